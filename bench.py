@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the TurboQuant encode-and-scan path on B200.
+
+Workload (the HBM-bound encode + scan case): dim 768, bits_per_coord 8
+(padded to D = 1024, 1036-byte codes), 10,000,000 rows drawn N(0,1) and
+L2-normalised per row, encoded on the GPU into a device-resident corpus; a
+step is distance_1_to_n for 64 independent normalised queries against it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  `value` is distance Gcodes/s over the whole job
+(codes scored per second, all ranks), device-resident corpus; `e2e` is the
+same metric through the public Python API with the corpus, the queries and the
+distances in pinned host memory (copies inside the timed region);
+`roofline` is the scan kernel's achieved HBM bandwidth against the measured
+copy peak; `cpu_baseline` is the reference library (compiled from its own
+sources into oracle/_ref) timed on this host's cores on a bounded sample.
+
+Under torchrun each rank scans its own 10M-code shard (weak scaling, no data
+exchange); timing is on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "turboquant-space_b200", "python"))
+
+METRIC = "distance Gcodes/s vs plain FP32 kernel at ≤1e-5 rel err; serving p99 ms at QPS"
+DIM, BITS, QUERIES = 768, 8, 64
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def l2n(x):
+    n = np.linalg.norm(x, axis=1, keepdims=True)
+    n[n == 0] = 1.0
+    return (x / n).astype(np.float32)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid):
+        self.uuid = device_uuid
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_module():
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if ref_dir not in sys.path:
+        sys.path.insert(0, ref_dir)
+    import _turboquant  # the reference's own pybind11 module, built from its sources
+    return _turboquant
+
+
+def cpu_scan(codes_host, queries, cores, kind_pref="reference"):
+    """Time distance_1_to_n of the reference (or, without its build, the
+    restatement) over `codes_host` for each query; returns (Gcodes/s, kind)."""
+    n = codes_host.shape[0]
+    try:
+        mod = reference_module()
+        sp = mod.TurboQuantSpace(DIM, bits_per_coord=BITS, num_threads=cores)
+        kind = "reference"
+    except Exception:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        sp = O.OracleSpace(DIM, BITS, num_threads=cores)
+        kind = "port"
+    sp.distance_1_to_n(queries[0], codes_host[: min(n, 10000)])  # warm the threads
+    t0 = time.perf_counter()
+    for q in queries:
+        sp.distance_1_to_n(q, codes_host)
+    dt = time.perf_counter() - t0
+    return len(queries) * n / dt / 1e9, kind
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU path on a bounded sample."""
+    if rank != 0:
+        return
+    cores = cpu_cores()
+    n_sample, q_sample = 1_000_000, 16
+    rng = np.random.default_rng(2)
+    X = np.concatenate([l2n(rng.standard_normal((250_000, DIM)).astype(np.float32))
+                        for _ in range(n_sample // 250_000)])
+    Q = l2n(np.random.default_rng(3).standard_normal((QUERIES, DIM)).astype(np.float32))[:q_sample]
+    try:
+        mod = reference_module()
+        sp = mod.TurboQuantSpace(DIM, bits_per_coord=BITS, num_threads=cores)
+        kind = "reference"
+    except Exception:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        sp = O.OracleSpace(DIM, BITS, num_threads=cores)
+        kind = "port"
+    codes = sp.encode_batch(X)
+    del X
+
+    def step():
+        for q in Q:
+            sp.distance_1_to_n(q, codes)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = q_sample * n_sample / dt / 1e9
+    sample = (f"{q_sample} queries x {n_sample} codes (768-d, 8-bit, normalised N(0,1) seed 2) "
+              f"per step, distance_1_to_n, {cores} OpenMP threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Gcodes/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "distance_1_to_n, dim 768, bits 8 (D 1024, 1036 B codes), "
+                               "CPU sample", "n_codes": n_sample, "queries": q_sample},
+        "cpu_baseline": {"value": round(value, 6), "unit": "Gcodes/s", "cores": cores,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": round(value, 6), "unit": "Gcodes/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=10_000_000, help="codes per GPU")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    import turboquant as tq
+    from turboquant._capi import check, lib
+
+    L = lib()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    space = tq.TurboQuantSpace(DIM, bits_per_coord=BITS, device=local)
+    h = space._h
+    cs = space.code_size_bytes()
+    D = space.padded_dim()
+    n = args.n
+    hbm_peak, peak_kind = peaks()
+
+    # ---- corpus: N(0,1) rows, L2-normalised, on this GPU (untimed) ----------
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(2 + 7919 * rank)
+    X = torch.empty((n, DIM), dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        step_rows = 1 << 20
+        for a in range(0, n, step_rows):
+            blk = X[a:a + step_rows]
+            blk.normal_(generator=gen)
+            nrm = blk.norm(dim=1, keepdim=True)
+            nrm[nrm == 0] = 1.0
+            blk.div_(nrm)
+    codes = torch.empty((n, cs), dtype=torch.uint8, device=dev)
+    stream.synchronize()
+
+    # ---- encode (bit-exact): timed separately -------------------------------
+    def encode():
+        check(L.tq_encode_batch_device(h, C.c_void_p(X.data_ptr()), n, C.c_void_p(codes.data_ptr()),
+                                       sptr))
+
+    encode()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    ev0.record(stream)
+    for _ in range(reps):
+        encode()
+    ev1.record(stream)
+    stream.synchronize()
+    enc_ms = ev0.elapsed_time(ev1) / reps
+    enc_bytes = n * (DIM * 4 + cs)
+
+    # parity sample of the full-size encode against the CPU checker
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    rows = np.sort(np.random.default_rng(99).choice(n, size=min(n, 512), replace=False))
+    ridx = torch.from_numpy(rows).to(dev)
+    Xs = X.index_select(0, ridx).cpu().numpy()
+    Cs = codes.index_select(0, ridx).cpu().numpy()
+    enc_exact = bool(np.array_equal(O.OracleSpace(DIM, BITS).encode_batch(Xs), Cs))
+    del X, ridx
+    torch.cuda.empty_cache()
+
+    # ---- queries and outputs --------------------------------------------------
+    Qh = l2n(np.random.default_rng(3 + 7919 * rank).standard_normal((QUERIES, DIM)).astype(np.float32))
+    Qd = torch.from_numpy(Qh).to(dev)
+    out = torch.empty((QUERIES, n), dtype=torch.float32, device=dev)
+    qptr = [C.c_void_p(Qd[i].data_ptr()) for i in range(QUERIES)]
+    optr = [C.c_void_p(out[i].data_ptr()) for i in range(QUERIES)]
+    cptr = C.c_void_p(codes.data_ptr())
+
+    def step():
+        for i in range(QUERIES):
+            check(L.tq_distance_1_to_n_device(h, qptr[i], cptr, n, optr[i], sptr))
+
+    # distance parity sample: query 0 against 2048 codes, vs the checker
+    step()
+    stream.synchronize()
+    csample = codes[:2048].cpu().numpy()
+    dref = O.OracleSpace(DIM, BITS).distance_1_to_n(Qh[0], csample)
+    meta = np.frombuffer(csample[:, D:D + 4].tobytes(), np.float32).astype(np.float64)
+    tscale = float(np.sum(Qh[0].astype(np.float64) ** 2)) + meta ** 2
+    dist_err = float(np.max(np.abs(out[0, :2048].cpu().numpy() - dref) /
+                            np.maximum(np.abs(dref), tscale)))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- timed region: K steps of 64 distance_1_to_n calls --------------------
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    barrier()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    with ClockSampler(uuid) as clk:
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        stream.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * QUERIES * n / (ms * 1e-3) / 1e9
+
+    # ---- the scan kernel alone: per-launch duration (prepared queries) --------
+    qrot = torch.empty((QUERIES, D), dtype=torch.float32, device=dev)
+    sq = torch.empty_like(qrot)
+    nrm = torch.empty((QUERIES, 2), dtype=torch.float32, device=dev)
+    check(L.tq_prepare_queries_device(h, C.c_void_p(Qd.data_ptr()), QUERIES, C.c_void_p(qrot.data_ptr()),
+                                      C.c_void_p(sq.data_ptr()), C.c_void_p(nrm.data_ptr()), sptr))
+    scan_args = [(C.c_void_p(qrot[i].data_ptr()), C.c_void_p(sq[i].data_ptr()),
+                  C.c_void_p(nrm[i].data_ptr()), optr[i]) for i in range(QUERIES)]
+    for a in scan_args[:4]:
+        check(L.tq_distance_1_to_n_prepared_device(h, a[0], a[1], a[2], cptr, n, a[3], sptr))
+    ev0.record(stream)
+    for a in scan_args:
+        check(L.tq_distance_1_to_n_prepared_device(h, a[0], a[1], a[2], cptr, n, a[3], sptr))
+    ev1.record(stream)
+    stream.synchronize()
+    scan_ms = ev0.elapsed_time(ev1) / QUERIES
+    scan_bytes = n * (cs + 4)
+    achieved = scan_bytes / (scan_ms * 1e-3) / 1e9
+
+    # ---- e2e: the public API with host buffers (rank-local) -------------------
+    e2e = None
+    if not args.no_e2e:
+        codes_h = torch.empty((n, cs), dtype=torch.uint8, pin_memory=True)
+        codes_h.copy_(codes)
+        out_h = torch.empty((QUERIES, n), dtype=torch.float32, pin_memory=True)
+        Q_h = torch.from_numpy(Qh).pin_memory()
+        cn, on, qn = codes_h.numpy(), out_h.numpy(), Q_h.numpy()
+        space.distance_m_to_n(qn, cn, out=on)  # warm-up
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            space.distance_m_to_n(qn, cn, out=on)
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        if dist is not None:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": round(world * QUERIES * n / e2e_s / 1e9, 4), "unit": "Gcodes/s",
+               "h2d_bytes_per_step": int(n * cs + QUERIES * DIM * 4),
+               "d2h_bytes_per_step": int(QUERIES * n * 4),
+               "ms_per_step": round(e2e_s * 1e3, 2),
+               "call": "TurboQuantSpace.distance_m_to_n(queries, codes, out=...) on pinned host arrays"}
+        del codes_h, out_h
+
+    # ---- CPU baseline: the reference on this host's cores, bounded sample ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = cpu_cores()
+        n_cpu = min(n, 1_000_000)
+        ch = codes[:n_cpu].cpu().numpy()
+        val, kind = cpu_scan(ch, Qh[:16], cores)
+        cpu = {"value": round(val, 6), "unit": "Gcodes/s", "cores": cores, "kind": kind,
+               "sample": f"16 queries x {n_cpu} codes of this corpus, distance_1_to_n"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "Gcodes/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (torch Philox N(0,1), rows L2-normalised; seeded per rank)",
+            "config": {"workload": "distance_1_to_n x 64 queries over a device-resident corpus of "
+                                   "10M codes: dim 768, bits 8 (D 1024, 1036 B/code)",
+                       "n_codes_per_gpu": n, "queries_per_step": QUERIES, "dim": DIM,
+                       "bits_per_coord": BITS, "code_bytes": cs,
+                       "l2": "corpus 10.4 GB per GPU > 126 MB L2: no flush needed",
+                       "parallelism": f"{world} independent shards" if world > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                         "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                         "traffic": None, "kernel": "scan_kernel<10,false,false>",
+                         "bytes_per_launch": scan_bytes, "ms_per_launch": round(scan_ms, 4),
+                         "peak_kind": peak_kind},
+            "encode": {"ms": round(enc_ms, 3), "Mvec_per_s": round(n / enc_ms / 1e3, 2),
+                       "GB_per_s": round(enc_bytes / enc_ms / 1e6, 1),
+                       "frac_hbm": round(enc_bytes / enc_ms / 1e6 / hbm_peak, 4),
+                       "bit_exact_sample_rows": len(rows), "bit_exact": enc_exact},
+            "distance_check": {"max_rel_err_vs_checker": dist_err, "codes_checked": 2048},
+            "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": args.steps * QUERIES * 2,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+/*
+ * turboquant_b200.h -- C ABI of the B200 (sm_100a) TurboQuant encode-and-scan
+ * library, libtqb200.so.
+ *
+ * This is the drop-in boundary for the reference's TurboQuantSpace
+ * (include/turboquant/space_turbo_quant.h:207-648) as its Python binding uses
+ * it (python/turboquant/bindings.cpp:53-218).  The reference exposes no C ABI
+ * (it is header-only C++ bound straight into pybind11); each function below
+ * names the reference member and binding it replaces.  Plain pointers and
+ * sizes only: no C++ or torch types cross this boundary, no exception escapes
+ * it, and every function reports failure through a tq_status plus a
+ * thread-local message (tq_last_error()).
+ *
+ * Codes are byte-identical to the reference layout: for padded dimension D
+ * (the next power of two >= max(dim, 4)) a code is `packed_bytes` of units
+ * unit = (sq_idx << 1) | qjl_bit -- two units per byte, even coordinate in the
+ * low nibble, when bits_per_coord <= 4; one unit per byte otherwise -- followed
+ * by the FP32 trailer [norm, gamma, sigma] (turbo_quant.h:101-185).
+ *
+ * Two families of entry points:
+ *   - host-pointer functions (tq_encode_batch, tq_distance_*) behave like the
+ *     reference methods: synchronous, all buffers in host memory, owned by the
+ *     caller.  Large inputs are streamed through the GPU in chunks.
+ *   - *_device functions take device pointers and a cudaStream_t (passed as
+ *     void*; NULL = the legacy default stream) and are stream-ordered: they
+ *     return once the work is enqueued.
+ */
+#ifndef TURBOQUANT_B200_H
+#define TURBOQUANT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tq_status {
+    TQ_OK = 0,
+    TQ_ERR_INVALID_ARGUMENT = 1, /* bad size/shape/value; the Python mirror raises ValueError */
+    TQ_ERR_CUDA = 2,             /* a CUDA runtime error (text in tq_last_error()) */
+    TQ_ERR_OUT_OF_MEMORY = 3,    /* device or pinned-host allocation failed */
+    TQ_ERR_NO_DEVICE = 4,        /* no usable sm_100 device */
+    TQ_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
+    TQ_ERR_BUSY = 6,             /* serving: a request was refused by admission */
+    TQ_ERR_NOT_SUPPORTED = 7     /* valid request this build does not implement */
+} tq_status;
+
+/* Arithmetic used by the M x N contractions. */
+typedef enum tq_precision {
+    TQ_PRECISION_FP32 = 0,      /* FP32 CUDA-core kernels: the drop-in */
+    TQ_PRECISION_SPLIT_BF16 = 1 /* tcgen05 tensor cores on hi+lo BF16 pairs, FP32 TMEM accumulators */
+} tq_precision;
+
+typedef struct tq_space tq_space;
+
+typedef struct tq_space_info {
+    size_t dim;          /* TurboQuantSpace::dim()            space_turbo_quant.h:315 */
+    size_t padded_dim;   /* TurboQuantSpace::paddedDim()      :316 */
+    size_t packed_bytes; /* TurboQuantSpace::packedBytes()    :320 */
+    size_t code_size;    /* TurboQuantSpace::codeSizeBytes()  :319 */
+    int bits_per_coord;  /* TurboQuantSpace::bitsPerCoord()   :321 */
+    int num_levels;      /* TurboQuantSpace::numLevels()      :323 */
+    int padded;          /* TurboQuantSpace::padded()         :317 */
+    int num_threads;     /* TurboQuantSpace::numThreads()     :318 (host threads; kept for API parity) */
+    int device;          /* CUDA device the space's tables live on */
+    uint64_t rot_seed;   /* :326 */
+    uint64_t qjl_seed;   /* :327 */
+    float scale;         /* TurboQuantSpace::scale()          :324 */
+} tq_space_info;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *tq_last_error(void);
+const char *tq_version(void);
+
+/* Replaces TurboQuantSpace::TurboQuantSpace (space_turbo_quant.h:250-311),
+ * bound at bindings.cpp:60-65.  Builds the Lloyd-Max table and both sign
+ * vectors on the host and uploads them to `device` (-1 = current device).
+ * Unlike the reference (asserts compiled out), dim < 1 or bits outside 2..9
+ * return TQ_ERR_INVALID_ARGUMENT.  The padding warning of :269-273 is printed
+ * to stderr the same way. */
+tq_status tq_space_create(size_t dim, int bits_per_coord, uint64_t rot_seed,
+                          uint64_t qjl_seed, int num_threads, int device,
+                          tq_space **out);
+void tq_space_destroy(tq_space *sp);
+tq_status tq_space_get_info(const tq_space *sp, tq_space_info *info);
+
+/* Host copies of the tables: centroids[num_levels], boundaries[num_levels-1],
+ * rot_signs[padded_dim], qjl_signs[padded_dim] (any pointer may be NULL).
+ * computeLloydMax space_turbo_quant.h:76-131; generateSigns turbo_quant.h:74-86. */
+tq_status tq_space_tables(const tq_space *sp, float *centroids, float *boundaries,
+                          float *rot_signs, float *qjl_signs);
+
+/* quantize (space_turbo_quant.h:332-337) of n normalised values on the host,
+ * through the same bucket table the encode kernel uses for bits >= 6 (the
+ * direct count otherwise).  A diagnostic: it lets the table's exactness be
+ * checked without a GPU.  idx[i] = #{j : z[i] > boundaries[j]} as uint8. */
+tq_status tq_space_quantize(const tq_space *sp, const float *z, size_t n, uint8_t *idx);
+
+/* ---- host-pointer entry points (synchronous) ----------------------------- */
+
+/* TurboQuantSpace::encodeBatch (space_turbo_quant.h:400-407); bindings.cpp:93-116.
+ * X: n x dim float32 row-major; out: n x code_size bytes.  Bit-exact. */
+tq_status tq_encode_batch(const tq_space *sp, const float *X, size_t n, uint8_t *out);
+
+/* TurboQuantSpace::distanceBatch1ToN (:577-585); bindings.cpp:156-172.
+ * query: dim floats; codes: n codes; out: n floats. */
+tq_status tq_distance_1_to_n(const tq_space *sp, const float *query, const uint8_t *codes,
+                             size_t n, float *out);
+
+/* TurboQuantSpace::distanceBatchMToN (:588-599); bindings.cpp:175-194.
+ * queries: m x dim; out: m x n row-major. */
+tq_status tq_distance_m_to_n(const tq_space *sp, const float *queries, size_t m,
+                             const uint8_t *codes, size_t n, float *out,
+                             tq_precision precision);
+
+/* TurboQuantSpace::distanceBatchMToNSymmetric (:602-615); bindings.cpp:197-218.
+ * MSE-only: gamma and the QJL bits are ignored, as in the reference. */
+tq_status tq_distance_m_to_n_symmetric(const tq_space *sp, const uint8_t *codes_a, size_t m,
+                                       const uint8_t *codes_b, size_t n, float *out,
+                                       tq_precision precision);
+
+/* ---- device-pointer entry points (stream-ordered) ------------------------ */
+
+/* encodeBatch on device buffers. */
+tq_status tq_encode_batch_device(const tq_space *sp, const float *X, size_t n, uint8_t *out,
+                                 void *stream);
+
+/* TurboQuantSpace::prepareQuery (:439-460) for m queries: q_rot and s_q are
+ * m x padded_dim, norms is m x 2 = (|q|^2, |q|). */
+tq_status tq_prepare_queries_device(const tq_space *sp, const float *queries, size_t m,
+                                    float *q_rot, float *s_q, float *norms, void *stream);
+
+/* distanceBatch1ToN on device buffers.  Scratch for the prepared query is
+ * taken from the stream-ordered pool of the device (cudaMallocAsync). */
+tq_status tq_distance_1_to_n_device(const tq_space *sp, const float *query,
+                                    const uint8_t *codes, size_t n, float *out, void *stream);
+
+/* The scan alone, for a query already prepared by tq_prepare_queries_device
+ * (q_rot, s_q: padded_dim floats; norms: 2 floats) -- the reference's
+ * distance(const TurboQuantPreparedQuery&, code) (:465-468) over n codes.
+ * Allocates nothing. */
+tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_rot,
+                                             const float *s_q, const float *norms,
+                                             const uint8_t *codes, size_t n, float *out,
+                                             void *stream);
+
+/* distanceBatchMToN on device buffers. */
+tq_status tq_distance_m_to_n_device(const tq_space *sp, const float *queries, size_t m,
+                                    const uint8_t *codes, size_t n, float *out,
+                                    tq_precision precision, void *stream);
+
+/* distanceBatchMToNSymmetric on device buffers. */
+tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t *codes_a,
+                                              size_t m, const uint8_t *codes_b, size_t n,
+                                              float *out, tq_precision precision,
+                                              void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TURBOQUANT_B200_H */

@@ -1,0 +1,414 @@
+/*
+ * tq_oracle.c -- plain-C restatement of TurboQuant's encode-and-scan path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the CPU checker; see tq_oracle.h).  Compiled with
+ * -ffp-contract=off and without fast-math: every fmaf() below is an FMA the
+ * reference's pinned build performs, every other operation rounds on its own.
+ */
+#include "tq_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef M_SQRT1_2
+#define M_SQRT1_2 0.70710678118654752440
+#endif
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+struct tqo_space {
+    size_t dim, D, packed_bytes, code_size;
+    int bits, num_levels, num_boundaries;
+    float scale, wht_scale;
+    float *centroids, *boundaries, *rot_signs, *qjl_signs;
+};
+
+/* The constants the reference's build folded (space_turbo_quant.h:348, 357-359):
+ *   `norm > 1e-10f` is evaluated as `norm_sq > fl(1e-10f * 1e-10f)`,
+ *   the floored sigma is 1e-10f and its inverse is fl(1 / 1e-10f). */
+static float f32_from_bits(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+#define NORMSQ_FLOOR f32_from_bits(0x1E3CE509u)   /* fl(1e-10f * 1e-10f) */
+#define SIGMA_FLOOR f32_from_bits(0x2EDBE6FFu)    /* 1e-10f */
+#define INV_SIGMA_FLOOR f32_from_bits(0x501502F9u) /* fl(1.0f / 1e-10f) */
+
+/* ---- splitmix64 + sign vectors: turbo_quant.h:27-39, 74-86 ---------------- */
+static uint64_t splitmix64_next(uint64_t *state) {
+    uint64_t z = (*state += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+void tqo_signs(size_t d, uint64_t seed, float *out) {
+    uint64_t state = seed;
+    for (size_t i = 0; i < d; ++i)
+        out[i] = (splitmix64_next(&state) & 1u) ? 1.0f : -1.0f;
+}
+
+/* ---- Lloyd-Max for N(0,1): space_turbo_quant.h:76-131 --------------------- */
+static double lm_phi(double x) { return exp(-0.5 * x * x) / sqrt(2.0 * M_PI); }
+static double lm_Phi(double x) { return 0.5 * erfc(-x * M_SQRT1_2); }
+static double lm_cond_mean(double a, double b) {
+    double denom = lm_Phi(b) - lm_Phi(a);
+    if (denom < 1e-15) return 0.5 * (a + b);
+    return (lm_phi(a) - lm_phi(b)) / denom;
+}
+
+void tqo_lloyd_max(int bits, float *centroids, float *boundaries) {
+    const int levels = 1 << bits;
+    const int half = levels / 2;
+    double *pos_c = (double *)malloc(sizeof(double) * (size_t)half);
+    double *pos_b = (double *)malloc(sizeof(double) * (size_t)(half > 1 ? half - 1 : 1));
+    double *new_c = (double *)malloc(sizeof(double) * (size_t)half);
+    for (int i = 0; i < half; ++i) pos_c[i] = (i + 0.5) * 3.5 / half;
+    for (int iter = 0; iter < 1000; ++iter) {
+        for (int i = 0; i < half - 1; ++i) pos_b[i] = 0.5 * (pos_c[i] + pos_c[i + 1]);
+        double max_delta = 0.0;
+        for (int i = 0; i < half; ++i) {
+            double lo = (i == 0) ? 0.0 : pos_b[i - 1];
+            double hi = (i == half - 1) ? 1e10 : pos_b[i];
+            new_c[i] = lm_cond_mean(lo, hi);
+            double dlt = fabs(new_c[i] - pos_c[i]);
+            if (dlt > max_delta) max_delta = dlt;
+        }
+        memcpy(pos_c, new_c, sizeof(double) * (size_t)half);
+        if (max_delta < 1e-12) break;
+    }
+    for (int i = 0; i < half; ++i) {
+        centroids[half + i] = (float)pos_c[i];
+        centroids[half - 1 - i] = -(float)pos_c[i];
+    }
+    boundaries[half - 1] = 0.0f;
+    for (int i = 0; i < half - 1; ++i) {
+        double b = 0.5 * (pos_c[i] + pos_c[i + 1]);
+        boundaries[half + i] = (float)b;
+        boundaries[half - 2 - i] = -(float)b;
+    }
+    free(pos_c); free(pos_b); free(new_c);
+}
+
+/* ---- geometry: space_turbo_quant.h:233-238, 258-266; turbo_quant.h:177-184 */
+size_t tqo_padded_dim(size_t dim) {
+    size_t d = dim < 4 ? 4 : dim, p = 1;
+    while (p < d) p <<= 1;
+    return p;
+}
+size_t tqo_packed_bytes(size_t D, int bits) { return bits <= 4 ? (D + 1) / 2 : D; }
+size_t tqo_code_size(size_t D, int bits) { return tqo_packed_bytes(D, bits) + 12; }
+
+tqo_space *tqo_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_seed) {
+    if (dim < 1 || bits < 2 || bits > 9) return NULL;
+    tqo_space *sp = (tqo_space *)calloc(1, sizeof(tqo_space));
+    sp->dim = dim;
+    sp->D = tqo_padded_dim(dim);
+    sp->bits = bits;
+    sp->packed_bytes = tqo_packed_bytes(sp->D, bits);
+    sp->code_size = sp->packed_bytes + 12;
+    sp->num_levels = 1 << (bits - 1);
+    sp->num_boundaries = sp->num_levels - 1;
+    /* space_turbo_quant.h:265-266: sqrt(float(pi)/2) / sqrt(float(D)) */
+    sp->scale = sqrtf((float)M_PI / 2.0f) / sqrtf((float)sp->D);
+    /* turbo_quant.h:69 */
+    sp->wht_scale = 1.0f / sqrtf((float)sp->D);
+    sp->centroids = (float *)malloc(sizeof(float) * (size_t)sp->num_levels);
+    sp->boundaries = (float *)malloc(sizeof(float) * (size_t)(sp->num_boundaries + 1));
+    tqo_lloyd_max(bits - 1, sp->centroids, sp->boundaries);
+    sp->rot_signs = (float *)malloc(sizeof(float) * sp->D);
+    sp->qjl_signs = (float *)malloc(sizeof(float) * sp->D);
+    tqo_signs(sp->D, rot_seed, sp->rot_signs);
+    tqo_signs(sp->D, qjl_seed, sp->qjl_signs);
+    return sp;
+}
+
+void tqo_destroy(tqo_space *sp) {
+    if (!sp) return;
+    free(sp->centroids); free(sp->boundaries); free(sp->rot_signs); free(sp->qjl_signs);
+    free(sp);
+}
+size_t tqo_space_padded_dim(const tqo_space *sp) { return sp->D; }
+size_t tqo_space_code_size(const tqo_space *sp) { return sp->code_size; }
+float tqo_space_scale(const tqo_space *sp) { return sp->scale; }
+const float *tqo_space_centroids(const tqo_space *sp) { return sp->centroids; }
+const float *tqo_space_boundaries(const tqo_space *sp) { return sp->boundaries; }
+const float *tqo_space_rot_signs(const tqo_space *sp) { return sp->rot_signs; }
+const float *tqo_space_qjl_signs(const tqo_space *sp) { return sp->qjl_signs; }
+
+/* ---- the pinned build's sum-of-squares tree --------------------------------
+ * Main loop: 8 lanes, lane k accumulates acc[k] = acc[k] + x[i]*x[i] for
+ * i = k mod 8 in increasing i (multiply and add round separately).  Then
+ * t[k] = acc[k] + acc[k+4] (k < 4) and s = (t0 + t2) + (t1 + t3).
+ * If 4..7 elements remain: t[k] = fma(x, x, t[k]) on the next 4 elements and
+ * s = (t0 + t2) + (t1 + t3) again (t starts at zero when n < 8).
+ * The last n mod 4 elements: s = fma(x, x, s) in order.                      */
+float tqo_sq_reduce(const float *x, size_t n) {
+    float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float s = 0.0f;
+    size_t base = 0;
+    if (n >= 8) {
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        size_t n8 = n & ~(size_t)7;
+        for (size_t i = 0; i < n8; i += 8)
+            for (int k = 0; k < 8; ++k) {
+                float p = x[i + k] * x[i + k];
+                acc[k] = acc[k] + p;
+            }
+        for (int k = 0; k < 4; ++k) t[k] = acc[k] + acc[k + 4];
+        s = (t[0] + t[2]) + (t[1] + t[3]);
+        base = n8;
+    }
+    size_t r = n - base;
+    if (r >= 4) {
+        for (int k = 0; k < 4; ++k) t[k] = fmaf(x[base + k], x[base + k], t[k]);
+        s = (t[0] + t[2]) + (t[1] + t[3]);
+        base += 4;
+        r -= 4;
+    }
+    for (size_t j = 0; j < r; ++j) s = fmaf(x[base + j], x[base + j], s);
+    return s;
+}
+
+/* ---- randomized Hadamard: turbo_quant.h:46-72, 89-99 ----------------------- */
+static void rht(float *v, const float *signs, size_t D, float wht_scale) {
+    for (size_t i = 0; i < D; ++i) v[i] = v[i] * signs[i];
+    for (size_t step = 1; step < D; step <<= 1)
+        for (size_t i = 0; i < D; i += step << 1)
+            for (size_t j = 0; j < step; ++j) {
+                float a = v[i + j], b = v[i + step + j];
+                v[i + j] = a + b;
+                v[i + step + j] = a - b;
+            }
+    for (size_t i = 0; i < D; ++i) v[i] = v[i] * wht_scale;
+}
+
+/* quantize: space_turbo_quant.h:332-337 (strict `>` count, uint8 result) */
+static uint8_t quantize(const tqo_space *sp, float v) {
+    uint8_t idx = 0;
+    for (int j = 0; j < sp->num_boundaries; ++j) idx = (uint8_t)(idx + (v > sp->boundaries[j]));
+    return idx;
+}
+
+/* encodeVector: space_turbo_quant.h:339-396 */
+static void encode_one(const tqo_space *sp, const float *raw, uint8_t *out,
+                       float *rot, float *res, uint8_t *idx) {
+    const size_t dim = sp->dim, D = sp->D;
+    float norm_sq = tqo_sq_reduce(raw, dim);
+    float norm = sqrtf(norm_sq);
+    float inv_norm = (norm_sq > NORMSQ_FLOOR) ? 1.0f / norm : 0.0f;
+    for (size_t i = 0; i < D; ++i) rot[i] = 0.0f;
+    for (size_t i = 0; i < dim; ++i) rot[i] = raw[i] * inv_norm;
+    rht(rot, sp->rot_signs, D, sp->wht_scale);
+
+    float var = tqo_sq_reduce(rot, D);
+    float sigma = sqrtf(var / (float)D);
+    float inv_sigma;
+    if (SIGMA_FLOOR > sigma) {
+        sigma = SIGMA_FLOOR;
+        inv_sigma = INV_SIGMA_FLOOR;
+    } else {
+        inv_sigma = 1.0f / sigma;
+    }
+    for (size_t i = 0; i < D; ++i) {
+        float normalized = rot[i] * inv_sigma;
+        idx[i] = quantize(sp, normalized);
+        res[i] = fmaf(-sp->centroids[idx[i]], sigma, rot[i]); /* contracted */
+    }
+    float gamma = sqrtf(tqo_sq_reduce(res, D));
+    rht(res, sp->qjl_signs, D, sp->wht_scale);
+
+    if (sp->bits <= 4) {
+        memset(out, 0, sp->packed_bytes);
+        for (size_t i = 0; i < D; ++i) {
+            uint8_t unit = (uint8_t)((idx[i] << 1) | (res[i] >= 0.0f ? 1u : 0u));
+            if ((i & 1) == 0) out[i >> 1] = unit;
+            else out[i >> 1] = (uint8_t)(out[i >> 1] | (unit << 4));
+        }
+    } else {
+        for (size_t i = 0; i < D; ++i)
+            out[i] = (uint8_t)((idx[i] << 1) | (res[i] >= 0.0f ? 1u : 0u));
+    }
+    float meta[3] = {norm, gamma, sigma};
+    memcpy(out + sp->packed_bytes, meta, 12);
+}
+
+void tqo_encode_batch(const tqo_space *sp, const float *X, size_t n, uint8_t *out,
+                      int num_threads) {
+    const size_t D = sp->D;
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel num_threads(num_threads)
+    {
+        float *rot = (float *)malloc(sizeof(float) * D);
+        float *res = (float *)malloc(sizeof(float) * D);
+        uint8_t *idx = (uint8_t *)malloc(D);
+#pragma omp for schedule(static)
+        for (long long i = 0; i < (long long)n; ++i)
+            encode_one(sp, X + (size_t)i * sp->dim, out + (size_t)i * sp->code_size, rot, res, idx);
+        free(rot); free(res); free(idx);
+    }
+}
+
+/* prepareQuery: space_turbo_quant.h:439-460 */
+void tqo_prepare_query(const tqo_space *sp, const float *q, float *q_rot, float *s_q,
+                       float *norms) {
+    const size_t dim = sp->dim, D = sp->D;
+    /* In the reference's batch drivers the |q|^2 loop accumulates into a
+     * struct member and is compiled as a plain sequential sum (:443-445). */
+    float qn2 = 0.0f;
+    for (size_t i = 0; i < dim; ++i) {
+        float p = q[i] * q[i];
+        qn2 = qn2 + p;
+    }
+    float qn = sqrtf(qn2);
+    float qinv = (qn2 > NORMSQ_FLOOR) ? 1.0f / qn : 0.0f;
+    for (size_t i = 0; i < D; ++i) q_rot[i] = 0.0f;
+    for (size_t i = 0; i < dim; ++i) q_rot[i] = q[i] * qinv;
+    rht(q_rot, sp->rot_signs, D, sp->wht_scale);
+    memcpy(s_q, q_rot, sizeof(float) * D);
+    rht(s_q, sp->qjl_signs, D, sp->wht_scale);
+    norms[0] = qn2;
+    norms[1] = qn;
+}
+
+static inline unsigned code_unit(const uint8_t *packed, size_t i, int bits) {
+    if (bits <= 4) {
+        uint8_t b = packed[i >> 1];
+        return (i & 1) ? (unsigned)(b >> 4) : (unsigned)(b & 0x0F);
+    }
+    return packed[i];
+}
+
+static inline void code_meta(const tqo_space *sp, const uint8_t *code, float m[3]) {
+    memcpy(m, code + sp->packed_bytes, 12);
+}
+
+/* distSearchScalar / distSearchScalarB4: space_turbo_quant.h:659-686, 951-983 */
+static float dist_search(const tqo_space *sp, const float *q_rot, const float *s_q,
+                         const float *norms, const uint8_t *code) {
+    float m[3];
+    code_meta(sp, code, m);
+    float ip_mse = 0.0f, dot_qjl = 0.0f;
+    for (size_t i = 0; i < sp->D; ++i) {
+        unsigned u = code_unit(code, i, sp->bits);
+        ip_mse = ip_mse + q_rot[i] * sp->centroids[u >> 1];
+        dot_qjl = dot_qjl + s_q[i] * ((u & 1) ? 1.0f : -1.0f);
+    }
+    ip_mse = ip_mse * m[2];
+    float correction = sp->scale * m[1] * dot_qjl;
+    float ip = (ip_mse + correction) * m[0] * norms[1];
+    float d = norms[0] + m[0] * m[0] - 2.0f * ip;
+    return d > 0.0f ? d : 0.0f;
+}
+
+/* distBuildScalar / distBuildScalarB4: space_turbo_quant.h:688-714, 985-1019 */
+static float dist_build(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+    float ma[3], mb[3];
+    code_meta(sp, a, ma);
+    code_meta(sp, b, mb);
+    float ip_rot = 0.0f;
+    for (size_t i = 0; i < sp->D; ++i) {
+        float ca = sp->centroids[code_unit(a, i, sp->bits) >> 1] * ma[2];
+        float cb = sp->centroids[code_unit(b, i, sp->bits) >> 1] * mb[2];
+        ip_rot = ip_rot + ca * cb;
+    }
+    float ip = ip_rot * ma[0] * mb[0];
+    float d = ma[0] * ma[0] + mb[0] * mb[0] - 2.0f * ip;
+    return d > 0.0f ? d : 0.0f;
+}
+
+void tqo_distance_1_to_n(const tqo_space *sp, const float *q, const uint8_t *codes,
+                         size_t n, float *out, int num_threads) {
+    float *q_rot = (float *)malloc(sizeof(float) * sp->D);
+    float *s_q = (float *)malloc(sizeof(float) * sp->D);
+    float norms[2];
+    tqo_prepare_query(sp, q, q_rot, s_q, norms);
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel for schedule(static) num_threads(num_threads)
+    for (long long i = 0; i < (long long)n; ++i)
+        out[i] = dist_search(sp, q_rot, s_q, norms, codes + (size_t)i * sp->code_size);
+    free(q_rot); free(s_q);
+}
+
+void tqo_distance_m_to_n(const tqo_space *sp, const float *Q, size_t m,
+                         const uint8_t *codes, size_t n, float *out, int num_threads) {
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel num_threads(num_threads)
+    {
+        float *q_rot = (float *)malloc(sizeof(float) * sp->D);
+        float *s_q = (float *)malloc(sizeof(float) * sp->D);
+        float norms[2];
+#pragma omp for schedule(static)
+        for (long long qi = 0; qi < (long long)m; ++qi) {
+            tqo_prepare_query(sp, Q + (size_t)qi * sp->dim, q_rot, s_q, norms);
+            for (size_t i = 0; i < n; ++i)
+                out[(size_t)qi * n + i] =
+                    dist_search(sp, q_rot, s_q, norms, codes + i * sp->code_size);
+        }
+        free(q_rot); free(s_q);
+    }
+}
+
+void tqo_distance_m_to_n_symmetric(const tqo_space *sp, const uint8_t *A, size_t m,
+                                   const uint8_t *B, size_t n, float *out,
+                                   int num_threads) {
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel for schedule(static) num_threads(num_threads)
+    for (long long i = 0; i < (long long)m; ++i)
+        for (size_t j = 0; j < n; ++j)
+            out[(size_t)i * n + j] =
+                dist_build(sp, A + (size_t)i * sp->code_size, B + j * sp->code_size);
+}
+
+/* ---- FP64 evaluation of the same formulas --------------------------------- */
+static void rht64(double *v, const float *signs, size_t D) {
+    for (size_t i = 0; i < D; ++i) v[i] *= (double)signs[i];
+    for (size_t step = 1; step < D; step <<= 1)
+        for (size_t i = 0; i < D; i += step << 1)
+            for (size_t j = 0; j < step; ++j) {
+                double a = v[i + j], b = v[i + step + j];
+                v[i + j] = a + b;
+                v[i + step + j] = a - b;
+            }
+    double s = 1.0 / sqrt((double)D);
+    for (size_t i = 0; i < D; ++i) v[i] *= s;
+}
+
+double tqo_distance_f64(const tqo_space *sp, const float *q, const uint8_t *code) {
+    const size_t D = sp->D;
+    double *q_rot = (double *)calloc(D, sizeof(double));
+    double *s_q = (double *)malloc(sizeof(double) * D);
+    double qn2 = 0.0;
+    for (size_t i = 0; i < sp->dim; ++i) qn2 += (double)q[i] * (double)q[i];
+    double qn = sqrt(qn2);
+    double qinv = qn > 1e-10 ? 1.0 / qn : 0.0;
+    for (size_t i = 0; i < sp->dim; ++i) q_rot[i] = (double)q[i] * qinv;
+    rht64(q_rot, sp->rot_signs, D);
+    memcpy(s_q, q_rot, sizeof(double) * D);
+    rht64(s_q, sp->qjl_signs, D);
+    float m[3];
+    code_meta(sp, code, m);
+    double ip_mse = 0.0, dot = 0.0;
+    for (size_t i = 0; i < D; ++i) {
+        unsigned u = code_unit(code, i, sp->bits);
+        ip_mse += q_rot[i] * (double)sp->centroids[u >> 1];
+        dot += s_q[i] * ((u & 1) ? 1.0 : -1.0);
+    }
+    double xn = m[0], gamma = m[1], sigma = m[2];
+    double ip = (ip_mse * sigma + (double)sp->scale * gamma * dot) * xn * qn;
+    double d = qn2 + xn * xn - 2.0 * ip;
+    free(q_rot); free(s_q);
+    return d > 0.0 ? d : 0.0;
+}
+
+double tqo_distance_symmetric_f64(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+    float ma[3], mb[3];
+    code_meta(sp, a, ma);
+    code_meta(sp, b, mb);
+    double ip = 0.0;
+    for (size_t i = 0; i < sp->D; ++i)
+        ip += ((double)sp->centroids[code_unit(a, i, sp->bits) >> 1] * ma[2]) *
+              ((double)sp->centroids[code_unit(b, i, sp->bits) >> 1] * mb[2]);
+    ip *= (double)ma[0] * (double)mb[0];
+    double d = (double)ma[0] * ma[0] + (double)mb[0] * mb[0] - 2.0 * ip;
+    return d > 0.0 ? d : 0.0;
+}

@@ -1,0 +1,207 @@
+"""Parity of the CUDA path with the reference, through the C ABI.
+
+Codes must be byte-identical (trailer floats included) to the reference's on
+the same inputs; distances must agree within DIST_RTOL (conftest.py) of the
+reference's, and their error against the FP64 evaluation of the same formula
+is stated.  Each test runs the product path (libtqb200.so); the oracle and the
+golden vectors are only the checker.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import turboquant as tq
+from conftest import (GOLDEN, GOLDEN_CASES, asym_term_scale, dist_close, load_case,
+                      sym_term_scale)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
+def test_encode_bit_exact_vs_golden(cuda_ok, dim, bits):
+    g = load_case(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    np.testing.assert_array_equal(s.encode_batch(g["X"]), g["codes"])
+
+
+@pytest.mark.parametrize("dim,bits", [(1, 2), (2, 9), (3, 4), (4, 8), (6, 8), (9, 5), (31, 4),
+                                      (32, 3), (63, 6), (64, 7), (130, 8), (256, 4), (511, 4),
+                                      (768, 8), (768, 4), (1024, 9), (1536, 4), (3000, 7),
+                                      (4096, 8), (8192, 4)])
+def test_encode_bit_exact_vs_oracle(cuda_ok, dim, bits):
+    rng = np.random.default_rng(dim * 13 + bits)
+    n = 257 if dim <= 1024 else 33          # not a multiple of 4: a ragged last quad
+    X = (rng.standard_normal((n, dim)) * rng.uniform(1e-3, 1e3, (n, 1))).astype(np.float32)
+    X[0] = 0.0
+    X[1, : max(1, dim // 2)] = 0.0
+    s = tq.TurboQuantSpace(dim, bits)
+    got = s.encode_batch(X)
+    want = O.OracleSpace(dim, bits).encode_batch(X)
+    bad = np.nonzero(np.any(got != want, axis=1))[0]
+    assert bad.size == 0, f"{bad.size} rows differ, first {bad[:5]}"
+
+
+def test_encode_cfg1_full_digest(cuda_ok):
+    """All 100,000 codes of the 128-d 4-bit plain-method case, against the reference's digest."""
+    X = np.random.default_rng(0).standard_normal((100_000, 128)).astype(np.float32)
+    codes = tq.TurboQuantSpace(128, 4).encode_batch(X)
+    with open(os.path.join(GOLDEN, "digests.json")) as f:
+        want = json.load(f)["cfg1_codes_sha256"]
+    assert hashlib.sha256(codes.tobytes()).hexdigest() == want
+
+
+def test_encode_cfg2_slice_digest(cuda_ok):
+    """100,000 rows of the normalised 768-d 8-bit corpus, against the reference's digest."""
+    rng = np.random.default_rng(2)
+    parts = []
+    for _ in range(2):
+        x = rng.standard_normal((50_000, 768)).astype(np.float32)
+        n = np.linalg.norm(x, axis=1, keepdims=True)
+        n[n == 0] = 1.0
+        parts.append((x / n).astype(np.float32))
+    codes = tq.TurboQuantSpace(768, 8).encode_batch(np.concatenate(parts))
+    with open(os.path.join(GOLDEN, "digests.json")) as f:
+        want = json.load(f)["cfg2_slice_codes_sha256"]
+    assert hashlib.sha256(codes.tobytes()).hexdigest() == want
+
+
+def test_encode_device_path_equals_host_path(cuda_ok):
+    import torch
+    rng = np.random.default_rng(11)
+    X = rng.standard_normal((1001, 768)).astype(np.float32)
+    s = tq.TurboQuantSpace(768, 8)
+    host = s.encode_batch(X)
+    dev = s.encode_batch(torch.from_numpy(X).cuda())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dev.cpu().numpy(), host)
+    out = torch.empty((1001, s.code_size_bytes()), dtype=torch.uint8, device="cuda")
+    s.encode_batch_into(torch.from_numpy(X).cuda(), out)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), host)
+
+
+def test_encode_single_and_into(cuda_ok):
+    g = load_case(768, 8)
+    s = tq.TurboQuantSpace(768, 8)
+    for i in range(5):
+        np.testing.assert_array_equal(s.encode(g["X"][i]), g["codes"][i])
+        buf = np.zeros(s.code_size_bytes(), np.uint8)
+        s.encode_into(g["X"][i], buf)
+        np.testing.assert_array_equal(buf, g["codes"][i])
+    out = np.zeros(g["codes"].shape, np.uint8)
+    s.encode_batch_into(g["X"], out)
+    np.testing.assert_array_equal(out, g["codes"])
+
+
+def test_encode_empty(cuda_ok):
+    s = tq.TurboQuantSpace(128, 4)
+    assert s.encode_batch(np.zeros((0, 128), np.float32)).shape == (0, 76)
+
+
+@pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
+def test_distance_1_to_n_vs_golden(cuda_ok, dim, bits):
+    g = load_case(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    cs = s.code_size_bytes()
+    d = s.distance_1_to_n(g["q"], g["codes"])
+    err, ok = dist_close(d, g["d1n"], asym_term_scale(g["q"], g["codes"], cs, cs - 12)[0])
+    assert ok, err.max()
+
+
+@pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
+def test_distance_m_to_n_vs_golden(cuda_ok, dim, bits):
+    g = load_case(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    cs = s.code_size_bytes()
+    d = s.distance_m_to_n(g["Q"], g["codes"])
+    assert d.shape == g["dmn"].shape
+    err, ok = dist_close(d, g["dmn"], asym_term_scale(g["Q"], g["codes"], cs, cs - 12))
+    assert ok, err.max()
+
+
+@pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
+def test_distance_symmetric_vs_golden(cuda_ok, dim, bits):
+    g = load_case(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    cs = s.code_size_bytes()
+    A = g["codes"][:8]
+    d = s.distance_m_to_n_symmetric(A, g["codes"])
+    err, ok = dist_close(d, g["dsym"], sym_term_scale(A, g["codes"], cs, cs - 12))
+    assert ok, err.max()
+
+
+def test_single_distances_match_batch(cuda_ok):
+    """distance / distance_symmetric equal the batch forms (test_turboquant.py:101-146)."""
+    g = load_case(128, 4)
+    s = tq.TurboQuantSpace(128, 4)
+    d = s.distance_1_to_n(g["q"], g["codes"])
+    for i in range(6):
+        assert abs(s.distance(g["q"], g["codes"][i]) - d[i]) < 1e-4
+    D = s.distance_m_to_n_symmetric(g["codes"][:3], g["codes"][:5])
+    for i in range(3):
+        for j in range(5):
+            assert abs(s.distance_symmetric(g["codes"][i], g["codes"][j]) - D[i, j]) < 1e-4
+
+
+def test_distance_cfg1_head_and_fp64_error(cuda_ok):
+    """The plain-method case end to end: GPU encode, then 1->N against the
+    reference's first 4096 distances; the error vs FP64 is stated."""
+    X = np.random.default_rng(0).standard_normal((100_000, 128)).astype(np.float32)
+    q = np.random.default_rng(1).standard_normal(128).astype(np.float32)
+    s = tq.TurboQuantSpace(128, 4)
+    codes = s.encode_batch(X)
+    d = s.distance_1_to_n(q, codes)
+    assert d.shape == (100_000,)
+    with np.load(os.path.join(GOLDEN, "cfg1_d1n_head.npz")) as z:
+        ref = z["d1n"]
+    scale = asym_term_scale(q, codes[:4096], 76, 64)[0]
+    err, ok = dist_close(d[:4096], ref, scale)
+    assert ok, err.max()
+    o = O.OracleSpace(128, 4)
+    f64 = np.array([o.distance_f64(q, codes[i]) for i in range(0, 100_000, 97)])
+    rel64 = np.abs(d[::97] - f64) / np.maximum(np.abs(f64), scale.max())
+    print(f"cfg1 distance max error vs FP64: {rel64.max():.3e} (relative to term scale)")
+    assert rel64.max() < 1e-5
+
+
+def test_distance_cfg2_head(cuda_ok):
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((50_000, 768)).astype(np.float32)
+    x = (x / np.linalg.norm(x, axis=1, keepdims=True)).astype(np.float32)
+    q = np.random.default_rng(3).standard_normal((64, 768)).astype(np.float32)
+    q = (q / np.linalg.norm(q, axis=1, keepdims=True)).astype(np.float32)
+    s = tq.TurboQuantSpace(768, 8)
+    codes = s.encode_batch(x[:4096])
+    d = s.distance_1_to_n(q[0], codes)
+    with np.load(os.path.join(GOLDEN, "cfg2_d1n_head.npz")) as z:
+        ref = z["d1n"]
+    err, ok = dist_close(d, ref, asym_term_scale(q[0], codes, 1036, 1024)[0])
+    assert ok, err.max()
+
+
+def test_device_distances_equal_host(cuda_ok):
+    import torch
+    g = load_case(768, 8)
+    s = tq.TurboQuantSpace(768, 8)
+    codes_d = torch.from_numpy(g["codes"]).cuda()
+    d1 = s.distance_1_to_n(torch.from_numpy(g["q"]).cuda(), codes_d)
+    dm = s.distance_m_to_n(torch.from_numpy(g["Q"]).cuda(), codes_d)
+    ds = s.distance_m_to_n_symmetric(codes_d[:8], codes_d)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d1.cpu().numpy(), s.distance_1_to_n(g["q"], g["codes"]))
+    np.testing.assert_array_equal(dm.cpu().numpy(), s.distance_m_to_n(g["Q"], g["codes"]))
+    np.testing.assert_array_equal(ds.cpu().numpy(),
+                                  s.distance_m_to_n_symmetric(g["codes"][:8], g["codes"]))
+
+
+def test_empty_and_single_row(cuda_ok):
+    s = tq.TurboQuantSpace(64, 8)
+    q = np.ones(64, np.float32)
+    assert s.distance_1_to_n(q, np.zeros(0, np.uint8)).shape == (0,)
+    codes = s.encode_batch(np.ones((1, 64), np.float32))
+    assert s.distance_1_to_n(q, codes).shape == (1,)
+    assert s.distance_m_to_n(np.ones((3, 64), np.float32), np.zeros(0, np.uint8)).shape == (3, 0)

@@ -1,0 +1,649 @@
+// tq_capi.cu -- the C ABI (include/turboquant_b200.h) over the sm_100a kernels.
+//
+// Host responsibilities: argument validation (the reference binding's checks,
+// python/turboquant/bindings.cpp:14-49, 159-209), table construction and
+// upload, device selection, stream-ordered scratch, and chunked host<->device
+// streaming for the host-pointer entry points.  No C++ exception crosses the
+// ABI: every entry point catches and converts to a tq_status.
+#include "turboquant_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "tq_internal.h"
+#include "tq_tables.h"
+
+struct tq_space {
+    size_t dim = 0, D = 0, packed_bytes = 0, code_size = 0;
+    int bits = 0, levels = 0, num_threads = 1, device = -1;
+    bool padded = false;
+    uint64_t rot_seed = 0, qjl_seed = 0;
+    std::vector<float> centroids, boundaries, rot_signs, qjl_signs;
+    tq::QuantLut qlut;
+    tq::Params P{};
+    tq::DevTables T{};
+    void *dev_block = nullptr;  // single device allocation holding the tables
+    std::mutex host_mu;         // serialises the host-pointer entry points
+    cudaStream_t host_stream[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+tq_status fail(tq_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+tq_status cuda_fail(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(TQ_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    return fail(TQ_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define TQ_CUDA(call, what)                          \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1, want = -1;
+    explicit DeviceGuard(int dev) : want(dev) {
+        cudaGetDevice(&prev);
+        if (prev != want) cudaSetDevice(want);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0 && prev != want) cudaSetDevice(prev);
+    }
+};
+
+int ilog2(size_t v) {
+    int l = 0;
+    while ((size_t(1) << l) < v) ++l;
+    return l;
+}
+
+tq_status need_device(const tq_space *sp) {
+    if (!sp) return fail(TQ_ERR_INVALID_ARGUMENT, "space is NULL");
+    if (sp->device < 0 || !sp->dev_block)
+        return fail(TQ_ERR_NO_DEVICE,
+                    "no CUDA device: the TurboQuant B200 kernels need an sm_100 GPU");
+    return TQ_OK;
+}
+
+bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+tq_status check_dev(const void *p, size_t bytes, const char *name) {
+    if (bytes == 0) return TQ_OK;
+    if (!p) return fail(TQ_ERR_INVALID_ARGUMENT, "%s: NULL pointer", name);
+    if (!is_device_ptr(p)) return fail(TQ_ERR_INVALID_ARGUMENT, "%s: not a device pointer", name);
+    return TQ_OK;
+}
+
+tq_status check_codes_align(const void *p, const char *name) {
+    if (reinterpret_cast<uintptr_t>(p) & 3)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "%s: device codes must be 4-byte aligned", name);
+    return TQ_OK;
+}
+
+// Stream-ordered scratch from the device's default pool.
+struct Scratch {
+    void *p = nullptr;
+    cudaStream_t st = nullptr;
+    ~Scratch() {
+        if (p) cudaFreeAsync(p, st);
+    }
+    cudaError_t alloc(size_t bytes, cudaStream_t s) {
+        st = s;
+        return cudaMallocAsync(&p, bytes, s);
+    }
+};
+
+constexpr size_t kChunkBytes = size_t(256) << 20;  // host streaming granularity
+
+tq_status ensure_host_streams(tq_space *sp) {
+    for (auto &s : sp->host_stream)
+        if (!s) TQ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    return TQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tq_last_error(void) { return g_err.c_str(); }
+const char *tq_version(void) { return "turboquant-b200 0.1.0 (sm_100a)"; }
+
+tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_seed,
+                          int num_threads, int device, tq_space **out) {
+    if (!out) return fail(TQ_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (dim < 1) return fail(TQ_ERR_INVALID_ARGUMENT, "TurboQuantSpace: dim must be >= 1");
+    if (bits < 2)
+        return fail(TQ_ERR_INVALID_ARGUMENT,
+                    "TurboQuantSpace: need at least 2 bits (1 MSE + 1 QJL)");
+    if (bits > 9)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "TurboQuantSpace: max 9 bits (8-bit MSE + 1 QJL)");
+    try {
+        auto *sp = new tq_space();
+        sp->dim = dim;
+        size_t D = 1;
+        while (D < (dim < 4 ? 4 : dim)) D <<= 1;  // roundUpPow2(max(dim, 4)) :233-238, 258
+        const int log2D = ilog2(D);
+        if (log2D > tq::kMaxLogD) {
+            delete sp;
+            return fail(TQ_ERR_NOT_SUPPORTED,
+                        "TurboQuantSpace: padded dim %zu exceeds the supported maximum %d", D,
+                        1 << tq::kMaxLogD);
+        }
+        sp->D = D;
+        sp->padded = D != dim;
+        sp->bits = bits;
+        sp->packed_bytes = bits <= 4 ? (D + 1) / 2 : D;  // turbo_quant.h:177-179
+        sp->code_size = sp->packed_bytes + 12;            // :182-184
+        sp->levels = 1 << (bits - 1);
+        sp->rot_seed = rot_seed;
+        sp->qjl_seed = qjl_seed;
+        sp->num_threads = num_threads > 0 ? num_threads : 1;
+        if (sp->padded)  // the reference's warning, space_turbo_quant.h:269-273
+            fprintf(stderr,
+                    "[TurboQuantSpace] warning: input dim %zu is not a power of 2 (or < 4); "
+                    "padding to %zu with zeros for internal computation.\n",
+                    dim, D);
+        tq::lloyd_max(bits - 1, sp->centroids, sp->boundaries);
+        sp->rot_signs = tq::sign_vector(D, rot_seed);
+        sp->qjl_signs = tq::sign_vector(D, qjl_seed);
+
+        tq::Params &P = sp->P;
+        P.dim = (int)dim;
+        P.D = (int)D;
+        P.log2D = log2D;
+        P.bits = bits;
+        P.nibble = bits <= 4;
+        P.levels = sp->levels;
+        P.nb = sp->levels - 1;
+        P.pb = (int)sp->packed_bytes;
+        P.cs = (int)sp->code_size;
+        // space_turbo_quant.h:265-266 and turbo_quant.h:69, in FP32 as written
+        P.scale = std::sqrt(static_cast<float>(M_PI) / 2.0f) / std::sqrt(static_cast<float>(D));
+        P.wht_scale = 1.0f / std::sqrt(static_cast<float>(D));
+        P.lutq = 0;
+        P.qlut_k = 0;
+        if (P.nb > 15 && tq::build_quant_lut(sp->boundaries, tq::kQlutBuckets, tq::kQlutMaxK, sp->qlut)) {
+            P.lutq = 1;
+            P.qlut_k = sp->qlut.k;
+            P.qlut_s = sp->qlut.s;
+            P.qlut_c = sp->qlut.c;
+        }
+
+        // device binding (optional: without a GPU the space answers geometry
+        // and table queries, and every compute entry point reports NO_DEVICE)
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+            cudaGetLastError();
+            ndev = 0;
+        }
+        if (ndev > 0) {
+            int dev = device;
+            if (dev < 0) cudaGetDevice(&dev);
+            if (dev >= ndev) {
+                delete sp;
+                return fail(TQ_ERR_INVALID_ARGUMENT, "device %d out of range (%d devices)", dev, ndev);
+            }
+            int major = 0;
+            cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+            if (major != 10) {
+                delete sp;
+                return fail(TQ_ERR_NO_DEVICE, "device %d is sm_%d*, these kernels are built for sm_100a",
+                            dev, major);
+            }
+            DeviceGuard g(dev);
+            const size_t mw = (D + 31) / 32;
+            const size_t off_c = 0, off_b = 4 * 256, off_q = off_b + 4 * (256 + tq::kQlutMaxK + 4);
+            const size_t off_r = off_q + tq::kQlutBuckets, off_j = off_r + 4 * mw;
+            const size_t total = off_j + 4 * mw;
+            std::vector<unsigned char> host(total, 0);
+            std::memcpy(host.data() + off_c, sp->centroids.data(), 4 * sp->levels);
+            std::vector<float> bnd(256 + tq::kQlutMaxK + 4, INFINITY);
+            std::copy(sp->boundaries.begin(), sp->boundaries.end(), bnd.begin());
+            std::memcpy(host.data() + off_b, bnd.data(), 4 * bnd.size());
+            if (P.lutq) std::memcpy(host.data() + off_q, sp->qlut.lo.data(), tq::kQlutBuckets);
+            std::vector<uint32_t> rm(mw, 0), qm(mw, 0);
+            for (size_t i = 0; i < D; ++i) {
+                if (sp->rot_signs[i] > 0) rm[i >> 5] |= 1u << (i & 31);
+                if (sp->qjl_signs[i] > 0) qm[i >> 5] |= 1u << (i & 31);
+            }
+            std::memcpy(host.data() + off_r, rm.data(), 4 * mw);
+            std::memcpy(host.data() + off_j, qm.data(), 4 * mw);
+            cudaError_t e = cudaMalloc(&sp->dev_block, total);
+            if (e != cudaSuccess) {
+                delete sp;
+                return cuda_fail(e, "cudaMalloc(tables)");
+            }
+            e = cudaMemcpy(sp->dev_block, host.data(), total, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(sp->dev_block);
+                delete sp;
+                return cuda_fail(e, "cudaMemcpy(tables)");
+            }
+            auto *base = static_cast<unsigned char *>(sp->dev_block);
+            sp->T.centroids = reinterpret_cast<const float *>(base + off_c);
+            sp->T.boundaries = reinterpret_cast<const float *>(base + off_b);
+            sp->T.qlut = base + off_q;
+            sp->T.rot_mask = reinterpret_cast<const uint32_t *>(base + off_r);
+            sp->T.qjl_mask = reinterpret_cast<const uint32_t *>(base + off_j);
+            sp->device = dev;
+            // keep freed scratch in the pool between calls
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t thr = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+            }
+        }
+        *out = sp;
+        return TQ_OK;
+    } catch (const std::bad_alloc &) {
+        return fail(TQ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (...) {
+        return fail(TQ_ERR_CUDA, "unexpected failure in tq_space_create");
+    }
+}
+
+void tq_space_destroy(tq_space *sp) {
+    if (!sp) return;
+    if (sp->device >= 0) {
+        DeviceGuard g(sp->device);
+        for (auto &s : sp->host_stream)
+            if (s) cudaStreamDestroy(s);
+        if (sp->dev_block) cudaFree(sp->dev_block);
+    }
+    delete sp;
+}
+
+tq_status tq_space_get_info(const tq_space *sp, tq_space_info *info) {
+    if (!sp || !info) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    info->dim = sp->dim;
+    info->padded_dim = sp->D;
+    info->packed_bytes = sp->packed_bytes;
+    info->code_size = sp->code_size;
+    info->bits_per_coord = sp->bits;
+    info->num_levels = sp->levels;
+    info->padded = sp->padded ? 1 : 0;
+    info->num_threads = sp->num_threads;
+    info->device = sp->device;
+    info->rot_seed = sp->rot_seed;
+    info->qjl_seed = sp->qjl_seed;
+    info->scale = sp->P.scale;
+    return TQ_OK;
+}
+
+tq_status tq_space_tables(const tq_space *sp, float *centroids, float *boundaries,
+                          float *rot_signs, float *qjl_signs) {
+    if (!sp) return fail(TQ_ERR_INVALID_ARGUMENT, "space is NULL");
+    if (centroids) std::memcpy(centroids, sp->centroids.data(), 4 * sp->centroids.size());
+    if (boundaries) std::memcpy(boundaries, sp->boundaries.data(), 4 * sp->boundaries.size());
+    if (rot_signs) std::memcpy(rot_signs, sp->rot_signs.data(), 4 * sp->rot_signs.size());
+    if (qjl_signs) std::memcpy(qjl_signs, sp->qjl_signs.data(), 4 * sp->qjl_signs.size());
+    return TQ_OK;
+}
+
+tq_status tq_space_quantize(const tq_space *sp, const float *z, size_t n, uint8_t *idx) {
+    if (!sp) return fail(TQ_ERR_INVALID_ARGUMENT, "space is NULL");
+    if (n && (!z || !idx)) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    const tq::Params &P = sp->P;
+    for (size_t i = 0; i < n; ++i) {
+        int c = 0;
+        if (P.lutq) {
+            const int j = tq::quant_bucket(z[i], P.qlut_s, P.qlut_c, tq::kQlutBuckets);
+            c = sp->qlut.lo[j];
+            const int lo = c;
+            for (int t = 0; t < P.qlut_k; ++t) {
+                const float b = (lo + t < P.nb) ? sp->boundaries[lo + t] : INFINITY;
+                c += (z[i] > b) ? 1 : 0;
+            }
+        } else {
+            for (int t = 0; t < P.nb; ++t) c += (z[i] > sp->boundaries[t]) ? 1 : 0;
+        }
+        idx[i] = static_cast<uint8_t>(c & 0xFF);
+    }
+    return TQ_OK;
+}
+
+// ---- device-pointer entry points -------------------------------------------
+
+tq_status tq_encode_batch_device(const tq_space *sp, const float *X, size_t n, uint8_t *out,
+                                 void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(X, n * sp->dim * 4, "X")) != TQ_OK) return st;
+    if ((st = check_dev(out, n * sp->code_size, "out")) != TQ_OK) return st;
+    TQ_CUDA(tq::launch_encode(sp->P, sp->T, X, n, out, (cudaStream_t)stream), "encode kernel");
+    return TQ_OK;
+}
+
+tq_status tq_prepare_queries_device(const tq_space *sp, const float *Q, size_t m, float *q_rot,
+                                    float *s_q, float *norms, void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (m == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(Q, m * sp->dim * 4, "queries")) != TQ_OK) return st;
+    if ((st = check_dev(q_rot, m * sp->D * 4, "q_rot")) != TQ_OK) return st;
+    if ((st = check_dev(s_q, m * sp->D * 4, "s_q")) != TQ_OK) return st;
+    if ((st = check_dev(norms, m * 8, "norms")) != TQ_OK) return st;
+    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, Q, m, q_rot, s_q, norms, (cudaStream_t)stream),
+            "prepare kernel");
+    return TQ_OK;
+}
+
+tq_status tq_distance_1_to_n_device(const tq_space *sp, const float *query,
+                                    const uint8_t *codes, size_t n, float *out, void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(query, sp->dim * 4, "query")) != TQ_OK) return st;
+    if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
+    if ((st = check_codes_align(codes, "codes")) != TQ_OK) return st;
+    if ((st = check_dev(out, n * 4, "out")) != TQ_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    Scratch scr;
+    TQ_CUDA(scr.alloc(sizeof(float) * (2 * sp->D + 2), s), "cudaMallocAsync(prepared query)");
+    float *q_rot = static_cast<float *>(scr.p), *s_q = q_rot + sp->D, *norms = s_q + sp->D;
+    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, query, 1, q_rot, s_q, norms, s), "prepare kernel");
+    TQ_CUDA(tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out, s), "scan kernel");
+    return TQ_OK;
+}
+
+tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_rot,
+                                             const float *s_q, const float *norms,
+                                             const uint8_t *codes, size_t n, float *out,
+                                             void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(q_rot, sp->D * 4, "q_rot")) != TQ_OK) return st;
+    if ((st = check_dev(s_q, sp->D * 4, "s_q")) != TQ_OK) return st;
+    if ((st = check_dev(norms, 8, "norms")) != TQ_OK) return st;
+    if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
+    if ((st = check_codes_align(codes, "codes")) != TQ_OK) return st;
+    if ((st = check_dev(out, n * 4, "out")) != TQ_OK) return st;
+    TQ_CUDA(tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out,
+                                   (cudaStream_t)stream),
+            "scan kernel");
+    return TQ_OK;
+}
+
+tq_status tq_distance_m_to_n_device(const tq_space *sp, const float *queries, size_t m,
+                                    const uint8_t *codes, size_t n, float *out,
+                                    tq_precision precision, void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if (m == 0 || n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(queries, m * sp->dim * 4, "queries")) != TQ_OK) return st;
+    if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
+    if ((st = check_codes_align(codes, "codes")) != TQ_OK) return st;
+    if ((st = check_dev(out, m * n * 4, "out")) != TQ_OK) return st;
+    if (precision == TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n is not built yet");
+    cudaStream_t s = (cudaStream_t)stream;
+    Scratch scr;
+    TQ_CUDA(scr.alloc(sizeof(float) * m * (2 * sp->D + 2), s), "cudaMallocAsync(prepared queries)");
+    float *q_rot = static_cast<float *>(scr.p), *s_q = q_rot + m * sp->D, *norms = s_q + m * sp->D;
+    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, queries, m, q_rot, s_q, norms, s), "prepare kernel");
+    TQ_CUDA(tq::launch_mton_fp32(sp->P, sp->T, q_rot, s_q, norms, m, codes, n, out, n, s),
+            "m_to_n kernel");
+    return TQ_OK;
+}
+
+tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t *A, size_t m,
+                                              const uint8_t *B, size_t n, float *out,
+                                              tq_precision precision, void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if (m == 0 || n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(A, m * sp->code_size, "codes_a")) != TQ_OK) return st;
+    if ((st = check_dev(B, n * sp->code_size, "codes_b")) != TQ_OK) return st;
+    if ((st = check_codes_align(A, "codes_a")) != TQ_OK) return st;
+    if ((st = check_codes_align(B, "codes_b")) != TQ_OK) return st;
+    if ((st = check_dev(out, m * n * 4, "out")) != TQ_OK) return st;
+    if (precision == TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n_symmetric is not built yet");
+    TQ_CUDA(tq::launch_mton_sym_fp32(sp->P, sp->T, A, m, B, n, out, n, (cudaStream_t)stream),
+            "symmetric m_to_n kernel");
+    return TQ_OK;
+}
+
+// ---- host-pointer entry points ---------------------------------------------
+// Inputs are streamed through the GPU in chunks of ~256 MB on two streams that
+// alternate, so the copies of one chunk overlap the kernels of the other.
+
+tq_status tq_encode_batch(const tq_space *csp, const float *X, size_t n, uint8_t *out) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    if (!X || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    const size_t row_bytes = sp->dim * 4;
+    size_t rows = std::max<size_t>(4, (kChunkBytes / row_bytes) & ~size_t(3));
+    rows = std::min(rows, n);
+    Scratch buf[2];
+    for (int k = 0; k < 2; ++k)
+        TQ_CUDA(buf[k].alloc(rows * (row_bytes + sp->code_size), sp->host_stream[k]),
+                "cudaMallocAsync(encode staging)");
+    size_t chunk = 0;
+    for (size_t r0 = 0; r0 < n; r0 += rows, ++chunk) {
+        const size_t nr = std::min(rows, n - r0);
+        cudaStream_t s = sp->host_stream[chunk & 1];
+        float *dX = static_cast<float *>(buf[chunk & 1].p);
+        uint8_t *dC = reinterpret_cast<uint8_t *>(dX) + rows * row_bytes;
+        TQ_CUDA(cudaMemcpyAsync(dX, X + r0 * sp->dim, nr * row_bytes, cudaMemcpyHostToDevice, s),
+                "H2D X");
+        TQ_CUDA(tq::launch_encode(sp->P, sp->T, dX, nr, dC, s), "encode kernel");
+        TQ_CUDA(cudaMemcpyAsync(out + r0 * sp->code_size, dC, nr * sp->code_size,
+                                cudaMemcpyDeviceToHost, s),
+                "D2H codes");
+    }
+    for (auto &s : sp->host_stream) TQ_CUDA(cudaStreamSynchronize(s), "encode");
+    return TQ_OK;
+}
+
+tq_status tq_distance_1_to_n(const tq_space *csp, const float *query, const uint8_t *codes,
+                             size_t n, float *out) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    if (!query || !codes || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    const size_t cs = sp->code_size;
+    size_t per = std::max<size_t>(1, kChunkBytes / cs);
+    per = std::min(per, n);
+    cudaStream_t s0 = sp->host_stream[0];
+    Scratch qs;
+    TQ_CUDA(qs.alloc(sizeof(float) * (sp->dim + 2 * sp->D + 2), s0), "cudaMallocAsync(query)");
+    float *dq = static_cast<float *>(qs.p), *q_rot = dq + sp->dim, *s_q = q_rot + sp->D,
+          *norms = s_q + sp->D;
+    TQ_CUDA(cudaMemcpyAsync(dq, query, sp->dim * 4, cudaMemcpyHostToDevice, s0), "H2D query");
+    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, dq, 1, q_rot, s_q, norms, s0), "prepare kernel");
+    cudaEvent_t ready;
+    TQ_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+    cudaEventRecord(ready, s0);
+    cudaStreamWaitEvent(sp->host_stream[1], ready, 0);
+    Scratch buf[2];
+    tq_status result = TQ_OK;
+    for (int k = 0; k < 2 && result == TQ_OK; ++k) {
+        cudaError_t e = buf[k].alloc(per * (cs + 4) + 16, sp->host_stream[k]);
+        if (e != cudaSuccess) result = cuda_fail(e, "cudaMallocAsync(scan staging)");
+    }
+    size_t chunk = 0;
+    for (size_t c0 = 0; c0 < n && result == TQ_OK; c0 += per, ++chunk) {
+        const size_t nc = std::min(per, n - c0);
+        cudaStream_t s = sp->host_stream[chunk & 1];
+        uint8_t *dC = static_cast<uint8_t *>(buf[chunk & 1].p);
+        float *dO = reinterpret_cast<float *>(dC + ((per * cs + 15) & ~size_t(15)));
+        cudaError_t e = cudaMemcpyAsync(dC, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, dC, nc, dO, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out + c0, dO, nc * 4, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) result = cuda_fail(e, "distance_1_to_n chunk");
+    }
+    for (auto &s : sp->host_stream) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess && result == TQ_OK) result = cuda_fail(e, "distance_1_to_n");
+    }
+    cudaEventDestroy(ready);
+    return result;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Shared driver of the two host-pointer M x N entry points: the row side
+// (prepared queries, or codes_a) is uploaded once, the column side (codes) is
+// streamed in chunks, and each [m, nc] output block is copied back into the
+// row-major [m, n] result with a pitched copy.
+template <typename Launch>
+tq_status mton_host(tq_space *sp, size_t m, const uint8_t *codes, size_t n, float *out,
+                    size_t row_side_bytes, const void *row_side_host,
+                    const Launch &launch_block) {
+    const size_t cs = sp->code_size;
+    size_t per = std::max<size_t>(1, std::min(kChunkBytes / cs, (kChunkBytes * 2) / (4 * m)));
+    per = std::min(per, n);
+    cudaStream_t s0 = sp->host_stream[0];
+    Scratch rs;
+    TQ_CUDA(rs.alloc(row_side_bytes, s0), "cudaMallocAsync(row side)");
+    TQ_CUDA(cudaMemcpyAsync(rs.p, row_side_host, row_side_bytes, cudaMemcpyHostToDevice, s0), "H2D rows");
+    tq_status result = TQ_OK;
+    void *prepared = nullptr;
+    {
+        cudaError_t e = launch_block(rs.p, nullptr, 0, nullptr, 0, s0, &prepared, true);
+        if (e != cudaSuccess) return cuda_fail(e, "row preparation");
+    }
+    cudaEvent_t ready;
+    TQ_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+    cudaEventRecord(ready, s0);
+    cudaStreamWaitEvent(sp->host_stream[1], ready, 0);
+    Scratch buf[2];
+    for (int k = 0; k < 2 && result == TQ_OK; ++k) {
+        cudaError_t e = buf[k].alloc(((per * cs + 15) & ~size_t(15)) + per * m * 4, sp->host_stream[k]);
+        if (e != cudaSuccess) result = cuda_fail(e, "cudaMallocAsync(m_to_n staging)");
+    }
+    size_t chunk = 0;
+    for (size_t c0 = 0; c0 < n && result == TQ_OK; c0 += per, ++chunk) {
+        const size_t nc = std::min(per, n - c0);
+        cudaStream_t s = sp->host_stream[chunk & 1];
+        uint8_t *dC = static_cast<uint8_t *>(buf[chunk & 1].p);
+        float *dO = reinterpret_cast<float *>(dC + ((per * cs + 15) & ~size_t(15)));
+        cudaError_t e = cudaMemcpyAsync(dC, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = launch_block(rs.p, dC, nc, dO, nc, s, &prepared, false);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(out + c0, n * 4, dO, nc * 4, nc * 4, m, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) result = cuda_fail(e, "m_to_n chunk");
+    }
+    for (auto &s : sp->host_stream) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess && result == TQ_OK) result = cuda_fail(e, "m_to_n");
+    }
+    cudaEventDestroy(ready);
+    if (prepared) cudaFree(prepared);
+    return result;
+}
+
+}  // namespace
+
+extern "C" {
+
+tq_status tq_distance_m_to_n(const tq_space *csp, const float *queries, size_t m,
+                             const uint8_t *codes, size_t n, float *out, tq_precision precision) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if (m == 0 || n == 0) return TQ_OK;
+    if (!queries || !codes || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (precision == TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n is not built yet");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    const size_t D = sp->D;
+    auto launch = [&](void *rows, const uint8_t *dC, size_t nc, float *dO, size_t ldo,
+                      cudaStream_t s, void **prepared, bool prep) -> cudaError_t {
+        if (prep) {
+            cudaError_t e = cudaMalloc(prepared, sizeof(float) * m * (2 * D + 2));
+            if (e != cudaSuccess) return e;
+            float *q_rot = static_cast<float *>(*prepared);
+            return tq::launch_prepare(sp->P, sp->T, static_cast<const float *>(rows), m, q_rot,
+                                      q_rot + m * D, q_rot + 2 * m * D, s);
+        }
+        float *q_rot = static_cast<float *>(*prepared);
+        return tq::launch_mton_fp32(sp->P, sp->T, q_rot, q_rot + m * D, q_rot + 2 * m * D, m, dC, nc,
+                                    dO, ldo, s);
+    };
+    return mton_host(sp, m, codes, n, out, m * sp->dim * 4, queries, launch);
+}
+
+tq_status tq_distance_m_to_n_symmetric(const tq_space *csp, const uint8_t *codes_a, size_t m,
+                                       const uint8_t *codes_b, size_t n, float *out,
+                                       tq_precision precision) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if (m == 0 || n == 0) return TQ_OK;
+    if (!codes_a || !codes_b || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (precision == TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n_symmetric is not built yet");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    auto launch = [&](void *rows, const uint8_t *dC, size_t nc, float *dO, size_t ldo,
+                      cudaStream_t s, void **, bool prep) -> cudaError_t {
+        if (prep) return cudaSuccess;
+        return tq::launch_mton_sym_fp32(sp->P, sp->T, static_cast<const uint8_t *>(rows), m, dC, nc,
+                                        dO, ldo, s);
+    };
+    return mton_host(sp, m, codes_b, n, out, m * sp->code_size, codes_a, launch);
+}
+
+}  // extern "C"

@@ -1,0 +1,822 @@
+// tq_kernels.cu -- sm_100a kernels of the TurboQuant encode-and-scan path.
+//
+//   encode_kernel   fused encodeVector (space_turbo_quant.h:339-396): norm,
+//                   sign flip + FWHT, sigma, Lloyd-Max quantize, residual,
+//                   gamma, QJL sign flip + FWHT, pack + trailer.  Bit-exact
+//                   with the reference's pinned Release build.
+//   prepare_kernel  prepareQuery (:439-460).
+//   scan_kernel     asymmetric distSearch* (:659-686, 951-983) over a code
+//                   stream (distanceBatch1ToN/MToN :577-599) and the MSE-only
+//                   symmetric distBuild* (:688-714, 985-1019) (MToNSymmetric
+//                   :602-615).
+//
+// Rounding discipline: every float operation whose rounding the reference
+// fixes is written with an explicit round-to-nearest intrinsic (__fadd_rn,
+// __fmul_rn, __fmaf_rn, __fdiv_rn, __fsqrt_rn) so that nvcc cannot contract
+// or reassociate it.
+#include "tq_internal.h"
+
+#include <cstdint>
+
+namespace tq {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float f32_bits(uint32_t u) { return __uint_as_float(u); }
+
+// Bijective index swizzle of a vector held in shared memory: the low 5 bits
+// (the bank) are XORed with bits 5-9 and 10-14.  It makes the FWHT passes'
+// group loads (contiguous or strided) and the 8-lane reduction chains
+// bank-conflict-free for the power-of-two sizes used here.
+__device__ __forceinline__ int swz(int e) { return e ^ (((e >> 5) ^ (e >> 10)) & 31); }
+
+// Multiply by the +-1 sign of element e (bit set = +1): an exact sign flip.
+__device__ __forceinline__ float apply_sign(float x, const uint32_t *mask, int e) {
+    const uint32_t bit = (mask[e >> 5] >> (e & 31)) & 1u;
+    return __uint_as_float(__float_as_uint(x) ^ ((bit ^ 1u) << 31));
+}
+
+// ---------------------------------------------------------------------------
+// Warp-level FWHT on a swizzled shared-memory vector of D = 2^LOG_D floats.
+// The butterflies run in stage order stride 1, 2, 4, ..., D/2 exactly as
+// whtInplaceScalar (turbo_quant.h:46-60) -- each output is a single rounding
+// of a + b or a - b of the previous stage, so the result is bit-identical.
+// Stages are grouped into passes of up to 5 (2^5 values per group held in
+// registers); a pass reads and writes the vector once.
+//   pass 1 also applies the pre-multiply (x * pre, rounded) and the sign flip
+//   (randomizedHadamard, turbo_quant.h:95-97); the last pass applies the
+//   1/sqrt(D) normalisation (turbo_quant.h:69-71).
+// ---------------------------------------------------------------------------
+template <int LOG_D>
+struct FwhtPlan {
+    static constexpr int PL = (LOG_D - 5 < 1) ? 1 : ((LOG_D - 5 > 5) ? 5 : LOG_D - 5);
+};
+
+template <int LOG_D, int S0, int R, bool FIRST, bool LAST, bool PREMUL>
+__device__ __forceinline__ void fwht_pass(float *buf, int lane, float pre, const uint32_t *mask,
+                                          float post) {
+    constexpr int D = 1 << LOG_D;
+    constexpr int NR = 1 << R;
+    constexpr int NG = D / NR;
+    constexpr int G = (NG + 31) / 32;
+#pragma unroll
+    for (int gi = 0; gi < G; ++gi) {
+        const int o = lane + 32 * gi;
+        if ((NG & 31) != 0 && o >= NG) break;
+        const int base = (o & ((1 << S0) - 1)) | ((o >> S0) << (S0 + R));
+        float v[NR];
+#pragma unroll
+        for (int t = 0; t < NR; ++t) {
+            const int e = base | (t << S0);
+            float x = buf[swz(e)];
+            if constexpr (FIRST) {
+                if constexpr (PREMUL) x = __fmul_rn(x, pre);
+                x = apply_sign(x, mask, e);
+            }
+            v[t] = x;
+        }
+#pragma unroll
+        for (int s = 0; s < R; ++s) {
+#pragma unroll
+            for (int t = 0; t < NR; ++t) {
+                if (!(t & (1 << s))) {
+                    const float a = v[t], b = v[t | (1 << s)];
+                    v[t] = __fadd_rn(a, b);
+                    v[t | (1 << s)] = __fsub_rn(a, b);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < NR; ++t) {
+            float x = v[t];
+            if constexpr (LAST) x = __fmul_rn(x, post);
+            buf[swz(base | (t << S0))] = x;
+        }
+    }
+}
+
+template <int LOG_D, int S0, bool PREMUL>
+__device__ __forceinline__ void fwht_from(float *buf, int lane, float pre, const uint32_t *mask,
+                                          float post) {
+    if constexpr (S0 < LOG_D) {
+        constexpr int PL = FwhtPlan<LOG_D>::PL;
+        constexpr int R = (LOG_D - S0 < PL) ? (LOG_D - S0) : PL;
+        fwht_pass<LOG_D, S0, R, S0 == 0, S0 + R == LOG_D, PREMUL>(buf, lane, pre, mask, post);
+        __syncwarp();
+        fwht_from<LOG_D, S0 + R, PREMUL>(buf, lane, pre, mask, post);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The reference's FP32 sum of squares as its pinned build evaluates it
+// (space_turbo_quant.h:343-344, 354-355, 370-371; restated in the CPU
+// checker): 8 accumulators acc[k] += x[i]^2 for i = k (mod 8) with separate
+// multiply and add roundings; t[k] = acc[k] + acc[k+4]; s = (t0+t2)+(t1+t3);
+// a 4-wide FMA step over the next 4 leftovers (from t, or from zero when
+// n < 8) and a scalar FMA tail.  Evaluated by the 8 lanes of group
+// g = lane/8 on the swizzled vector `buf`; all 8 lanes return the sum.  All
+// 32 lanes must call it.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float chain_sq_reduce(const float *buf, int n, int lane) {
+    const int k = lane & 7;
+    const int n8 = n & ~7;
+    float acc = 0.0f;
+#pragma unroll 8
+    for (int i = k; i < n8; i += 8) {
+        const float x = buf[swz(i)];
+        acc = __fadd_rn(acc, __fmul_rn(x, x));
+    }
+    const float hi = __shfl_down_sync(kFull, acc, 4, 8);
+    const float t = __fadd_rn(acc, hi);
+    float t0 = __shfl_sync(kFull, t, 0, 8);
+    float t1 = __shfl_sync(kFull, t, 1, 8);
+    float t2 = __shfl_sync(kFull, t, 2, 8);
+    float t3 = __shfl_sync(kFull, t, 3, 8);
+    float s = __fadd_rn(__fadd_rn(t0, t2), __fadd_rn(t1, t3));
+    int b = n8, r = n - n8;
+    if (r >= 4) {
+        const float x0 = buf[swz(b)], x1 = buf[swz(b + 1)];
+        const float x2 = buf[swz(b + 2)], x3 = buf[swz(b + 3)];
+        t0 = __fmaf_rn(x0, x0, t0);
+        t1 = __fmaf_rn(x1, x1, t1);
+        t2 = __fmaf_rn(x2, x2, t2);
+        t3 = __fmaf_rn(x3, x3, t3);
+        s = __fadd_rn(__fadd_rn(t0, t2), __fadd_rn(t1, t3));
+        b += 4;
+        r -= 4;
+    }
+    for (int j = 0; j < r; ++j) {
+        const float x = buf[swz(b + j)];
+        s = __fmaf_rn(x, x, s);
+    }
+    return s;
+}
+
+// quantize (space_turbo_quant.h:332-337): idx = #{j : z > B[j]}.
+// nb <= 15: the direct count.  Otherwise bucket j = clamp(fma(z, S, C)) of a
+// 2048-entry table gives lo = the number of boundaries every z of that bucket
+// exceeds, and only the next qlut_k boundaries are compared.  The host builds
+// the table from the exact float range of each bucket, so the count is exact.
+__device__ __forceinline__ int quantize(float z, const Params &P, const float *bnd,
+                                        const uint8_t *qlut) {
+    int idx = 0;
+    if (P.lutq) {
+        float y = __fmaf_rn(z, P.qlut_s, P.qlut_c);
+        y = fminf(fmaxf(y, 0.0f), (float)(kQlutBuckets - 1));
+        idx = qlut[(int)y];
+        const int lo = idx;
+        for (int t = 0; t < P.qlut_k; ++t) idx += (z > bnd[lo + t]) ? 1 : 0;
+    } else {
+        for (int t = 0; t < P.nb; ++t) idx += (z > bnd[t]) ? 1 : 0;
+    }
+    return idx & 0xFF;  // the reference accumulates into a uint8_t
+}
+
+// Shared table block of the encode / prepare kernels.
+constexpr int kTabCentOff = 0;                                  // float[256]
+constexpr int kTabBndOff = kTabCentOff + 4 * kMaxLevels;        // float[256 + 8]
+constexpr int kTabRotOff = kTabBndOff + 4 * (kMaxLevels + 8);   // u32[256]
+constexpr int kTabQjlOff = kTabRotOff + 4 * 256;                // u32[256]
+constexpr int kTabQlutOff = kTabQjlOff + 4 * 256;               // u8[2048]
+constexpr int kTabBytes = kTabQlutOff + kQlutBuckets;           // 6176 (16-aligned)
+static_assert(kTabBytes % 16 == 0, "table block must keep 16-byte alignment");
+
+__device__ __forceinline__ void load_tables(unsigned char *smem, const Params &P,
+                                            const DevTables &T, bool quant) {
+    float *cent = reinterpret_cast<float *>(smem + kTabCentOff);
+    float *bnd = reinterpret_cast<float *>(smem + kTabBndOff);
+    uint32_t *rot = reinterpret_cast<uint32_t *>(smem + kTabRotOff);
+    uint32_t *qjl = reinterpret_cast<uint32_t *>(smem + kTabQjlOff);
+    uint8_t *qlut = smem + kTabQlutOff;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int mw = (P.D + 31) >> 5;
+    for (int i = tid; i < mw; i += nt) {
+        rot[i] = T.rot_mask[i];
+        qjl[i] = T.qjl_mask[i];
+    }
+    if (quant) {
+        for (int i = tid; i < P.levels; i += nt) cent[i] = T.centroids[i];
+        for (int i = tid; i < P.nb + kQlutMaxK; i += nt) bnd[i] = T.boundaries[i];
+        if (P.lutq)
+            for (int i = tid; i < kQlutBuckets; i += nt) qlut[i] = T.qlut[i];
+    }
+}
+
+__host__ __device__ __forceinline__ int align16(int x) { return (x + 15) & ~15; }
+
+// Per-warp shared bytes of the encode kernel: 4 vectors of D+8 floats, 4 x D
+// quantizer indices, 4 staged codes.
+__host__ __device__ __forceinline__ int encode_warp_bytes(int D, int cs) {
+    return 16 * (D + 8) + 4 * D + align16(4 * cs);
+}
+
+// ---------------------------------------------------------------------------
+// encode: one warp per group of 4 consecutive rows ("quad").
+// ---------------------------------------------------------------------------
+template <int LOG_D>
+__global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X, size_t n,
+                                                     uint8_t *__restrict__ out, Params P,
+                                                     DevTables T) {
+    constexpr int D = 1 << LOG_D;
+    constexpr int VS = D + 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    load_tables(smem, P, T, true);
+    __syncthreads();
+    const float *s_cent = reinterpret_cast<const float *>(smem + kTabCentOff);
+    const float *s_bnd = reinterpret_cast<const float *>(smem + kTabBndOff);
+    const uint32_t *s_rot = reinterpret_cast<const uint32_t *>(smem + kTabRotOff);
+    const uint32_t *s_qjl = reinterpret_cast<const uint32_t *>(smem + kTabQjlOff);
+    const uint8_t *s_qlut = smem + kTabQlutOff;
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int cs = P.cs;
+    unsigned char *wbase = smem + kTabBytes + warp * encode_warp_bytes(D, cs);
+    float *buf = reinterpret_cast<float *>(wbase);
+    uint8_t *idxb = wbase + 16 * VS;
+    uint8_t *stage = idxb + 4 * D;
+    const int g = lane >> 3;
+    float *gbuf = buf + g * VS;
+    const bool vec4 = ((P.dim & 3) == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    const size_t nquads = (n + 3) >> 2;
+
+    for (size_t qd = (size_t)blockIdx.x * nwarps + warp; qd < nquads;
+         qd += (size_t)gridDim.x * nwarps) {
+        const size_t row0 = qd << 2;
+        const int nv = (n - row0 < 4) ? (int)(n - row0) : 4;
+
+        // A: rows -> shared memory, zero padded to D (space_turbo_quant.h:347-350)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            float *b = buf + v * VS;
+            if (v < nv) {
+                const float *src = X + (row0 + v) * (size_t)P.dim;
+                if (vec4) {
+                    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+                    for (int i4 = lane; i4 < (P.dim >> 2); i4 += 32) {
+                        const float4 x = __ldcs(s4 + i4);
+                        const int e = i4 << 2;
+                        b[swz(e)] = x.x;
+                        b[swz(e + 1)] = x.y;
+                        b[swz(e + 2)] = x.z;
+                        b[swz(e + 3)] = x.w;
+                    }
+                } else {
+                    for (int i = lane; i < P.dim; i += 32) b[swz(i)] = __ldcs(src + i);
+                }
+                for (int i = P.dim + lane; i < D; i += 32) b[swz(i)] = 0.0f;
+            } else {
+                for (int i = lane; i < D; i += 32) b[swz(i)] = 0.0f;
+            }
+        }
+        __syncwarp();
+
+        // B: norm (:342-348)
+        const float nsq = chain_sq_reduce(gbuf, P.dim, lane);
+        const float norm = __fsqrt_rn(nsq);
+        const float inv_norm = (nsq > f32_bits(kNormSqFloorBits)) ? __fdiv_rn(1.0f, norm) : 0.0f;
+
+        // C: rotated = RHT_rot(raw * inv_norm) (:349-351)
+#pragma unroll 1
+        for (int v = 0; v < 4; ++v) {
+            const float inv = __shfl_sync(kFull, inv_norm, 8 * v);
+            fwht_from<LOG_D, 0, true>(buf + v * VS, lane, inv, s_rot, P.wht_scale);
+        }
+
+        // D: sigma (:353-359)
+        const float var = chain_sq_reduce(gbuf, D, lane);
+        float sigma = __fsqrt_rn(__fdiv_rn(var, (float)D));
+        float inv_sigma;
+        if (f32_bits(kSigmaFloorBits) > sigma) {
+            sigma = f32_bits(kSigmaFloorBits);
+            inv_sigma = f32_bits(kInvSigmaFloorBits);
+        } else {
+            inv_sigma = __fdiv_rn(1.0f, sigma);
+        }
+
+        // E: quantize + residual (:361-367); the residual is one FMA
+#pragma unroll 1
+        for (int v = 0; v < 4; ++v) {
+            const float sg = __shfl_sync(kFull, sigma, 8 * v);
+            const float isg = __shfl_sync(kFull, inv_sigma, 8 * v);
+            float *b = buf + v * VS;
+            uint8_t *ib = idxb + v * D;
+            for (int i = lane; i < D; i += 32) {
+                const int p = swz(i);
+                const float x = b[p];
+                const int idx = quantize(__fmul_rn(x, isg), P, s_bnd, s_qlut);
+                b[p] = __fmaf_rn(-s_cent[idx], sg, x);
+                ib[i] = (uint8_t)idx;
+            }
+        }
+        __syncwarp();
+
+        // F: gamma (:369-372)
+        const float gamma = __fsqrt_rn(chain_sq_reduce(gbuf, D, lane));
+
+        // G: RHT_qjl(residual) (:374)
+#pragma unroll 1
+        for (int v = 0; v < 4; ++v) fwht_from<LOG_D, 0, false>(buf + v * VS, lane, 1.0f, s_qjl, P.wht_scale);
+
+        // H: pack units + trailer into the staging area (:375-395)
+        for (int v = 0; v < nv; ++v) {
+            const float *b = buf + v * VS;
+            const uint8_t *ib = idxb + v * D;
+            uint8_t *st = stage + v * cs;
+            if (P.nibble) {
+                for (int j = lane; j < P.pb; j += 32) {
+                    const unsigned u0 = ((unsigned)ib[2 * j] << 1) | (b[swz(2 * j)] >= 0.0f ? 1u : 0u);
+                    const unsigned u1 =
+                        ((unsigned)ib[2 * j + 1] << 1) | (b[swz(2 * j + 1)] >= 0.0f ? 1u : 0u);
+                    st[j] = (uint8_t)((u0 | (u1 << 4)) & 0xFFu);
+                }
+            } else {
+                for (int i = lane; i < D; i += 32)
+                    st[i] = (uint8_t)((((unsigned)ib[i] << 1) | (b[swz(i)] >= 0.0f ? 1u : 0u)) & 0xFFu);
+            }
+        }
+        if ((lane & 7) == 0 && g < nv) {
+            uint8_t *t = stage + g * cs + P.pb;
+            const uint32_t w[3] = {__float_as_uint(norm), __float_as_uint(gamma), __float_as_uint(sigma)};
+#pragma unroll
+            for (int q = 0; q < 12; ++q) t[q] = (uint8_t)(w[q >> 2] >> (8 * (q & 3)));
+        }
+        __syncwarp();
+
+        // I: staged codes -> global (one contiguous run of nv * cs bytes)
+        uint8_t *dst = out + row0 * (size_t)cs;
+        const int len = nv * cs;
+        if (((reinterpret_cast<uintptr_t>(dst) & 15) == 0) && ((len & 15) == 0)) {
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(stage);
+            uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+            for (int i = lane; i < (len >> 4); i += 32) __stcs(d4 + i, s4[i]);
+        } else if (((reinterpret_cast<uintptr_t>(dst) & 3) == 0) && ((len & 3) == 0)) {
+            const uint32_t *s1 = reinterpret_cast<const uint32_t *>(stage);
+            uint32_t *d1 = reinterpret_cast<uint32_t *>(dst);
+            for (int i = lane; i < (len >> 2); i += 32) d1[i] = s1[i];
+        } else {
+            for (int i = lane; i < len; i += 32) dst[i] = stage[i];
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// prepareQuery: one warp per query.
+// ---------------------------------------------------------------------------
+template <int LOG_D>
+__global__ void __launch_bounds__(256) prepare_kernel(const float *__restrict__ Q, size_t m,
+                                                      float *__restrict__ q_rot,
+                                                      float *__restrict__ s_q,
+                                                      float *__restrict__ norms, Params P,
+                                                      DevTables T) {
+    constexpr int D = 1 << LOG_D;
+    constexpr int VS = D + 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    load_tables(smem, P, T, false);
+    __syncthreads();
+    const uint32_t *s_rot = reinterpret_cast<const uint32_t *>(smem + kTabRotOff);
+    const uint32_t *s_qjl = reinterpret_cast<const uint32_t *>(smem + kTabQjlOff);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    float *buf = reinterpret_cast<float *>(smem + kTabBytes) + warp * VS;
+    for (size_t qi = (size_t)blockIdx.x * nwarps + warp; qi < m; qi += (size_t)gridDim.x * nwarps) {
+        const float *src = Q + qi * (size_t)P.dim;
+        for (int i = lane; i < D; i += 32) buf[swz(i)] = (i < P.dim) ? src[i] : 0.0f;
+        __syncwarp();
+        // |q|^2: the reference's batch drivers evaluate this loop as a plain
+        // sequential sum (:443-445).
+        float qn2 = 0.0f;
+        if (lane == 0) {
+            for (int i = 0; i < P.dim; ++i) {
+                const float x = buf[swz(i)];
+                qn2 = __fadd_rn(qn2, __fmul_rn(x, x));
+            }
+        }
+        qn2 = __shfl_sync(kFull, qn2, 0);
+        const float qn = __fsqrt_rn(qn2);
+        const float qinv = (qn2 > f32_bits(kNormSqFloorBits)) ? __fdiv_rn(1.0f, qn) : 0.0f;
+        fwht_from<LOG_D, 0, true>(buf, lane, qinv, s_rot, P.wht_scale);
+        float *qr = q_rot + qi * (size_t)D;
+        for (int i = lane; i < D; i += 32) qr[i] = buf[swz(i)];
+        fwht_from<LOG_D, 0, false>(buf, lane, 1.0f, s_qjl, P.wht_scale);
+        float *sq = s_q + qi * (size_t)D;
+        for (int i = lane; i < D; i += 32) sq[i] = buf[swz(i)];
+        if (lane == 0) {
+            norms[2 * qi] = qn2;
+            norms[2 * qi + 1] = qn;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scan: row i of the query side (blockIdx.y) against a stream of n codes.
+//   SYM = false: asymmetric distSearch; the row is a prepared query
+//                (q_rot, s_q, |q|^2, |q|).
+//   SYM = true:  MSE-only distBuild; the row is code a_i, decoded to
+//                c[idx] * sigma_a per coordinate.
+// A code of PB packed bytes is read as W = PB/4 32-bit words by LPC lanes
+// (WPL words each, coalesced); CPS codes share a warp step.  The query side
+// of each lane's positions sits in registers; centroids come from a
+// lane-replicated shared table (entry v of lane l at v*32 + l: conflict-free).
+// ---------------------------------------------------------------------------
+template <int LOG_D, bool NIBBLE>
+struct ScanShape {
+    static constexpr int D = 1 << LOG_D;
+    static constexpr int PB = NIBBLE ? D / 2 : D;
+    static constexpr int W = PB / 4;
+    static constexpr int LPC = W < 1 ? 1 : (W < 32 ? W : 32);
+    static constexpr int WPL = W / LPC;
+    static constexpr int CPS = 32 / LPC;
+    static constexpr int PPW = NIBBLE ? 8 : 4;
+    static constexpr int PPL = WPL * PPW;
+    static constexpr bool QREG = PPL <= 32;
+    static constexpr int U = QREG ? (WPL >= 8 ? 2 : 4) : 1;  // warp steps per iteration
+};
+
+template <int LOG_D, bool NIBBLE>
+__device__ __forceinline__ unsigned unit_of(uint32_t w, int b) {
+    return NIBBLE ? ((w >> (4 * b)) & 15u) : ((w >> (8 * b)) & 255u);
+}
+
+template <int LOG_D, bool NIBBLE, bool SYM>
+__global__ void __launch_bounds__(256) scan_kernel(const float *__restrict__ q_rot,
+                                                   const float *__restrict__ s_q,
+                                                   const float *__restrict__ norms,
+                                                   const uint8_t *__restrict__ codes_a,
+                                                   const uint8_t *__restrict__ codes, size_t n,
+                                                   float *__restrict__ out, size_t ldo, Params P,
+                                                   DevTables T) {
+    using S = ScanShape<LOG_D, NIBBLE>;
+    constexpr int PPL = S::PPL;
+    constexpr int NQ = S::QREG ? PPL : 1;
+    extern __shared__ __align__(16) float fsm[];
+    // one entry per value of (unit >> 1) a code byte can hold: 8 (nibble) or
+    // 128 (byte); entries past the table's levels read as 0
+    constexpr int LUTN = NIBBLE ? 8 : 128;
+    float *s_lut = fsm;                          // [LUTN * 32]
+    float *s_qa = fsm + LUTN * 32;               // !QREG: [PPL * 32] query side (q_rot or a)
+    float *s_qb = s_qa + (S::QREG ? 0 : PPL * 32);  // !QREG: [PPL * 32] -s_q
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int sl = lane % S::LPC, slot = lane / S::LPC;
+    const size_t row = blockIdx.y;
+    const int cs = P.cs;
+    for (int i = tid; i < LUTN * 32; i += blockDim.x) s_lut[i] = T.centroids[i >> 5];
+
+    // query side of this lane's positions p(j, b) = PPW * (sl + LPC * j) + b
+    float qa[NQ], qb[NQ];
+    float rn2 = 0.0f, rn = 0.0f;
+    if constexpr (!SYM) {
+        const float *qr = q_rot + row * (size_t)S::D;
+        const float *sq = s_q + row * (size_t)S::D;
+        rn2 = norms[2 * row];
+        rn = norms[2 * row + 1];
+#pragma unroll
+        for (int j = 0; j < S::WPL; ++j)
+#pragma unroll
+            for (int b = 0; b < S::PPW; ++b) {
+                const int p = S::PPW * (sl + S::LPC * j) + b;
+                const int r = j * S::PPW + b;
+                if constexpr (S::QREG) {
+                    qa[r] = qr[p];
+                    qb[r] = -sq[p];
+                } else if (tid < 32) {
+                    s_qa[r * 32 + lane] = qr[p];
+                    s_qb[r * 32 + lane] = -sq[p];
+                }
+            }
+    } else {
+        const uint8_t *ca = codes_a + row * (size_t)cs;
+        const float *ma = reinterpret_cast<const float *>(ca + S::PB);
+        const float sig_a = ma[2];
+        rn = ma[0];
+        rn2 = __fmul_rn(rn, rn);
+#pragma unroll
+        for (int j = 0; j < S::WPL; ++j) {
+            const uint32_t w = reinterpret_cast<const uint32_t *>(ca)[sl + S::LPC * j];
+#pragma unroll
+            for (int b = 0; b < S::PPW; ++b) {
+                const int r = j * S::PPW + b;
+                const float v = __fmul_rn(T.centroids[unit_of<LOG_D, NIBBLE>(w, b) >> 1], sig_a);
+                if constexpr (S::QREG) qa[r] = v;
+                else if (tid < 32) s_qa[r * 32 + lane] = v;
+            }
+        }
+    }
+    __syncthreads();
+
+    const size_t warps_total = (size_t)gridDim.x * (blockDim.x >> 5);
+    const size_t wg = (size_t)blockIdx.x * (blockDim.x >> 5) + (tid >> 5);
+    float *orow = out + row * ldo;
+    constexpr int STEP = S::CPS * S::U;
+    for (size_t c0 = wg * STEP; c0 < n; c0 += warps_total * STEP) {
+        uint32_t w[S::U][S::WPL];
+        float sig_b[S::U];
+#pragma unroll
+        for (int u = 0; u < S::U; ++u) {
+            const size_t c = c0 + (size_t)u * S::CPS + slot;
+            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + c * (size_t)cs);
+#pragma unroll
+            for (int j = 0; j < S::WPL; ++j) w[u][j] = (c < n) ? __ldg(cw + sl + S::LPC * j) : 0u;
+            if constexpr (SYM)
+                sig_b[u] = (c < n) ? __ldg(reinterpret_cast<const float *>(cw + S::W) + 2) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < S::U; ++u) {
+            float ip = 0.0f, dot = 0.0f;
+#pragma unroll
+            for (int j = 0; j < S::WPL; ++j) {
+#pragma unroll
+                for (int b = 0; b < S::PPW; ++b) {
+                    const int r = j * S::PPW + b;
+                    const unsigned un = unit_of<LOG_D, NIBBLE>(w[u][j], b);
+                    const float cv = s_lut[((un >> 1) << 5) + lane];
+                    const float a = S::QREG ? qa[r] : s_qa[r * 32 + lane];
+                    if constexpr (SYM) {
+                        // (c[a] sigma_a) * (c[b] sigma_b), each factor rounded (:709-710)
+                        ip = __fmaf_rn(a, __fmul_rn(cv, sig_b[u]), ip);
+                    } else {
+                        ip = __fmaf_rn(a, cv, ip);
+                        const float nb = S::QREG ? qb[r] : s_qb[r * 32 + lane];
+                        dot = __fadd_rn(dot, __uint_as_float(__float_as_uint(nb) ^ ((un & 1u) << 31)));
+                    }
+                }
+            }
+#pragma unroll
+            for (int off = S::LPC / 2; off > 0; off >>= 1) {
+                ip = __fadd_rn(ip, __shfl_xor_sync(kFull, ip, off));
+                if constexpr (!SYM) dot = __fadd_rn(dot, __shfl_xor_sync(kFull, dot, off));
+            }
+            const size_t c = c0 + (size_t)u * S::CPS + slot;
+            if (sl == 0 && c < n) {
+                const float *meta = reinterpret_cast<const float *>(codes + c * (size_t)cs + S::PB);
+                const float xn = meta[0];
+                float d;
+                if constexpr (SYM) {
+                    const float ipt = __fmul_rn(__fmul_rn(ip, rn), xn);  // ip_rot * n_a * n_b
+                    d = __fsub_rn(__fadd_rn(rn2, __fmul_rn(xn, xn)), __fmul_rn(2.0f, ipt));
+                } else {
+                    const float ip_mse = __fmul_rn(ip, meta[2]);
+                    const float corr = __fmul_rn(__fmul_rn(P.scale, meta[1]), dot);
+                    const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), xn), rn);
+                    d = __fsub_rn(__fadd_rn(rn2, __fmul_rn(xn, xn)), __fmul_rn(2.0f, ipt));
+                }
+                orow[c] = d > 0.0f ? d : 0.0f;
+            }
+        }
+    }
+}
+
+// Codes whose packed part is narrower than one 32-bit word (D = 4 with
+// nibble packing: 2 bytes) are scanned one thread per code with byte loads.
+template <bool SYM>
+__global__ void __launch_bounds__(256) scan_bytes_kernel(const float *__restrict__ q_rot,
+                                                         const float *__restrict__ s_q,
+                                                         const float *__restrict__ norms,
+                                                         const uint8_t *__restrict__ codes_a,
+                                                         const uint8_t *__restrict__ codes, size_t n,
+                                                         float *__restrict__ out, size_t ldo,
+                                                         Params P, DevTables T) {
+    const size_t row = blockIdx.y;
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    auto unit = [&](const uint8_t *code, int i) -> unsigned {
+        if (P.nibble) {
+            const unsigned b = code[i >> 1];
+            return (i & 1) ? (b >> 4) : (b & 15u);
+        }
+        return code[i];
+    };
+    const uint8_t *code = codes + c * (size_t)P.cs;
+    float mb[3];
+    for (int q = 0; q < 3; ++q) {
+        uint32_t w = 0;
+        for (int t = 0; t < 4; ++t) w |= (uint32_t)code[P.pb + 4 * q + t] << (8 * t);
+        mb[q] = __uint_as_float(w);
+    }
+    float d;
+    if constexpr (SYM) {
+        const uint8_t *ca = codes_a + row * (size_t)P.cs;
+        float ma[3];
+        for (int q = 0; q < 3; ++q) {
+            uint32_t w = 0;
+            for (int t = 0; t < 4; ++t) w |= (uint32_t)ca[P.pb + 4 * q + t] << (8 * t);
+            ma[q] = __uint_as_float(w);
+        }
+        float ip = 0.0f;
+        for (int i = 0; i < P.D; ++i)
+            ip = __fmaf_rn(__fmul_rn(T.centroids[unit(ca, i) >> 1], ma[2]),
+                           __fmul_rn(T.centroids[unit(code, i) >> 1], mb[2]), ip);
+        const float ipt = __fmul_rn(__fmul_rn(ip, ma[0]), mb[0]);
+        d = __fsub_rn(__fadd_rn(__fmul_rn(ma[0], ma[0]), __fmul_rn(mb[0], mb[0])), __fmul_rn(2.0f, ipt));
+    } else {
+        const float *qr = q_rot + row * (size_t)P.D;
+        const float *sq = s_q + row * (size_t)P.D;
+        float ip = 0.0f, dot = 0.0f;
+        for (int i = 0; i < P.D; ++i) {
+            const unsigned u = unit(code, i);
+            ip = __fmaf_rn(qr[i], T.centroids[u >> 1], ip);
+            dot = __fadd_rn(dot, (u & 1u) ? sq[i] : -sq[i]);
+        }
+        const float ip_mse = __fmul_rn(ip, mb[2]);
+        const float corr = __fmul_rn(__fmul_rn(P.scale, mb[1]), dot);
+        const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), mb[0]), norms[2 * row + 1]);
+        d = __fsub_rn(__fadd_rn(norms[2 * row], __fmul_rn(mb[0], mb[0])), __fmul_rn(2.0f, ipt));
+    }
+    out[row * ldo + c] = d > 0.0f ? d : 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Dispatch over log2(D).
+// ---------------------------------------------------------------------------
+template <template <int> class F, typename... Args>
+cudaError_t dispatch_logd(int log2D, Args &&...args) {
+    switch (log2D) {
+        case 2: return F<2>::run(args...);
+        case 3: return F<3>::run(args...);
+        case 4: return F<4>::run(args...);
+        case 5: return F<5>::run(args...);
+        case 6: return F<6>::run(args...);
+        case 7: return F<7>::run(args...);
+        case 8: return F<8>::run(args...);
+        case 9: return F<9>::run(args...);
+        case 10: return F<10>::run(args...);
+        case 11: return F<11>::run(args...);
+        case 12: return F<12>::run(args...);
+        case 13: return F<13>::run(args...);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int sm_count() {
+    static int count = 0;
+    if (count == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (count <= 0) count = 148;
+    }
+    return count;
+}
+
+constexpr int kSmemBudget = 227 * 1024;
+
+template <int LOG_D>
+struct EncodeRun {
+    static cudaError_t run(const Params &P, const DevTables &T, const float *X, size_t n,
+                           uint8_t *out, cudaStream_t st) {
+        const int D = 1 << LOG_D;
+        const int per_warp = encode_warp_bytes(D, P.cs);
+        int warps = (kSmemBudget - kTabBytes) / per_warp;
+        if (warps > 8) warps = 8;
+        if (warps < 1) return cudaErrorInvalidConfiguration;
+        const size_t smem = (size_t)kTabBytes + (size_t)warps * per_warp;
+        cudaError_t e = cudaFuncSetAttribute(encode_kernel<LOG_D>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel<LOG_D>, 32 * warps,
+                                                          smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        const size_t quads = (n + 3) / 4;
+        size_t blocks = (quads + warps - 1) / warps;
+        const size_t cap = (size_t)sm_count() * per_sm;
+        if (blocks > cap) blocks = cap;
+        if (blocks < 1) blocks = 1;
+        encode_kernel<LOG_D><<<(unsigned)blocks, 32 * warps, smem, st>>>(X, n, out, P, T);
+        return cudaGetLastError();
+    }
+};
+
+template <int LOG_D>
+struct PrepareRun {
+    static cudaError_t run(const Params &P, const DevTables &T, const float *Q, size_t m,
+                           float *q_rot, float *s_q, float *norms, cudaStream_t st) {
+        const int D = 1 << LOG_D;
+        int warps = (kSmemBudget - kTabBytes) / (4 * (D + 8));
+        if (warps > 8) warps = 8;
+        if (warps < 1) return cudaErrorInvalidConfiguration;
+        const size_t smem = (size_t)kTabBytes + (size_t)warps * 4 * (D + 8);
+        cudaError_t e = cudaFuncSetAttribute(prepare_kernel<LOG_D>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        size_t blocks = (m + warps - 1) / warps;
+        const size_t cap = (size_t)sm_count() * 4;
+        if (blocks > cap) blocks = cap;
+        if (blocks < 1) blocks = 1;
+        prepare_kernel<LOG_D><<<(unsigned)blocks, 32 * warps, smem, st>>>(Q, m, q_rot, s_q, norms, P, T);
+        return cudaGetLastError();
+    }
+};
+
+template <int LOG_D, bool NIBBLE, bool SYM>
+cudaError_t scan_launch(const Params &P, const DevTables &T, const float *q_rot, const float *s_q,
+                        const float *norms, const uint8_t *codes_a, size_t m,
+                        const uint8_t *codes, size_t n, float *out, size_t ldo, cudaStream_t st) {
+    using S = ScanShape<LOG_D, NIBBLE>;
+    if constexpr (S::W < 1) {
+        const unsigned bx = (unsigned)((n + 255) / 256);
+        for (size_t r0 = 0; r0 < m; r0 += 65535) {
+            const size_t rows = (m - r0 < 65535) ? (m - r0) : 65535;
+            scan_bytes_kernel<SYM><<<dim3(bx, (unsigned)rows), 256, 0, st>>>(
+                SYM ? nullptr : q_rot + r0 * (size_t)S::D, SYM ? nullptr : s_q + r0 * (size_t)S::D,
+                SYM ? nullptr : norms + 2 * r0, SYM ? codes_a + r0 * (size_t)P.cs : nullptr, codes, n,
+                out + r0 * ldo, ldo, P, T);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    } else {
+        const int threads = 256;
+        const size_t smem = sizeof(float) * ((size_t)(NIBBLE ? 8 : 128) * 32 + (S::QREG ? 0 : 2 * S::PPL * 32));
+        auto kern = scan_kernel<LOG_D, NIBBLE, SYM>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        const size_t steps = (n + S::CPS * S::U - 1) / (S::CPS * S::U);
+        size_t bx = (steps + (threads / 32) - 1) / (threads / 32);
+        size_t cap = (size_t)sm_count() * per_sm;
+        // spread the rows over the machine: each row gets its share of CTAs
+        if (m > 1) cap = (cap + m - 1) / m;
+        if (cap < 1) cap = 1;
+        if (bx > cap) bx = cap;
+        if (bx < 1) bx = 1;
+        for (size_t r0 = 0; r0 < m; r0 += 65535) {
+            const size_t rows = (m - r0 < 65535) ? (m - r0) : 65535;
+            dim3 grid((unsigned)bx, (unsigned)rows);
+            const float *qr = SYM ? nullptr : q_rot + r0 * (size_t)S::D;
+            const float *sq = SYM ? nullptr : s_q + r0 * (size_t)S::D;
+            const float *nm = SYM ? nullptr : norms + 2 * r0;
+            const uint8_t *ca = SYM ? codes_a + r0 * (size_t)P.cs : nullptr;
+            kern<<<grid, threads, smem, st>>>(qr, sq, nm, ca, codes, n, out + r0 * ldo, ldo, P, T);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+}
+
+template <int LOG_D>
+struct ScanRun {
+    static cudaError_t run(const Params &P, const DevTables &T, const float *q_rot,
+                           const float *s_q, const float *norms, const uint8_t *codes_a, size_t m,
+                           const uint8_t *codes, size_t n, float *out, size_t ldo, bool sym,
+                           cudaStream_t st) {
+        if (P.nibble) {
+            return sym ? scan_launch<LOG_D, true, true>(P, T, q_rot, s_q, norms, codes_a, m, codes,
+                                                        n, out, ldo, st)
+                       : scan_launch<LOG_D, true, false>(P, T, q_rot, s_q, norms, codes_a, m,
+                                                         codes, n, out, ldo, st);
+        }
+        return sym ? scan_launch<LOG_D, false, true>(P, T, q_rot, s_q, norms, codes_a, m, codes, n,
+                                                     out, ldo, st)
+                   : scan_launch<LOG_D, false, false>(P, T, q_rot, s_q, norms, codes_a, m, codes,
+                                                      n, out, ldo, st);
+    }
+};
+
+}  // namespace
+
+cudaError_t launch_encode(const Params &P, const DevTables &T, const float *X, size_t n,
+                          uint8_t *out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    return dispatch_logd<EncodeRun>(P.log2D, P, T, X, n, out, st);
+}
+
+cudaError_t launch_prepare(const Params &P, const DevTables &T, const float *Q, size_t m,
+                           float *q_rot, float *s_q, float *norms, cudaStream_t st) {
+    if (m == 0) return cudaSuccess;
+    return dispatch_logd<PrepareRun>(P.log2D, P, T, Q, m, q_rot, s_q, norms, st);
+}
+
+cudaError_t launch_scan_1_to_n(const Params &P, const DevTables &T, const float *q_rot,
+                               const float *s_q, const float *norms, const uint8_t *codes,
+                               size_t n, float *out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    return dispatch_logd<ScanRun>(P.log2D, P, T, q_rot, s_q, norms, (const uint8_t *)nullptr,
+                                  (size_t)1, codes, n, out, n, false, st);
+}
+
+cudaError_t launch_mton_fp32(const Params &P, const DevTables &T, const float *q_rot,
+                             const float *s_q, const float *norms, size_t m,
+                             const uint8_t *codes, size_t n, float *out, size_t ldo,
+                             cudaStream_t st) {
+    if (n == 0 || m == 0) return cudaSuccess;
+    return dispatch_logd<ScanRun>(P.log2D, P, T, q_rot, s_q, norms, (const uint8_t *)nullptr, m,
+                                  codes, n, out, ldo, false, st);
+}
+
+cudaError_t launch_mton_sym_fp32(const Params &P, const DevTables &T, const uint8_t *A,
+                                 size_t m, const uint8_t *B, size_t n, float *out, size_t ldo,
+                                 cudaStream_t st) {
+    if (n == 0 || m == 0) return cudaSuccess;
+    return dispatch_logd<ScanRun>(P.log2D, P, T, (const float *)nullptr, (const float *)nullptr,
+                                  (const float *)nullptr, A, m, B, n, out, ldo, true, st);
+}
+
+}  // namespace tq

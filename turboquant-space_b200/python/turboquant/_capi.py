@@ -1,0 +1,112 @@
+"""ctypes binding of libtqb200.so (include/turboquant_b200.h).
+
+The library is loaded from this directory; there is no fallback: without the
+built library (or without an sm_100 GPU for the compute calls) every call
+fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtqb200.so")
+
+TQ_OK = 0
+TQ_ERR_INVALID_ARGUMENT = 1
+TQ_ERR_CUDA = 2
+TQ_ERR_OUT_OF_MEMORY = 3
+TQ_ERR_NO_DEVICE = 4
+TQ_ERR_TIMEOUT = 5
+TQ_ERR_BUSY = 6
+TQ_ERR_NOT_SUPPORTED = 7
+
+PRECISION = {"fp32": 0, "split_bf16": 1}
+
+# Every symbol include/turboquant_b200.h declares.
+EXPORTS = (
+    "tq_last_error", "tq_version", "tq_space_create", "tq_space_destroy", "tq_space_get_info",
+    "tq_space_tables", "tq_space_quantize", "tq_encode_batch", "tq_distance_1_to_n", "tq_distance_m_to_n",
+    "tq_distance_m_to_n_symmetric", "tq_encode_batch_device", "tq_prepare_queries_device",
+    "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device", "tq_distance_m_to_n_device",
+    "tq_distance_m_to_n_symmetric_device",
+)
+
+
+class SpaceInfo(C.Structure):
+    _fields_ = [
+        ("dim", C.c_size_t), ("padded_dim", C.c_size_t), ("packed_bytes", C.c_size_t),
+        ("code_size", C.c_size_t), ("bits_per_coord", C.c_int), ("num_levels", C.c_int),
+        ("padded", C.c_int), ("num_threads", C.c_int), ("device", C.c_int),
+        ("rot_seed", C.c_uint64), ("qjl_seed", C.c_uint64), ("scale", C.c_float),
+    ]
+
+
+class TQError(RuntimeError):
+    """A failure reported by libtqb200 (CUDA error, out of memory, no device...)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libtqb200.so not found at {LIB_PATH}: build it with "
+            "`make -C turboquant-space_b200` (or __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    vp, sz, fp, u8p = C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p
+    st = C.c_int
+    L.tq_last_error.restype = C.c_char_p
+    L.tq_version.restype = C.c_char_p
+    L.tq_space_create.restype = st
+    L.tq_space_create.argtypes = [sz, C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_int,
+                                  C.POINTER(vp)]
+    L.tq_space_destroy.restype = None
+    L.tq_space_destroy.argtypes = [vp]
+    L.tq_space_get_info.restype = st
+    L.tq_space_get_info.argtypes = [vp, C.POINTER(SpaceInfo)]
+    L.tq_space_tables.restype = st
+    L.tq_space_tables.argtypes = [vp, fp, fp, fp, fp]
+    L.tq_space_quantize.restype = st
+    L.tq_space_quantize.argtypes = [vp, fp, sz, u8p]
+    L.tq_encode_batch.restype = st
+    L.tq_encode_batch.argtypes = [vp, fp, sz, u8p]
+    L.tq_distance_1_to_n.restype = st
+    L.tq_distance_1_to_n.argtypes = [vp, fp, u8p, sz, fp]
+    L.tq_distance_m_to_n.restype = st
+    L.tq_distance_m_to_n.argtypes = [vp, fp, sz, u8p, sz, fp, C.c_int]
+    L.tq_distance_m_to_n_symmetric.restype = st
+    L.tq_distance_m_to_n_symmetric.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int]
+    L.tq_encode_batch_device.restype = st
+    L.tq_encode_batch_device.argtypes = [vp, fp, sz, u8p, vp]
+    L.tq_prepare_queries_device.restype = st
+    L.tq_prepare_queries_device.argtypes = [vp, fp, sz, fp, fp, fp, vp]
+    L.tq_distance_1_to_n_device.restype = st
+    L.tq_distance_1_to_n_device.argtypes = [vp, fp, u8p, sz, fp, vp]
+    L.tq_distance_1_to_n_prepared_device.restype = st
+    L.tq_distance_1_to_n_prepared_device.argtypes = [vp, fp, fp, fp, u8p, sz, fp, vp]
+    L.tq_distance_m_to_n_device.restype = st
+    L.tq_distance_m_to_n_device.argtypes = [vp, fp, sz, u8p, sz, fp, C.c_int, vp]
+    L.tq_distance_m_to_n_symmetric_device.restype = st
+    L.tq_distance_m_to_n_symmetric_device.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int, vp]
+    _LIB = L
+    return L
+
+
+def check(status: int) -> None:
+    if status == TQ_OK:
+        return
+    msg = lib().tq_last_error().decode(errors="replace")
+    if status == TQ_ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    if status == TQ_ERR_OUT_OF_MEMORY:
+        raise MemoryError(msg)
+    raise TQError(status, msg)
