@@ -1,0 +1,39 @@
+// tq_mton.h -- operand planes and contraction kernels of the M x N distances
+// (tq_mton.cu: decode + FP32 SGEMM; tq_tc.cu: split-BF16 tcgen05 GEMM).
+#pragma once
+
+#include "tq_internal.h"
+
+namespace tq {
+
+constexpr int kPlaneF32 = 0;   // one FP32 plane
+constexpr int kPlaneBF16 = 1;  // hi and lo BF16 planes, x = hi + lo
+constexpr int kPlaneRowAlign = 128;
+
+// Rows [0, rows) of `codes` -> planes of rows_pad x K (K = D symmetric, 2D
+// asymmetric), zero rows beyond `rows`; s1/s2 per-row scalars (rows_pad).
+cudaError_t launch_planes_from_codes(const Params &P, const DevTables &T, const uint8_t *codes,
+                                     size_t rows, size_t rows_pad, bool sym, int fmt, void *plane0,
+                                     void *plane1, float *s1, float *s2, cudaStream_t st);
+
+// Prepared queries -> planes of rows_pad x 2D and r1 = |q|, r2 = |q|^2.
+cudaError_t launch_planes_from_prepared(const float *q_rot, const float *s_q, const float *norms,
+                                        size_t rows, size_t rows_pad, int D, int fmt, void *plane0,
+                                        void *plane1, float *r1, float *r2, cudaStream_t st);
+
+// out[i, j] = max(0, r2_i + c2_j - 2 (C_ij r1_i) c1_j), C = A B^T in FP32.
+cudaError_t launch_sgemm_dist(const float *A, const float *B, int K, size_t m, size_t m_pad,
+                              size_t n, size_t n_pad, const float *r1, const float *r2,
+                              const float *c1, const float *c2, float *out, size_t ldo,
+                              cudaStream_t st);
+
+// The same with C = Ah Bh^T + Ah Bl^T + Al Bh^T on tcgen05 tensor cores
+// (FP32 accumulators in tensor memory).  K % 64 == 0, m_pad % 128 == 0,
+// n_pad % 256 == 0.  `err` (device int) is set non-zero if a bounded wait in
+// the kernel gave up.
+cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const void *Bl, int K,
+                           size_t m, size_t m_pad, size_t n, size_t n_pad, const float *r1,
+                           const float *r2, const float *c1, const float *c2, float *out,
+                           size_t ldo, int *err, cudaStream_t st);
+
+}  // namespace tq
