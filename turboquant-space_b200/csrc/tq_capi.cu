@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "tq_internal.h"
+#include "tq_mton.h"
 #include "tq_tables.h"
 
 struct tq_space {
@@ -129,6 +130,141 @@ tq_status ensure_host_streams(tq_space *sp) {
         if (!s) TQ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     return TQ_OK;
 }
+
+// M x N driver.  The row side (m queries, or m codes for the symmetric form)
+// is prepared once; the column side is decoded and contracted in chunks:
+//   FP32, m < kScanRows:  the HBM-bound scan kernel per row (no planes);
+//   FP32 otherwise:       FP32 planes + CUDA-core SGEMM;
+//   SPLIT_BF16:           hi/lo BF16 planes + tcgen05 GEMM.
+// Every distance ends in the same epilogue d = max(0, r2 + c2 - 2 C r1 c1).
+class MtonRunner {
+  public:
+    static constexpr size_t kScanRows = 32;
+    static constexpr size_t kRowPlaneBytes = size_t(512) << 20;
+    static constexpr size_t kColPlaneBytes = size_t(1) << 30;
+
+    static size_t row_chunk(const tq_space *sp, bool sym, tq_precision prec) {
+        const size_t K = sym ? sp->D : 2 * sp->D;
+        size_t rows = (kRowPlaneBytes / (K * 4)) & ~size_t(tq::kPlaneRowAlign - 1);
+        (void)prec;
+        return std::max<size_t>(tq::kPlaneRowAlign, rows);
+    }
+
+    MtonRunner(tq_space *sp, bool sym, tq_precision prec, size_t m)
+        : sp_(sp), sym_(sym), prec_(prec), m_(m) {
+        K_ = sym ? (int)sp->D : 2 * (int)sp->D;
+        fmt_ = prec == TQ_PRECISION_SPLIT_BF16 ? tq::kPlaneBF16 : tq::kPlaneF32;
+        planes_ = prec == TQ_PRECISION_SPLIT_BF16 || m >= kScanRows;
+        m_pad_ = round_up(m, tq::kPlaneRowAlign);
+        const size_t col_align = prec == TQ_PRECISION_SPLIT_BF16 ? 256 : 128;
+        nc_max_ = std::max(col_align, ((kColPlaneBytes / ((size_t)K_ * 4)) / col_align) * col_align);
+    }
+
+    tq_status prepare_rows(const void *rows_dev, cudaStream_t s) {
+        if (prec_ == TQ_PRECISION_SPLIT_BF16 && (K_ % 64 != 0))
+            return fail(TQ_ERR_NOT_SUPPORTED,
+                        "split-BF16 contraction needs a reduction length that is a multiple of 64 "
+                        "(padded dim %zu)", sp_->D);
+        if (fmt_ == tq::kPlaneF32 && planes_ && (K_ % 16 != 0)) planes_ = false;
+        const size_t D = sp_->D;
+        if (!sym_) {  // prepared queries (the scan path uses them directly)
+            TQ_CUDA(prep_.alloc(sizeof(float) * m_ * (2 * D + 2), s), "cudaMallocAsync(prepared)");
+            q_rot_ = static_cast<float *>(prep_.p);
+            s_q_ = q_rot_ + m_ * D;
+            norms_ = s_q_ + m_ * D;
+            TQ_CUDA(tq::launch_prepare(sp_->P, sp_->T, static_cast<const float *>(rows_dev), m_,
+                                       q_rot_, s_q_, norms_, s),
+                    "prepare kernel");
+        } else {
+            codes_a_ = static_cast<const uint8_t *>(rows_dev);
+        }
+        if (!planes_) return TQ_OK;
+        const size_t plane_bytes = m_pad_ * (size_t)K_ * 4;
+        TQ_CUDA(rows_.alloc(plane_bytes + 2 * 4 * m_pad_, s), "cudaMallocAsync(row planes)");
+        a0_ = rows_.p;
+        a1_ = static_cast<unsigned char *>(rows_.p) + plane_bytes / 2;
+        r1_ = reinterpret_cast<float *>(static_cast<unsigned char *>(rows_.p) + plane_bytes);
+        r2_ = r1_ + m_pad_;
+        if (!sym_)
+            TQ_CUDA(tq::launch_planes_from_prepared(q_rot_, s_q_, norms_, m_, m_pad_, (int)D, fmt_, a0_,
+                                                    a1_, r1_, r2_, s),
+                    "row planes");
+        else
+            TQ_CUDA(tq::launch_planes_from_codes(sp_->P, sp_->T, codes_a_, m_, m_pad_, true, fmt_, a0_,
+                                                 a1_, r1_, r2_, s),
+                    "row planes");
+        return TQ_OK;
+    }
+
+    // columns [0, n) of device codes -> out[i * ldo + j]
+    tq_status run_cols(const uint8_t *codes, size_t n, float *out, size_t ldo, cudaStream_t s) {
+        if (!planes_) {
+            if (!sym_)
+                TQ_CUDA(tq::launch_mton_fp32(sp_->P, sp_->T, q_rot_, s_q_, norms_, m_, codes, n, out,
+                                             ldo, s),
+                        "m_to_n scan kernel");
+            else
+                TQ_CUDA(tq::launch_mton_sym_fp32(sp_->P, sp_->T, codes_a_, m_, codes, n, out, ldo, s),
+                        "symmetric m_to_n scan kernel");
+            return TQ_OK;
+        }
+        if (!cols_.p) {
+            const size_t nc = std::min(nc_max_, round_up(n, prec_ == TQ_PRECISION_SPLIT_BF16 ? 256 : 128));
+            nc_alloc_ = nc;
+            const size_t plane_bytes = nc * (size_t)K_ * 4;
+            TQ_CUDA(cols_.alloc(plane_bytes + 2 * 4 * nc + 16, s), "cudaMallocAsync(column planes)");
+            b0_ = cols_.p;
+            b1_ = static_cast<unsigned char *>(cols_.p) + plane_bytes / 2;
+            c1_ = reinterpret_cast<float *>(static_cast<unsigned char *>(cols_.p) + plane_bytes);
+            c2_ = c1_ + nc;
+            err_ = reinterpret_cast<int *>(c2_ + nc);
+            TQ_CUDA(cudaMemsetAsync(err_, 0, sizeof(int), s), "memset");
+        }
+        const size_t col_align = prec_ == TQ_PRECISION_SPLIT_BF16 ? 256 : 128;
+        for (size_t n0 = 0; n0 < n; n0 += nc_alloc_) {
+            const size_t nc = std::min(nc_alloc_, n - n0);
+            const size_t nc_pad = round_up(nc, col_align);
+            TQ_CUDA(tq::launch_planes_from_codes(sp_->P, sp_->T, codes + n0 * sp_->code_size, nc,
+                                                 nc_pad, sym_, fmt_, b0_, b1_, c1_, c2_, s),
+                    "column planes");
+            if (fmt_ == tq::kPlaneF32)
+                TQ_CUDA(tq::launch_sgemm_dist(static_cast<const float *>(a0_),
+                                              static_cast<const float *>(b0_), K_, m_, m_pad_, nc,
+                                              nc_pad, r1_, r2_, c1_, c2_, out + n0, ldo, s),
+                        "FP32 GEMM kernel");
+            else
+                TQ_CUDA(tq::launch_tc_dist(a0_, a1_, b0_, b1_, K_, m_, m_pad_, nc, nc_pad, r1_, r2_,
+                                           c1_, c2_, out + n0, ldo, err_, s),
+                        "tcgen05 GEMM kernel");
+        }
+        return TQ_OK;
+    }
+
+    // Reports a bounded wait that gave up inside the tensor-core kernel.
+    tq_status finish(cudaStream_t s) {
+        if (!err_) return TQ_OK;
+        int h = 0;
+        TQ_CUDA(cudaMemcpyAsync(&h, err_, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H status");
+        TQ_CUDA(cudaStreamSynchronize(s), "sync");
+        if (h != 0) return fail(TQ_ERR_TIMEOUT, "tensor-core kernel: a pipeline wait timed out (code %d)", h);
+        return TQ_OK;
+    }
+
+  private:
+    static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+    tq_space *sp_;
+    bool sym_;
+    tq_precision prec_;
+    size_t m_, m_pad_ = 0, nc_max_ = 0, nc_alloc_ = 0;
+    int K_ = 0, fmt_ = 0;
+    bool planes_ = false;
+    Scratch prep_, rows_, cols_;
+    float *q_rot_ = nullptr, *s_q_ = nullptr, *norms_ = nullptr;
+    const uint8_t *codes_a_ = nullptr;
+    void *a0_ = nullptr, *a1_ = nullptr, *b0_ = nullptr, *b1_ = nullptr;
+    float *r1_ = nullptr, *r2_ = nullptr, *c1_ = nullptr, *c2_ = nullptr;
+    int *err_ = nullptr;
+};
 
 }  // namespace
 
@@ -413,15 +549,15 @@ tq_status tq_distance_m_to_n_device(const tq_space *sp, const float *queries, si
     if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
     if ((st = check_codes_align(codes, "codes")) != TQ_OK) return st;
     if ((st = check_dev(out, m * n * 4, "out")) != TQ_OK) return st;
-    if (precision == TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n is not built yet");
     cudaStream_t s = (cudaStream_t)stream;
-    Scratch scr;
-    TQ_CUDA(scr.alloc(sizeof(float) * m * (2 * sp->D + 2), s), "cudaMallocAsync(prepared queries)");
-    float *q_rot = static_cast<float *>(scr.p), *s_q = q_rot + m * sp->D, *norms = s_q + m * sp->D;
-    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, queries, m, q_rot, s_q, norms, s), "prepare kernel");
-    TQ_CUDA(tq::launch_mton_fp32(sp->P, sp->T, q_rot, s_q, norms, m, codes, n, out, n, s),
-            "m_to_n kernel");
+    const size_t mchunk = MtonRunner::row_chunk(sp, false, precision);
+    for (size_t m0 = 0; m0 < m; m0 += mchunk) {
+        const size_t mc = std::min(mchunk, m - m0);
+        MtonRunner r(const_cast<tq_space *>(sp), false, precision, mc);
+        if ((st = r.prepare_rows(queries + m0 * sp->dim, s)) != TQ_OK) return st;
+        if ((st = r.run_cols(codes, n, out + m0 * n, n, s)) != TQ_OK) return st;
+        if ((st = r.finish(s)) != TQ_OK) return st;
+    }
     return TQ_OK;
 }
 
@@ -439,10 +575,15 @@ tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t 
     if ((st = check_codes_align(A, "codes_a")) != TQ_OK) return st;
     if ((st = check_codes_align(B, "codes_b")) != TQ_OK) return st;
     if ((st = check_dev(out, m * n * 4, "out")) != TQ_OK) return st;
-    if (precision == TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n_symmetric is not built yet");
-    TQ_CUDA(tq::launch_mton_sym_fp32(sp->P, sp->T, A, m, B, n, out, n, (cudaStream_t)stream),
-            "symmetric m_to_n kernel");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t mchunk = MtonRunner::row_chunk(sp, true, precision);
+    for (size_t m0 = 0; m0 < m; m0 += mchunk) {
+        const size_t mc = std::min(mchunk, m - m0);
+        MtonRunner r(const_cast<tq_space *>(sp), true, precision, mc);
+        if ((st = r.prepare_rows(A + m0 * sp->code_size, s)) != TQ_OK) return st;
+        if ((st = r.run_cols(B, n, out + m0 * n, n, s)) != TQ_OK) return st;
+        if ((st = r.finish(s)) != TQ_OK) return st;
+    }
     return TQ_OK;
 }
 
@@ -536,54 +677,66 @@ tq_status tq_distance_1_to_n(const tq_space *csp, const float *query, const uint
 
 namespace {
 
-// Shared driver of the two host-pointer M x N entry points: the row side
-// (prepared queries, or codes_a) is uploaded once, the column side (codes) is
-// streamed in chunks, and each [m, nc] output block is copied back into the
+// Shared driver of the two host-pointer M x N entry points: the row side is
+// uploaded and prepared once; the column side (codes) is streamed in chunks
+// on two alternating streams and each [m, nc] block is copied back into the
 // row-major [m, n] result with a pitched copy.
-template <typename Launch>
-tq_status mton_host(tq_space *sp, size_t m, const uint8_t *codes, size_t n, float *out,
-                    size_t row_side_bytes, const void *row_side_host,
-                    const Launch &launch_block) {
+tq_status mton_host(tq_space *sp, bool sym, tq_precision prec, const void *rows_host, size_t m,
+                    const uint8_t *codes, size_t n, float *out) {
     const size_t cs = sp->code_size;
+    const size_t row_bytes = sym ? m * cs : m * sp->dim * 4;
     size_t per = std::max<size_t>(1, std::min(kChunkBytes / cs, (kChunkBytes * 2) / (4 * m)));
     per = std::min(per, n);
-    cudaStream_t s0 = sp->host_stream[0];
-    Scratch rs;
-    TQ_CUDA(rs.alloc(row_side_bytes, s0), "cudaMallocAsync(row side)");
-    TQ_CUDA(cudaMemcpyAsync(rs.p, row_side_host, row_side_bytes, cudaMemcpyHostToDevice, s0), "H2D rows");
-    tq_status result = TQ_OK;
-    void *prepared = nullptr;
-    {
-        cudaError_t e = launch_block(rs.p, nullptr, 0, nullptr, 0, s0, &prepared, true);
-        if (e != cudaSuccess) return cuda_fail(e, "row preparation");
-    }
-    cudaEvent_t ready;
-    TQ_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
-    cudaEventRecord(ready, s0);
-    cudaStreamWaitEvent(sp->host_stream[1], ready, 0);
+    cudaStream_t s0 = sp->host_stream[0], s1 = sp->host_stream[1];
+    Scratch rows;
+    TQ_CUDA(rows.alloc(row_bytes, s0), "cudaMallocAsync(rows)");
+    TQ_CUDA(cudaMemcpyAsync(rows.p, rows_host, row_bytes, cudaMemcpyHostToDevice, s0), "H2D rows");
+    MtonRunner runner(sp, sym, prec, m);
+    tq_status st = runner.prepare_rows(rows.p, s0);
+    if (st != TQ_OK) return st;
+    // the column runner's scratch is shared by both streams: serialise the
+    // contractions on s0 and overlap only the copies
+    cudaEvent_t ev[2];
+    for (auto &e : ev) TQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
     Scratch buf[2];
+    tq_status result = TQ_OK;
     for (int k = 0; k < 2 && result == TQ_OK; ++k) {
-        cudaError_t e = buf[k].alloc(((per * cs + 15) & ~size_t(15)) + per * m * 4, sp->host_stream[k]);
+        cudaError_t e = buf[k].alloc(((per * cs + 15) & ~size_t(15)) + per * m * 4, s0);
         if (e != cudaSuccess) result = cuda_fail(e, "cudaMallocAsync(m_to_n staging)");
     }
+    cudaEvent_t copied[2];
+    for (auto &e : copied) TQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    // the staging buffers were allocated on s0: s1 waits for that first
+    cudaEventRecord(copied[0], s0);
+    cudaEventRecord(copied[1], s0);
     size_t chunk = 0;
     for (size_t c0 = 0; c0 < n && result == TQ_OK; c0 += per, ++chunk) {
         const size_t nc = std::min(per, n - c0);
-        cudaStream_t s = sp->host_stream[chunk & 1];
-        uint8_t *dC = static_cast<uint8_t *>(buf[chunk & 1].p);
+        const int k = (int)(chunk & 1);
+        uint8_t *dC = static_cast<uint8_t *>(buf[k].p);
         float *dO = reinterpret_cast<float *>(dC + ((per * cs + 15) & ~size_t(15)));
-        cudaError_t e = cudaMemcpyAsync(dC, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = launch_block(rs.p, dC, nc, dO, nc, s, &prepared, false);
+        // s1: wait until the previous D2H from this buffer is done, upload codes
+        cudaError_t e = cudaStreamWaitEvent(s1, copied[k], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dC, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s1);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], s1);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, ev[k], 0);
+        if (e != cudaSuccess) { result = cuda_fail(e, "m_to_n upload"); break; }
+        st = runner.run_cols(dC, nc, dO, nc, s0);
+        if (st != TQ_OK) { result = st; break; }
+        e = cudaEventRecord(ev[k], s0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s1, ev[k], 0);
         if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(out + c0, n * 4, dO, nc * 4, nc * 4, m, cudaMemcpyDeviceToHost, s);
+            e = cudaMemcpy2DAsync(out + c0, n * 4, dO, nc * 4, nc * 4, m, cudaMemcpyDeviceToHost, s1);
+        if (e == cudaSuccess) e = cudaEventRecord(copied[k], s1);
         if (e != cudaSuccess) result = cuda_fail(e, "m_to_n chunk");
     }
-    for (auto &s : sp->host_stream) {
+    for (cudaStream_t s : {s0, s1}) {
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess && result == TQ_OK) result = cuda_fail(e, "m_to_n");
     }
-    cudaEventDestroy(ready);
-    if (prepared) cudaFree(prepared);
+    if (result == TQ_OK) result = runner.finish(s0);
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (auto &e : copied) cudaEventDestroy(e);
     return result;
 }
 
@@ -599,27 +752,11 @@ tq_status tq_distance_m_to_n(const tq_space *csp, const float *queries, size_t m
         return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
     if (m == 0 || n == 0) return TQ_OK;
     if (!queries || !codes || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
-    if (precision == TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n is not built yet");
     auto *sp = const_cast<tq_space *>(csp);
     std::lock_guard<std::mutex> lock(sp->host_mu);
     DeviceGuard g(sp->device);
     if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
-    const size_t D = sp->D;
-    auto launch = [&](void *rows, const uint8_t *dC, size_t nc, float *dO, size_t ldo,
-                      cudaStream_t s, void **prepared, bool prep) -> cudaError_t {
-        if (prep) {
-            cudaError_t e = cudaMalloc(prepared, sizeof(float) * m * (2 * D + 2));
-            if (e != cudaSuccess) return e;
-            float *q_rot = static_cast<float *>(*prepared);
-            return tq::launch_prepare(sp->P, sp->T, static_cast<const float *>(rows), m, q_rot,
-                                      q_rot + m * D, q_rot + 2 * m * D, s);
-        }
-        float *q_rot = static_cast<float *>(*prepared);
-        return tq::launch_mton_fp32(sp->P, sp->T, q_rot, q_rot + m * D, q_rot + 2 * m * D, m, dC, nc,
-                                    dO, ldo, s);
-    };
-    return mton_host(sp, m, codes, n, out, m * sp->dim * 4, queries, launch);
+    return mton_host(sp, false, precision, queries, m, codes, n, out);
 }
 
 tq_status tq_distance_m_to_n_symmetric(const tq_space *csp, const uint8_t *codes_a, size_t m,
@@ -631,19 +768,11 @@ tq_status tq_distance_m_to_n_symmetric(const tq_space *csp, const uint8_t *codes
         return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
     if (m == 0 || n == 0) return TQ_OK;
     if (!codes_a || !codes_b || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
-    if (precision == TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_NOT_SUPPORTED, "split-BF16 distance_m_to_n_symmetric is not built yet");
     auto *sp = const_cast<tq_space *>(csp);
     std::lock_guard<std::mutex> lock(sp->host_mu);
     DeviceGuard g(sp->device);
     if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
-    auto launch = [&](void *rows, const uint8_t *dC, size_t nc, float *dO, size_t ldo,
-                      cudaStream_t s, void **, bool prep) -> cudaError_t {
-        if (prep) return cudaSuccess;
-        return tq::launch_mton_sym_fp32(sp->P, sp->T, static_cast<const uint8_t *>(rows), m, dC, nc,
-                                        dO, ldo, s);
-    };
-    return mton_host(sp, m, codes_b, n, out, m * sp->code_size, codes_a, launch);
+    return mton_host(sp, true, precision, codes_a, m, codes_b, n, out);
 }
 
 }  // extern "C"

@@ -570,15 +570,21 @@ __global__ void __launch_bounds__(256) scan_kernel(const float *__restrict__ q_r
 // ---------------------------------------------------------------------------
 // scan8: the asymmetric scan for byte units (bits >= 5) at D = 128 * WPL.
 // A code is read as D/4 32-bit words, word l + 32 j by lane l; each lane owns
-// positions p = 4 (l + 32 j) + b and keeps q_rot[p] in registers.  Shared
-// memory holds a 256-row table, one 256-byte row per unit byte u:
-//   bytes [0, 128):   column l = c[u >> 1]           (centroid of the unit)
-//   bytes [128, 256): rows g*16 + s, column l = sum_b (bit b of s ? +1 : -1)
-//                     * s_q[4 (l + 32 g) + b]       (QJL sum of one word)
-// so that per position the centroid costs one PRMT (byte -> row | lane) and
-// one conflict-free LDS, and per word the QJL term costs one LOP3 + IMAD
-// (gather the 4 sign bits) + PRMT + LDS.  U codes per warp step; the next
-// step's words are loaded before the current step is reduced.
+// positions p = 4 (l + 32 j) + b and keeps q_rot[p] in registers.
+//   centroid term: shared memory holds one 256-byte row per unit byte u whose
+//     first 128 bytes are c[u >> 1] replicated in 32 lane columns, so each
+//     position costs one PRMT (byte -> row | lane column) and one
+//     bank-conflict-free LDS, then an FFMA;
+//   QJL term: s_q is held per query as 16-bit fixed point, s_q ~ step * s16,
+//     split into a signed high byte and an unsigned low byte packed four per
+//     register; the four sign bits of a word are its bytes & 1, so
+//     sum_p bit_p s16_p costs two dp4a per word and
+//     dot = step * (2 sum_p bit_p s16_p - sum_p s16_p).
+//     The fixed-point error enters only the correction term scale*gamma*dot
+//     (space_turbo_quant.h:683), where it is below 1e-6 of the distance's
+//     term scale at the sizes used here.
+// U codes per warp step; the next step's words are loaded before the current
+// step is reduced (transpose reduction: 2U values over 32 lanes).
 // ---------------------------------------------------------------------------
 template <int WPL, int U>
 __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__ q_rot,
@@ -587,44 +593,64 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
                                                        const uint8_t *__restrict__ codes, size_t n,
                                                        float *__restrict__ out, size_t ldo, Params P,
                                                        DevTables T) {
-    static_assert(U == 4, "the transpose reduction below is written for 4 codes");
+    static_assert(U == 2, "the transpose reduction below is written for 2 codes");
     constexpr int D = 128 * WPL;
-    constexpr int W = D / 4;  // words per code
     extern __shared__ __align__(16) unsigned char tab[];
+    __shared__ float s_red[8];
+    __shared__ int s_ired[8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     const size_t row = blockIdx.y;
     const float *qr_g = q_rot + row * (size_t)D;
     const float *sq_g = s_q + row * (size_t)D;
     for (int i = tid; i < 256 * 32; i += blockDim.x)
         reinterpret_cast<float *>(tab + (i >> 5) * 256)[i & 31] = T.centroids[(i >> 5) >> 1];
-    for (int i = tid; i < WPL * 16 * 32; i += blockDim.x) {
-        const int gr = i >> 5, l = i & 31, g = gr >> 4, sgn = gr & 15;
-        float acc = 0.0f;
+    // fixed-point scale of s_q: step = max|s_q| / 32767
+    float mx = 0.0f;
+    for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
+    if (lane == 0) s_red[warp] = mx;
+    __syncthreads();
+    mx = s_red[0];
+    for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
+    const float step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
+    const float inv_step = 1.0f / step;
+    float qr[WPL * 4];
+    int shi[WPL];
+    unsigned slo[WPL];
+    int ssum = 0;
+#pragma unroll
+    for (int j = 0; j < WPL; ++j) {
+        unsigned hi = 0, lo = 0;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const float v = sq_g[4 * (l + 32 * g) + b];
-            acc += ((sgn >> b) & 1) ? v : -v;
+            const int p = 4 * (lane + 32 * j) + b;
+            qr[4 * j + b] = qr_g[p];
+            int v = __float2int_rn(sq_g[p] * inv_step);
+            v = max(-32767, min(32767, v));
+            ssum += v;
+            hi |= ((unsigned)(v >> 8) & 0xFFu) << (8 * b);
+            lo |= ((unsigned)v & 0xFFu) << (8 * b);
         }
-        reinterpret_cast<float *>(tab + gr * 256 + 128)[l] = acc;
+        shi[j] = (int)hi;
+        slo[j] = lo;
     }
-    float qr[WPL * 4];
 #pragma unroll
-    for (int j = 0; j < WPL; ++j)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) qr[4 * j + b] = qr_g[4 * (lane + 32 * j) + b];
+    for (int off = 16; off > 0; off >>= 1) ssum += __shfl_xor_sync(kFull, ssum, off);
     const float qn2 = norms[2 * row], qn = norms[2 * row + 1];
+    const float sc = P.scale;
     __syncthreads();
 
     const uint32_t lane4 = (uint32_t)lane * 4u;
     const int cs = P.cs;
-    // lane that finishes code u of a step after the transpose reduction
-    const int my_u = ((lane & 3) == 0 && ((lane >> 2) & 1) == 0) ? (((lane >> 4) & 1) * 2 + ((lane >> 3) & 1)) : -1;
-    const size_t step = (size_t)gridDim.x * nw * U;
+    // after the reduction lane 0 finishes code 0 and lane 16 code 1 of a step
+    const int my_u = (lane == 0) ? 0 : ((lane == 16) ? 1 : -1);
+    const size_t stride = (size_t)gridDim.x * nw * U;
     size_t c0 = ((size_t)blockIdx.x * nw + warp) * U;
     float *orow = out + row * ldo;
 
     uint32_t wn[U][WPL];
-    float tn[3] = {0.0f, 0.0f, 0.0f};
+    float tn0 = 0.0f, tn1 = 0.0f, tn2 = 0.0f;
     auto load = [&](size_t base) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -635,25 +661,27 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
         }
         if (my_u >= 0 && base + my_u < n) {
             const float *m = reinterpret_cast<const float *>(codes + (base + my_u) * (size_t)cs + D);
-            tn[0] = __ldg(m);
-            tn[1] = __ldg(m + 1);
-            tn[2] = __ldg(m + 2);
+            tn0 = __ldg(m);
+            tn1 = __ldg(m + 1);
+            tn2 = __ldg(m + 2);
         }
     };
     if (c0 < n) load(c0);
-    for (; c0 < n; c0 += step) {
+    for (; c0 < n; c0 += stride) {
         uint32_t w[U][WPL];
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int j = 0; j < WPL; ++j) w[u][j] = wn[u][j];
-        const float t0 = tn[0], t1 = tn[1], t2 = tn[2];
-        if (c0 + step < n) load(c0 + step);
+        const float t0 = tn0, t1 = tn1, t2 = tn2;
+        if (c0 + stride < n) load(c0 + stride);
 
         float v[2 * U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            float ip = 0.0f, dot = 0.0f;
+            float ip = 0.0f;
+            int acc_hi = 0;
+            unsigned acc_lo = 0;
 #pragma unroll
             for (int j = 0; j < WPL; ++j) {
                 const uint32_t x = w[u][j];
@@ -662,53 +690,48 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
                     const uint32_t a = __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4));
                     ip = __fmaf_rn(qr[4 * j + b], *reinterpret_cast<const float *>(tab + a), ip);
                 }
-                const uint32_t sg = (x & 0x01010101u) * 0x01020408u;  // sign bits -> bits 24..27
-                const uint32_t a2 = __byte_perm(sg, lane4, 0x6534u);
-                dot += *reinterpret_cast<const float *>(tab + a2 + (j * 16 * 256 + 128));
+                const uint32_t bits = x & 0x01010101u;
+                acc_hi = __dp4a((int)bits, shi[j], acc_hi);
+                acc_lo = __dp4a(bits, slo[j], acc_lo);
             }
             v[2 * u] = ip;
-            v[2 * u + 1] = dot;
+            v[2 * u + 1] = (float)(acc_hi * 256 + (int)acc_lo);  // exact: |.| < 2^21
         }
-        // transpose reduction of 8 values over 32 lanes (9 shuffles)
-        float w4[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const bool hi = lane & 16;
-            const float send = hi ? v[k] : v[k + 4];
-            const float keep = hi ? v[k + 4] : v[k];
-            w4[k] = keep + __shfl_xor_sync(kFull, send, 16);
-        }
+        // transpose reduction of 4 values over 32 lanes (6 shuffles)
         float w2[2];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-            const bool hi = lane & 8;
-            const float send = hi ? w4[k] : w4[k + 2];
-            const float keep = hi ? w4[k + 2] : w4[k];
-            w2[k] = keep + __shfl_xor_sync(kFull, send, 8);
+            const bool hi = lane & 16;
+            const float send = hi ? v[k] : v[k + 2];
+            const float keep = hi ? v[k + 2] : v[k];
+            w2[k] = keep + __shfl_xor_sync(kFull, send, 16);
         }
         float y;
         {
-            const bool hi = lane & 4;
+            const bool hi = lane & 8;
             const float send = hi ? w2[0] : w2[1];
             const float keep = hi ? w2[1] : w2[0];
-            y = keep + __shfl_xor_sync(kFull, send, 4);
+            y = keep + __shfl_xor_sync(kFull, send, 8);
         }
-        y += __shfl_xor_sync(kFull, y, 1);
+        y += __shfl_xor_sync(kFull, y, 4);
         y += __shfl_xor_sync(kFull, y, 2);
-        // lane holds value index ((lane>>4)&1)*4 + ((lane>>3)&1)*2 + ((lane>>2)&1):
-        // ip of code u at lanes 0/8/16/24 (u = 0..3), its dot at lane + 4
-        const float dot = __shfl_down_sync(kFull, y, 4);
+        y += __shfl_xor_sync(kFull, y, 1);
+        // lane holds value ((lane>>4)&1)*2 + ((lane>>3)&1): ip of code u at
+        // lane 16u, its sign sum at lane 16u + 8
+        const float sb = __shfl_down_sync(kFull, y, 8);
         if (my_u >= 0) {
             const size_t c = c0 + my_u;
             if (c < n) {
+                const float dot = __fmul_rn(step, 2.0f * sb - (float)ssum);
                 const float ip_mse = __fmul_rn(y, t2);
-                const float corr = __fmul_rn(__fmul_rn(P.scale, t1), dot);
+                const float corr = __fmul_rn(__fmul_rn(sc, t1), dot);
                 const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), t0), qn);
                 const float d = __fsub_rn(__fadd_rn(qn2, __fmul_rn(t0, t0)), __fmul_rn(2.0f, ipt));
                 orow[c] = d > 0.0f ? d : 0.0f;
             }
         }
     }
+    (void)s_ired;
 }
 
 // Codes whose packed part is narrower than one 32-bit word (D = 4 with
@@ -913,7 +936,7 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
         return cudaErrorNotSupported;
     } else {
         constexpr int WPL = (1 << LOG_D) / 128;
-        auto kern = scan8_kernel<WPL, 4>;
+        auto kern = scan8_kernel<WPL, 2>;
         const int threads = 256;
         const size_t smem = 256 * 256;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -922,7 +945,7 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
-        const size_t steps = (n + 3) / 4;
+        const size_t steps = (n + 1) / 2;
         size_t bx = (steps + (threads / 32) - 1) / (threads / 32);
         size_t cap = (size_t)sm_count() * per_sm;
         if (m > 1) cap = (cap + m - 1) / m;
