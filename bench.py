@@ -192,6 +192,131 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+def mixture_rows(torch, gen, dev, n, dim, centres, std=0.3, chunk=1 << 18):
+    """Rows of a Gaussian mixture (uniform weights over `centres`), L2-normalised."""
+    out = torch.empty((n, dim), dtype=torch.float32, device=dev)
+    k = centres.shape[0]
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        lab = torch.randint(0, k, (b - a,), generator=gen, device=dev)
+        blk = centres.index_select(0, lab)
+        blk.add_(torch.randn((b - a, dim), generator=gen, device=dev).mul_(std))
+        nrm = blk.norm(dim=1, keepdim=True)
+        nrm[nrm == 0] = 1.0
+        out[a:b] = blk / nrm
+    return out
+
+
+def normal_rows(torch, gen, dev, n, dim, chunk=1 << 20):
+    out = torch.empty((n, dim), dtype=torch.float32, device=dev)
+    for a in range(0, n, chunk):
+        blk = out[a:a + chunk]
+        blk.normal_(generator=gen)
+        nrm = blk.norm(dim=1, keepdim=True)
+        nrm[nrm == 0] = 1.0
+        blk.div_(nrm)
+    return out
+
+
+def run_mton(args, sym):
+    """Dense M x N contractions, FP32 CUDA cores vs split-BF16 tcgen05.
+
+    mton: 1,000,000 codes of normalised N(0,1) 768-d rows (4-bit), 4096
+          normalised queries -> 4096 x 1,000,000 asymmetric distances.
+    sym:  2048 x 2,000,000 codes of a 1024-centre Gaussian mixture at 1536-d
+          (padded to 2048), 4-bit -> symmetric distances."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import turboquant as tq
+    from turboquant._capi import check, lib
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    L = lib()
+    stream = torch.cuda.Stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    gen = torch.Generator(device=dev)
+    if sym:
+        dim, bits, m, n = 1536, 4, 2048, args.n if args.n != 10_000_000 else 2_000_000
+        gen.manual_seed(6)
+        centres = torch.randn((1024, dim), generator=gen, device=dev)
+        Arows = mixture_rows(torch, gen, dev, m, dim, centres)
+        gen.manual_seed(7)
+        Brows = mixture_rows(torch, gen, dev, n, dim, centres)
+    else:
+        dim, bits, m, n = 768, 4, 4096, args.n if args.n != 10_000_000 else 1_000_000
+        gen.manual_seed(4)
+        Brows = normal_rows(torch, gen, dev, n, dim)
+        gen.manual_seed(5)
+        Arows = normal_rows(torch, gen, dev, m, dim)
+    space = tq.TurboQuantSpace(dim, bits_per_coord=bits, device=0)
+    h = space._h
+    cs, D = space.code_size_bytes(), space.padded_dim()
+    codes = torch.empty((n, cs), dtype=torch.uint8, device=dev)
+    check(L.tq_encode_batch_device(h, C.c_void_p(Brows.data_ptr()), n, C.c_void_p(codes.data_ptr()), sptr))
+    if sym:
+        acodes = torch.empty((m, cs), dtype=torch.uint8, device=dev)
+        check(L.tq_encode_batch_device(h, C.c_void_p(Arows.data_ptr()), m, C.c_void_p(acodes.data_ptr()), sptr))
+    stream.synchronize()
+    Qh = Arows.cpu().numpy() if not sym else None
+    del Brows
+    out = torch.empty((m, n), dtype=torch.float32, device=dev)
+
+    def call(prec):
+        if sym:
+            check(L.tq_distance_m_to_n_symmetric_device(h, C.c_void_p(acodes.data_ptr()), m,
+                                                        C.c_void_p(codes.data_ptr()), n,
+                                                        C.c_void_p(out.data_ptr()), prec, sptr))
+        else:
+            check(L.tq_distance_m_to_n_device(h, C.c_void_p(Arows.data_ptr()), m,
+                                              C.c_void_p(codes.data_ptr()), n,
+                                              C.c_void_p(out.data_ptr()), prec, sptr))
+
+    flops = float(m) * n * (2 * D if sym else 4 * D)
+    res = {}
+    rng = np.random.default_rng(10)
+    ii = rng.integers(0, m, 10_000)
+    jj = rng.integers(0, n, 10_000)
+    ch = codes.index_select(0, torch.from_numpy(jj).to(dev)).cpu().numpy()
+    o = O.OracleSpace(dim, bits)
+    if sym:
+        ah = acodes.index_select(0, torch.from_numpy(ii).to(dev)).cpu().numpy()
+        f64 = np.array([o.distance_symmetric_f64(ah[k], ch[k]) for k in range(10_000)])
+        ma = np.frombuffer(ah[:, D // 2:D // 2 + 4].tobytes(), np.float32).astype(np.float64)
+    else:
+        f64 = np.array([o.distance_f64(Qh[i], ch[k]) for k, i in enumerate(ii)])
+        ma = np.linalg.norm(Qh[ii].astype(np.float64), axis=1)
+    mb = np.frombuffer(ch[:, cs - 12:cs - 8].tobytes(), np.float32).astype(np.float64)
+    tscale = np.maximum(np.abs(f64), ma ** 2 + mb ** 2)
+    flat = torch.from_numpy(ii * n + jj).to(dev)
+    for name, prec, reps in (("fp32", 0, max(1, args.steps // 5)), ("split_bf16", 1, args.steps)):
+        call(prec)
+        stream.synchronize()
+        got = out.view(-1).index_select(0, flat).cpu().numpy().astype(np.float64)
+        err = float(np.max(np.abs(got - f64) / tscale))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            call(prec)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {"ms": round(ms, 3), "TFLOP_s": round(flops / (ms * 1e-3) / 1e12, 2),
+                     "Gdist_s": round(m * n / (ms * 1e-3) / 1e9, 3),
+                     "max_rel_err_vs_fp64": err, "reps": reps}
+    print(json.dumps({
+        "metric": METRIC, "workload": "sym" if sym else "mton",
+        "config": {"dim": dim, "padded_dim": D, "bits_per_coord": bits, "m": m, "n": n,
+                   "flops_per_pair": 2 * D if sym else 4 * D,
+                   "data": ("1024-centre Gaussian mixture, std 0.3, rows L2-normalised"
+                            if sym else "N(0,1) rows L2-normalised"),
+                   "error_sample": "10,000 (i, j) pairs, seed 10, vs the FP64 evaluation"},
+        "results": res,
+        "speedup_split_bf16_vs_fp32": round(res["fp32"]["ms"] / res["split_bf16"]["ms"], 2),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,8 +327,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("scan", "mton", "sym"), default="scan",
+                    help="scan (default): the 1->N scan benchmark; mton/sym: the dense M x N "
+                         "contractions, FP32 vs split-BF16")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload != "scan":
+        run_mton(args, args.workload == "sym")
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

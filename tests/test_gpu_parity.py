@@ -253,3 +253,62 @@ def test_mton_device_gemm_equals_host(cuda_ok):
     dv = s.distance_m_to_n(torch.from_numpy(Q).cuda(), torch.from_numpy(codes).cuda())
     torch.cuda.synchronize()
     np.testing.assert_array_equal(dv.cpu().numpy(), h)
+
+
+# ---- split-BF16 tcgen05 contraction ------------------------------------------
+TC_CASES = [(768, 4), (1536, 4), (384, 4), (1024, 8), (100, 8), (64, 6)]
+
+
+@pytest.mark.parametrize("dim,bits", TC_CASES)
+def test_distance_m_to_n_split_bf16_vs_oracle(cuda_ok, dim, bits):
+    rng = np.random.default_rng(dim + 3 * bits)
+    X = rng.standard_normal((517, dim)).astype(np.float32)
+    X = (X / np.linalg.norm(X, axis=1, keepdims=True)).astype(np.float32)
+    Q = rng.standard_normal((141, dim)).astype(np.float32)
+    Q = (Q / np.linalg.norm(Q, axis=1, keepdims=True)).astype(np.float32)
+    s = tq.TurboQuantSpace(dim, bits)
+    codes = s.encode_batch(X)
+    d = s.distance_m_to_n(Q, codes, precision="split_bf16")
+    ref = O.OracleSpace(dim, bits).distance_m_to_n(Q, codes)
+    cs = s.code_size_bytes()
+    err, ok = dist_close(d, ref, asym_term_scale(Q, codes, cs, cs - 12))
+    print(f"split-BF16 asym {dim}/{bits}: max err {err.max():.2e}")
+    assert ok, err.max()
+
+
+@pytest.mark.parametrize("dim,bits", TC_CASES)
+def test_distance_symmetric_split_bf16_vs_oracle(cuda_ok, dim, bits):
+    rng = np.random.default_rng(dim + 5 * bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    A = s.encode_batch(rng.standard_normal((130, dim)).astype(np.float32))
+    B = s.encode_batch(rng.standard_normal((600, dim)).astype(np.float32))
+    d = s.distance_m_to_n_symmetric(A, B, precision="split_bf16")
+    ref = O.OracleSpace(dim, bits).distance_m_to_n_symmetric(A, B)
+    cs = s.code_size_bytes()
+    err, ok = dist_close(d, ref, sym_term_scale(A, B, cs, cs - 12))
+    print(f"split-BF16 sym {dim}/{bits}: max err {err.max():.2e}")
+    assert ok, err.max()
+
+
+def test_split_bf16_error_vs_fp64(cuda_ok):
+    """Error of the tensor-core form against the FP64 evaluation, 10,000 sampled pairs."""
+    rng = np.random.default_rng(10)
+    dim, bits = 768, 4
+    X = rng.standard_normal((4096, dim)).astype(np.float32)
+    X = (X / np.linalg.norm(X, axis=1, keepdims=True)).astype(np.float32)
+    Q = rng.standard_normal((256, dim)).astype(np.float32)
+    Q = (Q / np.linalg.norm(Q, axis=1, keepdims=True)).astype(np.float32)
+    s = tq.TurboQuantSpace(dim, bits)
+    codes = s.encode_batch(X)
+    d_tc = s.distance_m_to_n(Q, codes, precision="split_bf16")
+    d_32 = s.distance_m_to_n(Q, codes)
+    o = O.OracleSpace(dim, bits)
+    ii = rng.integers(0, 256, 10_000)
+    jj = rng.integers(0, 4096, 10_000)
+    f64 = np.array([o.distance_f64(Q[i], codes[j]) for i, j in zip(ii, jj)])
+    scale = np.maximum(np.abs(f64), asym_term_scale(Q, codes, 524, 512)[ii, jj])
+    e_tc = np.abs(d_tc[ii, jj] - f64) / scale
+    e_32 = np.abs(d_32[ii, jj] - f64) / scale
+    print(f"vs FP64 over 10k pairs: split-BF16 max {e_tc.max():.2e} mean {e_tc.mean():.2e}; "
+          f"FP32 max {e_32.max():.2e} mean {e_32.mean():.2e}")
+    assert e_tc.max() < 1e-5 and e_32.max() < 1e-5

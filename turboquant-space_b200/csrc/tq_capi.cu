@@ -678,65 +678,76 @@ tq_status tq_distance_1_to_n(const tq_space *csp, const float *query, const uint
 namespace {
 
 // Shared driver of the two host-pointer M x N entry points: the row side is
-// uploaded and prepared once; the column side (codes) is streamed in chunks
-// on two alternating streams and each [m, nc] block is copied back into the
-// row-major [m, n] result with a pitched copy.
+// uploaded and prepared once; the column side (codes) is streamed in chunks.
+// Three streams: uploads (host_stream[1]), contractions (host_stream[0]) and
+// downloads (a third stream), so that the H2D of chunk k+1, the kernels of
+// chunk k and the pitched D2H of chunk k-1 overlap on separate engines.
 tq_status mton_host(tq_space *sp, bool sym, tq_precision prec, const void *rows_host, size_t m,
                     const uint8_t *codes, size_t n, float *out) {
     const size_t cs = sp->code_size;
     const size_t row_bytes = sym ? m * cs : m * sp->dim * 4;
     size_t per = std::max<size_t>(1, std::min(kChunkBytes / cs, (kChunkBytes * 2) / (4 * m)));
     per = std::min(per, n);
-    cudaStream_t s0 = sp->host_stream[0], s1 = sp->host_stream[1];
+    cudaStream_t sc = sp->host_stream[0], su = sp->host_stream[1];
+    cudaStream_t sd = nullptr;
+    TQ_CUDA(cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking), "cudaStreamCreate");
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sguard{sd};
     Scratch rows;
-    TQ_CUDA(rows.alloc(row_bytes, s0), "cudaMallocAsync(rows)");
-    TQ_CUDA(cudaMemcpyAsync(rows.p, rows_host, row_bytes, cudaMemcpyHostToDevice, s0), "H2D rows");
+    TQ_CUDA(rows.alloc(row_bytes, sc), "cudaMallocAsync(rows)");
+    TQ_CUDA(cudaMemcpyAsync(rows.p, rows_host, row_bytes, cudaMemcpyHostToDevice, sc), "H2D rows");
     MtonRunner runner(sp, sym, prec, m);
-    tq_status st = runner.prepare_rows(rows.p, s0);
+    tq_status st = runner.prepare_rows(rows.p, sc);
     if (st != TQ_OK) return st;
-    // the column runner's scratch is shared by both streams: serialise the
-    // contractions on s0 and overlap only the copies
-    cudaEvent_t ev[2];
-    for (auto &e : ev) TQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    const size_t cbytes = (per * cs + 15) & ~size_t(15);
     Scratch buf[2];
-    tq_status result = TQ_OK;
-    for (int k = 0; k < 2 && result == TQ_OK; ++k) {
-        cudaError_t e = buf[k].alloc(((per * cs + 15) & ~size_t(15)) + per * m * 4, s0);
-        if (e != cudaSuccess) result = cuda_fail(e, "cudaMallocAsync(m_to_n staging)");
+    for (int k = 0; k < 2; ++k)
+        TQ_CUDA(buf[k].alloc(cbytes + per * m * 4, sc), "cudaMallocAsync(m_to_n staging)");
+    cudaEvent_t uploaded[2], computed[2], downloaded[2];
+    for (int k = 0; k < 2; ++k) {
+        TQ_CUDA(cudaEventCreateWithFlags(&uploaded[k], cudaEventDisableTiming), "event");
+        TQ_CUDA(cudaEventCreateWithFlags(&computed[k], cudaEventDisableTiming), "event");
+        TQ_CUDA(cudaEventCreateWithFlags(&downloaded[k], cudaEventDisableTiming), "event");
+        // the staging buffers were allocated on sc: the other streams start after it
+        cudaEventRecord(downloaded[k], sc);
+        cudaEventRecord(computed[k], sc);
     }
-    cudaEvent_t copied[2];
-    for (auto &e : copied) TQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-    // the staging buffers were allocated on s0: s1 waits for that first
-    cudaEventRecord(copied[0], s0);
-    cudaEventRecord(copied[1], s0);
+    tq_status result = TQ_OK;
     size_t chunk = 0;
     for (size_t c0 = 0; c0 < n && result == TQ_OK; c0 += per, ++chunk) {
         const size_t nc = std::min(per, n - c0);
         const int k = (int)(chunk & 1);
         uint8_t *dC = static_cast<uint8_t *>(buf[k].p);
-        float *dO = reinterpret_cast<float *>(dC + ((per * cs + 15) & ~size_t(15)));
-        // s1: wait until the previous D2H from this buffer is done, upload codes
-        cudaError_t e = cudaStreamWaitEvent(s1, copied[k], 0);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dC, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s1);
-        if (e == cudaSuccess) e = cudaEventRecord(ev[k], s1);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, ev[k], 0);
+        float *dO = reinterpret_cast<float *>(dC + cbytes);
+        // upload into buffer k once the contraction that last read it is done
+        cudaError_t e = cudaStreamWaitEvent(su, computed[k], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dC, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, su);
+        if (e == cudaSuccess) e = cudaEventRecord(uploaded[k], su);
+        // contract once uploaded and once the previous download of dO is done
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, uploaded[k], 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, downloaded[k], 0);
         if (e != cudaSuccess) { result = cuda_fail(e, "m_to_n upload"); break; }
-        st = runner.run_cols(dC, nc, dO, nc, s0);
+        st = runner.run_cols(dC, nc, dO, nc, sc);
         if (st != TQ_OK) { result = st; break; }
-        e = cudaEventRecord(ev[k], s0);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s1, ev[k], 0);
+        e = cudaEventRecord(computed[k], sc);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sd, computed[k], 0);
         if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(out + c0, n * 4, dO, nc * 4, nc * 4, m, cudaMemcpyDeviceToHost, s1);
-        if (e == cudaSuccess) e = cudaEventRecord(copied[k], s1);
+            e = cudaMemcpy2DAsync(out + c0, n * 4, dO, nc * 4, nc * 4, m, cudaMemcpyDeviceToHost, sd);
+        if (e == cudaSuccess) e = cudaEventRecord(downloaded[k], sd);
         if (e != cudaSuccess) result = cuda_fail(e, "m_to_n chunk");
     }
-    for (cudaStream_t s : {s0, s1}) {
+    for (cudaStream_t s : {su, sc, sd}) {
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess && result == TQ_OK) result = cuda_fail(e, "m_to_n");
     }
-    if (result == TQ_OK) result = runner.finish(s0);
-    for (auto &e : ev) cudaEventDestroy(e);
-    for (auto &e : copied) cudaEventDestroy(e);
+    if (result == TQ_OK) result = runner.finish(sc);
+    for (int k = 0; k < 2; ++k) {
+        cudaEventDestroy(uploaded[k]);
+        cudaEventDestroy(computed[k]);
+        cudaEventDestroy(downloaded[k]);
+    }
     return result;
 }
 
