@@ -567,6 +567,24 @@ __global__ void __launch_bounds__(256) scan_kernel(const float *__restrict__ q_r
     }
 }
 
+// Packed FP32x2 FMA (two independent IEEE FMAs on a register pair).
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float sum2(unsigned long long v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return lo + hi;
+}
+
 // ---------------------------------------------------------------------------
 // scan8: the asymmetric scan for byte units (bits >= 5) at D = 128 * WPL.
 // A code is read as D/4 32-bit words, word l + 32 j by lane l; each lane owns
@@ -597,7 +615,6 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
     constexpr int D = 128 * WPL;
     extern __shared__ __align__(16) unsigned char tab[];
     __shared__ float s_red[8];
-    __shared__ int s_ired[8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     const size_t row = blockIdx.y;
     const float *qr_g = q_rot + row * (size_t)D;
@@ -615,7 +632,7 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
     for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
     const float step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
     const float inv_step = 1.0f / step;
-    float qr[WPL * 4];
+    unsigned long long qr2[WPL * 2];  // q_rot of positions (4 (lane + 32 j) + 2 h, +1)
     int shi[WPL];
     unsigned slo[WPL];
     int ssum = 0;
@@ -625,7 +642,7 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const int p = 4 * (lane + 32 * j) + b;
-            qr[4 * j + b] = qr_g[p];
+            if (b & 1) qr2[2 * j + (b >> 1)] = pack2(qr_g[p - 1], qr_g[p]);
             int v = __float2int_rn(sq_g[p] * inv_step);
             v = max(-32767, min(32767, v));
             ssum += v;
@@ -679,22 +696,25 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
         float v[2 * U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            float ip = 0.0f;
+            unsigned long long acc2 = 0ull;  // (even, odd) position partial sums
             int acc_hi = 0;
             unsigned acc_lo = 0;
 #pragma unroll
             for (int j = 0; j < WPL; ++j) {
                 const uint32_t x = w[u][j];
+                float cv[4];
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
                     const uint32_t a = __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4));
-                    ip = __fmaf_rn(qr[4 * j + b], *reinterpret_cast<const float *>(tab + a), ip);
+                    cv[b] = *reinterpret_cast<const float *>(tab + a);
                 }
+                acc2 = ffma2(qr2[2 * j], pack2(cv[0], cv[1]), acc2);
+                acc2 = ffma2(qr2[2 * j + 1], pack2(cv[2], cv[3]), acc2);
                 const uint32_t bits = x & 0x01010101u;
                 acc_hi = __dp4a((int)bits, shi[j], acc_hi);
                 acc_lo = __dp4a(bits, slo[j], acc_lo);
             }
-            v[2 * u] = ip;
+            v[2 * u] = sum2(acc2);
             v[2 * u + 1] = (float)(acc_hi * 256 + (int)acc_lo);  // exact: |.| < 2^21
         }
         // transpose reduction of 4 values over 32 lanes (6 shuffles)
@@ -731,7 +751,6 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
             }
         }
     }
-    (void)s_ired;
 }
 
 // Codes whose packed part is narrower than one 32-bit word (D = 4 with
