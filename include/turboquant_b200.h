@@ -145,6 +145,31 @@ tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_
                                              const uint8_t *codes, size_t n, float *out,
                                              void *stream);
 
+/* distance_1_to_n on device buffers for callers that cannot allocate device
+ * memory: for example code that runs inside a memory budget fixed up front
+ * (a serving process that reserved its pool at start-up), a framework
+ * plug-in whose enqueue step is not allowed to allocate, or a latency path
+ * that cannot afford the synchronisation of cudaMalloc/cudaFree.  It has no
+ * counterpart in the reference (whose CPU code never allocates device memory).
+ *
+ * It computes exactly what tq_distance_1_to_n_device computes, but keeps the
+ * prepared query (2 * padded_dim + 2 floats) in a fixed array that the
+ * library holds in device memory on every GPU that loads it, until the
+ * process exits: 16,386 floats (64 KiB + 8 bytes), enough for the largest
+ * padded_dim this library supports (8192).  Larger requests are rejected
+ * with TQ_ERR_INVALID_ARGUMENT.  No call allocates or frees device memory.
+ *
+ * The first call on a device looks up that device's copy of the array
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the one array, and it keeps the last call's
+ * contents; each call rewrites every value it reads before reading it, so
+ * nothing needs clearing.  Calls whose work overlaps on the GPU (different
+ * streams, or different host threads without ordering) race on the array:
+ * order them on one stream or serialise them. */
+tq_status tq_distance_1_to_n_device_noalloc(const tq_space *sp, const float *query,
+                                            const uint8_t *codes, size_t n, float *out,
+                                            void *stream);
+
 /* distanceBatchMToN on device buffers. */
 tq_status tq_distance_m_to_n_device(const tq_space *sp, const float *queries, size_t m,
                                     const uint8_t *codes, size_t n, float *out,

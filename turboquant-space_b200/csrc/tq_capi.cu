@@ -536,6 +536,70 @@ tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_
     return TQ_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Fixed device scratch of tq_distance_1_to_n_device_noalloc: the prepared
+// query (q_rot, s_q, |q|^2, |q|) of the largest supported padded dim.
+constexpr size_t kNoAllocScratchFloats = 2 * (size_t(1) << tq::kMaxLogD) + 2;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocSlot {
+    std::once_flag once;
+    float *ptr = nullptr;
+    cudaError_t err = cudaSuccess;
+};
+NoAllocSlot g_noalloc_slots[kNoAllocMaxDevices];
+
+// Device address of this device's copy of the array (looked up once per
+// device, with that device current; the host-side name is not a device
+// address).
+tq_status noalloc_scratch(int device, float **out) {
+    if (device < 0 || device >= kNoAllocMaxDevices)
+        return fail(TQ_ERR_NOT_SUPPORTED, "device %d: no static scratch slot", device);
+    NoAllocSlot &slot = g_noalloc_slots[device];
+    std::call_once(slot.once, [&] {
+        void *p = nullptr;
+        slot.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (slot.err == cudaSuccess) slot.ptr = static_cast<float *>(p);
+    });
+    if (slot.err != cudaSuccess) return cuda_fail(slot.err, "cudaGetSymbolAddress(static scratch)");
+    *out = slot.ptr;
+    return TQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tq_status tq_distance_1_to_n_device_noalloc(const tq_space *sp, const float *query,
+                                            const uint8_t *codes, size_t n, float *out,
+                                            void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    const size_t need = 2 * sp->D + 2;
+    if (need > kNoAllocScratchFloats)
+        return fail(TQ_ERR_INVALID_ARGUMENT,
+                    "distance_1_to_n_device_noalloc: padded dim %zu needs %zu floats of scratch, "
+                    "the static scratch holds %zu",
+                    sp->D, need, kNoAllocScratchFloats);
+    if (n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(query, sp->dim * 4, "query")) != TQ_OK) return st;
+    if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
+    if ((st = check_codes_align(codes, "codes")) != TQ_OK) return st;
+    if ((st = check_dev(out, n * 4, "out")) != TQ_OK) return st;
+    float *scratch = nullptr;
+    if ((st = noalloc_scratch(sp->device, &scratch)) != TQ_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    float *q_rot = scratch, *s_q = scratch + sp->D, *norms = scratch + 2 * sp->D;
+    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, query, 1, q_rot, s_q, norms, s), "prepare kernel");
+    TQ_CUDA(tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out, s), "scan kernel");
+    return TQ_OK;
+}
+
 tq_status tq_distance_m_to_n_device(const tq_space *sp, const float *queries, size_t m,
                                     const uint8_t *codes, size_t n, float *out,
                                     tq_precision precision, void *stream) {

@@ -28,7 +28,8 @@ EXPORTS = (
     "tq_last_error", "tq_version", "tq_space_create", "tq_space_destroy", "tq_space_get_info",
     "tq_space_tables", "tq_space_quantize", "tq_encode_batch", "tq_distance_1_to_n", "tq_distance_m_to_n",
     "tq_distance_m_to_n_symmetric", "tq_encode_batch_device", "tq_prepare_queries_device",
-    "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device", "tq_distance_m_to_n_device",
+    "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device",
+    "tq_distance_1_to_n_device_noalloc", "tq_distance_m_to_n_device",
     "tq_distance_m_to_n_symmetric_device",
 )
 
@@ -93,6 +94,8 @@ def lib() -> C.CDLL:
     L.tq_distance_1_to_n_device.argtypes = [vp, fp, u8p, sz, fp, vp]
     L.tq_distance_1_to_n_prepared_device.restype = st
     L.tq_distance_1_to_n_prepared_device.argtypes = [vp, fp, fp, fp, u8p, sz, fp, vp]
+    L.tq_distance_1_to_n_device_noalloc.restype = st
+    L.tq_distance_1_to_n_device_noalloc.argtypes = [vp, fp, u8p, sz, fp, vp]
     L.tq_distance_m_to_n_device.restype = st
     L.tq_distance_m_to_n_device.argtypes = [vp, fp, sz, u8p, sz, fp, C.c_int, vp]
     L.tq_distance_m_to_n_symmetric_device.restype = st
