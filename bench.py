@@ -317,6 +317,96 @@ def run_mton(args, sym):
     }), flush=True)
 
 
+def run_serve(args):
+    """Serving over a device-resident corpus: 20,000,000 codes of a 1024-centre
+    Gaussian mixture at dim 384 (padded 512), 4-bit; requests of m ~ U{1..256}
+    queries from the same mixture ask for exact top-10; Poisson arrivals at each
+    swept rate for one window; p50/p99 request latency (submit -> result on the
+    host) and goodput (completed requests / window) per rate."""
+    import threading
+    import torch
+    import turboquant as tq
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    dim, bits = 384, 4
+    n = args.n if args.n != 10_000_000 else 20_000_000
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(8)
+    centres = torch.randn((1024, dim), generator=gen, device=dev)
+    space = tq.TurboQuantSpace(dim, bits_per_coord=bits, device=0)
+    cs = space.code_size_bytes()
+    codes = torch.empty((n, cs), dtype=torch.uint8, device=dev)
+    chunk = 1 << 20
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        X = mixture_rows(torch, gen, dev, b - a, dim, centres)
+        codes[a:b] = space.encode_batch(X)
+    del X
+    gen.manual_seed(9)
+    pool = mixture_rows(torch, gen, dev, 262_144, dim, centres).cpu().numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    index = space.index(codes)
+    build_s = time.perf_counter() - t0
+    del codes
+    torch.cuda.empty_cache()
+    server = index.serve(k=10, max_rows=1024, slots=2)
+    tuning = server.tuning()
+    rates = [float(r) for r in args.rates.split(",")]
+    rng = np.random.default_rng(9)
+    results = []
+    for rate in rates:
+        server.reset_stats()
+        reqs, refused = [], 0
+        t_start = time.perf_counter()
+        t_next = t_start
+        off = 0
+        while True:
+            t_next += rng.exponential(1.0 / rate)
+            if t_next - t_start > args.window:
+                break
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            m = int(rng.integers(1, 257))
+            if off + m > pool.shape[0]:
+                off = 0
+            try:
+                reqs.append(server.submit(pool[off:off + m]))
+            except tq.BusyError:
+                refused += 1
+            off += m
+        offered_s = time.perf_counter() - t_start
+        lat = []
+        for r in reqs:
+            r.wait()
+            lat.append(r.latency_ms)
+        drain_s = time.perf_counter() - t_start
+        st = server.stats(latencies=False)
+        lat = np.array(lat) if lat else np.array([np.nan])
+        results.append({
+            "rate_req_s": rate, "window_s": round(offered_s, 2), "offered": len(reqs) + refused,
+            "admitted": len(reqs), "refused": refused,
+            "goodput_req_s": round(len(reqs) / drain_s, 2),
+            "rows_per_s": round(st["rows"] / drain_s, 1),
+            "p50_ms": round(float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(float(np.percentile(lat, 99)), 2),
+            "batches": st["batches"], "mean_rows_per_batch": round(st["rows"] / max(1, st["batches"]), 1),
+        })
+        print(json.dumps({"serve_rate": results[-1]}), flush=True)
+    server.close()
+    print(json.dumps({
+        "metric": METRIC, "workload": "serve",
+        "config": {"dim": dim, "padded_dim": space.padded_dim(), "bits_per_coord": bits,
+                   "n_codes": n, "k": 10, "request_rows": "U{1..256}", "arrivals": "Poisson",
+                   "window_s": args.window, "max_batch_rows": 1024, "slots": 2,
+                   "data": "1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 8/9)"},
+        "index_build_s": round(build_s, 2), "tuning": tuning, "results": results,
+    }), flush=True)
+    index.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -327,11 +417,17 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("scan", "mton", "sym"), default="scan",
+    ap.add_argument("--rates", default="5,20,40,60,1000,50000",
+                    help="serve: request rates (req/s) to sweep")
+    ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
+    ap.add_argument("--workload", choices=("scan", "mton", "sym", "serve"), default="scan",
                     help="scan (default): the 1->N scan benchmark; mton/sym: the dense M x N "
                          "contractions, FP32 vs split-BF16")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "serve":
+        run_serve(args)
+        return
     if args.workload != "scan":
         run_mton(args, args.workload == "sym")
         return

@@ -181,6 +181,51 @@ tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t 
                                               float *out, tq_precision precision,
                                               void *stream);
 
+/* ---- serving: device-resident index + continuous-batching top-k server ---
+ * The reference has no index or serving loop (README.md:81-83); these entry
+ * points serve exact top-k asymmetric search (distSearch, space_turbo_quant.h
+ * :659-686) over a corpus kept in HBM.  Results are ascending by distance,
+ * ties broken by the smaller code index (a stable argsort). */
+typedef struct tq_index tq_index;
+typedef struct tq_server tq_server;
+typedef struct tq_request tq_request;
+
+typedef struct tq_server_stats {
+    uint64_t submitted, rejected, completed, batches, rows;
+    size_t queued_rows;
+    int slots, max_rows;
+} tq_server_stats;
+
+/* Decode n codes (host or device memory) once into the index's BF16 operand
+ * planes (4 * 2 * padded_dim bytes per code) in HBM. */
+tq_status tq_index_create(const tq_space *sp, const uint8_t *codes, size_t n, int codes_on_device,
+                          tq_index **out);
+void tq_index_destroy(tq_index *ix);
+
+/* A server answering top-k (k <= 16) for requests of up to max_rows queries
+ * (a multiple of 128).  `slots` batches may be in flight at once (fewer if
+ * they do not fit in half of the free device memory); kernel_variant -1
+ * autotunes the contraction's tile shape per batch-size bucket; queue_rows
+ * bounds the queued query rows (0: 16 x max_rows), beyond which submit
+ * returns TQ_ERR_BUSY. */
+tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int kernel_variant,
+                           size_t queue_rows, tq_server **out);
+/* Queue m query rows (m x dim float32, copied); non-blocking. */
+tq_status tq_server_submit(tq_server *sv, const float *queries, size_t m, tq_request **out);
+/* Wait (timeout_ms < 0: forever) and copy the m x k results and the latency. */
+tq_status tq_request_wait(tq_request *r, int timeout_ms, float *dist, int64_t *idx,
+                          double *latency_ms);
+int tq_request_done(tq_request *r);
+void tq_request_release(tq_request *r);
+/* Counters and up to `cap` recorded request latencies (milliseconds). */
+tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latencies, size_t cap,
+                          size_t *n_latencies);
+tq_status tq_server_reset_stats(tq_server *sv);
+/* The autotuner's choice per bucket: rows, kernel variant, measured ms. */
+tq_status tq_server_tuning(tq_server *sv, int *bucket_rows, int *variant, float *ms, int cap,
+                           int *n);
+void tq_server_destroy(tq_server *sv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,27 +19,15 @@
 #include <string>
 #include <vector>
 
+#include "tq_host.h"
 #include "tq_internal.h"
 #include "tq_mton.h"
 #include "tq_tables.h"
 
-struct tq_space {
-    size_t dim = 0, D = 0, packed_bytes = 0, code_size = 0;
-    int bits = 0, levels = 0, num_threads = 1, device = -1;
-    bool padded = false;
-    uint64_t rot_seed = 0, qjl_seed = 0;
-    std::vector<float> centroids, boundaries, rot_signs, qjl_signs;
-    tq::QuantLut qlut;
-    tq::Params P{};
-    tq::DevTables T{};
-    void *dev_block = nullptr;  // single device allocation holding the tables
-    std::mutex host_mu;         // serialises the host-pointer entry points
-    cudaStream_t host_stream[2] = {nullptr, nullptr};
-};
-
-namespace {
 
 thread_local std::string g_err;
+
+namespace tq {
 
 tq_status fail(tq_status st, const char *fmt, ...) {
     char buf[512];
@@ -57,35 +45,27 @@ tq_status cuda_fail(cudaError_t e, const char *what) {
     return fail(TQ_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define TQ_CUDA(call, what)                          \
-    do {                                             \
-        cudaError_t e_ = (call);                     \
-        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-    } while (0)
-
-struct DeviceGuard {
-    int prev = -1, want = -1;
-    explicit DeviceGuard(int dev) : want(dev) {
-        cudaGetDevice(&prev);
-        if (prev != want) cudaSetDevice(want);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0 && prev != want) cudaSetDevice(prev);
-    }
-};
-
-int ilog2(size_t v) {
-    int l = 0;
-    while ((size_t(1) << l) < v) ++l;
-    return l;
-}
-
 tq_status need_device(const tq_space *sp) {
     if (!sp) return fail(TQ_ERR_INVALID_ARGUMENT, "space is NULL");
     if (sp->device < 0 || !sp->dev_block)
         return fail(TQ_ERR_NO_DEVICE,
                     "no CUDA device: the TurboQuant B200 kernels need an sm_100 GPU");
     return TQ_OK;
+}
+
+}  // namespace tq
+
+using tq::cuda_fail;
+using tq::DeviceGuard;
+using tq::fail;
+using tq::need_device;
+
+namespace {
+
+int ilog2(size_t v) {
+    int l = 0;
+    while ((size_t(1) << l) < v) ++l;
+    return l;
 }
 
 bool is_device_ptr(const void *p) {

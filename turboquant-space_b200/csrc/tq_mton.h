@@ -36,4 +36,20 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
                            const float *r2, const float *c1, const float *c2, float *out,
                            size_t ldo, int *err, cudaStream_t st);
 
+// Top-k over a device-resident index: C = A B^T as above, reduced per row to the
+// k (<= 16) smallest (distance, index) pairs, ties to the smaller index.
+// The row count is read from m_dev; `grid` CTAs split the rows into 128-row
+// blocks and the columns into slices; partials hold grid * 128 * 16 entries.
+// Variant 0: 128 x 256 tiles, 2 stages; variant 1: 128 x 128 tiles, 3 stages.
+constexpr int kTopKMax = 16;
+int tc_topk_variants();
+cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
+                           const void *Bh, const void *Bl, size_t n_pad, int K, const int *m_dev,
+                           size_t n, const float *r1, const float *r2, const float *c1,
+                           const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
+                           cudaStream_t st);
+cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
+                              const int *part_i, int k, size_t max_rows, float *out_d,
+                              long long *out_i, cudaStream_t st);
+
 }  // namespace tq

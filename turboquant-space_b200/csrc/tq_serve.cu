@@ -1,0 +1,614 @@
+// tq_serve.cu -- device-resident index and the continuous-batching search server.
+//
+// The reference has no index or serving loop (README.md:81-83); this is the
+// north-star serving path built on the same distance contraction:
+//
+//   tq_index   the corpus decoded once into hi/lo BF16 planes
+//              B[j] = [sigma_j c[idx_j] | scale gamma_j (+-1)_j] (K = 2D) plus
+//              |x_j| and |x_j|^2, resident in HBM.
+//   slot       buffers for one batch of up to `max_rows` query rows and one CUDA
+//              graph per row bucket (128, 256, 512, ... max_rows) capturing
+//              H2D queries -> prepareQuery -> query planes -> tcgen05 top-k ->
+//              merge -> D2H results; the kernels read the batch's row count
+//              from device memory, so the graph replays for any batch size.
+//   server     a scheduler thread.  Requests are queued on submit; whenever a
+//              slot is free the queued requests are packed in arrival order
+//              into one batch (continuous batching: requests that arrive while
+//              other batches are on the GPU join the next batch) and the
+//              bucket's graph is launched on the slot's stream.  Slots run on
+//              separate streams, so one batch's copies and query preparation
+//              overlap another's contraction.  Admission: the slots are sized
+//              from the device's free memory at creation, and submit refuses a
+//              request (TQ_ERR_BUSY) when the queued rows would exceed the
+//              queue capacity.
+//   autotune   per bucket, each kernel variant (tile shape x stage depth) is
+//              timed on the index and the fastest is captured into the graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "tq_host.h"
+#include "tq_mton.h"
+
+struct tq_index {
+    tq_space *sp = nullptr;
+    size_t n = 0, n_pad = 0;
+    int K = 0;
+    void *planes = nullptr;  // hi plane, then lo plane: n_pad x K BF16 each
+    float *c1 = nullptr, *c2 = nullptr;
+    int device = -1;
+};
+
+namespace {
+
+using tq::cuda_fail;
+using tq::DeviceGuard;
+using tq::fail;
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+struct tq_request {
+    std::vector<float> queries;  // m x dim
+    size_t m = 0;
+    int k = 0;
+    std::vector<float> dist;     // m x k
+    std::vector<long long> idx;  // m x k
+    double t_submit = 0, t_done = 0;
+    tq_status status = TQ_OK;
+    bool done = false;
+    std::mutex mu;
+    std::condition_variable cv;
+};
+
+namespace {
+
+struct Slot {
+    int max_rows = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    float *h_q = nullptr;
+    int *h_m = nullptr;
+    int *h_err = nullptr;
+    float *h_d = nullptr;
+    long long *h_i = nullptr;
+    void *d_block = nullptr;  // one device allocation for all buffers below
+    float *d_q = nullptr, *d_prep = nullptr, *d_r1 = nullptr, *d_r2 = nullptr, *d_pd = nullptr,
+          *d_od = nullptr;
+    int *d_m = nullptr, *d_pi = nullptr, *d_err = nullptr;
+    void *d_ap = nullptr;  // query planes: max_rows x K x 2 BF16 planes
+    long long *d_oi = nullptr;
+    std::vector<int> bucket_rows;
+    std::vector<cudaGraphExec_t> graphs;
+    std::vector<tq_request *> batch;  // requests in flight in this slot
+    size_t batch_rows = 0;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct tq_server {
+    tq_index *index = nullptr;
+    int k = 10;
+    int grid = 148;
+    int max_rows = 1024;
+    size_t queue_rows_cap = 0;
+    std::vector<Slot> slots;
+    std::vector<int> bucket_variant;  // autotuned kernel variant per bucket
+    std::vector<double> bucket_ms;
+    std::deque<tq_request *> pending;
+    size_t pending_rows = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread worker;
+    bool stop = false;
+    // stats
+    uint64_t submitted = 0, rejected = 0, completed = 0, batches = 0, rows_done = 0;
+    std::vector<float> latencies_ms;  // ring of the most recent completions
+    size_t lat_pos = 0;
+    double busy_ms = 0;
+};
+
+namespace {
+
+int bucket_index(const tq_server *sv, size_t rows) {
+    const auto &b = sv->slots[0].bucket_rows;
+    for (size_t i = 0; i < b.size(); ++i)
+        if (rows <= (size_t)b[i]) return (int)i;
+    return (int)b.size() - 1;
+}
+
+// Enqueue the batch pipeline of `rows_cap` rows with kernel variant `var` on
+// the slot's stream (used both for graph capture and for autotuning runs).
+cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool copies) {
+    tq_index *ix = sv->index;
+    tq_space *sp = ix->sp;
+    const size_t D = sp->D;
+    const size_t K = (size_t)ix->K;
+    cudaStream_t st = sl.stream;
+    cudaError_t e = cudaSuccess;
+    if (copies) {
+        e = cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)rows_cap * sp->dim * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.d_m, sl.h_m, sizeof(int), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    float *q_rot = sl.d_prep, *s_q = q_rot + (size_t)rows_cap * D, *norms = s_q + (size_t)rows_cap * D;
+    e = tq::launch_prepare(sp->P, sp->T, sl.d_q, rows_cap, q_rot, s_q, norms, st);
+    if (e != cudaSuccess) return e;
+    unsigned char *ah = static_cast<unsigned char *>(sl.d_ap);
+    unsigned char *al = ah + (size_t)rows_cap * K * 2;
+    e = tq::launch_planes_from_prepared(q_rot, s_q, norms, rows_cap, rows_cap, (int)D, tq::kPlaneBF16,
+                                        ah, al, sl.d_r1, sl.d_r2, st);
+    if (e != cudaSuccess) return e;
+    unsigned char *bh = static_cast<unsigned char *>(ix->planes);
+    unsigned char *bl = bh + ix->n_pad * K * 2;
+    e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, sl.d_m, ix->n, sl.d_r1,
+                           sl.d_r2, ix->c1, ix->c2, sv->k, sl.d_pd, sl.d_pi, sl.d_err, sv->grid, st);
+    if (e != cudaSuccess) return e;
+    e = tq::launch_topk_merge(sl.d_m, sv->grid, sl.d_pd, sl.d_pi, sv->k, rows_cap, sl.d_od, sl.d_oi, st);
+    if (e != cudaSuccess) return e;
+    if (copies) {
+        e = cudaMemcpyAsync(sl.h_d, sl.d_od, (size_t)rows_cap * sv->k * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(sl.h_i, sl.d_oi, (size_t)rows_cap * sv->k * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_err, sl.d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    }
+    return e;
+}
+
+tq_status slot_alloc(tq_server *sv, Slot &sl) {
+    tq_index *ix = sv->index;
+    tq_space *sp = ix->sp;
+    const size_t R = (size_t)sv->max_rows, D = sp->D, K = (size_t)ix->K, k = (size_t)sv->k;
+    sl.max_rows = sv->max_rows;
+    TQ_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    TQ_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "cudaEventCreate");
+    TQ_CUDA(cudaMallocHost(&sl.h_q, R * sp->dim * 4), "cudaMallocHost(queries)");
+    TQ_CUDA(cudaMallocHost(&sl.h_m, 16), "cudaMallocHost(m)");
+    TQ_CUDA(cudaMallocHost(&sl.h_err, 16), "cudaMallocHost(err)");
+    *sl.h_err = 0;
+    TQ_CUDA(cudaMallocHost(&sl.h_d, R * k * 4), "cudaMallocHost(dist)");
+    TQ_CUDA(cudaMallocHost(&sl.h_i, R * k * 8), "cudaMallocHost(idx)");
+    std::memset(sl.h_q, 0, R * sp->dim * 4);
+    // device block layout (each part 256-byte aligned)
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = round_up(off + bytes, 256);
+        return o;
+    };
+    const size_t o_q = take(R * sp->dim * 4), o_m = take(16), o_prep = take(R * (2 * D + 2) * 4);
+    const size_t o_ap = take(R * K * 4), o_r1 = take(R * 4), o_r2 = take(R * 4);
+    const size_t parts = (size_t)sv->grid * 128 * tq::kTopKMax;
+    const size_t o_pd = take(parts * 4), o_pi = take(parts * 4), o_od = take(R * k * 4);
+    const size_t o_oi = take(R * k * 8), o_err = take(16);
+    TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
+    TQ_CUDA(cudaMemset(sl.d_block, 0, off), "cudaMemset(slot)");
+    auto *base = static_cast<unsigned char *>(sl.d_block);
+    sl.d_q = reinterpret_cast<float *>(base + o_q);
+    sl.d_m = reinterpret_cast<int *>(base + o_m);
+    sl.d_prep = reinterpret_cast<float *>(base + o_prep);
+    sl.d_ap = base + o_ap;
+    sl.d_r1 = reinterpret_cast<float *>(base + o_r1);
+    sl.d_r2 = reinterpret_cast<float *>(base + o_r2);
+    sl.d_pd = reinterpret_cast<float *>(base + o_pd);
+    sl.d_pi = reinterpret_cast<int *>(base + o_pi);
+    sl.d_od = reinterpret_cast<float *>(base + o_od);
+    sl.d_oi = reinterpret_cast<long long *>(base + o_oi);
+    sl.d_err = reinterpret_cast<int *>(base + o_err);
+    for (int b = 128; b < sv->max_rows; b *= 2) sl.bucket_rows.push_back(b);
+    sl.bucket_rows.push_back(sv->max_rows);
+    return TQ_OK;
+}
+
+void slot_free(Slot &sl) {
+    for (auto g : sl.graphs)
+        if (g) cudaGraphExecDestroy(g);
+    sl.graphs.clear();
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+    if (sl.d_block) cudaFree(sl.d_block);
+    if (sl.h_q) cudaFreeHost(sl.h_q);
+    if (sl.h_m) cudaFreeHost(sl.h_m);
+    if (sl.h_err) cudaFreeHost(sl.h_err);
+    if (sl.h_d) cudaFreeHost(sl.h_d);
+    if (sl.h_i) cudaFreeHost(sl.h_i);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
+    sl = Slot();
+}
+
+// Time each kernel variant for each bucket on slot 0 (full buckets of zero
+// queries: the work does not depend on the values) and keep the fastest.
+tq_status autotune(tq_server *sv, int fixed_variant) {
+    Slot &sl = sv->slots[0];
+    const int nb = (int)sl.bucket_rows.size();
+    sv->bucket_variant.assign(nb, fixed_variant >= 0 ? fixed_variant : 0);
+    sv->bucket_ms.assign(nb, 0.0);
+    cudaEvent_t e0, e1;
+    TQ_CUDA(cudaEventCreate(&e0), "event");
+    TQ_CUDA(cudaEventCreate(&e1), "event");
+    for (int b = 0; b < nb; ++b) {
+        const int rows = sl.bucket_rows[b];
+        *sl.h_m = rows;
+        TQ_CUDA(cudaMemcpyAsync(sl.d_m, sl.h_m, sizeof(int), cudaMemcpyHostToDevice, sl.stream), "H2D m");
+        double best = 1e30;
+        for (int v = 0; v < tq::tc_topk_variants(); ++v) {
+            if (fixed_variant >= 0 && v != fixed_variant) continue;
+            TQ_CUDA(enqueue_batch(sv, sl, rows, v, false), "autotune warm-up");
+            TQ_CUDA(cudaEventRecord(e0, sl.stream), "event");
+            TQ_CUDA(enqueue_batch(sv, sl, rows, v, false), "autotune run");
+            TQ_CUDA(cudaEventRecord(e1, sl.stream), "event");
+            TQ_CUDA(cudaEventSynchronize(e1), "autotune sync");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                sv->bucket_variant[b] = v;
+            }
+        }
+        sv->bucket_ms[b] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int herr = 0;
+    TQ_CUDA(cudaMemcpy(&herr, sl.d_err, sizeof(int), cudaMemcpyDeviceToHost), "D2H status");
+    if (herr) return fail(TQ_ERR_TIMEOUT, "top-k kernel: a pipeline wait timed out (code %d)", herr);
+    return TQ_OK;
+}
+
+tq_status capture_graphs(tq_server *sv, Slot &sl) {
+    for (size_t b = 0; b < sl.bucket_rows.size(); ++b) {
+        cudaGraph_t g = nullptr;
+        TQ_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaError_t e = enqueue_batch(sv, sl, sl.bucket_rows[b], sv->bucket_variant[b], true);
+        cudaError_t e2 = cudaStreamEndCapture(sl.stream, &g);
+        if (e != cudaSuccess) return cuda_fail(e, "capture batch");
+        if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
+        cudaGraphExec_t ex = nullptr;
+        e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+        sl.graphs.push_back(ex);
+    }
+    return TQ_OK;
+}
+
+void finish_request(tq_server *sv, tq_request *r, double t) {
+    {
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->t_done = t;
+        r->done = true;
+    }
+    r->cv.notify_all();
+    const float lat = (float)(t - r->t_submit);
+    if (sv->latencies_ms.size() < 1u << 20) {
+        sv->latencies_ms.push_back(lat);
+    } else {
+        sv->latencies_ms[sv->lat_pos] = lat;
+        sv->lat_pos = (sv->lat_pos + 1) % sv->latencies_ms.size();
+    }
+}
+
+// The scheduler: completes finished batches, then packs queued requests into
+// every free slot.
+void worker_loop(tq_server *sv) {
+    DeviceGuard g(sv->index->device);
+    const size_t dim = sv->index->sp->dim;
+    const int k = sv->k;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    while (true) {
+        bool any_busy = false;
+        for (auto &sl : sv->slots) {
+            if (!sl.busy) continue;
+            const cudaError_t q = cudaEventQuery(sl.done);
+            if (q == cudaErrorNotReady) {
+                any_busy = true;
+                continue;
+            }
+            const double t = now_ms();
+            const int herr = (q == cudaSuccess) ? *sl.h_err : 0;
+            size_t row = 0;
+            for (tq_request *r : sl.batch) {
+                if (q != cudaSuccess || herr) {
+                    r->status = q != cudaSuccess ? TQ_ERR_CUDA : TQ_ERR_TIMEOUT;
+                } else {
+                    std::memcpy(r->dist.data(), sl.h_d + row * k, r->m * k * sizeof(float));
+                    std::memcpy(r->idx.data(), sl.h_i + row * k, r->m * k * sizeof(long long));
+                }
+                row += r->m;
+                finish_request(sv, r, t);
+            }
+            sv->completed += sl.batch.size();
+            sv->rows_done += sl.batch_rows;
+            sl.batch.clear();
+            sl.batch_rows = 0;
+            sl.busy = false;
+        }
+        if (sv->stop && sv->pending.empty() && !any_busy) break;
+        for (auto &sl : sv->slots) {
+            if (sl.busy || sv->pending.empty()) continue;
+            size_t rows = 0;
+            while (!sv->pending.empty() && rows + sv->pending.front()->m <= (size_t)sv->max_rows) {
+                tq_request *r = sv->pending.front();
+                sv->pending.pop_front();
+                sv->pending_rows -= r->m;
+                std::memcpy(sl.h_q + rows * dim, r->queries.data(), r->m * dim * sizeof(float));
+                rows += r->m;
+                sl.batch.push_back(r);
+            }
+            if (sl.batch.empty()) continue;
+            *sl.h_m = (int)rows;
+            sl.batch_rows = rows;
+            const int b = bucket_index(sv, rows);
+            cudaError_t e = cudaGraphLaunch(sl.graphs[b], sl.stream);
+            if (e == cudaSuccess) e = cudaEventRecord(sl.done, sl.stream);
+            if (e != cudaSuccess) {
+                for (tq_request *r : sl.batch) {
+                    r->status = TQ_ERR_CUDA;
+                    finish_request(sv, r, now_ms());
+                }
+                sl.batch.clear();
+                continue;
+            }
+            sl.busy = true;
+            any_busy = true;
+            ++sv->batches;
+        }
+        if (any_busy) {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+            lk.lock();
+        } else {
+            sv->cv.wait_for(lk, std::chrono::milliseconds(5),
+                            [&] { return sv->stop || !sv->pending.empty(); });
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n,
+                          int codes_on_device, tq_index **out) {
+    if (!out) return fail(TQ_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    tq_status st = tq::need_device(csp);
+    if (st != TQ_OK) return st;
+    if (n == 0 || !codes) return fail(TQ_ERR_INVALID_ARGUMENT, "index: empty corpus");
+    if (n > 0x7ffffff0ull) return fail(TQ_ERR_INVALID_ARGUMENT, "index: more than 2^31 codes");
+    auto *sp = const_cast<tq_space *>(csp);
+    const size_t K = 2 * sp->D;
+    if (K % 64) return fail(TQ_ERR_NOT_SUPPORTED, "index: padded dim must be a multiple of 32");
+    DeviceGuard g(sp->device);
+    auto *ix = new tq_index();
+    ix->sp = sp;
+    ix->n = n;
+    ix->n_pad = round_up(n, 256);
+    ix->K = (int)K;
+    ix->device = sp->device;
+    const size_t plane = ix->n_pad * K * 2;
+    cudaError_t e = cudaMalloc(&ix->planes, 2 * plane + 2 * ix->n_pad * 4 + 256);
+    if (e != cudaSuccess) {
+        delete ix;
+        return cuda_fail(e, "cudaMalloc(index planes)");
+    }
+    ix->c1 = reinterpret_cast<float *>(static_cast<unsigned char *>(ix->planes) + 2 * plane);
+    ix->c2 = ix->c1 + ix->n_pad;
+    auto *hi = static_cast<unsigned char *>(ix->planes);
+    auto *lo = hi + plane;
+    const size_t chunk = 1 << 20;
+    uint8_t *stage = nullptr;
+    if (!codes_on_device) {
+        e = cudaMalloc(&stage, std::min(chunk, n) * sp->code_size + 16);
+        if (e != cudaSuccess) {
+            cudaFree(ix->planes);
+            delete ix;
+            return cuda_fail(e, "cudaMalloc(index staging)");
+        }
+    }
+    for (size_t r0 = 0; r0 < ix->n_pad && e == cudaSuccess; r0 += chunk) {
+        const size_t rows_pad = std::min(chunk, ix->n_pad - r0);
+        const size_t rows = r0 < n ? std::min(rows_pad, n - r0) : 0;
+        const uint8_t *src = codes + r0 * sp->code_size;
+        if (!codes_on_device && rows) {
+            e = cudaMemcpy(stage, src, rows * sp->code_size, cudaMemcpyHostToDevice);
+            src = stage;
+        }
+        if (e == cudaSuccess)
+            e = tq::launch_planes_from_codes(sp->P, sp->T, rows ? src : stage ? stage : codes, rows,
+                                             rows_pad, false, tq::kPlaneBF16, hi + r0 * K * 2,
+                                             lo + r0 * K * 2, ix->c1 + r0, ix->c2 + r0, nullptr);
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (stage) cudaFree(stage);
+    if (e != cudaSuccess) {
+        cudaFree(ix->planes);
+        delete ix;
+        return cuda_fail(e, "index build");
+    }
+    *out = ix;
+    return TQ_OK;
+}
+
+void tq_index_destroy(tq_index *ix) {
+    if (!ix) return;
+    DeviceGuard g(ix->device);
+    if (ix->planes) cudaFree(ix->planes);
+    delete ix;
+}
+
+tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int kernel_variant,
+                           size_t queue_rows, tq_server **out) {
+    if (!out || !ix) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (k < 1 || k > tq::kTopKMax) return fail(TQ_ERR_INVALID_ARGUMENT, "k must be in 1..%d", tq::kTopKMax);
+    if (max_rows < 128 || max_rows % 128) return fail(TQ_ERR_INVALID_ARGUMENT, "max_rows must be a positive multiple of 128");
+    if (slots < 1 || slots > 8) return fail(TQ_ERR_INVALID_ARGUMENT, "slots must be in 1..8");
+    if (kernel_variant >= tq::tc_topk_variants()) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown kernel variant");
+    DeviceGuard g(ix->device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+    if (max_rows / 128 > sms) return fail(TQ_ERR_INVALID_ARGUMENT, "max_rows too large for this GPU");
+    auto *sv = new tq_server();
+    sv->index = ix;
+    sv->k = k;
+    sv->grid = sms;
+    sv->max_rows = max_rows;
+    sv->queue_rows_cap = queue_rows ? queue_rows : (size_t)16 * max_rows;
+    // admission by free device memory: no more slots than fit in half the free memory
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t D = ix->sp->D, K = (size_t)ix->K, R = (size_t)max_rows;
+    const size_t slot_bytes = R * (ix->sp->dim * 4 + (2 * D + 2) * 4 + K * 4 + 8 + (size_t)k * 12) +
+                              (size_t)sms * 128 * tq::kTopKMax * 8 + 4096;
+    const size_t fit = std::max<size_t>(1, (free_b / 2) / slot_bytes);
+    slots = (int)std::min<size_t>((size_t)slots, fit);
+    sv->slots.resize(slots);
+    tq_status st = TQ_OK;
+    for (auto &sl : sv->slots)
+        if ((st = slot_alloc(sv, sl)) != TQ_OK) break;
+    if (st == TQ_OK) st = autotune(sv, kernel_variant);
+    for (auto &sl : sv->slots) {
+        if (st != TQ_OK) break;
+        st = capture_graphs(sv, sl);
+    }
+    if (st != TQ_OK) {
+        for (auto &sl : sv->slots) slot_free(sl);
+        delete sv;
+        return st;
+    }
+    sv->worker = std::thread(worker_loop, sv);
+    *out = sv;
+    return TQ_OK;
+}
+
+tq_status tq_server_submit(tq_server *sv, const float *queries, size_t m, tq_request **out) {
+    if (!sv || !out || (m && !queries)) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (m == 0 || m > (size_t)sv->max_rows)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "request rows must be in 1..%d", sv->max_rows);
+    const size_t dim = sv->index->sp->dim;
+    auto *r = new tq_request();
+    r->queries.assign(queries, queries + m * dim);
+    r->m = m;
+    r->k = sv->k;
+    r->dist.assign(m * sv->k, 0.0f);
+    r->idx.assign(m * sv->k, -1);
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        ++sv->submitted;
+        if (sv->stop || sv->pending_rows + m > sv->queue_rows_cap) {
+            ++sv->rejected;
+            delete r;
+            return fail(TQ_ERR_BUSY, "server queue full (%zu rows queued)", sv->pending_rows);
+        }
+        r->t_submit = now_ms();
+        sv->pending.push_back(r);
+        sv->pending_rows += m;
+    }
+    sv->cv.notify_one();
+    *out = r;
+    return TQ_OK;
+}
+
+tq_status tq_request_wait(tq_request *r, int timeout_ms, float *dist, int64_t *idx,
+                          double *latency_ms) {
+    if (!r) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL request");
+    std::unique_lock<std::mutex> lk(r->mu);
+    if (timeout_ms < 0) {
+        r->cv.wait(lk, [&] { return r->done; });
+    } else if (!r->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return r->done; })) {
+        return fail(TQ_ERR_TIMEOUT, "request not finished within %d ms", timeout_ms);
+    }
+    if (r->status != TQ_OK) return fail(r->status, "request failed on the device");
+    if (dist) std::memcpy(dist, r->dist.data(), r->dist.size() * sizeof(float));
+    if (idx) std::memcpy(idx, r->idx.data(), r->idx.size() * sizeof(long long));
+    if (latency_ms) *latency_ms = r->t_done - r->t_submit;
+    return TQ_OK;
+}
+
+int tq_request_done(tq_request *r) {
+    if (!r) return 0;
+    std::lock_guard<std::mutex> lk(r->mu);
+    return r->done ? 1 : 0;
+}
+
+void tq_request_release(tq_request *r) {
+    if (!r) return;
+    {
+        std::unique_lock<std::mutex> lk(r->mu);
+        r->cv.wait(lk, [&] { return r->done; });
+    }
+    delete r;
+}
+
+tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latencies, size_t cap,
+                          size_t *n_lat) {
+    if (!sv || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    out->submitted = sv->submitted;
+    out->rejected = sv->rejected;
+    out->completed = sv->completed;
+    out->batches = sv->batches;
+    out->rows = sv->rows_done;
+    out->queued_rows = sv->pending_rows;
+    out->slots = (int)sv->slots.size();
+    out->max_rows = sv->max_rows;
+    size_t nl = std::min(cap, sv->latencies_ms.size());
+    if (latencies && nl) std::memcpy(latencies, sv->latencies_ms.data(), nl * sizeof(float));
+    if (n_lat) *n_lat = latencies ? nl : sv->latencies_ms.size();
+    return TQ_OK;
+}
+
+tq_status tq_server_reset_stats(tq_server *sv) {
+    if (!sv) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL server");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->submitted = sv->rejected = sv->completed = sv->batches = sv->rows_done = 0;
+    sv->latencies_ms.clear();
+    sv->lat_pos = 0;
+    return TQ_OK;
+}
+
+tq_status tq_server_tuning(tq_server *sv, int *bucket_rows, int *variant, float *ms, int cap, int *n) {
+    if (!sv) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL server");
+    const auto &b = sv->slots[0].bucket_rows;
+    const int nb = (int)std::min<size_t>(b.size(), (size_t)cap);
+    for (int i = 0; i < nb; ++i) {
+        if (bucket_rows) bucket_rows[i] = b[i];
+        if (variant) variant[i] = sv->bucket_variant[i];
+        if (ms) ms[i] = (float)sv->bucket_ms[i];
+    }
+    if (n) *n = (int)b.size();
+    return TQ_OK;
+}
+
+void tq_server_destroy(tq_server *sv) {
+    if (!sv) return;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+    }
+    sv->cv.notify_all();
+    if (sv->worker.joinable()) sv->worker.join();
+    DeviceGuard g(sv->index->device);
+    for (auto &sl : sv->slots) slot_free(sl);
+    delete sv;
+}
+
+}  // extern "C"

@@ -120,6 +120,16 @@ __device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, ui
         : "memory");
 }
 
+__device__ __forceinline__ void umma_i(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
@@ -306,6 +316,290 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// tc_topk_kernel: the same contraction over a device-resident index, with the
+// distances reduced to a per-row top-k instead of being stored.  The number of
+// query rows m is read from device memory (so that one captured launch serves
+// batches of any size up to the buffers' capacity).  CTA c takes row block
+// c / S and the contiguous slice c % S of the column tiles, S = grid / row
+// blocks; each epilogue thread keeps its row's best k (distance, index) pairs,
+// ties broken by the smaller index, and writes them to the partial buffers
+// part_d / part_i [(block * S + slice) * 128 + row][kTopKMax].
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool better(float d, int i, float bd, int bi) {
+    return d < bd || (d == bd && i < bi);
+}
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_topk_kernel(
+    const __grid_constant__ CUtensorMap tm_ah, const __grid_constant__ CUtensorMap tm_al,
+    const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl, int K,
+    const int *__restrict__ m_dev, unsigned nb_tiles, size_t n, const float *__restrict__ r1,
+    const float *__restrict__ r2, const float *__restrict__ c1, const float *__restrict__ c2, int k,
+    float *__restrict__ part_d, int *__restrict__ part_i, int *err) {
+    constexpr int B_BYTES = BN * TC_BK * 2;
+    constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * B_BYTES;
+    constexpr int TMEM_COLS = 2 * BN;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(TC_BM >> 4) << 24);
+    const int m = *m_dev;
+    const int num_mb = (m + TC_BM - 1) / TC_BM;
+    if (num_mb <= 0 || num_mb > (int)gridDim.x) return;
+    const int S = (int)gridDim.x / num_mb;
+    if ((int)blockIdx.x >= num_mb * S) return;  // uniform over the CTA
+    const int mb = (int)blockIdx.x / S, slice = (int)blockIdx.x % S;
+    const unsigned nb0 = (unsigned)(((size_t)nb_tiles * slice) / S);
+    const unsigned nb1 = (unsigned)(((size_t)nb_tiles * (slice + 1)) / S);
+    const unsigned ntiles = nb1 - nb0;
+
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    // bars: full[STAGES], empty[STAGES], tfull[2], tempty[2], drain; then the TMEM slot
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
+    const uint32_t tfull0 = smem_u32(bars + 2 * STAGES), tempty0 = smem_u32(bars + 2 * STAGES + 2);
+    const uint32_t drain = smem_u32(bars + 2 * STAGES + 4);
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < STAGES; ++st) {
+            mbar_init(full0 + 8 * st, 1);
+            mbar_init(empty0 + 8 * st, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(tfull0 + 8 * b, 1);
+            mbar_init(tempty0 + 8 * b, 128);
+        }
+        mbar_init(drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int KB = K / TC_BK;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (unsigned t = 0; t < ntiles && ok; ++t) {
+                const int nb = (int)(nb0 + t);
+                for (int kb = 0; kb < KB; ++kb, ++it) {
+                    const uint32_t st = it % STAGES, ph = (it / STAGES) & 1u;
+                    if (!mbar_wait(empty0 + 8 * st, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
+                    const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
+                    const uint32_t fb = full0 + 8 * st;
+                    mbar_expect_tx(fb, STAGE_BYTES);
+                    tma_load_2d(base, &tm_ah, kb * TC_BK, mb * TC_BM, fb);
+                    tma_load_2d(base + TC_A_BYTES, &tm_al, kb * TC_BK, mb * TC_BM, fb);
+                    tma_load_2d(base + 2 * TC_A_BYTES, &tm_bh, kb * TC_BK, nb * BN, fb);
+                    tma_load_2d(base + 2 * TC_A_BYTES + B_BYTES, &tm_bl, kb * TC_BK, nb * BN, fb);
+                }
+            }
+            const uint32_t drain_n = it < (uint32_t)STAGES ? it : (uint32_t)STAGES;
+            for (uint32_t q = 0; q < drain_n; ++q) {
+                const uint32_t j = it - 1 - q;
+                mbar_wait(full0 + 8 * (j % STAGES), (j / STAGES) & 1u, err, kErrFull);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (unsigned t = 0; t < ntiles && ok; ++t) {
+                const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
+                if (!mbar_wait(tempty0 + 8 * b, tph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + b * BN;
+                for (int kb = 0; kb < KB; ++kb, ++it) {
+                    const uint32_t st = it % STAGES, ph = (it / STAGES) & 1u;
+                    if (!mbar_wait(full0 + 8 * st, ph, err, kErrFull)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
+                    const uint32_t ah = base, al = base + TC_A_BYTES;
+                    const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + B_BYTES;
+#pragma unroll
+                    for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                        const uint32_t koff = kk * 32;
+                        const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+                        umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), IDESC, acc);
+                        umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), IDESC, 1u);
+                        umma_i(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), IDESC, 1u);
+                    }
+                    umma_commit(empty0 + 8 * st);
+                }
+                if (ok) umma_commit(tfull0 + 8 * b);
+            }
+            umma_commit(drain);
+            mbar_wait(drain, 0, err, kErrFull);
+        }
+    } else {
+        const int q = warp & 3;
+        const int row_in_tile = 32 * q + lane;
+        const int row = mb * TC_BM + row_in_tile;
+        const bool row_ok = row < m;
+        const float rr1 = row_ok ? __ldg(r1 + row) : 0.0f;
+        const float rr2 = row_ok ? __ldg(r2 + row) : 0.0f;
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+#pragma unroll
+        for (int t = 0; t < kTopKMax; ++t) {
+            bd[t] = INFINITY;
+            bi[t] = 0x7fffffff;
+        }
+        float thr_d = INFINITY;
+        int thr_i = 0x7fffffff;
+        for (unsigned t = 0; t < ntiles; ++t) {
+            const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
+            if (!mbar_wait(tfull0 + 8 * b, tph, err, kErrTmemFull)) break;
+            tc_fence_after();
+            const size_t colbase = (size_t)(nb0 + t) * BN;
+#pragma unroll 1
+            for (int ch = 0; ch < BN / 32; ++ch) {
+                uint32_t r[32];
+                __syncwarp();
+                tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + b * BN + ch * 32, r);
+                const size_t col0 = colbase + ch * 32;
+                if (row_ok) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const size_t col = col0 + j;
+                        if (col >= n) break;
+                        const float ipt = __fmul_rn(__fmul_rn(__uint_as_float(r[j]), rr1), __ldg(c1 + col));
+                        float d = __fsub_rn(__fadd_rn(rr2, __ldg(c2 + col)), __fmul_rn(2.0f, ipt));
+                        d = d > 0.0f ? d : 0.0f;
+                        const int ci = (int)col;
+                        if (better(d, ci, thr_d, thr_i)) {
+                            float cd = d;
+                            int cx = ci;
+#pragma unroll
+                            for (int u = 0; u < kTopKMax; ++u) {
+                                if (u < k) {
+                                    const bool sw = better(cd, cx, bd[u], bi[u]);
+                                    const float td = bd[u];
+                                    const int ti = bi[u];
+                                    bd[u] = sw ? cd : td;
+                                    bi[u] = sw ? cx : ti;
+                                    cd = sw ? td : cd;
+                                    cx = sw ? ti : cx;
+                                }
+                            }
+#pragma unroll
+                            for (int u = 0; u < kTopKMax; ++u)
+                                if (u == k - 1) {
+                                    thr_d = bd[u];
+                                    thr_i = bi[u];
+                                }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            tc_fence_before();
+            mbar_arrive(tempty0 + 8 * b);
+        }
+        if (row_ok) {
+            const size_t o = ((size_t)blockIdx.x * TC_BM + row_in_tile) * kTopKMax;
+#pragma unroll
+            for (int u = 0; u < kTopKMax; ++u)
+                if (u < k) {
+                    part_d[o + u] = bd[u];
+                    part_i[o + u] = bi[u];
+                }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// Merge of the per-slice candidates: one warp per query row.  Each lane keeps
+// the best k of its slices, then k rounds of a warp arg-min on (d, index)
+// produce the sorted top-k.
+__global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__ m_dev, int slices_cap,
+                                                         int grid_ctas, const float *__restrict__ part_d,
+                                                         const int *__restrict__ part_i, int k,
+                                                         float *__restrict__ out_d,
+                                                         long long *__restrict__ out_i) {
+    const int m = *m_dev;
+    const int num_mb = (m + TC_BM - 1) / TC_BM;
+    if (num_mb <= 0 || num_mb > grid_ctas) return;
+    const int S = grid_ctas / num_mb;
+    (void)slices_cap;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < m; row += gridDim.x * wpb) {
+        const int mb = row / TC_BM, rit = row % TC_BM;
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+#pragma unroll
+        for (int t = 0; t < kTopKMax; ++t) {
+            bd[t] = INFINITY;
+            bi[t] = 0x7fffffff;
+        }
+        for (int sl = lane; sl < S; sl += 32) {
+            const size_t o = ((size_t)(mb * S + sl) * TC_BM + rit) * kTopKMax;
+            for (int u = 0; u < k; ++u) {
+                float cd = part_d[o + u];
+                int cx = part_i[o + u];
+#pragma unroll
+                for (int v = 0; v < kTopKMax; ++v) {
+                    if (v < k) {
+                        const bool sw = better(cd, cx, bd[v], bi[v]);
+                        const float td = bd[v];
+                        const int ti = bi[v];
+                        bd[v] = sw ? cd : td;
+                        bi[v] = sw ? cx : ti;
+                        cd = sw ? td : cd;
+                        cx = sw ? ti : cx;
+                    }
+                }
+            }
+        }
+        // k rounds: warp arg-min of each lane's current head
+        int head = 0;
+        for (int u = 0; u < k; ++u) {
+            float hd = INFINITY;
+            int hx = 0x7fffffff;
+#pragma unroll
+            for (int v = 0; v < kTopKMax; ++v)
+                if (v == head) {
+                    hd = bd[v];
+                    hx = bi[v];
+                }
+            float wd = hd;
+            int wx = hx;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float od = __shfl_xor_sync(0xffffffffu, wd, off);
+                const int ox = __shfl_xor_sync(0xffffffffu, wx, off);
+                if (better(od, ox, wd, wx)) {
+                    wd = od;
+                    wx = ox;
+                }
+            }
+            if (hx == wx && hd == wd && head < k) ++head;  // the winning lane pops its head
+            if (lane == 0) {
+                out_d[(size_t)row * k + u] = wd;
+                out_i[(size_t)row * k + u] = (wx == 0x7fffffff) ? -1 : (long long)wx;
+            }
+        }
+    }
+}
+
 // ---- host: tensor maps ------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -333,7 +627,54 @@ bool make_map(CUtensorMap *map, const void *base, int K, size_t rows, int box_ro
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <int BN, int STAGES>
+cudaError_t topk_variant(const void *Ah, const void *Al, size_t rows_pad, const void *Bh,
+                         const void *Bl, size_t n_pad, int K, const int *m_dev, size_t n,
+                         const float *r1, const float *r2, const float *c1, const float *c2, int k,
+                         float *part_d, int *part_i, int *err, int grid, cudaStream_t st) {
+    if (K % TC_BK || rows_pad % TC_BM || n_pad % BN) return cudaErrorInvalidValue;
+    for (const void *p : {Ah, Al, Bh, Bl})
+        if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
+    alignas(64) CUtensorMap mah, mal, mbh, mbl;
+    if (!make_map(&mah, Ah, K, rows_pad, TC_BM) || !make_map(&mal, Al, K, rows_pad, TC_BM) ||
+        !make_map(&mbh, Bh, K, n_pad, BN) || !make_map(&mbl, Bl, K, n_pad, BN))
+        return cudaErrorInvalidValue;
+    constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * BN * TC_BK * 2;
+    const size_t smem = (size_t)STAGES * STAGE_BYTES + 256 + 1024;
+    auto kern = tc_topk_kernel<BN, STAGES>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, m_dev, (unsigned)(n_pad / BN), n, r1,
+                                         r2, c1, c2, k, part_d, part_i, err);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+int tc_topk_variants() { return 2; }
+
+cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
+                           const void *Bh, const void *Bl, size_t n_pad, int K, const int *m_dev,
+                           size_t n, const float *r1, const float *r2, const float *c1,
+                           const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
+                           cudaStream_t st) {
+    if (k < 1 || k > kTopKMax) return cudaErrorInvalidValue;
+    if (variant == 1)
+        return topk_variant<128, 3>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, m_dev, n, r1, r2, c1, c2, k,
+                                    part_d, part_i, err, grid, st);
+    return topk_variant<256, 2>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, m_dev, n, r1, r2, c1, c2, k,
+                                part_d, part_i, err, grid, st);
+}
+
+cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
+                              const int *part_i, int k, size_t max_rows, float *out_d,
+                              long long *out_i, cudaStream_t st) {
+    const int wpb = 8;
+    const unsigned blocks = (unsigned)((max_rows + wpb - 1) / wpb);
+    topk_merge_kernel<<<blocks ? blocks : 1, 32 * wpb, 0, st>>>(m_dev, grid_ctas, grid_ctas, part_d,
+                                                                part_i, k, out_d, out_i);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const void *Bl, int K,
                            size_t m, size_t m_pad, size_t n, size_t n_pad, const float *r1,

@@ -21,7 +21,7 @@ import numpy as np
 from . import _capi
 from ._capi import TQError, check, lib
 
-__all__ = ["TurboQuantSpace", "TQError"]
+__all__ = ["TurboQuantSpace", "TQError", "Index", "Server", "BusyError"]
 __version__ = "0.1.0"
 
 
@@ -375,7 +375,14 @@ class TurboQuantSpace:
         check(lib().tq_distance_m_to_n_symmetric(self._h, _ptr(a), m, _ptr(b), n, _ptr(out), prec))
         return out
 
+    def index(self, codes):
+        """A device-resident search index over `codes` (see turboquant.serving)."""
+        return Index(self, codes)
+
     def __repr__(self):
         return (f"TurboQuantSpace(dim={self.dim()}, bits_per_coord={self.bits_per_coord()}, "
                 f"padded_dim={self.padded_dim()}, code_size_bytes={self.code_size_bytes()}, "
                 f"device={self.device()})")
+
+
+from .serving import BusyError, Index, Server  # noqa: E402

@@ -30,8 +30,19 @@ EXPORTS = (
     "tq_distance_m_to_n_symmetric", "tq_encode_batch_device", "tq_prepare_queries_device",
     "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device",
     "tq_distance_1_to_n_device_noalloc", "tq_distance_m_to_n_device",
-    "tq_distance_m_to_n_symmetric_device",
+    "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
+    "tq_server_create", "tq_server_submit", "tq_request_wait", "tq_request_done",
+    "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning",
+    "tq_server_destroy",
 )
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64), ("rejected", C.c_uint64), ("completed", C.c_uint64),
+        ("batches", C.c_uint64), ("rows", C.c_uint64), ("queued_rows", C.c_size_t),
+        ("slots", C.c_int), ("max_rows", C.c_int),
+    ]
 
 
 class SpaceInfo(C.Structure):
@@ -100,6 +111,28 @@ def lib() -> C.CDLL:
     L.tq_distance_m_to_n_device.argtypes = [vp, fp, sz, u8p, sz, fp, C.c_int, vp]
     L.tq_distance_m_to_n_symmetric_device.restype = st
     L.tq_distance_m_to_n_symmetric_device.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int, vp]
+    L.tq_index_create.restype = st
+    L.tq_index_create.argtypes = [vp, u8p, sz, C.c_int, C.POINTER(vp)]
+    L.tq_index_destroy.restype = None
+    L.tq_index_destroy.argtypes = [vp]
+    L.tq_server_create.restype = st
+    L.tq_server_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, sz, C.POINTER(vp)]
+    L.tq_server_submit.restype = st
+    L.tq_server_submit.argtypes = [vp, fp, sz, C.POINTER(vp)]
+    L.tq_request_wait.restype = st
+    L.tq_request_wait.argtypes = [vp, C.c_int, fp, vp, C.POINTER(C.c_double)]
+    L.tq_request_done.restype = C.c_int
+    L.tq_request_done.argtypes = [vp]
+    L.tq_request_release.restype = None
+    L.tq_request_release.argtypes = [vp]
+    L.tq_server_get_stats.restype = st
+    L.tq_server_get_stats.argtypes = [vp, C.POINTER(ServerStats), fp, sz, C.POINTER(C.c_size_t)]
+    L.tq_server_reset_stats.restype = st
+    L.tq_server_reset_stats.argtypes = [vp]
+    L.tq_server_tuning.restype = st
+    L.tq_server_tuning.argtypes = [vp, vp, vp, vp, C.c_int, C.POINTER(C.c_int)]
+    L.tq_server_destroy.restype = None
+    L.tq_server_destroy.argtypes = [vp]
     _LIB = L
     return L
 
