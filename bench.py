@@ -107,6 +107,26 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def shard_seed(base, rank):
+    """Seed of this rank's shard: each rank draws and scans its own codes."""
+    return base + 7919 * rank
+
+
+def max_over_ranks(value, dist, device=None):
+    """The slowest rank's figure (timing is the max over ranks)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(codes_per_rank, queries, world, ms):
+    """Whole-job distance Gcodes/s: every rank scored `queries` x its codes in `ms`."""
+    return world * queries * codes_per_rank / (ms * 1e-3) / 1e9
+
+
 def cpu_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -465,7 +485,7 @@ def main():
 
     # ---- corpus: N(0,1) rows, L2-normalised, on this GPU (untimed) ----------
     gen = torch.Generator(device=dev)
-    gen.manual_seed(2 + 7919 * rank)
+    gen.manual_seed(shard_seed(2, rank))
     X = torch.empty((n, DIM), dtype=torch.float32, device=dev)
     with torch.cuda.stream(stream):
         step_rows = 1 << 20
@@ -506,7 +526,7 @@ def main():
     torch.cuda.empty_cache()
 
     # ---- queries and outputs --------------------------------------------------
-    Qh = l2n(np.random.default_rng(3 + 7919 * rank).standard_normal((QUERIES, DIM)).astype(np.float32))
+    Qh = l2n(np.random.default_rng(shard_seed(3, rank)).standard_normal((QUERIES, DIM)).astype(np.float32))
     Qd = torch.from_numpy(Qh).to(dev)
     out = torch.empty((QUERIES, n), dtype=torch.float32, device=dev)
     qptr = [C.c_void_p(Qd[i].data_ptr()) for i in range(QUERIES)]
@@ -549,12 +569,8 @@ def main():
         ev1.record(stream)
         stream.synchronize()
     barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * QUERIES * n / (ms * 1e-3) / 1e9
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
+    value = job_throughput(n, QUERIES, world, ms)
 
     # ---- the scan kernel alone: per-launch duration (prepared queries) --------
     qrot = torch.empty((QUERIES, D), dtype=torch.float32, device=dev)
@@ -588,12 +604,8 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             space.distance_m_to_n(qn, cn, out=on)
-        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-        if dist is not None:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": round(world * QUERIES * n / e2e_s / 1e9, 4), "unit": "Gcodes/s",
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, dist, dev)
+        e2e = {"value": round(job_throughput(n, QUERIES, world, e2e_s * 1e3), 4), "unit": "Gcodes/s",
                "h2d_bytes_per_step": int(n * cs + QUERIES * DIM * 4),
                "d2h_bytes_per_step": int(QUERIES * n * 4),
                "ms_per_step": round(e2e_s * 1e3, 2),
