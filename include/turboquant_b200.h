@@ -181,6 +181,12 @@ tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t 
                                               float *out, tq_precision precision,
                                               void *stream);
 
+/* Self-test of the device-side failure path: a kernel waits, with a limit of
+ * about budget_ms, on a barrier that nothing signals.  Returns TQ_ERR_TIMEOUT
+ * when the wait gave up and reported it (the expected outcome; the context
+ * stays usable), TQ_OK if it did not. */
+tq_status tq_selftest_bounded_wait(int device, int budget_ms);
+
 /* ---- serving: device-resident index + continuous-batching top-k server ---
  * The reference has no index or serving loop (README.md:81-83); these entry
  * points serve exact top-k asymmetric search (distSearch, space_turbo_quant.h

@@ -312,3 +312,14 @@ def test_split_bf16_error_vs_fp64(cuda_ok):
     print(f"vs FP64 over 10k pairs: split-BF16 max {e_tc.max():.2e} mean {e_tc.mean():.2e}; "
           f"FP32 max {e_32.max():.2e} mean {e_32.mean():.2e}")
     assert e_tc.max() < 1e-5 and e_32.max() < 1e-5
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(cuda_ok):
+    """A device-side wait on a barrier nothing signals gives up after its limit
+    and reports TQ_ERR_TIMEOUT; the next launch on the same context works."""
+    from turboquant import _capi
+    st = _capi.lib().tq_selftest_bounded_wait(0, 200)
+    assert st == _capi.TQ_ERR_TIMEOUT, _capi.lib().tq_last_error()
+    g = load_case(128, 4)
+    s = tq.TurboQuantSpace(128, 4)
+    np.testing.assert_array_equal(s.encode_batch(g["X"]), g["codes"])

@@ -52,4 +52,9 @@ cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part
                               const int *part_i, int k, size_t max_rows, float *out_d,
                               long long *out_i, cudaStream_t st);
 
+// One thread waits on an mbarrier nothing arrives at; after budget_cycles the
+// wait gives up and writes a non-zero code to *err (the failure path of every
+// bounded wait in the tensor-core kernels).
+cudaError_t launch_bounded_wait_selftest(int *err, long long budget_cycles, cudaStream_t st);
+
 }  // namespace tq

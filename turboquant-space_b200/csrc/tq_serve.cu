@@ -598,6 +598,31 @@ tq_status tq_server_tuning(tq_server *sv, int *bucket_rows, int *variant, float 
     return TQ_OK;
 }
 
+tq_status tq_selftest_bounded_wait(int device, int budget_ms) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(TQ_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0) cudaGetDevice(&device);
+    if (budget_ms < 1 || budget_ms > 10000) return fail(TQ_ERR_INVALID_ARGUMENT, "budget_ms must be in 1..10000");
+    DeviceGuard g(device);
+    int clock_khz = 0;
+    cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, device);
+    if (clock_khz <= 0) clock_khz = 2000000;
+    int *err = nullptr;
+    TQ_CUDA(cudaMalloc(&err, sizeof(int)), "cudaMalloc");
+    cudaError_t e = cudaMemset(err, 0, sizeof(int));
+    if (e == cudaSuccess) e = tq::launch_bounded_wait_selftest(err, (long long)clock_khz * budget_ms, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(err);
+    if (e != cudaSuccess) return cuda_fail(e, "bounded-wait self-test");
+    if (h != 0) return fail(TQ_ERR_TIMEOUT, "device wait gave up after ~%d ms (code %d)", budget_ms, h);
+    return TQ_OK;
+}
+
 void tq_server_destroy(tq_server *sv) {
     if (!sv) return;
     {

@@ -600,6 +600,26 @@ __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__
     }
 }
 
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing
+// arrives at, with a budget of `budget_cycles`; the wait must give up and
+// record kErrSelfTest in *err instead of hanging.
+constexpr int kErrSelfTest = 9;
+__global__ void bounded_wait_selftest_kernel(int *err, long long budget_cycles) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    const uint32_t b = smem_u32(&bar);
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const long long t0 = clock64();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(b, 0)) return;  // cannot happen: no arrival
+        if ((it & 255u) == 0 && clock64() - t0 > budget_cycles) {
+            atomicCAS(err, 0, kErrSelfTest);
+            return;
+        }
+    }
+}
+
 // ---- host: tensor maps ------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -652,6 +672,11 @@ cudaError_t topk_variant(const void *Ah, const void *Al, size_t rows_pad, const 
 }  // namespace
 
 int tc_topk_variants() { return 2; }
+
+cudaError_t launch_bounded_wait_selftest(int *err, long long budget_cycles, cudaStream_t st) {
+    bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(err, budget_cycles);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
                            const void *Bh, const void *Bl, size_t n_pad, int K, const int *m_dev,
