@@ -308,7 +308,7 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
         P.wht_scale = 1.0f / std::sqrt(static_cast<float>(D));
         P.lutq = 0;
         P.qlut_k = 0;
-        if (P.nb > 15 && tq::build_quant_lut(sp->boundaries, tq::kQlutBuckets, tq::kQlutMaxK, sp->qlut)) {
+        if (tq::build_quant_lut(sp->boundaries, tq::kQlutBuckets, tq::kQlutMaxK, sp->qlut)) {
             P.lutq = 1;
             P.qlut_k = sp->qlut.k;
             P.qlut_s = sp->qlut.s;

@@ -173,6 +173,25 @@ __device__ __forceinline__ int quantize(float z, const Params &P, const float *b
     return idx & 0xFF;  // the reference accumulates into a uint8_t
 }
 
+// quantize with one shared loop: the bucket table narrows the range to
+// [lo, lo + k) (k = 1 for every Lloyd-Max table of b = 2..9), the direct count
+// (no table) to [0, nb).  Kept out of line of the unrolled callers: one loop.
+__device__ __forceinline__ int quantize_compact(float z, const Params &P, const float *bnd,
+                                                const uint8_t *qlut) {
+    int idx = 0, t1 = P.nb;
+    if (P.lutq) {
+        float y = __fmaf_rn(z, P.qlut_s, P.qlut_c);
+        y = fminf(fmaxf(y, 0.0f), (float)(kQlutBuckets - 1));
+        idx = qlut[(int)y];
+        if (P.qlut_k == 1) return (idx + ((z > bnd[idx]) ? 1 : 0)) & 0xFF;
+        t1 = idx + P.qlut_k;
+    }
+    const int t0 = idx;
+#pragma unroll 1
+    for (int t = t0; t < t1; ++t) idx += (z > bnd[t]) ? 1 : 0;
+    return idx & 0xFF;
+}
+
 // Shared table block of the encode / prepare kernels.
 constexpr int kTabCentOff = 0;                                  // float[256]
 constexpr int kTabBndOff = kTabCentOff + 4 * kMaxLevels;        // float[256 + 8]
@@ -358,6 +377,382 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
             for (int i = lane; i < len; i += 32) dst[i] = stage[i];
         }
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// encode2: the same computation for D = 256, 512, 1024 (E = D/32 = 8, 16, 32
+// values per lane) with the FWHT held in registers.
+//   layout A: lane l holds elements l*E + t; stages 0..log2(E)-1 in registers,
+//             stages log2(E)..4 (E < 32) with lane shuffles;
+//   one shared-memory transpose;
+//   layout B: lane l holds elements 32 t + l; stages 5.. in registers.
+// Butterflies of register stride >= 2 use packed FP32x2 add/sub: each half is
+// an independent IEEE add or subtract, so every stage output is still the
+// single rounding of a + b or a - b and the stage order is unchanged.
+// The vector buffer uses a 16-byte-chunk swizzle (chunk column XOR a function
+// of the 128-byte row) that keeps the float4 layout-A accesses, the layout-B
+// accesses and the 8-lane reduction chains free of bank conflicts.
+// ---------------------------------------------------------------------------
+typedef unsigned long long u64;
+
+__device__ __forceinline__ u64 fadd2(u64 a, u64 b) {
+    u64 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 fsub2(u64 a, u64 b) {
+    u64 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 fmul2(u64 a, u64 b) {
+    u64 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 mk2(float lo, float hi) {
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void un2(u64 v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+template <int E>
+struct Swz {
+    __device__ static __forceinline__ int g(int row) {
+        if constexpr (E >= 32) return row & 7;
+        else if constexpr (E == 16) return row & 3;
+        else return row & 1;
+    }
+    // physical float offset of element e
+    __device__ static __forceinline__ int elem(int e) {
+        const int c = e >> 2, row = c >> 3;
+        return ((row << 3) | ((c ^ g(row)) & 7)) << 2 | (e & 3);
+    }
+    // physical float offset of chunk c (4 floats)
+    __device__ static __forceinline__ int chunk(int c) {
+        const int row = c >> 3;
+        return ((row << 3) | ((c ^ g(row)) & 7)) << 2;
+    }
+};
+
+// The reference's sum-of-squares tree (as chain_sq_reduce) on a Swz<E> buffer.
+// FULL: n = D (a multiple of 32), so there are no leftovers.
+template <int E, bool FULL>
+__device__ __forceinline__ float chain_sq_reduce2(const float *buf, int n, int lane) {
+    if constexpr (FULL) n = 32 * E;
+    const int k = lane & 7, kh = k >> 2, kw = k & 3;
+    const int steps = (n & ~7) >> 3;
+    float acc = 0.0f;
+    int m = 0;
+#pragma unroll 1
+    for (; m + 4 <= steps; m += 4) {
+        const int r = m >> 2, gg = Swz<E>::g(r);
+        const float *base = buf + r * 32 + kw;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float x = base[((2 * i + kh) ^ gg) << 2];
+            acc = __fadd_rn(acc, __fmul_rn(x, x));
+        }
+    }
+    if constexpr (!FULL) {
+#pragma unroll 1
+        for (; m < steps; ++m) {
+            const float x = buf[Swz<E>::elem(k + 8 * m)];
+            acc = __fadd_rn(acc, __fmul_rn(x, x));
+        }
+    }
+    const float hi = __shfl_down_sync(kFull, acc, 4, 8);
+    const float t = __fadd_rn(acc, hi);
+    float t0 = __shfl_sync(kFull, t, 0, 8);
+    float t1 = __shfl_sync(kFull, t, 1, 8);
+    float t2 = __shfl_sync(kFull, t, 2, 8);
+    float t3 = __shfl_sync(kFull, t, 3, 8);
+    float s = __fadd_rn(__fadd_rn(t0, t2), __fadd_rn(t1, t3));
+    if constexpr (FULL) return s;
+    int b = n & ~7, r = n - b;
+    if (r >= 4) {
+        const float x0 = buf[Swz<E>::elem(b)], x1 = buf[Swz<E>::elem(b + 1)];
+        const float x2 = buf[Swz<E>::elem(b + 2)], x3 = buf[Swz<E>::elem(b + 3)];
+        t0 = __fmaf_rn(x0, x0, t0);
+        t1 = __fmaf_rn(x1, x1, t1);
+        t2 = __fmaf_rn(x2, x2, t2);
+        t3 = __fmaf_rn(x3, x3, t3);
+        s = __fadd_rn(__fadd_rn(t0, t2), __fadd_rn(t1, t3));
+        b += 4;
+        r -= 4;
+    }
+    for (int j = 0; j < r; ++j) {
+        const float x = buf[Swz<E>::elem(b + j)];
+        s = __fmaf_rn(x, x, s);
+    }
+    return s;
+}
+
+// In-register butterfly stage of register stride 2^SREG over E values held as
+// E/2 pairs (p[i] = values 2i, 2i+1).
+template <int E, int SREG>
+__device__ __forceinline__ void reg_stage(u64 (&p)[E / 2]) {
+    if constexpr (SREG == 0) {
+#pragma unroll
+        for (int i = 0; i < E / 2; ++i) {
+            float a, b;
+            un2(p[i], a, b);
+            p[i] = mk2(__fadd_rn(a, b), __fsub_rn(a, b));
+        }
+    } else {
+        constexpr int PS = 1 << (SREG - 1);
+#pragma unroll
+        for (int i = 0; i < E / 2; ++i) {
+            if (!(i & PS)) {
+                const u64 a = p[i], b = p[i + PS];
+                p[i] = fadd2(a, b);
+                p[i + PS] = fsub2(a, b);
+            }
+        }
+    }
+}
+
+template <int E, int SREG = 0>
+__device__ __forceinline__ void reg_stages(u64 (&p)[E / 2]) {
+    if constexpr ((1 << SREG) < E) {
+        reg_stage<E, SREG>(p);
+        reg_stages<E, SREG + 1>(p);
+    }
+}
+
+// Cross-lane stages of layout A (element bits log2(E)..4 are lane bits).
+template <int E, int LB = 0>
+__device__ __forceinline__ void lane_stages(u64 (&p)[E / 2], int lane) {
+    constexpr int LE = (E >= 32) ? 5 : (E == 16 ? 4 : 3);
+    if constexpr (LE + LB < 5) {
+        const int mask = 1 << LB;
+        const bool high = lane & mask;
+#pragma unroll
+        for (int i = 0; i < E / 2; ++i) {
+            const u64 y = __shfl_xor_sync(kFull, p[i], mask);
+            const u64 x = high ? (p[i] ^ 0x8000000080000000ull) : p[i];
+            p[i] = fadd2(y, x);  // low lane: y + x; high lane: y - x (= low - high)
+        }
+        lane_stages<E, LB + 1>(p, lane);
+    }
+}
+
+// RHT of one vector held in `buf` (Swz<E>): optional pre-multiply, sign flip
+// from `sbits` (bit t: element lane*E + t is +1), FWHT, post-multiply.  The
+// result is left in layout B in `out` (E values: element 32 t + lane).
+template <int E, bool PREMUL>
+__device__ __forceinline__ void rht2(float *buf, int lane, float pre, uint32_t sbits, float post,
+                                     float (&out)[E]) {
+    u64 p[E / 2];
+#pragma unroll
+    for (int k = 0; k < E / 4; ++k) {
+        const float4 x = *reinterpret_cast<const float4 *>(buf + Swz<E>::chunk(lane * (E / 4) + k));
+        p[2 * k] = mk2(x.x, x.y);
+        p[2 * k + 1] = mk2(x.z, x.w);
+    }
+    const u64 pre2 = mk2(pre, pre);
+#pragma unroll
+    for (int i = 0; i < E / 2; ++i) {
+        if constexpr (PREMUL) p[i] = fmul2(p[i], pre2);
+        const u64 flip = ((u64)((~sbits >> (2 * i)) & 1u) << 31) | ((u64)((~sbits >> (2 * i + 1)) & 1u) << 63);
+        p[i] ^= flip;
+    }
+    reg_stages<E>(p);
+    lane_stages<E>(p, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < E / 4; ++k) {
+        float a, b, c, d;
+        un2(p[2 * k], a, b);
+        un2(p[2 * k + 1], c, d);
+        *reinterpret_cast<float4 *>(buf + Swz<E>::chunk(lane * (E / 4) + k)) = make_float4(a, b, c, d);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < E / 2; ++i)
+        p[i] = mk2(buf[Swz<E>::elem(32 * (2 * i) + lane)], buf[Swz<E>::elem(32 * (2 * i + 1) + lane)]);
+    reg_stages<E>(p);
+    const u64 post2 = mk2(post, post);
+#pragma unroll
+    for (int i = 0; i < E / 2; ++i) {
+        p[i] = fmul2(p[i], post2);
+        un2(p[i], out[2 * i], out[2 * i + 1]);
+    }
+    __syncwarp();
+}
+
+// Per-warp shared bytes of encode2: 4 vectors of D+8 floats, the quantizer
+// indices of 4 vectors (D bytes each, one 32-bit word per lane and 4
+// positions), 4 staged codes.
+template <int LOG_D>
+__host__ __device__ constexpr int encode2_warp_bytes_c(int cs) {
+    return 16 * ((1 << LOG_D) + 8) + 4 * (1 << LOG_D) + align16(4 * cs);
+}
+
+template <int LOG_D, bool NIBBLE>
+__global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ X, size_t n,
+                                                      uint8_t *__restrict__ out, Params P,
+                                                      DevTables T) {
+    constexpr int D = 1 << LOG_D;
+    constexpr int E = D / 32;
+    constexpr int VS = D + 8;
+    static_assert(E >= 8 && E <= 32, "encode2 covers D = 256..1024");
+    extern __shared__ __align__(16) unsigned char smem[];
+    load_tables(smem, P, T, true);
+    __syncthreads();
+    const float *s_cent = reinterpret_cast<const float *>(smem + kTabCentOff);
+    const float *s_bnd = reinterpret_cast<const float *>(smem + kTabBndOff);
+    const uint32_t *s_rot = reinterpret_cast<const uint32_t *>(smem + kTabRotOff);
+    const uint32_t *s_qjl = reinterpret_cast<const uint32_t *>(smem + kTabQjlOff);
+    const uint8_t *s_qlut = smem + kTabQlutOff;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int cs = P.cs;
+    unsigned char *wbase = smem + kTabBytes + warp * encode2_warp_bytes_c<LOG_D>(cs);
+    float *buf = reinterpret_cast<float *>(wbase);
+    uint32_t *idxw = reinterpret_cast<uint32_t *>(wbase + 16 * VS);  // [4][E/4][32]
+    uint8_t *stage = wbase + 16 * VS + 4 * D;
+    const int g = lane >> 3;
+    // sign bits of this lane's layout-A elements lane*E .. lane*E + E-1
+    const int bit0 = lane * E;
+    const uint32_t emask = (E >= 32) ? 0xffffffffu : ((1u << E) - 1u);
+    const uint32_t rbits = (s_rot[bit0 >> 5] >> (bit0 & 31)) & emask;
+    const uint32_t qbits = (s_qjl[bit0 >> 5] >> (bit0 & 31)) & emask;
+    const bool vec4 = ((P.dim & 3) == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    const size_t nquads = (n + 3) >> 2;
+
+    // The warps of a block step through the phases together (block barriers
+    // between phase groups), so the block executes one phase's code at a time.
+    for (size_t base = (size_t)blockIdx.x * nwarps; base < nquads; base += (size_t)gridDim.x * nwarps) {
+        const size_t qd = base + warp;
+        const bool active = qd < nquads;
+        const size_t row0 = qd << 2;
+        const int nv = !active ? 0 : ((n - row0 < 4) ? (int)(n - row0) : 4);
+        float norm = 0.0f, inv_norm = 0.0f;
+        // A: rows -> buffers (zero padded); B: norm
+        if (active) {
+            if (vec4) {
+                const int d4 = P.dim >> 2;
+#pragma unroll 4
+                for (int i = lane; i < D; i += 32) {  // i = v * (D/4) + chunk
+                    const int v = i / (D / 4), i4 = i % (D / 4);
+                    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (v < nv && i4 < d4)
+                        x = __ldcs(reinterpret_cast<const float4 *>(X + (row0 + v) * (size_t)P.dim) + i4);
+                    *reinterpret_cast<float4 *>(buf + v * VS + Swz<E>::chunk(i4)) = x;
+                }
+            } else {
+#pragma unroll 1
+                for (int v = 0; v < 4; ++v) {
+                    const float *src = X + (row0 + v) * (size_t)P.dim;
+#pragma unroll 1
+                    for (int i = lane; i < D; i += 32)
+                        buf[v * VS + Swz<E>::elem(i)] = (v < nv && i < P.dim) ? __ldcs(src + i) : 0.0f;
+                }
+            }
+            __syncwarp();
+            const float nsq = chain_sq_reduce2<E, false>(buf + g * VS, P.dim, lane);
+            norm = __fsqrt_rn(nsq);
+            inv_norm = (nsq > f32_bits(kNormSqFloorBits)) ? __fdiv_rn(1.0f, norm) : 0.0f;
+        }
+        __syncthreads();
+        // C: rotated = RHT_rot(raw * inv_norm), written back in layout B; D: sigma
+        float sigma = 0.0f, inv_sigma = 0.0f;
+        if (active) {
+#pragma unroll 1
+            for (int v = 0; v < 4; ++v) {
+                float *b = buf + v * VS;
+                float x[E];
+                rht2<E, true>(b, lane, __shfl_sync(kFull, inv_norm, 8 * v), rbits, P.wht_scale, x);
+#pragma unroll
+                for (int t = 0; t < E; ++t) b[Swz<E>::elem(32 * t + lane)] = x[t];
+            }
+            __syncwarp();
+            const float var = chain_sq_reduce2<E, true>(buf + g * VS, D, lane);
+            sigma = __fsqrt_rn(__fdiv_rn(var, (float)D));
+            if (f32_bits(kSigmaFloorBits) > sigma) {
+                sigma = f32_bits(kSigmaFloorBits);
+                inv_sigma = f32_bits(kInvSigmaFloorBits);
+            } else {
+                inv_sigma = __fdiv_rn(1.0f, sigma);
+            }
+        }
+        __syncthreads();
+        // E: quantize + residual in layout B, four indices per lane-word into
+        // the per-warp index array; F: gamma
+        float gamma = 0.0f;
+        if (active) {
+#pragma unroll 1
+            for (int v = 0; v < 4; ++v) {
+                const float sg = __shfl_sync(kFull, sigma, 8 * v);
+                const float isg = __shfl_sync(kFull, inv_sigma, 8 * v);
+                float *b = buf + v * VS;
+#pragma unroll 2
+                for (int t4 = 0; t4 < E / 4; ++t4) {
+                    uint32_t word = 0u;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int p = Swz<E>::elem(32 * (4 * t4 + q) + lane);
+                        const float x = b[p];
+                        const int idx = quantize_compact(__fmul_rn(x, isg), P, s_bnd, s_qlut);
+                        b[p] = __fmaf_rn(-s_cent[idx], sg, x);
+                        word |= (uint32_t)idx << (8 * q);
+                    }
+                    idxw[(v * (E / 4) + t4) * 32 + lane] = word;
+                }
+            }
+            __syncwarp();
+            gamma = __fsqrt_rn(chain_sq_reduce2<E, true>(buf + g * VS, D, lane));
+        }
+        __syncthreads();
+        // G: RHT_qjl(residual), pack units + trailer; H: staged codes -> global
+        if (active) {
+#pragma unroll 1
+            for (int v = 0; v < nv; ++v) {
+                float x[E];
+                rht2<E, false>(buf + v * VS, lane, 1.0f, qbits, P.wht_scale, x);
+                uint8_t *st = stage + v * cs;
+#pragma unroll
+                for (int t4 = 0; t4 < E / 4; ++t4) {
+                    const uint32_t word = idxw[(v * (E / 4) + t4) * 32 + lane];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int t = 4 * t4 + q;
+                        const uint32_t idx = (word >> (8 * q)) & 0xFFu;
+                        const uint32_t unit = ((idx << 1) | (x[t] >= 0.0f ? 1u : 0u)) & 0xFFu;
+                        const int e = 32 * t + lane;
+                        if constexpr (NIBBLE) {
+                            const uint32_t up = __shfl_down_sync(kFull, unit, 1);
+                            if (!(lane & 1)) st[e >> 1] = (uint8_t)((unit | (up << 4)) & 0xFFu);
+                        } else {
+                            st[e] = (uint8_t)unit;
+                        }
+                    }
+                }
+            }
+            if ((lane & 7) == 0 && g < nv) {
+                uint8_t *t = stage + g * cs + P.pb;
+                const uint32_t w[3] = {__float_as_uint(norm), __float_as_uint(gamma), __float_as_uint(sigma)};
+#pragma unroll
+                for (int q = 0; q < 12; ++q) t[q] = (uint8_t)(w[q >> 2] >> (8 * (q & 3)));
+            }
+            __syncwarp();
+            uint8_t *dst = out + row0 * (size_t)cs;
+            const int len = nv * cs;
+            if (((reinterpret_cast<uintptr_t>(dst) & 15) == 0) && ((len & 15) == 0)) {
+                const uint4 *s4 = reinterpret_cast<const uint4 *>(stage);
+                uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+#pragma unroll 1
+                for (int i = lane; i < (len >> 4); i += 32) __stcs(d4 + i, s4[i]);
+            } else {
+#pragma unroll 1
+                for (int i = lane; i < len; i += 32) dst[i] = stage[i];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -753,6 +1148,169 @@ __global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__
     }
 }
 
+// scan8b: the scan8 arithmetic with the per-code overhead moved out of the
+// step.  A warp owns batches of 16 consecutive codes and runs them as 8 steps
+// of 2 codes; the word registers of the next step are loaded (ping-pong, no
+// copies) before the current step is reduced, and code indices past the end
+// are clamped to the last code, so the loads need no bounds checks.  After
+// each step's transpose reduction the 8-lane group holding a value keeps it in
+// the lane whose (lane & 7) is the step, so after 8 steps lane l holds value
+// kind (l >> 3) & 1 of code 2 (l & 7) + (l >> 4): 16 lanes then finish the 16
+// codes together (trailer loaded at the start of the batch, one store each).
+// Per code this is the same sequence of roundings as scan8.
+// ---------------------------------------------------------------------------
+template <int WPL>
+__global__ void __launch_bounds__(256, 2) scan8b_kernel(const float *__restrict__ q_rot,
+                                                        const float *__restrict__ s_q,
+                                                        const float *__restrict__ norms,
+                                                        const uint8_t *__restrict__ codes, size_t n,
+                                                        float *__restrict__ out, size_t ldo, Params P,
+                                                        DevTables T) {
+    constexpr int D = 128 * WPL;
+    extern __shared__ __align__(16) unsigned char tab[];
+    __shared__ float s_red[8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const size_t row = blockIdx.y;
+    const float *qr_g = q_rot + row * (size_t)D;
+    const float *sq_g = s_q + row * (size_t)D;
+    for (int i = tid; i < 256 * 32; i += blockDim.x)
+        reinterpret_cast<float *>(tab + (i >> 5) * 256)[i & 31] = T.centroids[(i >> 5) >> 1];
+    float mx = 0.0f;
+    for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
+    if (lane == 0) s_red[warp] = mx;
+    __syncthreads();
+    mx = s_red[0];
+    for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
+    const float step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
+    const float inv_step = 1.0f / step;
+    unsigned long long qr2[WPL * 2];
+    int shi[WPL];
+    unsigned slo[WPL];
+    int ssum = 0;
+#pragma unroll
+    for (int j = 0; j < WPL; ++j) {
+        unsigned hi = 0, lo = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int p = 4 * (lane + 32 * j) + b;
+            if (b & 1) qr2[2 * j + (b >> 1)] = pack2(qr_g[p - 1], qr_g[p]);
+            int v = __float2int_rn(sq_g[p] * inv_step);
+            v = max(-32767, min(32767, v));
+            ssum += v;
+            hi |= ((unsigned)(v >> 8) & 0xFFu) << (8 * b);
+            lo |= ((unsigned)v & 0xFFu) << (8 * b);
+        }
+        shi[j] = (int)hi;
+        slo[j] = lo;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ssum += __shfl_xor_sync(kFull, ssum, off);
+    const float qn2 = norms[2 * row], qn = norms[2 * row + 1];
+    const float sc = P.scale;
+    __syncthreads();
+
+    const uint32_t lane4 = (uint32_t)lane * 4u;
+    const size_t cs = (size_t)P.cs;
+    const size_t last = n - 1;
+    const size_t nbatch = (n + 15) >> 4;
+    const size_t bstride = (size_t)gridDim.x * nw;
+    size_t bt = (size_t)blockIdx.x * nw + warp;
+    if (bt >= nbatch) return;
+    const int ecode = 2 * (lane & 7) + (lane >> 4);  // the code this lane finishes
+    const bool eowner = !(lane & 8);
+    float *orow = out + row * ldo;
+
+    auto load = [&](uint32_t (&w)[2][WPL], size_t c0) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const size_t c = (c0 + u < last) ? c0 + u : last;
+            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + c * cs);
+#pragma unroll
+            for (int j = 0; j < WPL; ++j) w[u][j] = __ldg(cw + lane + 32 * j);
+        }
+    };
+    // one step: 2 codes -> the transpose-reduced value of this lane's group
+    auto reduce_step = [&](const uint32_t (&w)[2][WPL]) -> float {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            unsigned long long acc2 = 0ull;
+            int acc_hi = 0;
+            unsigned acc_lo = 0;
+#pragma unroll
+            for (int j = 0; j < WPL; ++j) {
+                const uint32_t x = w[u][j];
+                float cv[4];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const uint32_t a = __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4));
+                    cv[b] = *reinterpret_cast<const float *>(tab + a);
+                }
+                acc2 = ffma2(qr2[2 * j], pack2(cv[0], cv[1]), acc2);
+                acc2 = ffma2(qr2[2 * j + 1], pack2(cv[2], cv[3]), acc2);
+                const uint32_t bits = x & 0x01010101u;
+                acc_hi = __dp4a((int)bits, shi[j], acc_hi);
+                acc_lo = __dp4a(bits, slo[j], acc_lo);
+            }
+            v[2 * u] = sum2(acc2);
+            v[2 * u + 1] = (float)(acc_hi * 256 + (int)acc_lo);
+        }
+        float w2[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const bool hi = lane & 16;
+            const float send = hi ? v[k] : v[k + 2];
+            const float keep = hi ? v[k + 2] : v[k];
+            w2[k] = keep + __shfl_xor_sync(kFull, send, 16);
+        }
+        float y;
+        {
+            const bool hi = lane & 8;
+            const float send = hi ? w2[0] : w2[1];
+            const float keep = hi ? w2[1] : w2[0];
+            y = keep + __shfl_xor_sync(kFull, send, 8);
+        }
+        y += __shfl_xor_sync(kFull, y, 4);
+        y += __shfl_xor_sync(kFull, y, 2);
+        y += __shfl_xor_sync(kFull, y, 1);
+        return y;
+    };
+
+    uint32_t wa[2][WPL], wb[2][WPL];
+    load(wa, bt << 4);
+    for (;;) {
+        const size_t cbase = bt << 4;
+        const size_t next_bt = bt + bstride;
+        // trailer of the code this lane finishes (used after the 8 steps)
+        const size_t ce = cbase + (size_t)ecode;
+        const float *tm = reinterpret_cast<const float *>(codes + (ce < last ? ce : last) * cs + D);
+        const float t0 = __ldg(tm), t1 = __ldg(tm + 1), t2 = __ldg(tm + 2);
+        float R = 0.0f;
+#pragma unroll 1
+        for (int s = 0; s < 8; s += 2) {
+            load(wb, cbase + 2 * s + 2);
+            const float ya = reduce_step(wa);
+            R = ((lane & 7) == s) ? ya : R;
+            load(wa, (s + 2 < 8) ? cbase + 2 * s + 4 : (next_bt << 4));
+            const float yb = reduce_step(wb);
+            R = ((lane & 7) == s + 1) ? yb : R;
+        }
+        const float sb = __shfl_down_sync(kFull, R, 8);
+        if (eowner && ce < n) {
+            const float dot = __fmul_rn(step, 2.0f * sb - (float)ssum);
+            const float ip_mse = __fmul_rn(R, t2);
+            const float corr = __fmul_rn(__fmul_rn(sc, t1), dot);
+            const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), t0), qn);
+            const float d = __fsub_rn(__fadd_rn(qn2, __fmul_rn(t0, t0)), __fmul_rn(2.0f, ipt));
+            orow[ce] = d > 0.0f ? d : 0.0f;
+        }
+        bt = next_bt;
+        if (bt >= nbatch) break;
+    }
+}
+
 // Codes whose packed part is narrower than one 32-bit word (D = 4 with
 // nibble packing: 2 bytes) are scanned one thread per code with byte loads.
 template <bool SYM>
@@ -847,10 +1405,37 @@ int sm_count() {
 
 constexpr int kSmemBudget = 227 * 1024;
 
+template <int LOG_D, bool NIBBLE>
+cudaError_t encode2_launch(const Params &P, const DevTables &T, const float *X, size_t n,
+                           uint8_t *out, cudaStream_t st) {
+    const int per_warp = encode2_warp_bytes_c<LOG_D>(P.cs);
+    int warps = (kSmemBudget - kTabBytes) / per_warp;
+    if (warps > 4) warps = 4;
+    if (warps < 1) return cudaErrorInvalidConfiguration;
+    const size_t smem = (size_t)kTabBytes + (size_t)warps * per_warp;
+    cudaError_t e = cudaFuncSetAttribute(encode2_kernel<LOG_D, NIBBLE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode2_kernel<LOG_D, NIBBLE>, 32 * warps, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const size_t quads = (n + 3) / 4;
+    size_t blocks = (quads + warps - 1) / warps;
+    const size_t cap = (size_t)sm_count() * per_sm;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    encode2_kernel<LOG_D, NIBBLE><<<(unsigned)blocks, 32 * warps, smem, st>>>(X, n, out, P, T);
+    return cudaGetLastError();
+}
+
 template <int LOG_D>
 struct EncodeRun {
     static cudaError_t run(const Params &P, const DevTables &T, const float *X, size_t n,
                            uint8_t *out, cudaStream_t st) {
+        if constexpr (LOG_D >= 8 && LOG_D <= 10)
+            return P.nibble ? encode2_launch<LOG_D, true>(P, T, X, n, out, st)
+                            : encode2_launch<LOG_D, false>(P, T, X, n, out, st);
         const int D = 1 << LOG_D;
         const int per_warp = encode_warp_bytes(D, P.cs);
         int warps = (kSmemBudget - kTabBytes) / per_warp;
@@ -955,7 +1540,7 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
         return cudaErrorNotSupported;
     } else {
         constexpr int WPL = (1 << LOG_D) / 128;
-        auto kern = scan8_kernel<WPL, 2>;
+        auto kern = scan8b_kernel<WPL>;
         const int threads = 256;
         const size_t smem = 256 * 256;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -964,8 +1549,8 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
-        const size_t steps = (n + 1) / 2;
-        size_t bx = (steps + (threads / 32) - 1) / (threads / 32);
+        const size_t batches = (n + 15) / 16;
+        size_t bx = (batches + (threads / 32) - 1) / (threads / 32);
         size_t cap = (size_t)sm_count() * per_sm;
         if (m > 1) cap = (cap + m - 1) / m;
         if (cap < 1) cap = 1;

@@ -100,7 +100,8 @@ bool build_quant_lut(const std::vector<float> &boundaries, int buckets, int max_
     for (int i = 1; i < nb; ++i)
         if (!(boundaries[i - 1] < boundaries[i])) return false;
     const float lo = boundaries.front(), hi = boundaries.back();
-    const float width = (hi - lo) / static_cast<float>(buckets);
+    // one boundary (bits = 2): any positive width gives lo = 0 and k = 1
+    const float width = (hi > lo) ? (hi - lo) / static_cast<float>(buckets) : 1.0f;
     const float r0 = lo - width, r1 = hi + width;
     lut.s = static_cast<float>(buckets) / (r1 - r0);
     lut.c = -r0 * lut.s;
