@@ -36,6 +36,10 @@ sys.path.insert(0, os.path.join(ROOT, "turboquant-space_b200", "python"))
 
 METRIC = "distance Gcodes/s vs plain FP32 kernel at ≤1e-5 rel err; serving p99 ms at QPS"
 DIM, BITS, QUERIES = 768, 8, 64
+# DRAM bytes (read + write) per code of one scan launch, from the ncu capture of
+# a 1M-code launch of the 768-d 8-bit corpus: 1.036052 GB read + 6.99 MB
+# written.  Traffic grows with the code count, so the bench scales it per code.
+SCAN_TRAFFIC_PER_CODE = (1.036052e9 + 6.991e6) / 1e6
 
 
 def peaks():
@@ -636,7 +640,11 @@ def main():
                        "parallelism": f"{world} independent shards" if world > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
-                         "traffic": None, "kernel": "scan_kernel<10,false,false>",
+                         "traffic": int(round(SCAN_TRAFFIC_PER_CODE * n)),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                           "1M-code launch, scaled per code "
+                                           "(profiles/scan8t_kernel_1M_768d_b8.md)",
+                         "kernel": "scan8t_kernel<8,16,2,true> (1->N, 16 warps x 2-stage rings)",
                          "bytes_per_launch": scan_bytes, "ms_per_launch": round(scan_ms, 4),
                          "peak_kind": peak_kind},
             "encode": {"ms": round(enc_ms, 3), "Mvec_per_s": round(n / enc_ms / 1e3, 2),

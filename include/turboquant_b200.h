@@ -181,6 +181,16 @@ tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t 
                                               float *out, tq_precision precision,
                                               void *stream);
 
+/* The device status word of the space's stream-ordered kernels.  Every wait in
+ * the staged 1->N scan is bounded; a wait that gives up (a copy that never
+ * completes) writes a non-zero code here and the kernel returns without
+ * finishing its codes.  Synchronise the streams the space's *_device calls ran
+ * on, then call this: it reports the code in *code (0 = none), clears it, and
+ * returns TQ_ERR_TIMEOUT when it was set.  The host-pointer entry points check
+ * it themselves.  No counterpart in the reference (CPU code never waits on a
+ * device). */
+tq_status tq_space_take_device_status(const tq_space *sp, int *code);
+
 /* Self-test of the device-side failure path: a kernel waits, with a limit of
  * about budget_ms, on a barrier that nothing signals.  Returns TQ_ERR_TIMEOUT
  * when the wait gave up and reported it (the expected outcome; the context

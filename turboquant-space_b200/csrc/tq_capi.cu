@@ -84,6 +84,17 @@ tq_status check_dev(const void *p, size_t bytes, const char *name) {
     return TQ_OK;
 }
 
+// Reads and clears the space's device status word (after the caller's
+// synchronisation); TQ_ERR_TIMEOUT when a bounded device wait gave up.
+tq_status take_status(const tq_space *sp, int *code_out) {
+    int code = 0;
+    TQ_CUDA(cudaMemcpy(&code, sp->T.status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+    if (code_out) *code_out = code;
+    if (code == 0) return TQ_OK;
+    TQ_CUDA(cudaMemset(sp->T.status, 0, sizeof(int)), "clear status");
+    return fail(TQ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", code);
+}
+
 tq_status check_codes_align(const void *p, const char *name) {
     if (reinterpret_cast<uintptr_t>(p) & 3)
         return fail(TQ_ERR_INVALID_ARGUMENT, "%s: device codes must be 4-byte aligned", name);
@@ -340,7 +351,8 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
             const size_t mw = (D + 31) / 32;
             const size_t off_c = 0, off_b = 4 * 256, off_q = off_b + 4 * (256 + tq::kQlutMaxK + 4);
             const size_t off_r = off_q + tq::kQlutBuckets, off_j = off_r + 4 * mw;
-            const size_t total = off_j + 4 * mw;
+            const size_t off_s = (off_j + 4 * mw + 15) & ~size_t(15);
+            const size_t total = off_s + 16;
             std::vector<unsigned char> host(total, 0);
             std::memcpy(host.data() + off_c, sp->centroids.data(), 4 * sp->levels);
             std::vector<float> bnd(256 + tq::kQlutMaxK + 4, INFINITY);
@@ -371,6 +383,7 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
             sp->T.qlut = base + off_q;
             sp->T.rot_mask = reinterpret_cast<const uint32_t *>(base + off_r);
             sp->T.qjl_mask = reinterpret_cast<const uint32_t *>(base + off_j);
+            sp->T.status = reinterpret_cast<int *>(base + off_s);
             sp->device = dev;
             // keep freed scratch in the pool between calls
             cudaMemPool_t pool;
@@ -494,6 +507,14 @@ tq_status tq_distance_1_to_n_device(const tq_space *sp, const float *query,
     TQ_CUDA(tq::launch_prepare(sp->P, sp->T, query, 1, q_rot, s_q, norms, s), "prepare kernel");
     TQ_CUDA(tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out, s), "scan kernel");
     return TQ_OK;
+}
+
+tq_status tq_space_take_device_status(const tq_space *sp, int *code) {
+    if (code) *code = 0;
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    DeviceGuard g(sp->device);
+    return take_status(sp, code);
 }
 
 tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_rot,
@@ -714,6 +735,7 @@ tq_status tq_distance_1_to_n(const tq_space *csp, const float *query, const uint
         if (e != cudaSuccess && result == TQ_OK) result = cuda_fail(e, "distance_1_to_n");
     }
     cudaEventDestroy(ready);
+    if (result == TQ_OK) result = take_status(sp, nullptr);
     return result;
 }
 

@@ -50,6 +50,7 @@ struct DevTables {
     const uint8_t *qlut;      // [kQlutBuckets]: boundaries below the bucket
     const uint32_t *rot_mask; // [D/32 rounded up]: bit i set <=> rot sign +1
     const uint32_t *qjl_mask; // [D/32 rounded up]
+    int *status;              // stream-ordered kernels' error word (0 = ok)
 };
 
 // ---- kernel launchers (tq_kernels.cu); all stream-ordered -------------------

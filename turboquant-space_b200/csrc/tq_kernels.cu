@@ -14,6 +14,7 @@
 // fixes is written with an explicit round-to-nearest intrinsic (__fadd_rn,
 // __fmul_rn, __fmaf_rn, __fdiv_rn, __fsqrt_rn) so that nvcc cannot contract
 // or reassociate it.
+#include "tq_async.cuh"
 #include "tq_internal.h"
 
 #include <cstdint>
@@ -1311,6 +1312,304 @@ __global__ void __launch_bounds__(256, 2) scan8b_kernel(const float *__restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// scan8t: the 1->N byte-unit scan (scan8's arithmetic) fed from shared memory.
+// The corpus is read as groups of 4 consecutive codes: 4 cs bytes, a multiple
+// of 16, so a group is one untiled bulk copy.  Warp w of the grid owns groups
+// w, w + TW, w + 2 TW, ... (TW = warps in the grid) and streams them with
+// cp.async.bulk into a private ring of S stages, one mbarrier per stage; lane
+// 0 refills a stage as soon as the warp has read it.  The bytes in flight per
+// SM are therefore set by the rings (NW x (S - 1) groups), not by registers.
+// Lane l reads word l + 32 j of every code from shared memory: consecutive
+// words, so the reads are conflict-free at any code offset.
+// Each stage gives 8 values (centroid dot and sign sum of 4 codes) that one
+// transpose reduction leaves in the lane groups of 4; across a batch of 4
+// stages lane l keeps the value of stage l & 3, and the 16 lanes with bit 2
+// clear then finish the batch's 16 codes (trailer, distance, store).
+// The last n mod 4 codes are read with plain loads by the warp that would own
+// group n / 4.  The caller guarantees a 16-byte aligned corpus.
+// ---------------------------------------------------------------------------
+constexpr int kErrScanWait = 5;  // status code: a scan stage never arrived
+
+template <int WPL>
+struct Scan8Query {
+    unsigned long long qr2[2 * WPL];  // q_rot of positions 4 (lane + 32 j) + {0,1}, {2,3}
+    int shi[WPL];                     // s_q fixed point, signed high bytes
+    unsigned slo[WPL];                // s_q fixed point, unsigned low bytes
+};
+
+// Per-query set-up shared by the byte-unit scans: the lane-replicated centroid
+// table (256 rows of 256 bytes, entry of lane l at row * 256 + 4 l), the
+// fixed-point step of s_q (max |s_q| / 32767), this lane's query registers and
+// the sum of all fixed-point s_q.  Ends with a block barrier.
+template <int WPL>
+__device__ __forceinline__ void scan8_setup(const float *__restrict__ qr_g,
+                                            const float *__restrict__ sq_g, unsigned char *tab,
+                                            const DevTables &T, float *s_red, Scan8Query<WPL> &Q,
+                                            int &ssum, float &step) {
+    constexpr int D = 128 * WPL;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int i = tid; i < 256 * 32; i += blockDim.x)
+        reinterpret_cast<float *>(tab + (i >> 5) * 256)[i & 31] = T.centroids[(i >> 5) >> 1];
+    float mx = 0.0f;
+    for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
+    if (lane == 0) s_red[warp] = mx;
+    __syncthreads();
+    mx = s_red[0];
+    for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
+    step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
+    const float inv_step = 1.0f / step;
+    int sum = 0;
+#pragma unroll
+    for (int j = 0; j < WPL; ++j) {
+        unsigned hi = 0, lo = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int p = 4 * (lane + 32 * j) + b;
+            if (b & 1) Q.qr2[2 * j + (b >> 1)] = pack2(qr_g[p - 1], qr_g[p]);
+            int v = __float2int_rn(sq_g[p] * inv_step);
+            v = max(-32767, min(32767, v));
+            sum += v;
+            hi |= ((unsigned)(v >> 8) & 0xFFu) << (8 * b);
+            lo |= ((unsigned)v & 0xFFu) << (8 * b);
+        }
+        Q.shi[j] = (int)hi;
+        Q.slo[j] = lo;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+    ssum = sum;
+    __syncthreads();
+}
+
+// This lane's share of one code: the centroid dot over its 4 WPL positions and
+// the fixed-point sign sum (exact integer, |.| < 2^21).
+template <int WPL, bool PACK>
+__device__ __forceinline__ void scan8_terms(const uint32_t (&w)[WPL], const Scan8Query<WPL> &Q,
+                                            const unsigned char *tab, uint32_t lane4, float &ip,
+                                            float &sg) {
+    int acc_hi = 0;
+    unsigned acc_lo = 0;
+    if constexpr (PACK) {
+        unsigned long long acc2 = 0ull;
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) {
+            const uint32_t x = w[j];
+            float cv[4];
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                cv[b] = *reinterpret_cast<const float *>(
+                    tab + __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4)));
+            acc2 = ffma2(Q.qr2[2 * j], pack2(cv[0], cv[1]), acc2);
+            acc2 = ffma2(Q.qr2[2 * j + 1], pack2(cv[2], cv[3]), acc2);
+            const uint32_t bits = x & 0x01010101u;
+            acc_hi = __dp4a((int)bits, Q.shi[j], acc_hi);
+            acc_lo = __dp4a(bits, Q.slo[j], acc_lo);
+        }
+        ip = sum2(acc2);
+    } else {
+        float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) {
+            const uint32_t x = w[j];
+            float q[4];
+            asm("mov.b64 {%0, %1}, %2;" : "=f"(q[0]), "=f"(q[1]) : "l"(Q.qr2[2 * j]));
+            asm("mov.b64 {%0, %1}, %2;" : "=f"(q[2]), "=f"(q[3]) : "l"(Q.qr2[2 * j + 1]));
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const float c = *reinterpret_cast<const float *>(
+                    tab + __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4)));
+                if (b & 1) a1 = __fmaf_rn(q[b], c, a1);
+                else a0 = __fmaf_rn(q[b], c, a0);
+            }
+            const uint32_t bits = x & 0x01010101u;
+            acc_hi = __dp4a((int)bits, Q.shi[j], acc_hi);
+            acc_lo = __dp4a(bits, Q.slo[j], acc_lo);
+        }
+        ip = a0 + a1;
+    }
+    sg = (float)(acc_hi * 256 + (int)acc_lo);
+}
+
+// Transpose reduction of 8 values over the warp (9 shuffles).  On return every
+// lane holds the warp sum of value 4 b4 + 2 b3 + b2 (b_i = bit i of the lane).
+__device__ __forceinline__ float transpose8(const float (&v)[8], int lane) {
+    float a[4];
+    const bool h16 = lane & 16;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float send = h16 ? v[k] : v[k + 4];
+        const float keep = h16 ? v[k + 4] : v[k];
+        a[k] = keep + __shfl_xor_sync(kFull, send, 16);
+    }
+    float b[2];
+    const bool h8 = lane & 8;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float send = h8 ? a[k] : a[k + 2];
+        const float keep = h8 ? a[k + 2] : a[k];
+        b[k] = keep + __shfl_xor_sync(kFull, send, 8);
+    }
+    const bool h4 = lane & 4;
+    float y = (h4 ? b[1] : b[0]) + __shfl_xor_sync(kFull, h4 ? b[0] : b[1], 4);
+    y += __shfl_xor_sync(kFull, y, 2);
+    y += __shfl_xor_sync(kFull, y, 1);
+    return y;
+}
+
+// The reference's distance epilogue (distSearch*, space_turbo_quant.h:683-685)
+// from the reduced centroid dot `ipr`, the fixed-point sign sum `sb` and the
+// code's trailer (norm t0, gamma t1, sigma t2).
+__device__ __forceinline__ float scan8_distance(float ipr, float sb, float t0, float t1, float t2,
+                                                float step, int ssum, float sc, float qn2,
+                                                float qn) {
+    const float dot = __fmul_rn(step, 2.0f * sb - (float)ssum);
+    const float ip_mse = __fmul_rn(ipr, t2);
+    const float corr = __fmul_rn(__fmul_rn(sc, t1), dot);
+    const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), t0), qn);
+    const float d = __fsub_rn(__fadd_rn(qn2, __fmul_rn(t0, t0)), __fmul_rn(2.0f, ipt));
+    return d > 0.0f ? d : 0.0f;
+}
+
+template <int WPL, int NW, int S>
+constexpr int scan8t_smem_bytes() {
+    return 65536 + NW * S * (4 * (128 * WPL + 12) + 8);
+}
+
+template <int WPL, int NW, int S, bool PACK>
+__global__ void __launch_bounds__(NW * 32, 1) scan8t_kernel(const float *__restrict__ q_rot,
+                                                            const float *__restrict__ s_q,
+                                                            const float *__restrict__ norms,
+                                                            const uint8_t *__restrict__ codes,
+                                                            size_t n, float *__restrict__ out,
+                                                            Params P, DevTables T) {
+    constexpr int D = 128 * WPL;
+    static_assert(S >= 2, "the ring needs two stages");
+    constexpr uint32_t GB = 4u * (D + 12);  // bytes per group of 4 codes
+    constexpr int CW = (D + 12) / 4;        // words per code
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ float s_red[NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *tab = smem;
+    unsigned char *ring = smem + 65536 + (size_t)warp * S * GB;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 65536 + (size_t)NW * S * GB) + warp * S;
+    int *err = T.status;
+
+    const size_t G = n >> 2;
+    const size_t TW = (size_t)gridDim.x * NW;
+    const size_t gw = (size_t)blockIdx.x * NW + warp;
+    const size_t K = gw < G ? (G - gw + TW - 1) / TW : 0;  // groups of this warp
+    // ring set-up and the first S copies, before the table build
+    if (lane == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(smem_u32(bars + s), 1);
+        mbar_init_fence();
+        for (int s = 0; s < S && (size_t)s < K; ++s) {
+            const uint32_t bar = smem_u32(bars + s);
+            mbar_expect_tx(bar, GB);
+            bulk_load(smem_u32(ring + s * GB), codes + (gw + (size_t)s * TW) * GB, GB, bar);
+        }
+    }
+    Scan8Query<WPL> Q;
+    int ssum;
+    float step;
+    scan8_setup<WPL>(q_rot, s_q, tab, T, s_red, Q, ssum, step);
+    const float qn2 = norms[0], qn = norms[1], sc = P.scale;
+    const uint32_t lane4 = (uint32_t)lane * 4u;
+    const bool kind0 = !(lane & 4);                               // holds a centroid dot
+    const int ec = 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1);      // code of the group
+
+    const size_t src_step = TW * GB;
+    const uint8_t *src_next = codes + (gw + (size_t)S * TW) * GB;  // next group to fetch
+    int s = 0;
+    uint32_t ph = 0;
+    size_t k = 0;
+    bool ok = true;
+    for (size_t k0 = 0; k0 < K; k0 += 4) {
+        const size_t ke = k0 + (lane & 3);
+        const bool ev = kind0 && ke < K;
+        const size_t ce = 4 * (gw + ke * TW) + ec;
+        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
+        if (ev) {
+            const float *tm = reinterpret_cast<const float *>(codes + ce * (D + 12) + D);
+            t0 = __ldg(tm);
+            t1 = __ldg(tm + 1);
+            t2 = __ldg(tm + 2);
+        }
+        float R = 0.0f;
+        const int nst = (K - k0 < 4) ? (int)(K - k0) : 4;
+#pragma unroll 1
+        for (int i = 0; i < nst; ++i, ++k) {
+            const uint32_t bar = smem_u32(bars + s);
+            ok = __all_sync(kFull, mbar_wait(bar, ph, err, kErrScanWait));
+            if (!ok) break;
+            const uint32_t *sw = reinterpret_cast<const uint32_t *>(ring + s * GB);
+            uint32_t w[4][WPL];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int j = 0; j < WPL; ++j) w[c][j] = sw[c * CW + lane + 32 * j];
+            float v[8];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                scan8_terms<WPL, PACK>(w[c], Q, tab, lane4, v[2 * c], v[2 * c + 1]);
+            const float y = transpose8(v, lane);
+            R = ((lane & 3) == i) ? y : R;
+            __syncwarp();
+            if (lane == 0 && k + S < K) {
+                fence_proxy_async_smem();
+                mbar_expect_tx(bar, GB);
+                bulk_load(smem_u32(ring + s * GB), src_next, GB, bar);
+                src_next += src_step;
+            }
+            if (++s == S) {
+                s = 0;
+                ph ^= 1u;
+            }
+        }
+        if (!ok) break;
+        const float sb = __shfl_down_sync(kFull, R, 4);
+        if (ev) out[ce] = scan8_distance(R, sb, t0, t1, t2, step, ssum, sc, qn2, qn);
+    }
+    if (!ok) {
+        // wait (bounded) for this warp's copies still in flight, then leave
+        if (lane == 0) {
+            for (size_t j = k; j < K && j < k + S; ++j) {
+                mbar_drain(smem_u32(bars + s), ph);
+                if (++s == S) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+        }
+        return;
+    }
+    // the last n mod 4 codes, read straight from global memory
+    const size_t r = n - 4 * G;
+    if (r > 0 && gw == G % TW) {
+        uint32_t w[4][WPL];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const size_t cc = 4 * G + ((size_t)c < r ? (size_t)c : r - 1);
+            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + cc * (D + 12));
+#pragma unroll
+            for (int j = 0; j < WPL; ++j) w[c][j] = __ldg(cw + lane + 32 * j);
+        }
+        float v[8];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) scan8_terms<WPL, PACK>(w[c], Q, tab, lane4, v[2 * c], v[2 * c + 1]);
+        const float y = transpose8(v, lane);
+        const float sb = __shfl_down_sync(kFull, y, 4);
+        if (kind0 && (lane & 3) == 0 && (size_t)ec < r) {
+            const size_t ce = 4 * G + ec;
+            const float *tm = reinterpret_cast<const float *>(codes + ce * (D + 12) + D);
+            out[ce] = scan8_distance(y, sb, __ldg(tm), __ldg(tm + 1), __ldg(tm + 2), step, ssum, sc,
+                                     qn2, qn);
+        }
+    }
+}
+
 // Codes whose packed part is narrower than one 32-bit word (D = 4 with
 // nibble packing: 2 bytes) are scanned one thread per code with byte loads.
 template <bool SYM>
@@ -1532,6 +1831,29 @@ cudaError_t scan_launch(const Params &P, const DevTables &T, const float *q_rot,
     }
 }
 
+// The staged 1->N scan: one CTA per SM (its shared memory is the centroid
+// table plus NW rings), at most as many warps as there are groups of 4 codes.
+// 16 warps (4 per scheduler) with ~8 KB rings measured fastest on B200 at
+// 10M x 1036-byte codes (12 warps x 3 stages: 80%, 16 x 2: 85% of the copy
+// bandwidth; 13 or 14 warps are slower than 12).
+template <int WPL, int NW, int S, bool PACK>
+cudaError_t scan8t_launch(const Params &P, const DevTables &T, const float *q_rot,
+                          const float *s_q, const float *norms, const uint8_t *codes, size_t n,
+                          float *out, cudaStream_t st) {
+    auto kern = scan8t_kernel<WPL, NW, S, PACK>;
+    constexpr int smem = scan8t_smem_bytes<WPL, NW, S>();
+    static_assert(smem <= kSmemBudget - 64, "scan8t rings exceed shared memory");
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const size_t groups = n / 4;
+    size_t blocks = (groups + NW - 1) / NW;
+    const size_t cap = (size_t)sm_count();
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, NW * 32, smem, st>>>(q_rot, s_q, norms, codes, n, out, P, T);
+    return cudaGetLastError();
+}
+
 template <int LOG_D>
 cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot, const float *s_q,
                          const float *norms, size_t m, const uint8_t *codes, size_t n, float *out,
@@ -1540,6 +1862,9 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
         return cudaErrorNotSupported;
     } else {
         constexpr int WPL = (1 << LOG_D) / 128;
+        if (m == 1 && (reinterpret_cast<uintptr_t>(codes) & 15) == 0)
+            return scan8t_launch<WPL, 16, 8400 / (4 * (128 * WPL + 12)), true>(
+                P, T, q_rot, s_q, norms, codes, n, out, st);
         auto kern = scan8b_kernel<WPL>;
         const int threads = 256;
         const size_t smem = 256 * 256;

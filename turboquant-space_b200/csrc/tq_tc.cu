@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "tq_async.cuh"
 #include "tq_mton.h"
 
 namespace tq {
@@ -36,55 +37,8 @@ constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;   // 32 KB
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // 96 KB
 constexpr int TC_TMEM_COLS = 512;
 constexpr int TC_THREADS = 192;
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
-
 // error codes written to *err
 constexpr int kErrFull = 1, kErrEmpty = 2, kErrTmemFull = 3, kErrTmemEmpty = 4;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: true when the phase completed; false after the budget ran out
-// (error recorded) or when another role already recorded an error.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err, int code) {
-    const long long t0 = clock64();
-    for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 1023u) == 0) {
-            if (*reinterpret_cast<volatile int *>(err) != 0) return false;
-            if (clock64() - t0 > kWaitCycles) {
-                atomicCAS(err, 0, code);
-                return false;
-            }
-        }
-    }
-}
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
                                             uint32_t bar) {

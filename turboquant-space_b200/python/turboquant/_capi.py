@@ -33,7 +33,7 @@ EXPORTS = (
     "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
     "tq_server_create", "tq_server_submit", "tq_request_wait", "tq_request_done",
     "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning",
-    "tq_server_destroy", "tq_selftest_bounded_wait",
+    "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status",
 )
 
 
@@ -133,6 +133,8 @@ def lib() -> C.CDLL:
     L.tq_server_tuning.argtypes = [vp, vp, vp, vp, C.c_int, C.POINTER(C.c_int)]
     L.tq_selftest_bounded_wait.restype = st
     L.tq_selftest_bounded_wait.argtypes = [C.c_int, C.c_int]
+    L.tq_space_take_device_status.restype = st
+    L.tq_space_take_device_status.argtypes = [vp, C.POINTER(C.c_int)]
     L.tq_server_destroy.restype = None
     L.tq_server_destroy.argtypes = [vp]
     _LIB = L
