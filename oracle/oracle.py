@@ -77,6 +77,14 @@ def lib():
         L.tqo_distance_f64.argtypes = [C.c_void_p, _fp, _u8p]
         L.tqo_distance_symmetric_f64.restype = C.c_double
         L.tqo_distance_symmetric_f64.argtypes = [C.c_void_p, _u8p, _u8p]
+        L.tqo_rotated_coords_batch.argtypes = [C.c_void_p, _fp, _sz, _fp, C.c_int]
+        L.tqo_distance_m_to_n_symmetric_qjl.argtypes = [C.c_void_p, _u8p, _sz, _u8p, _sz, _fp,
+                                                        C.c_int, C.c_int]
+        L.tqo_prepare_symmetric.argtypes = [C.c_void_p, _u8p, _fp, _fp, _fp]
+        L.tqo_distance_1_to_n_symmetric_full.argtypes = [C.c_void_p, _fp, _fp, _fp, _u8p, _sz,
+                                                         _fp, C.c_int]
+        L.tqo_distance_symmetric_qjl_f64.restype = C.c_double
+        L.tqo_distance_symmetric_qjl_f64.argtypes = [C.c_void_p, _u8p, _u8p, C.c_int]
         _LIB = L
     return _LIB
 
@@ -176,6 +184,48 @@ class OracleSpace:
         a = np.ascontiguousarray(a, dtype=np.uint8)
         b = np.ascontiguousarray(b, dtype=np.uint8)
         return float(self._L.tqo_distance_symmetric_f64(self._h, _u8(a), _u8(b)))
+
+
+    # rotatedCoordsBatch and the QJL-corrected symmetric distances
+    SYM_VARIANTS = {"light": 0, "full": 1, "full_prepared": 2}
+
+    def rotated_coords_batch(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.empty((X.shape[0], self.D), np.float32)
+        self._L.tqo_rotated_coords_batch(self._h, _f32(X), X.shape[0], _f32(out), self.threads)
+        return out
+
+    def distance_m_to_n_symmetric_qjl(self, A, B, variant):
+        A = np.ascontiguousarray(A, dtype=np.uint8)
+        B = np.ascontiguousarray(B, dtype=np.uint8)
+        m, n = A.size // self.cs, B.size // self.cs
+        out = np.empty((m, n), np.float32)
+        self._L.tqo_distance_m_to_n_symmetric_qjl(self._h, _u8(A), m, _u8(B), n, _f32(out),
+                                                  self.SYM_VARIANTS[variant], self.threads)
+        return out
+
+    def prepare_symmetric_query(self, code):
+        code = np.ascontiguousarray(code, dtype=np.uint8)
+        recon = np.empty(self.D, np.float32)
+        sign = np.empty(self.D, np.float32)
+        sc = np.empty(5, np.float32)
+        self._L.tqo_prepare_symmetric(self._h, _u8(code), _f32(recon), _f32(sign), _f32(sc))
+        return recon, sign, sc
+
+    def distance_1_to_n_symmetric_full(self, prepared, codes):
+        recon, sign, sc = (np.ascontiguousarray(a, dtype=np.float32) for a in prepared)
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        n = codes.size // self.cs
+        out = np.empty(n, np.float32)
+        self._L.tqo_distance_1_to_n_symmetric_full(self._h, _f32(recon), _f32(sign), _f32(sc),
+                                                   _u8(codes), n, _f32(out), self.threads)
+        return out
+
+    def distance_symmetric_qjl_f64(self, a, b, variant):
+        a = np.ascontiguousarray(a, dtype=np.uint8)
+        b = np.ascontiguousarray(b, dtype=np.uint8)
+        return float(self._L.tqo_distance_symmetric_qjl_f64(self._h, _u8(a), _u8(b),
+                                                            self.SYM_VARIANTS[variant]))
 
 
 def sq_reduce(x):

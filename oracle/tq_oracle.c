@@ -412,3 +412,221 @@ double tqo_distance_symmetric_f64(const tqo_space *sp, const uint8_t *a, const u
     double d = (double)ma[0] * ma[0] + (double)mb[0] * mb[0] - 2.0 * ip;
     return d > 0.0 ? d : 0.0;
 }
+
+/* ---- rotatedCoordsBatch: space_turbo_quant.h:411-435 ----------------------
+ * |x|^2 with the same reduction tree as encodeVector (same loop shape), the
+ * guard `norm_sq > 1e-20f`, inv_norm = 1 / sqrt(norm_sq), the rotation RHT,
+ * var over D, inv_sigma = sqrt(D / var) (guard var > 1e-20f, else 1). */
+void tqo_rotated_coords_batch(const tqo_space *sp, const float *X, size_t n, float *out,
+                              int num_threads) {
+    const size_t dim = sp->dim, D = sp->D;
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel for schedule(static) num_threads(num_threads)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+        const float *raw = X + (size_t)ii * dim;
+        float *dst = out + (size_t)ii * D;
+        float norm_sq = tqo_sq_reduce(raw, dim);
+        float inv_norm = (norm_sq > 1e-20f) ? 1.0f / sqrtf(norm_sq) : 0.0f;
+        for (size_t j = 0; j < D; ++j) dst[j] = 0.0f;
+        for (size_t j = 0; j < dim; ++j) dst[j] = raw[j] * inv_norm;
+        rht(dst, sp->rot_signs, D, sp->wht_scale);
+        float var = tqo_sq_reduce(dst, D);
+        float inv_sigma = (var > 1e-20f) ? sqrtf((float)D / var) : 1.0f;
+        for (size_t j = 0; j < D; ++j) dst[j] = dst[j] * inv_sigma;
+    }
+}
+
+/* ---- QJL-corrected symmetric distances: space_turbo_quant.h:483-572, 731-945
+ * Sums are evaluated in index order as written in the reference's scalar
+ * functions (its build may vectorise them; the bar for distances is 1e-5). */
+static float pi_over_2d(const tqo_space *sp) {
+    return (float)M_PI / (2.0f * (float)sp->D);
+}
+
+static float clampf_(float v, float lim) {
+    return v > lim ? lim : (v < -lim ? -lim : v);
+}
+
+/* distBuildFullScalar (:731-800) */
+static float dist_build_full(const tqo_space *sp, const uint8_t *a, const uint8_t *b,
+                             float *ra, float *rb) {
+    const size_t D = sp->D;
+    float ma[3], mb[3];
+    code_meta(sp, a, ma);
+    code_meta(sp, b, mb);
+    float ip_mse = 0.0f;
+    for (size_t i = 0; i < D; ++i) {
+        float ca = sp->centroids[code_unit(a, i, sp->bits) >> 1] * ma[2];
+        float cb = sp->centroids[code_unit(b, i, sp->bits) >> 1] * mb[2];
+        ip_mse = ip_mse + ca * cb;
+        ra[i] = ca;
+        rb[i] = cb;
+    }
+    rht(ra, sp->qjl_signs, D, sp->wht_scale);
+    rht(rb, sp->qjl_signs, D, sp->wht_scale);
+    float t_ab = 0.0f, t_ba = 0.0f, t_ss = 0.0f;
+    for (size_t i = 0; i < D; ++i) {
+        float sa = (code_unit(a, i, sp->bits) & 1) ? 1.0f : -1.0f;
+        float sb = (code_unit(b, i, sp->bits) & 1) ? 1.0f : -1.0f;
+        t_ab = t_ab + ra[i] * sb;
+        t_ba = t_ba + sa * rb[i];
+        t_ss = t_ss + sa * sb;
+    }
+    float term2 = sp->scale * mb[1] * t_ab;
+    float term3 = sp->scale * ma[1] * t_ba;
+    float term4 = pi_over_2d(sp) * ma[1] * mb[1] * t_ss;
+    float corr = clampf_(term2 + term3 + term4, fabsf(ip_mse));
+    float ip = (ip_mse + corr) * ma[0] * mb[0];
+    float d = ma[0] * ma[0] + mb[0] * mb[0] - 2.0f * ip;
+    return d > 0.0f ? d : 0.0f;
+}
+
+/* distBuildLightScalar (:884-925) */
+static float dist_build_light(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+    const size_t D = sp->D;
+    float ma[3], mb[3];
+    code_meta(sp, a, ma);
+    code_meta(sp, b, mb);
+    float ip_mse = 0.0f;
+    int agree = 0;
+    for (size_t i = 0; i < D; ++i) {
+        unsigned ua = code_unit(a, i, sp->bits), ub = code_unit(b, i, sp->bits);
+        ip_mse = ip_mse + (sp->centroids[ua >> 1] * ma[2]) * (sp->centroids[ub >> 1] * mb[2]);
+        agree += ((ua ^ ub) & 1u) == 0 ? 1 : 0;
+    }
+    float dot_signs = (float)(2 * agree - (int)D);
+    float corr = clampf_(pi_over_2d(sp) * ma[1] * mb[1] * dot_signs, fabsf(ip_mse));
+    float ip = (ip_mse + corr) * ma[0] * mb[0];
+    float d = ma[0] * ma[0] + mb[0] * mb[0] - 2.0f * ip;
+    return d > 0.0f ? d : 0.0f;
+}
+
+/* prepareSymmetricQuery (:498-530): recon_q = RHT_qjl(c[idx] * sigma),
+ * sign_q = +-1, s[0..4] = norm, gamma, sigma, scale * gamma,
+ * (pi / (2 D)) * gamma. */
+void tqo_prepare_symmetric(const tqo_space *sp, const uint8_t *code, float *recon_q,
+                           float *sign_q, float *s) {
+    const size_t D = sp->D;
+    float m[3];
+    code_meta(sp, code, m);
+    for (size_t i = 0; i < D; ++i) {
+        unsigned u = code_unit(code, i, sp->bits);
+        recon_q[i] = sp->centroids[u >> 1] * m[2];
+        sign_q[i] = (u & 1) ? 1.0f : -1.0f;
+    }
+    rht(recon_q, sp->qjl_signs, D, sp->wht_scale);
+    s[0] = m[0];
+    s[1] = m[1];
+    s[2] = m[2];
+    s[3] = sp->scale * m[1];
+    s[4] = pi_over_2d(sp) * m[1];
+}
+
+/* distBuildFullPreparedScalar (:809-878) */
+static float dist_build_full_prepared(const tqo_space *sp, const float *recon_q,
+                                      const float *sign_q, const float *s, const uint8_t *b,
+                                      float *rb) {
+    const size_t D = sp->D;
+    float mb[3];
+    code_meta(sp, b, mb);
+    for (size_t i = 0; i < D; ++i)
+        rb[i] = sp->centroids[code_unit(b, i, sp->bits) >> 1] * mb[2];
+    rht(rb, sp->qjl_signs, D, sp->wht_scale);
+    float d_rr = 0.0f, d_rs = 0.0f, d_sr = 0.0f, d_ss = 0.0f;
+    for (size_t i = 0; i < D; ++i) {
+        float sb = (code_unit(b, i, sp->bits) & 1) ? 1.0f : -1.0f;
+        d_rr = d_rr + recon_q[i] * rb[i];
+        d_rs = d_rs + recon_q[i] * sb;
+        d_sr = d_sr + sign_q[i] * rb[i];
+        d_ss = d_ss + sign_q[i] * sb;
+    }
+    float term2 = sp->scale * mb[1] * d_rs;
+    float term3 = s[3] * d_sr;
+    float term4 = s[4] * mb[1] * d_ss;
+    float corr = clampf_(term2 + term3 + term4, fabsf(d_rr));
+    float ip = (d_rr + corr) * s[0] * mb[0];
+    float d = s[0] * s[0] + mb[0] * mb[0] - 2.0f * ip;
+    return d > 0.0f ? d : 0.0f;
+}
+
+void tqo_distance_m_to_n_symmetric_qjl(const tqo_space *sp, const uint8_t *A, size_t m,
+                                       const uint8_t *B, size_t n, float *out, int variant,
+                                       int num_threads) {
+    const size_t D = sp->D, cs = sp->code_size;
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel num_threads(num_threads)
+    {
+        float *ra = (float *)malloc(sizeof(float) * D);
+        float *rb = (float *)malloc(sizeof(float) * D);
+        float *sq = (float *)malloc(sizeof(float) * D);
+        float s[5];
+#pragma omp for schedule(static)
+        for (long long i = 0; i < (long long)m; ++i) {
+            const uint8_t *a = A + (size_t)i * cs;
+            if (variant == TQO_SYM_FULL_PREPARED) tqo_prepare_symmetric(sp, a, ra, sq, s);
+            for (size_t j = 0; j < n; ++j) {
+                const uint8_t *b = B + j * cs;
+                float d;
+                if (variant == TQO_SYM_LIGHT) d = dist_build_light(sp, a, b);
+                else if (variant == TQO_SYM_FULL) d = dist_build_full(sp, a, b, ra, rb);
+                else d = dist_build_full_prepared(sp, ra, sq, s, b, rb);
+                out[(size_t)i * n + j] = d;
+            }
+        }
+        free(ra); free(rb); free(sq);
+    }
+}
+
+void tqo_distance_1_to_n_symmetric_full(const tqo_space *sp, const float *recon_q,
+                                        const float *sign_q, const float *s,
+                                        const uint8_t *B, size_t n, float *out,
+                                        int num_threads) {
+    const size_t D = sp->D;
+    if (num_threads <= 0) num_threads = 1;
+#pragma omp parallel num_threads(num_threads)
+    {
+        float *rb = (float *)malloc(sizeof(float) * D);
+#pragma omp for schedule(static)
+        for (long long j = 0; j < (long long)n; ++j)
+            out[j] = dist_build_full_prepared(sp, recon_q, sign_q, s,
+                                              B + (size_t)j * sp->code_size, rb);
+        free(rb);
+    }
+}
+
+/* FP64 evaluation of the three corrected formulas on the same codes (the
+ * prepared variant's ip_mse is the post-Hadamard dot, equal in exact
+ * arithmetic to the full variant's pre-Hadamard one). */
+double tqo_distance_symmetric_qjl_f64(const tqo_space *sp, const uint8_t *a, const uint8_t *b,
+                                      int variant) {
+    const size_t D = sp->D;
+    float ma[3], mb[3];
+    code_meta(sp, a, ma);
+    code_meta(sp, b, mb);
+    double *ra = (double *)malloc(sizeof(double) * D);
+    double *rb = (double *)malloc(sizeof(double) * D);
+    double ip_mse = 0.0, t_ab = 0.0, t_ba = 0.0, t_ss = 0.0;
+    for (size_t i = 0; i < D; ++i) {
+        ra[i] = (double)sp->centroids[code_unit(a, i, sp->bits) >> 1] * ma[2];
+        rb[i] = (double)sp->centroids[code_unit(b, i, sp->bits) >> 1] * mb[2];
+        ip_mse += ra[i] * rb[i];
+    }
+    rht64(ra, sp->qjl_signs, D);
+    rht64(rb, sp->qjl_signs, D);
+    for (size_t i = 0; i < D; ++i) {
+        double sa = (code_unit(a, i, sp->bits) & 1) ? 1.0 : -1.0;
+        double sb = (code_unit(b, i, sp->bits) & 1) ? 1.0 : -1.0;
+        t_ab += ra[i] * sb;
+        t_ba += sa * rb[i];
+        t_ss += sa * sb;
+    }
+    free(ra); free(rb);
+    const double p2d = M_PI / (2.0 * (double)D), scale = sqrt(M_PI / 2.0) / sqrt((double)D);
+    double corr = p2d * ma[1] * mb[1] * t_ss;
+    if (variant != TQO_SYM_LIGHT) corr += scale * mb[1] * t_ab + scale * ma[1] * t_ba;
+    double lim = fabs(ip_mse);
+    corr = corr > lim ? lim : (corr < -lim ? -lim : corr);
+    double ip = (ip_mse + corr) * ma[0] * mb[0];
+    double d = (double)ma[0] * ma[0] + (double)mb[0] * mb[0] - 2.0 * ip;
+    return d > 0.0 ? d : 0.0;
+}

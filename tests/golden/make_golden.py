@@ -16,7 +16,11 @@ The inputs follow the reference's own test pattern
 python/tests/test_turboquant.py:17-19) and its benchmark's row normalisation
 (python/benchmarks/run_benchmark.py:229-232).
 
-Usage:  python tests/golden/make_golden.py
+* ``qjl_<dim>_<bits>.npz`` (``make_golden.py qjl``): rotated_coords_batch and
+  the QJL-corrected symmetric distances of the reference module on the same
+  inputs.
+
+Usage:  python tests/golden/make_golden.py [qjl]
 """
 from __future__ import annotations
 
@@ -129,5 +133,36 @@ def main():
     print(json.dumps(meta, indent=1))
 
 
+# (dim, bits) cases of the rotated-coordinate diagnostic and the QJL-corrected
+# symmetric distances (reference module methods rotated_coords_batch,
+# distance_m_to_n_symmetric_{light,full,full_prepared},
+# prepare_symmetric_query + distance_1_to_n_symmetric_full).
+QJL_CASES = [(128, 4), (768, 8), (1536, 4), (384, 4), (7, 4), (33, 6), (100, 9), (1000, 3)]
+
+
+def qjl_main():
+    """``qjl_<dim>_<bits>.npz``: the reference module's outputs on the inputs
+    and codes of ``case_<dim>_<bits>.npz`` (the first 8 rows against all 32)."""
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    R = O.import_ref_module()
+    for dim, bits in QJL_CASES:
+        r = R.TurboQuantSpace(dim, bits)
+        X, _, _ = case_inputs(dim, bits)
+        codes = r.encode_batch(X)
+        prev = np.load(os.path.join(HERE, f"case_{dim}_{bits}.npz"))["codes"]
+        assert np.array_equal(prev, codes), "inputs differ from case_<dim>_<bits>.npz"
+        np.savez_compressed(
+            os.path.join(HERE, f"qjl_{dim}_{bits}.npz"),
+            rot=r.rotated_coords_batch(X[:8]),
+            dlight=r.distance_m_to_n_symmetric_light(codes[:8], codes),
+            dfull=r.distance_m_to_n_symmetric_full(codes[:8], codes),
+            dfullp=r.distance_m_to_n_symmetric_full_prepared(codes[:8], codes),
+            d1full=r.distance_1_to_n_symmetric_full(r.prepare_symmetric_query(codes[5]), codes))
+        print("qjl", dim, bits)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["qjl"]:
+        qjl_main()
+    else:
+        main()
