@@ -52,6 +52,13 @@ typedef enum tq_precision {
     TQ_PRECISION_SPLIT_BF16 = 1 /* tcgen05 tensor cores on hi+lo BF16 pairs, FP32 TMEM accumulators */
 } tq_precision;
 
+/* The QJL-corrected symmetric distances (space_turbo_quant.h:483-572, 731-945). */
+typedef enum tq_sym_variant {
+    TQ_SYM_LIGHT = 0,        /* distBuildLightScalar (:902-945): MSE + sign-agreement term */
+    TQ_SYM_FULL = 1,         /* distBuildFullScalar (:731-800): all four inner-product terms */
+    TQ_SYM_FULL_PREPARED = 2 /* distBuildFullPreparedScalar (:808-878): row code prepared once */
+} tq_sym_variant;
+
 typedef struct tq_space tq_space;
 
 typedef struct tq_space_info {
@@ -180,6 +187,45 @@ tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t 
                                               size_t m, const uint8_t *codes_b, size_t n,
                                               float *out, tq_precision precision,
                                               void *stream);
+
+/* ---- beside the encode-and-scan path ------------------------------------ */
+
+/* rotatedCoordsBatch (space_turbo_quant.h:411-435; bindings.cpp:119-132):
+ * out[n, padded_dim] = the sigma-normalised post-rotation coordinates,
+ * bit-identical to the reference.  Host pointers, synchronous. */
+tq_status tq_rotated_coords_batch(const tq_space *sp, const float *X, size_t n, float *out);
+/* The same on device buffers, stream-ordered. */
+tq_status tq_rotated_coords_batch_device(const tq_space *sp, const float *X, size_t n, float *out,
+                                         void *stream);
+
+/* distanceBatchMToNSymmetric{Light,Full,FullPrepared} (:557-572, 618-647,
+ * bindings.cpp:221-266, 312-334): out[m, n] row-major.  Host pointers,
+ * synchronous.  Each code is reconstructed and passed through the QJL
+ * Hadamard once; the pair terms are two FP32 contractions on the GPU. */
+tq_status tq_distance_m_to_n_symmetric_qjl(const tq_space *sp, const uint8_t *codes_a, size_t m,
+                                           const uint8_t *codes_b, size_t n, float *out,
+                                           tq_sym_variant variant);
+/* The same on device buffers, stream-ordered. */
+tq_status tq_distance_m_to_n_symmetric_qjl_device(const tq_space *sp, const uint8_t *codes_a,
+                                                  size_t m, const uint8_t *codes_b, size_t n,
+                                                  float *out, tq_sym_variant variant,
+                                                  void *stream);
+
+/* prepareSymmetricQuery (:499-535; bindings.cpp:276-282) of one code (host
+ * pointers): recon_q[padded_dim] = RHT_qjl(c * sigma), sign_q[padded_dim] =
+ * +-1, scalars[5] = {norm, gamma, sigma, scale * gamma, (pi / 2D) * gamma}. */
+tq_status tq_prepare_symmetric_query(const tq_space *sp, const uint8_t *code, float *recon_q,
+                                     float *sign_q, float *scalars);
+/* distanceBatch1ToNSymmetricFull (:544-553; bindings.cpp:293-310) on a
+ * prepared code.  Host pointers, synchronous. */
+tq_status tq_distance_1_to_n_symmetric_full(const tq_space *sp, const float *recon_q,
+                                            const float *sign_q, const float *scalars,
+                                            const uint8_t *codes, size_t n, float *out);
+/* The same with every buffer in device memory, stream-ordered. */
+tq_status tq_distance_1_to_n_symmetric_full_device(const tq_space *sp, const float *recon_q,
+                                                   const float *sign_q, const float *scalars,
+                                                   const uint8_t *codes, size_t n, float *out,
+                                                   void *stream);
 
 /* The device status word of the space's stream-ordered kernels.  Every wait in
  * the staged 1->N scan is bounded; a wait that gives up (a copy that never

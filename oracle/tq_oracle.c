@@ -481,7 +481,7 @@ static float dist_build_full(const tqo_space *sp, const uint8_t *a, const uint8_
     return d > 0.0f ? d : 0.0f;
 }
 
-/* distBuildLightScalar (:884-925) */
+/* distBuildLightScalar (:902-945) */
 static float dist_build_light(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
     const size_t D = sp->D;
     float ma[3], mb[3];
@@ -501,7 +501,7 @@ static float dist_build_light(const tqo_space *sp, const uint8_t *a, const uint8
     return d > 0.0f ? d : 0.0f;
 }
 
-/* prepareSymmetricQuery (:498-530): recon_q = RHT_qjl(c[idx] * sigma),
+/* prepareSymmetricQuery (:499-535): recon_q = RHT_qjl(c[idx] * sigma),
  * sign_q = +-1, s[0..4] = norm, gamma, sigma, scale * gamma,
  * (pi / (2 D)) * gamma. */
 void tqo_prepare_symmetric(const tqo_space *sp, const uint8_t *code, float *recon_q,
@@ -522,7 +522,7 @@ void tqo_prepare_symmetric(const tqo_space *sp, const uint8_t *code, float *reco
     s[4] = pi_over_2d(sp) * m[1];
 }
 
-/* distBuildFullPreparedScalar (:809-878) */
+/* distBuildFullPreparedScalar (:808-878) */
 static float dist_build_full_prepared(const tqo_space *sp, const float *recon_q,
                                       const float *sign_q, const float *s, const uint8_t *b,
                                       float *rb) {

@@ -90,7 +90,7 @@ void tqo_rotated_coords_batch(const tqo_space *sp, const float *X, size_t n, flo
 /* QJL-corrected symmetric distances (space_turbo_quant.h:483-572, 731-945):
  * LIGHT adds the sign-agreement term only, FULL all four inner-product terms
  * (two reconstructions + QJL Hadamards per pair), FULL_PREPARED prepares the
- * row code once (prepareSymmetricQuery :498-530) and uses the post-Hadamard
+ * row code once (prepareSymmetricQuery :499-535) and uses the post-Hadamard
  * dot as the MSE term.  The correction is clamped to +-|ip_mse|. */
 enum { TQO_SYM_LIGHT = 0, TQO_SYM_FULL = 1, TQO_SYM_FULL_PREPARED = 2 };
 void tqo_distance_m_to_n_symmetric_qjl(const tqo_space *sp, const uint8_t *A, size_t m,
@@ -100,7 +100,7 @@ void tqo_distance_m_to_n_symmetric_qjl(const tqo_space *sp, const uint8_t *A, si
  * s = {norm, gamma, sigma, scale * gamma, (pi / (2 D)) * gamma}. */
 void tqo_prepare_symmetric(const tqo_space *sp, const uint8_t *code, float *recon_q,
                            float *sign_q, float *s);
-/* distanceBatch1ToNSymmetricFull (:535-545) on a prepared row code. */
+/* distanceBatch1ToNSymmetricFull (:544-553) on a prepared row code. */
 void tqo_distance_1_to_n_symmetric_full(const tqo_space *sp, const float *recon_q,
                                         const float *sign_q, const float *s,
                                         const uint8_t *B, size_t n, float *out,

@@ -853,3 +853,265 @@ tq_status tq_distance_m_to_n_symmetric(const tq_space *csp, const uint8_t *codes
 }
 
 }  // extern "C"
+
+// ---- rotated coordinates and QJL-corrected symmetric distances -------------
+namespace {
+
+constexpr size_t kSymqChunkBytes = size_t(512) << 20;  // column planes per chunk
+
+// Row planes built once (from row codes, or from a prepared code), column
+// planes built per chunk; one two-accumulator contraction per chunk.
+struct SymqRunner {
+    const tq_space *sp;
+    int mode, ldk1, ldk2;
+    size_t m = 0, per = 0;
+    Scratch rows, cols;
+    float *P1a = nullptr, *P2a = nullptr, *sa = nullptr;
+
+    SymqRunner(const tq_space *s, int md) : sp(s), mode(md) {
+        ldk1 = tq::symq_ldk((int)s->D);
+        ldk2 = tq::symq_ldk(tq::symq_k2(md, (int)s->D));
+    }
+    size_t row_floats() const { return (size_t)ldk1 + ldk2 + 8; }
+    tq_status alloc_rows(size_t rows_, cudaStream_t s) {
+        m = rows_;
+        TQ_CUDA(rows.alloc(sizeof(float) * row_floats() * m, s), "cudaMallocAsync(row planes)");
+        P1a = static_cast<float *>(rows.p);
+        P2a = P1a + m * ldk1;
+        sa = P2a + m * ldk2;
+        return TQ_OK;
+    }
+    tq_status prepare_rows(const uint8_t *A, size_t rows_, cudaStream_t s) {
+        tq_status st = alloc_rows(rows_, s);
+        if (st != TQ_OK) return st;
+        TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, A, m, mode, true, P1a, ldk1, P2a, ldk2, sa, s),
+                "symmetric planes kernel");
+        return TQ_OK;
+    }
+    tq_status prepare_row_from_prepared(const float *recon, const float *sign, const float *sc,
+                                        cudaStream_t s) {
+        tq_status st = alloc_rows(1, s);
+        if (st != TQ_OK) return st;
+        TQ_CUDA(tq::launch_symq_prepared_row(recon, sign, sc, (int)sp->D, P1a, ldk1, P2a, ldk2, sa, s),
+                "prepared row kernel");
+        return TQ_OK;
+    }
+    // out[:, 0:n] (leading dimension ldo) for n column codes
+    tq_status run_cols(const uint8_t *B, size_t n, float *out, size_t ldo, cudaStream_t s) {
+        if (!per) {
+            per = std::max<size_t>(64, kSymqChunkBytes / (sizeof(float) * row_floats()));
+            per = std::min(per, std::max<size_t>(n, 1));
+            TQ_CUDA(cols.alloc(sizeof(float) * row_floats() * per, s), "cudaMallocAsync(column planes)");
+        }
+        float *P1b = static_cast<float *>(cols.p), *P2b = P1b + per * ldk1, *sb = P2b + per * ldk2;
+        for (size_t c0 = 0; c0 < n; c0 += per) {
+            const size_t nc = std::min(per, n - c0);
+            TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, B + c0 * sp->code_size, nc, mode, false, P1b,
+                                           ldk1, P2b, ldk2, sb, s),
+                    "symmetric planes kernel");
+            TQ_CUDA(tq::launch_symq_gemm(P1a, P2a, sa, m, P1b, P2b, sb, nc, ldk1, ldk2, out + c0, ldo, s),
+                    "symmetric contraction kernel");
+        }
+        return TQ_OK;
+    }
+};
+
+int sym_mode(tq_sym_variant v) {
+    switch (v) {
+        case TQ_SYM_LIGHT: return tq::SYMQ_LIGHT;
+        case TQ_SYM_FULL: return tq::SYMQ_FULL;
+        case TQ_SYM_FULL_PREPARED: return tq::SYMQ_FULL_PREPARED;
+        default: return -1;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+tq_status tq_rotated_coords_batch_device(const tq_space *sp, const float *X, size_t n, float *out,
+                                         void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(X, n * sp->dim * 4, "X")) != TQ_OK) return st;
+    if ((st = check_dev(out, n * sp->D * 4, "out")) != TQ_OK) return st;
+    TQ_CUDA(tq::launch_rotated_coords(sp->P, sp->T, X, n, out, (cudaStream_t)stream),
+            "rotated coordinates kernel");
+    return TQ_OK;
+}
+
+tq_status tq_rotated_coords_batch(const tq_space *csp, const float *X, size_t n, float *out) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    if (!X || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    cudaStream_t s = sp->host_stream[0];
+    const size_t in_row = sp->dim * 4, out_row = sp->D * 4;
+    const size_t rows = std::min(n, std::max<size_t>(1, kChunkBytes / (in_row + out_row)));
+    Scratch buf;
+    TQ_CUDA(buf.alloc(rows * (in_row + out_row), s), "cudaMallocAsync(rotated staging)");
+    float *dX = static_cast<float *>(buf.p);
+    float *dO = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(dX) + rows * in_row);
+    for (size_t r0 = 0; r0 < n; r0 += rows) {
+        const size_t nr = std::min(rows, n - r0);
+        TQ_CUDA(cudaMemcpyAsync(dX, X + r0 * sp->dim, nr * in_row, cudaMemcpyHostToDevice, s), "H2D X");
+        TQ_CUDA(tq::launch_rotated_coords(sp->P, sp->T, dX, nr, dO, s), "rotated coordinates kernel");
+        TQ_CUDA(cudaMemcpyAsync(out + r0 * sp->D, dO, nr * out_row, cudaMemcpyDeviceToHost, s), "D2H");
+    }
+    TQ_CUDA(cudaStreamSynchronize(s), "rotated_coords_batch");
+    return TQ_OK;
+}
+
+tq_status tq_distance_m_to_n_symmetric_qjl_device(const tq_space *sp, const uint8_t *A, size_t m,
+                                                  const uint8_t *B, size_t n, float *out,
+                                                  tq_sym_variant variant, void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    const int mode = sym_mode(variant);
+    if (mode < 0) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown symmetric variant %d", (int)variant);
+    if (m == 0 || n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(A, m * sp->code_size, "codes_a")) != TQ_OK) return st;
+    if ((st = check_dev(B, n * sp->code_size, "codes_b")) != TQ_OK) return st;
+    if ((st = check_dev(out, m * n * 4, "out")) != TQ_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    SymqRunner r(sp, mode);
+    if ((st = r.prepare_rows(A, m, s)) != TQ_OK) return st;
+    return r.run_cols(B, n, out, n, s);
+}
+
+tq_status tq_distance_m_to_n_symmetric_qjl(const tq_space *csp, const uint8_t *codes_a, size_t m,
+                                           const uint8_t *codes_b, size_t n, float *out,
+                                           tq_sym_variant variant) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    const int mode = sym_mode(variant);
+    if (mode < 0) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown symmetric variant %d", (int)variant);
+    if (m == 0 || n == 0) return TQ_OK;
+    if (!codes_a || !codes_b || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    cudaStream_t s = sp->host_stream[0];
+    const size_t cs = sp->code_size;
+    Scratch dA;
+    TQ_CUDA(dA.alloc(m * cs, s), "cudaMallocAsync(codes_a)");
+    TQ_CUDA(cudaMemcpyAsync(dA.p, codes_a, m * cs, cudaMemcpyHostToDevice, s), "H2D codes_a");
+    SymqRunner r(sp, mode);
+    if ((st = r.prepare_rows(static_cast<uint8_t *>(dA.p), m, s)) != TQ_OK) return st;
+    size_t per = std::max<size_t>(1, std::min(kChunkBytes / cs, (kChunkBytes * 2) / (4 * m)));
+    per = std::min(per, n);
+    Scratch buf;
+    const size_t cbytes = (per * cs + 15) & ~size_t(15);
+    TQ_CUDA(buf.alloc(cbytes + per * m * 4, s), "cudaMallocAsync(symmetric staging)");
+    uint8_t *dB = static_cast<uint8_t *>(buf.p);
+    float *dO = reinterpret_cast<float *>(dB + cbytes);
+    for (size_t c0 = 0; c0 < n; c0 += per) {
+        const size_t nc = std::min(per, n - c0);
+        TQ_CUDA(cudaMemcpyAsync(dB, codes_b + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s), "H2D codes_b");
+        if ((st = r.run_cols(dB, nc, dO, nc, s)) != TQ_OK) return st;
+        TQ_CUDA(cudaMemcpy2DAsync(out + c0, n * 4, dO, nc * 4, nc * 4, m, cudaMemcpyDeviceToHost, s),
+                "D2H distances");
+    }
+    TQ_CUDA(cudaStreamSynchronize(s), "distance_m_to_n_symmetric (QJL)");
+    return TQ_OK;
+}
+
+tq_status tq_prepare_symmetric_query(const tq_space *csp, const uint8_t *code, float *recon_q,
+                                     float *sign_q, float *scalars) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (!code || !recon_q || !sign_q || !scalars) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    cudaStream_t s = sp->host_stream[0];
+    const int ldk1 = tq::symq_ldk((int)sp->D), ldk2 = tq::symq_ldk((int)sp->D);
+    Scratch buf;
+    const size_t cbytes = (sp->code_size + 15) & ~size_t(15);
+    TQ_CUDA(buf.alloc(cbytes + sizeof(float) * (ldk1 + ldk2 + 8), s), "cudaMallocAsync(prepare)");
+    uint8_t *dc = static_cast<uint8_t *>(buf.p);
+    float *P1 = reinterpret_cast<float *>(dc + cbytes), *P2 = P1 + ldk1, *sc = P2 + ldk2;
+    TQ_CUDA(cudaMemcpyAsync(dc, code, sp->code_size, cudaMemcpyHostToDevice, s), "H2D code");
+    TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, dc, 1, tq::SYMQ_PREPARE, true, P1, ldk1, P2, ldk2,
+                                   sc, s),
+            "symmetric planes kernel");
+    float sc8[8];
+    TQ_CUDA(cudaMemcpyAsync(recon_q, P1, sp->D * 4, cudaMemcpyDeviceToHost, s), "D2H recon");
+    TQ_CUDA(cudaMemcpyAsync(sign_q, P2, sp->D * 4, cudaMemcpyDeviceToHost, s), "D2H sign");
+    TQ_CUDA(cudaMemcpyAsync(sc8, sc, sizeof(sc8), cudaMemcpyDeviceToHost, s), "D2H scalars");
+    TQ_CUDA(cudaStreamSynchronize(s), "prepare_symmetric_query");
+    scalars[0] = sc8[1];  // norm
+    scalars[1] = sc8[3];  // gamma
+    scalars[2] = sc8[4];  // sigma
+    scalars[3] = sc8[5];  // scale * gamma
+    scalars[4] = sc8[6];  // (pi / 2D) * gamma
+    return TQ_OK;
+}
+
+tq_status tq_distance_1_to_n_symmetric_full_device(const tq_space *sp, const float *recon_q,
+                                                   const float *sign_q, const float *scalars,
+                                                   const uint8_t *codes, size_t n, float *out,
+                                                   void *stream) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    DeviceGuard g(sp->device);
+    if ((st = check_dev(recon_q, sp->D * 4, "recon_q")) != TQ_OK) return st;
+    if ((st = check_dev(sign_q, sp->D * 4, "sign_q")) != TQ_OK) return st;
+    if ((st = check_dev(scalars, 5 * 4, "scalars")) != TQ_OK) return st;
+    if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
+    if ((st = check_dev(out, n * 4, "out")) != TQ_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    SymqRunner r(sp, tq::SYMQ_FULL_PREPARED);
+    if ((st = r.prepare_row_from_prepared(recon_q, sign_q, scalars, s)) != TQ_OK) return st;
+    return r.run_cols(codes, n, out, n, s);
+}
+
+tq_status tq_distance_1_to_n_symmetric_full(const tq_space *csp, const float *recon_q,
+                                            const float *sign_q, const float *scalars,
+                                            const uint8_t *codes, size_t n, float *out) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (n == 0) return TQ_OK;
+    if (!recon_q || !sign_q || !scalars || !codes || !out)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    cudaStream_t s = sp->host_stream[0];
+    const size_t D = sp->D, cs = sp->code_size;
+    Scratch q;
+    TQ_CUDA(q.alloc(sizeof(float) * (2 * D + 8), s), "cudaMallocAsync(prepared code)");
+    float *dr = static_cast<float *>(q.p), *ds = dr + D, *dsc = ds + D;
+    TQ_CUDA(cudaMemcpyAsync(dr, recon_q, D * 4, cudaMemcpyHostToDevice, s), "H2D recon_q");
+    TQ_CUDA(cudaMemcpyAsync(ds, sign_q, D * 4, cudaMemcpyHostToDevice, s), "H2D sign_q");
+    TQ_CUDA(cudaMemcpyAsync(dsc, scalars, 5 * 4, cudaMemcpyHostToDevice, s), "H2D scalars");
+    SymqRunner r(sp, tq::SYMQ_FULL_PREPARED);
+    if ((st = r.prepare_row_from_prepared(dr, ds, dsc, s)) != TQ_OK) return st;
+    const size_t per = std::min(n, std::max<size_t>(1, kChunkBytes / (cs + 4)));
+    Scratch buf;
+    const size_t cbytes = (per * cs + 15) & ~size_t(15);
+    TQ_CUDA(buf.alloc(cbytes + per * 4, s), "cudaMallocAsync(symmetric staging)");
+    uint8_t *dB = static_cast<uint8_t *>(buf.p);
+    float *dO = reinterpret_cast<float *>(dB + cbytes);
+    for (size_t c0 = 0; c0 < n; c0 += per) {
+        const size_t nc = std::min(per, n - c0);
+        TQ_CUDA(cudaMemcpyAsync(dB, codes + c0 * cs, nc * cs, cudaMemcpyHostToDevice, s), "H2D codes");
+        if ((st = r.run_cols(dB, nc, dO, nc, s)) != TQ_OK) return st;
+        TQ_CUDA(cudaMemcpyAsync(out + c0, dO, nc * 4, cudaMemcpyDeviceToHost, s), "D2H distances");
+    }
+    TQ_CUDA(cudaStreamSynchronize(s), "distance_1_to_n_symmetric_full");
+    return TQ_OK;
+}
+
+}  // extern "C"

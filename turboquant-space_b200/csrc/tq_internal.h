@@ -69,4 +69,22 @@ cudaError_t launch_mton_sym_fp32(const Params &P, const DevTables &T, const uint
                                  size_t m, const uint8_t *B, size_t n, float *out, size_t ldo,
                                  cudaStream_t st);
 
+// ---- rotated coordinates and QJL-corrected symmetric distances (tq_symq.cu)
+cudaError_t launch_rotated_coords(const Params &P, const DevTables &T, const float *X, size_t n,
+                                  float *out, cudaStream_t st);
+// Plane modes: the three distance variants and the prepared-code export
+// (P1 = recon, P2 = signs).
+enum SymqMode { SYMQ_LIGHT = 0, SYMQ_FULL = 1, SYMQ_FULL_PREPARED = 2, SYMQ_PREPARE = 3 };
+int symq_ldk(int K);            // K rounded up to the GEMM's K step
+int symq_k2(int mode, int D);   // columns of the correction plane
+cudaError_t launch_symq_planes(const Params &P, const DevTables &T, const uint8_t *codes,
+                               size_t rows, int mode, bool row_side, float *P1, int ldk1,
+                               float *P2, int ldk2, float *scal, cudaStream_t st);
+cudaError_t launch_symq_prepared_row(const float *recon, const float *sign, const float *sc, int D,
+                                     float *P1, int ldk1, float *P2, int ldk2, float *scal,
+                                     cudaStream_t st);
+cudaError_t launch_symq_gemm(const float *P1a, const float *P2a, const float *sa, size_t m,
+                             const float *P1b, const float *P2b, const float *sb, size_t n,
+                             int ldk1, int ldk2, float *out, size_t ldo, cudaStream_t st);
+
 }  // namespace tq

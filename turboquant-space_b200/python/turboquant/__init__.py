@@ -21,7 +21,7 @@ import numpy as np
 from . import _capi
 from ._capi import TQError, check, lib
 
-__all__ = ["TurboQuantSpace", "TQError", "Index", "Server", "BusyError"]
+__all__ = ["TurboQuantSpace", "PreparedSymCode", "TQError", "Index", "Server", "BusyError"]
 __version__ = "0.1.0"
 
 
@@ -150,6 +150,32 @@ def _stream_and_device(obj):
     torch = _torch()
     dev = obj.device if hasattr(obj, "device") else torch.device("cuda", torch.cuda.current_device())
     return torch.cuda.current_stream(dev).cuda_stream, dev
+
+
+class PreparedSymCode:
+    """TurboQuantPreparedSymCode (space_turbo_quant.h:158-166): one code
+    reconstructed and passed through the QJL Hadamard (recon_q), its +-1 QJL
+    signs (sign_q) and the scalars [norm, gamma, sigma, scale * gamma,
+    (pi / 2D) * gamma], held on the host as float32 arrays."""
+
+    __slots__ = ("recon_q", "sign_q", "scalars")
+
+    def __init__(self, recon_q, sign_q, scalars):
+        self.recon_q = np.ascontiguousarray(recon_q, dtype=np.float32)
+        self.sign_q = np.ascontiguousarray(sign_q, dtype=np.float32)
+        self.scalars = np.ascontiguousarray(scalars, dtype=np.float32)
+
+    @property
+    def norm_q(self):
+        return float(self.scalars[0])
+
+    @property
+    def gamma_q(self):
+        return float(self.scalars[1])
+
+    @property
+    def sigma_q(self):
+        return float(self.scalars[2])
 
 
 class TurboQuantSpace:
@@ -373,6 +399,107 @@ class TurboQuantSpace:
         b, n = _codes_host(codes_b, cs)
         out = _out_host(out, (m, n))
         check(lib().tq_distance_m_to_n_symmetric(self._h, _ptr(a), m, _ptr(b), n, _ptr(out), prec))
+        return out
+
+    # -- rotated coordinates (bindings.cpp:119-132) ---------------------------
+    def rotated_coords_batch(self, X):
+        """(n, padded_dim) sigma-normalised post-rotation coordinates
+        (rotatedCoordsBatch, space_turbo_quant.h:411-435), bit-identical."""
+        D = self.padded_dim()
+        if _is_device(X):
+            ptr, shape = _float_dev(X, self.dim(), "input", 2)
+            torch = _torch()
+            stream, dev = _stream_and_device(X)
+            out = torch.empty((shape[0], D), dtype=torch.float32, device=dev)
+            check(lib().tq_rotated_coords_batch_device(self._h, C.c_void_p(ptr), shape[0],
+                                                       C.c_void_p(out.data_ptr()),
+                                                       C.c_void_p(stream)))
+            return out
+        data = _float_host(X, self.dim(), "input", 2)
+        out = np.empty((data.shape[0], D), np.float32)
+        check(lib().tq_rotated_coords_batch(self._h, _ptr(data), data.shape[0], _ptr(out)))
+        return out
+
+    # -- QJL-corrected symmetric distances (bindings.cpp:221-334) --------------
+    def _symmetric_qjl(self, codes_a, codes_b, variant):
+        cs = self.code_size_bytes()
+        v = _capi.SYM_VARIANT[variant]
+        if _is_device(codes_a) or _is_device(codes_b):
+            aptr, m = _codes_dev(codes_a, cs)
+            bptr, n = _codes_dev(codes_b, cs)
+            torch = _torch()
+            stream, dev = _stream_and_device(codes_b)
+            out = torch.empty((m, n), dtype=torch.float32, device=dev)
+            check(lib().tq_distance_m_to_n_symmetric_qjl_device(
+                self._h, C.c_void_p(aptr), m, C.c_void_p(bptr), n, C.c_void_p(out.data_ptr()), v,
+                C.c_void_p(stream)))
+            return out
+        mva, mvb = memoryview(codes_a), memoryview(codes_b)
+        if mva.itemsize != 1 or mvb.itemsize != 1:
+            raise ValueError("codes must be uint8")
+        if mva.nbytes % cs != 0 or mvb.nbytes % cs != 0:
+            raise ValueError("codes size not a multiple of code_size_bytes")
+        a, m = _codes_host(codes_a, cs)
+        b, n = _codes_host(codes_b, cs)
+        out = np.empty((m, n), np.float32)
+        check(lib().tq_distance_m_to_n_symmetric_qjl(self._h, _ptr(a), m, _ptr(b), n, _ptr(out), v))
+        return out
+
+    def distance_m_to_n_symmetric_full(self, codes_a, codes_b):
+        """distanceBatchMToNSymmetricFull: MSE + all four QJL terms (:618-631, 731-800)."""
+        return self._symmetric_qjl(codes_a, codes_b, "full")
+
+    def distance_m_to_n_symmetric_light(self, codes_a, codes_b):
+        """distanceBatchMToNSymmetricLight: MSE + the sign-agreement term (:634-647, 902-945)."""
+        return self._symmetric_qjl(codes_a, codes_b, "light")
+
+    def distance_m_to_n_symmetric_full_prepared(self, codes_a, codes_b):
+        """distanceBatchMToNSymmetricFullPrepared: row codes prepared once (:557-572, 808-878)."""
+        return self._symmetric_qjl(codes_a, codes_b, "full_prepared")
+
+    def prepare_symmetric_query(self, code):
+        """prepareSymmetricQuery (:499-535) of one code: a PreparedSymCode."""
+        mv = _bytes_host(code, "code", False)
+        if mv.nbytes != self.code_size_bytes():
+            raise ValueError("code: wrong byte size")
+        c = np.ascontiguousarray(np.asarray(mv).reshape(-1).view(np.uint8))
+        D = self.padded_dim()
+        recon = np.empty(D, np.float32)
+        sign = np.empty(D, np.float32)
+        sc = np.empty(5, np.float32)
+        check(lib().tq_prepare_symmetric_query(self._h, _ptr(c), _ptr(recon), _ptr(sign), _ptr(sc)))
+        return PreparedSymCode(recon, sign, sc)
+
+    def distance_symmetric_full_prepared(self, pq, code_b):
+        """distanceSymmetricFullPrepared (:538-541): one prepared code x one code."""
+        mv = _bytes_host(code_b, "code_b", False)
+        if mv.nbytes != self.code_size_bytes():
+            raise ValueError("code_b: wrong byte size")
+        b = np.ascontiguousarray(np.asarray(mv).reshape(-1).view(np.uint8))
+        return float(self.distance_1_to_n_symmetric_full(pq, b)[0])
+
+    def distance_1_to_n_symmetric_full(self, pq, codes):
+        """distanceBatch1ToNSymmetricFull (:544-553): a prepared code x n codes."""
+        if not isinstance(pq, PreparedSymCode):
+            raise TypeError("pq: expected a PreparedSymCode")
+        cs = self.code_size_bytes()
+        if _is_device(codes):
+            cptr, n = _codes_dev(codes, cs)
+            torch = _torch()
+            stream, dev = _stream_and_device(codes)
+            r = torch.from_numpy(pq.recon_q).to(dev)
+            sg = torch.from_numpy(pq.sign_q).to(dev)
+            sc = torch.from_numpy(pq.scalars).to(dev)
+            out = torch.empty(n, dtype=torch.float32, device=dev)
+            check(lib().tq_distance_1_to_n_symmetric_full_device(
+                self._h, C.c_void_p(r.data_ptr()), C.c_void_p(sg.data_ptr()),
+                C.c_void_p(sc.data_ptr()), C.c_void_p(cptr), n, C.c_void_p(out.data_ptr()),
+                C.c_void_p(stream)))
+            return out
+        c, n = _codes_host(codes, cs)
+        out = np.empty(n, np.float32)
+        check(lib().tq_distance_1_to_n_symmetric_full(self._h, _ptr(pq.recon_q), _ptr(pq.sign_q),
+                                                      _ptr(pq.scalars), _ptr(c), n, _ptr(out)))
         return out
 
     def index(self, codes):

@@ -34,7 +34,13 @@ EXPORTS = (
     "tq_server_create", "tq_server_submit", "tq_request_wait", "tq_request_done",
     "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning",
     "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status",
+    "tq_rotated_coords_batch", "tq_rotated_coords_batch_device",
+    "tq_distance_m_to_n_symmetric_qjl", "tq_distance_m_to_n_symmetric_qjl_device",
+    "tq_prepare_symmetric_query", "tq_distance_1_to_n_symmetric_full",
+    "tq_distance_1_to_n_symmetric_full_device",
 )
+
+SYM_VARIANT = {"light": 0, "full": 1, "full_prepared": 2}
 
 
 class ServerStats(C.Structure):
@@ -135,6 +141,20 @@ def lib() -> C.CDLL:
     L.tq_selftest_bounded_wait.argtypes = [C.c_int, C.c_int]
     L.tq_space_take_device_status.restype = st
     L.tq_space_take_device_status.argtypes = [vp, C.POINTER(C.c_int)]
+    L.tq_rotated_coords_batch.restype = st
+    L.tq_rotated_coords_batch.argtypes = [vp, fp, sz, fp]
+    L.tq_rotated_coords_batch_device.restype = st
+    L.tq_rotated_coords_batch_device.argtypes = [vp, fp, sz, fp, vp]
+    L.tq_distance_m_to_n_symmetric_qjl.restype = st
+    L.tq_distance_m_to_n_symmetric_qjl.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int]
+    L.tq_distance_m_to_n_symmetric_qjl_device.restype = st
+    L.tq_distance_m_to_n_symmetric_qjl_device.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int, vp]
+    L.tq_prepare_symmetric_query.restype = st
+    L.tq_prepare_symmetric_query.argtypes = [vp, u8p, fp, fp, fp]
+    L.tq_distance_1_to_n_symmetric_full.restype = st
+    L.tq_distance_1_to_n_symmetric_full.argtypes = [vp, fp, fp, fp, u8p, sz, fp]
+    L.tq_distance_1_to_n_symmetric_full_device.restype = st
+    L.tq_distance_1_to_n_symmetric_full_device.argtypes = [vp, fp, fp, fp, u8p, sz, fp, vp]
     L.tq_server_destroy.restype = None
     L.tq_server_destroy.argtypes = [vp]
     _LIB = L
