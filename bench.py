@@ -341,6 +341,101 @@ def run_mton(args, sym):
     }), flush=True)
 
 
+def run_symq(args):
+    """QJL-corrected symmetric distances (light, full, full-prepared): 2048 row
+    codes x 200,000 column codes of a 1024-centre Gaussian mixture at 1536-d
+    (padded 2048), 4-bit, device-resident.  Each variant is timed on the GPU
+    (CUDA events) and checked against the FP64 evaluation of its formula on
+    2,000 sampled pairs; the reference's own CPU code (oracle/_ref) is timed
+    on a bounded sample (128 x 512 pairs) on the host cores."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import turboquant as tq
+    from turboquant._capi import SYM_VARIANT, check, lib
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    L = lib()
+    stream = torch.cuda.Stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    dim, bits, m = 1536, 4, 2048
+    n = args.n if args.n != 10_000_000 else 200_000
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(6)
+    centres = torch.randn((1024, dim), generator=gen, device=dev)
+    Arows = mixture_rows(torch, gen, dev, m, dim, centres)
+    gen.manual_seed(7)
+    Brows = mixture_rows(torch, gen, dev, n, dim, centres)
+    space = tq.TurboQuantSpace(dim, bits_per_coord=bits, device=0)
+    h = space._h
+    cs, D = space.code_size_bytes(), space.padded_dim()
+    acodes = torch.empty((m, cs), dtype=torch.uint8, device=dev)
+    codes = torch.empty((n, cs), dtype=torch.uint8, device=dev)
+    check(L.tq_encode_batch_device(h, C.c_void_p(Arows.data_ptr()), m, C.c_void_p(acodes.data_ptr()), sptr))
+    check(L.tq_encode_batch_device(h, C.c_void_p(Brows.data_ptr()), n, C.c_void_p(codes.data_ptr()), sptr))
+    stream.synchronize()
+    del Arows, Brows
+    out = torch.empty((m, n), dtype=torch.float32, device=dev)
+    rng = np.random.default_rng(10)
+    ii, jj = rng.integers(0, m, 2000), rng.integers(0, n, 2000)
+    ah = acodes.index_select(0, torch.from_numpy(ii).to(dev)).cpu().numpy()
+    ch = codes.index_select(0, torch.from_numpy(jj).to(dev)).cpu().numpy()
+    o = O.OracleSpace(dim, bits)
+    na = np.frombuffer(ah[:, cs - 12:cs - 8].tobytes(), np.float32).astype(np.float64)
+    nb = np.frombuffer(ch[:, cs - 12:cs - 8].tobytes(), np.float32).astype(np.float64)
+    flat = torch.from_numpy(ii * n + jj).to(dev)
+    ref_mod = None
+    try:
+        ref_mod = O.import_ref_module()
+    except Exception:  # the reference build is optional
+        ref_mod = None
+    a_cpu, b_cpu = acodes[:128].cpu().numpy(), codes[:512].cpu().numpy()
+    res = {}
+    for variant in ("light", "full", "full_prepared"):
+        v = SYM_VARIANT[variant]
+
+        def call():
+            check(L.tq_distance_m_to_n_symmetric_qjl_device(
+                h, C.c_void_p(acodes.data_ptr()), m, C.c_void_p(codes.data_ptr()), n,
+                C.c_void_p(out.data_ptr()), v, sptr))
+
+        call()
+        stream.synchronize()
+        got = out.view(-1).index_select(0, flat).cpu().numpy().astype(np.float64)
+        f64 = np.array([o.distance_symmetric_qjl_f64(ah[k], ch[k], variant) for k in range(2000)])
+        err = float(np.max(np.abs(got - f64) / np.maximum(np.abs(f64), na ** 2 + nb ** 2)))
+        reps = max(1, args.steps // 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        k_total = D + (3 * D if variant != "light" else D)
+        r = {"ms": round(ms, 3), "Gdist_s": round(m * n / (ms * 1e-3) / 1e9, 3),
+             "TFLOP_s_issued": round(2.0 * k_total * m * n / (ms * 1e-3) / 1e12, 2),
+             "max_rel_err_vs_fp64": err, "reps": reps}
+        if ref_mod is not None:
+            rs = ref_mod.TurboQuantSpace(dim, bits, num_threads=cpu_cores())
+            fn = getattr(rs, f"distance_m_to_n_symmetric_{variant}")
+            fn(a_cpu[:4], b_cpu[:4])
+            t0 = time.perf_counter()
+            fn(a_cpu, b_cpu)
+            dt = time.perf_counter() - t0
+            r["cpu_reference"] = {"Gdist_s": round(a_cpu.shape[0] * b_cpu.shape[0] / dt / 1e9, 6),
+                                  "cores": cpu_cores(), "sample": "128 x 512 pairs of the same codes"}
+        res[variant] = r
+    print(json.dumps({
+        "metric": METRIC, "workload": "symq",
+        "config": {"dim": dim, "padded_dim": D, "bits_per_coord": bits, "m": m, "n": n,
+                   "data": "1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 6/7)",
+                   "error_sample": "2,000 (i, j) pairs, seed 10, vs the FP64 evaluation"},
+        "results": res,
+    }), flush=True)
+
+
 def run_serve(args):
     """Serving over a device-resident corpus: 20,000,000 codes of a 1024-centre
     Gaussian mixture at dim 384 (padded 512), 4-bit; requests of m ~ U{1..256}
@@ -444,13 +539,17 @@ def main():
     ap.add_argument("--rates", default="5,20,40,60,1000,50000",
                     help="serve: request rates (req/s) to sweep")
     ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
-    ap.add_argument("--workload", choices=("scan", "mton", "sym", "serve"), default="scan",
+    ap.add_argument("--workload", choices=("scan", "mton", "sym", "symq", "serve"), default="scan",
                     help="scan (default): the 1->N scan benchmark; mton/sym: the dense M x N "
-                         "contractions, FP32 vs split-BF16")
+                         "contractions, FP32 vs split-BF16; symq: the QJL-corrected symmetric "
+                         "distances; serve: the serving loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == "serve":
         run_serve(args)
+        return
+    if args.workload == "symq":
+        run_symq(args)
         return
     if args.workload != "scan":
         run_mton(args, args.workload == "sym")
