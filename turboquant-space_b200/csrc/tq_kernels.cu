@@ -189,9 +189,9 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
 // Butterflies of register stride >= 2 use packed FP32x2 add/sub: each half is
 // an independent IEEE add or subtract, so every stage output is still the
 // single rounding of a + b or a - b and the stage order is unchanged.
-// The vector buffer uses a 16-byte-chunk swizzle (chunk column XOR a function
-// of the 128-byte row) that keeps the float4 layout-A accesses, the layout-B
-// accesses and the 8-lane reduction chains free of bank conflicts.
+// The vector buffer is row-padded (PadLayout below): the float4 layout-A
+// accesses, the layout-B accesses and the 8-lane reduction chains are free of
+// bank conflicts without per-access index arithmetic.
 // ---------------------------------------------------------------------------
 typedef unsigned long long u64;
 
@@ -219,48 +219,59 @@ __device__ __forceinline__ void un2(u64 v, float &lo, float &hi) {
     asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
 }
 
+// Vector buffer layout of encode2: element e at e + 4 (e >> 5), i.e. every
+// 32-float row is followed by 4 floats of padding.  The layout-A float4
+// accesses (lane l: elements E l .. E l + E - 1), the layout-B accesses
+// (lane l: elements 32 t + l) and the 8-lane reduction chains are all free of
+// bank conflicts, and with the unrolled indices every address is a per-lane
+// base plus an immediate offset.  VecRow<D> floats per vector (a multiple of
+// 32 plus 8, so that the 4 vectors of a warp start 8 banks apart).
 template <int E>
-struct Swz {
-    __device__ static __forceinline__ int g(int row) {
-        if constexpr (E >= 32) return row & 7;
-        else if constexpr (E == 16) return row & 3;
-        else return row & 1;
-    }
+struct PadLayout {
     // physical float offset of element e
-    __device__ static __forceinline__ int elem(int e) {
-        const int c = e >> 2, row = c >> 3;
-        return ((row << 3) | ((c ^ g(row)) & 7)) << 2 | (e & 3);
-    }
-    // physical float offset of chunk c (4 floats)
-    __device__ static __forceinline__ int chunk(int c) {
-        const int row = c >> 3;
-        return ((row << 3) | ((c ^ g(row)) & 7)) << 2;
-    }
+    __device__ static __forceinline__ int elem(int e) { return e + ((e >> 5) << 2); }
+    // physical float offset of chunk c (elements 4c .. 4c + 3)
+    __device__ static __forceinline__ int chunk(int c) { return (c << 2) + ((c >> 3) << 2); }
 };
 
-// The reference's sum-of-squares tree (as chain_sq_reduce) on a Swz<E> buffer.
-// FULL: n = D (a multiple of 32), so there are no leftovers.
+template <int D>
+__host__ __device__ constexpr int vec_row_floats() {
+    return D + D / 8 + 8;
+}
+
+// The reference's sum-of-squares tree (as chain_sq_reduce) on a PadLayout
+// buffer.  FULL: n = D (a multiple of 32), so there are no leftovers.  Chain k
+// (lane k of the 8-lane group) reads elements k + 8 m: four per 32-float row.
 template <int E, bool FULL>
 __device__ __forceinline__ float chain_sq_reduce2(const float *buf, int n, int lane) {
     if constexpr (FULL) n = 32 * E;
-    const int k = lane & 7, kh = k >> 2, kw = k & 3;
+    const int k = lane & 7;
     const int steps = (n & ~7) >> 3;
     float acc = 0.0f;
     int m = 0;
+    // 16 steps (4 rows) per iteration: the loads run ahead of the chain
+#pragma unroll 1
+    for (; m + 16 <= steps; m += 16) {
+        const float *base = buf + (m >> 2) * 36 + k;
+        float xs[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) xs[i] = base[(i >> 2) * 36 + 8 * (i & 3)];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc = __fadd_rn(acc, __fmul_rn(xs[i], xs[i]));
+    }
 #pragma unroll 1
     for (; m + 4 <= steps; m += 4) {
-        const int r = m >> 2, gg = Swz<E>::g(r);
-        const float *base = buf + r * 32 + kw;
+        const float *base = buf + (m >> 2) * 36 + k;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const float x = base[((2 * i + kh) ^ gg) << 2];
+            const float x = base[8 * i];
             acc = __fadd_rn(acc, __fmul_rn(x, x));
         }
     }
     if constexpr (!FULL) {
 #pragma unroll 1
         for (; m < steps; ++m) {
-            const float x = buf[Swz<E>::elem(k + 8 * m)];
+            const float x = buf[PadLayout<E>::elem(k + 8 * m)];
             acc = __fadd_rn(acc, __fmul_rn(x, x));
         }
     }
@@ -274,8 +285,8 @@ __device__ __forceinline__ float chain_sq_reduce2(const float *buf, int n, int l
     if constexpr (FULL) return s;
     int b = n & ~7, r = n - b;
     if (r >= 4) {
-        const float x0 = buf[Swz<E>::elem(b)], x1 = buf[Swz<E>::elem(b + 1)];
-        const float x2 = buf[Swz<E>::elem(b + 2)], x3 = buf[Swz<E>::elem(b + 3)];
+        const float x0 = buf[PadLayout<E>::elem(b)], x1 = buf[PadLayout<E>::elem(b + 1)];
+        const float x2 = buf[PadLayout<E>::elem(b + 2)], x3 = buf[PadLayout<E>::elem(b + 3)];
         t0 = __fmaf_rn(x0, x0, t0);
         t1 = __fmaf_rn(x1, x1, t1);
         t2 = __fmaf_rn(x2, x2, t2);
@@ -285,7 +296,7 @@ __device__ __forceinline__ float chain_sq_reduce2(const float *buf, int n, int l
         r -= 4;
     }
     for (int j = 0; j < r; ++j) {
-        const float x = buf[Swz<E>::elem(b + j)];
+        const float x = buf[PadLayout<E>::elem(b + j)];
         s = __fmaf_rn(x, x, s);
     }
     return s;
@@ -340,7 +351,7 @@ __device__ __forceinline__ void lane_stages(u64 (&p)[E / 2], int lane) {
     }
 }
 
-// RHT of one vector held in `buf` (Swz<E>): optional pre-multiply, sign flip
+// RHT of one vector held in `buf` (PadLayout<E>): optional pre-multiply, sign flip
 // from `sbits` (bit t: element lane*E + t is +1), FWHT, post-multiply.  The
 // result is left in layout B in `out` (E values: element 32 t + lane).
 template <int E, bool PREMUL>
@@ -349,7 +360,7 @@ __device__ __forceinline__ void rht2(float *buf, int lane, float pre, uint32_t s
     u64 p[E / 2];
 #pragma unroll
     for (int k = 0; k < E / 4; ++k) {
-        const float4 x = *reinterpret_cast<const float4 *>(buf + Swz<E>::chunk(lane * (E / 4) + k));
+        const float4 x = *reinterpret_cast<const float4 *>(buf + PadLayout<E>::chunk(lane * (E / 4) + k));
         p[2 * k] = mk2(x.x, x.y);
         p[2 * k + 1] = mk2(x.z, x.w);
     }
@@ -368,12 +379,12 @@ __device__ __forceinline__ void rht2(float *buf, int lane, float pre, uint32_t s
         float a, b, c, d;
         un2(p[2 * k], a, b);
         un2(p[2 * k + 1], c, d);
-        *reinterpret_cast<float4 *>(buf + Swz<E>::chunk(lane * (E / 4) + k)) = make_float4(a, b, c, d);
+        *reinterpret_cast<float4 *>(buf + PadLayout<E>::chunk(lane * (E / 4) + k)) = make_float4(a, b, c, d);
     }
     __syncwarp();
 #pragma unroll
     for (int i = 0; i < E / 2; ++i)
-        p[i] = mk2(buf[Swz<E>::elem(32 * (2 * i) + lane)], buf[Swz<E>::elem(32 * (2 * i + 1) + lane)]);
+        p[i] = mk2(buf[PadLayout<E>::elem(32 * (2 * i) + lane)], buf[PadLayout<E>::elem(32 * (2 * i + 1) + lane)]);
     reg_stages<E>(p);
     const u64 post2 = mk2(post, post);
 #pragma unroll
@@ -384,12 +395,12 @@ __device__ __forceinline__ void rht2(float *buf, int lane, float pre, uint32_t s
     __syncwarp();
 }
 
-// Per-warp shared bytes of encode2: 4 vectors of D+8 floats, the quantizer
-// indices of 4 vectors (D bytes each, one 32-bit word per lane and 4
-// positions), 4 staged codes.
+// Per-warp shared bytes of encode2: 4 padded vectors, the quantizer indices
+// of 4 vectors (D bytes each, one 32-bit word per lane and 4 positions), 4
+// staged codes.
 template <int LOG_D>
 __host__ __device__ constexpr int encode2_warp_bytes_c(int cs) {
-    return 16 * ((1 << LOG_D) + 8) + 4 * (1 << LOG_D) + align16(4 * cs);
+    return 16 * vec_row_floats<(1 << LOG_D)>() + 4 * (1 << LOG_D) + align16(4 * cs);
 }
 
 template <int LOG_D, bool NIBBLE>
@@ -398,7 +409,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                                                       DevTables T) {
     constexpr int D = 1 << LOG_D;
     constexpr int E = D / 32;
-    constexpr int VS = D + 8;
+    constexpr int VS = vec_row_floats<D>();
     static_assert(E >= 8 && E <= 32, "encode2 covers D = 256..1024");
     extern __shared__ __align__(16) unsigned char smem[];
     load_tables(smem, P, T, true);
@@ -431,25 +442,41 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
         const size_t row0 = qd << 2;
         const int nv = !active ? 0 : ((n - row0 < 4) ? (int)(n - row0) : 4);
         float norm = 0.0f, inv_norm = 0.0f;
+        // the rows of this warp's next quad go to L2 while this one is encoded
+        if (vec4 && lane == 0) {
+            const size_t nrow0 = (qd + (size_t)gridDim.x * nwarps) << 2;
+            if (nrow0 < n) {
+                const size_t rows = (n - nrow0 < 4) ? (n - nrow0) : 4;
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(X + nrow0 * (size_t)P.dim),
+                             "r"((uint32_t)(rows * (size_t)P.dim * 4)) : "memory");
+            }
+        }
         // A: rows -> buffers (zero padded); B: norm
         if (active) {
             if (vec4) {
+                // every 16-byte chunk as an async copy (all in flight at
+                // once); the zero padding past dim as plain stores
                 const int d4 = P.dim >> 2;
 #pragma unroll 4
                 for (int i = lane; i < D; i += 32) {  // i = v * (D/4) + chunk
                     const int v = i / (D / 4), i4 = i % (D / 4);
-                    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (v < nv && i4 < d4)
-                        x = __ldcs(reinterpret_cast<const float4 *>(X + (row0 + v) * (size_t)P.dim) + i4);
-                    *reinterpret_cast<float4 *>(buf + v * VS + Swz<E>::chunk(i4)) = x;
+                    float *dst = buf + v * VS + PadLayout<E>::chunk(i4);
+                    if (v < nv && i4 < d4) {
+                        const float *src = X + (row0 + v) * (size_t)P.dim + 4 * i4;
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)),
+                                     "l"(src) : "memory");
+                    } else {
+                        *reinterpret_cast<float4 *>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
                 }
+                asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
             } else {
 #pragma unroll 1
                 for (int v = 0; v < 4; ++v) {
                     const float *src = X + (row0 + v) * (size_t)P.dim;
 #pragma unroll 1
                     for (int i = lane; i < D; i += 32)
-                        buf[v * VS + Swz<E>::elem(i)] = (v < nv && i < P.dim) ? __ldcs(src + i) : 0.0f;
+                        buf[v * VS + PadLayout<E>::elem(i)] = (v < nv && i < P.dim) ? __ldcs(src + i) : 0.0f;
                 }
             }
             __syncwarp();
@@ -467,7 +494,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 float x[E];
                 rht2<E, true>(b, lane, __shfl_sync(kFull, inv_norm, 8 * v), rbits, P.wht_scale, x);
 #pragma unroll
-                for (int t = 0; t < E; ++t) b[Swz<E>::elem(32 * t + lane)] = x[t];
+                for (int t = 0; t < E; ++t) b[PadLayout<E>::elem(32 * t + lane)] = x[t];
             }
             __syncwarp();
             const float var = chain_sq_reduce2<E, true>(buf + g * VS, D, lane);
@@ -484,24 +511,46 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
         // the per-warp index array; F: gamma
         float gamma = 0.0f;
         if (active) {
+            // Every Lloyd-Max table of b = 6..9 has at most one boundary per
+            // bucket (qlut_k = 1): idx = lo + (z > B[lo]) with no loop and no
+            // branch, so the unrolled elements' load chains overlap.
+            const bool fastq = P.lutq && P.qlut_k == 1;
 #pragma unroll 1
             for (int v = 0; v < 4; ++v) {
                 const float sg = __shfl_sync(kFull, sigma, 8 * v);
                 const float isg = __shfl_sync(kFull, inv_sigma, 8 * v);
                 float *b = buf + v * VS;
-#pragma unroll 2
-                for (int t4 = 0; t4 < E / 4; ++t4) {
-                    uint32_t word = 0u;
+                // This lane's E values are loaded first, quantized in
+                // registers and stored afterwards: a store into the buffer
+                // between two of its loads would order every element's chain
+                // of table loads after the previous one's.
+                float xr[E];
+                uint32_t wq[E / 4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int p = Swz<E>::elem(32 * (4 * t4 + q) + lane);
-                        const float x = b[p];
-                        const int idx = quantize_compact(__fmul_rn(x, isg), P, s_bnd, s_qlut);
-                        b[p] = __fmaf_rn(-s_cent[idx], sg, x);
-                        word |= (uint32_t)idx << (8 * q);
+                for (int t = 0; t < E; ++t) xr[t] = b[PadLayout<E>::elem(32 * t + lane)];
+                if (fastq) {
+#pragma unroll
+                    for (int t = 0; t < E; ++t) {
+                        const float z = __fmul_rn(xr[t], isg);
+                        float y = __fmaf_rn(z, P.qlut_s, P.qlut_c);
+                        y = fminf(fmaxf(y, 0.0f), (float)(kQlutBuckets - 1));
+                        int idx = s_qlut[(int)y];
+                        idx = (idx + ((z > s_bnd[idx]) ? 1 : 0)) & 0xFF;
+                        xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
+                        wq[t >> 2] = ((t & 3) ? wq[t >> 2] : 0u) | ((uint32_t)idx << (8 * (t & 3)));
                     }
-                    idxw[(v * (E / 4) + t4) * 32 + lane] = word;
+                } else {
+#pragma unroll
+                    for (int t = 0; t < E; ++t) {
+                        const int idx = quantize_compact(__fmul_rn(xr[t], isg), P, s_bnd, s_qlut);
+                        xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
+                        wq[t >> 2] = ((t & 3) ? wq[t >> 2] : 0u) | ((uint32_t)idx << (8 * (t & 3)));
+                    }
                 }
+#pragma unroll
+                for (int t = 0; t < E; ++t) b[PadLayout<E>::elem(32 * t + lane)] = xr[t];
+#pragma unroll
+                for (int t4 = 0; t4 < E / 4; ++t4) idxw[(v * (E / 4) + t4) * 32 + lane] = wq[t4];
             }
             __syncwarp();
             gamma = __fsqrt_rn(chain_sq_reduce2<E, true>(buf + g * VS, D, lane));
@@ -514,9 +563,12 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 float x[E];
                 rht2<E, false>(buf + v * VS, lane, 1.0f, qbits, P.wht_scale, x);
                 uint8_t *st = stage + v * cs;
+                uint32_t wq[E / 4];  // all index words first: no load after a store
+#pragma unroll
+                for (int t4 = 0; t4 < E / 4; ++t4) wq[t4] = idxw[(v * (E / 4) + t4) * 32 + lane];
 #pragma unroll
                 for (int t4 = 0; t4 < E / 4; ++t4) {
-                    const uint32_t word = idxw[(v * (E / 4) + t4) * 32 + lane];
+                    const uint32_t word = wq[t4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int t = 4 * t4 + q;
