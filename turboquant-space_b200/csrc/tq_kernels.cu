@@ -1323,22 +1323,137 @@ __device__ __forceinline__ float scan8_distance(float ipr, float sb, float t0, f
     return d > 0.0f ? d : 0.0f;
 }
 
-template <int WPL, int NW, int S>
-constexpr int scan8t_smem_bytes() {
-    return 65536 + NW * S * (4 * (128 * WPL + 12) + 8);
+// ---------------------------------------------------------------------------
+// Unit policies of the staged scan.  A code's packed part is PB = 128 WPL
+// bytes, read by lane l as words l + 32 j (j < WPL).
+//   ByteUnits   (bits >= 5, D = 128 WPL): one unit per byte; one 4-byte lookup
+//               per coordinate (scan8_terms).
+//   NibbleUnits (bits <= 4, D = 256 WPL): two units per byte; the table row of
+//               byte value u holds the pair (c[lo >> 1], c[hi >> 1]) of its
+//               low and high nibble in each lane column (8 bytes), so one
+//               8-byte lookup gives both coordinates of a byte and feeds a
+//               packed FP32x2 FMA with the query pair (q[2b], q[2b + 1]).
+// Both tables are 256 rows x 256 bytes (64 KB), lane-replicated.
+// ---------------------------------------------------------------------------
+template <int WPL>
+struct ByteUnits {
+    static constexpr int kWPL = WPL, PB = 128 * WPL;
+    using Query = Scan8Query<WPL>;
+    __device__ static __forceinline__ void setup(const float *qr, const float *sq, unsigned char *tab,
+                                                 const DevTables &T, float *s_red, Query &Q,
+                                                 int &ssum, float &step) {
+        scan8_setup<WPL>(qr, sq, tab, T, s_red, Q, ssum, step);
+    }
+    __device__ static __forceinline__ void terms(const uint32_t (&w)[WPL], const Query &Q,
+                                                 const unsigned char *tab, int lane, float &ip,
+                                                 float &sg) {
+        scan8_terms<WPL, true>(w, Q, tab, (uint32_t)lane * 4u, ip, sg);
+    }
+};
+
+template <int WPL>
+struct NibbleQuery {
+    unsigned long long qr2[4 * WPL];  // (q[2b], q[2b + 1]) of byte b = 4 (lane + 32 j) + k
+    int she[WPL], sho[WPL];           // s_q fixed point of the even / odd coordinates, high bytes
+    unsigned sle[WPL], slo[WPL];      // ... low bytes
+};
+
+template <int WPL>
+struct NibbleUnits {
+    static constexpr int kWPL = WPL, PB = 128 * WPL;
+    static constexpr int D = 256 * WPL;
+    using Query = NibbleQuery<WPL>;
+    __device__ static __forceinline__ void setup(const float *qr_g, const float *sq_g,
+                                                 unsigned char *tab, const DevTables &T,
+                                                 float *s_red, Query &Q, int &ssum, float &step) {
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+        for (int i = tid; i < 256 * 64; i += blockDim.x) {
+            const int u = i >> 6, half = i & 1;  // row u, float (lane, half) of the row
+            const int unit = half ? (u >> 4) : (u & 15);
+            reinterpret_cast<float *>(tab + u * 256)[i & 63] = T.centroids[unit >> 1];
+        }
+        float mx = 0.0f;
+        for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
+        if (lane == 0) s_red[warp] = mx;
+        __syncthreads();
+        mx = s_red[0];
+        for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
+        step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
+        const float inv_step = 1.0f / step;
+        int sum = 0;
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) {
+            unsigned eh = 0, el = 0, oh = 0, ol = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int b = 4 * (lane + 32 * j) + k;
+                Q.qr2[4 * j + k] = pack2(qr_g[2 * b], qr_g[2 * b + 1]);
+                int ve = __float2int_rn(sq_g[2 * b] * inv_step);
+                int vo = __float2int_rn(sq_g[2 * b + 1] * inv_step);
+                ve = max(-32767, min(32767, ve));
+                vo = max(-32767, min(32767, vo));
+                sum += ve + vo;
+                eh |= ((unsigned)(ve >> 8) & 0xFFu) << (8 * k);
+                el |= ((unsigned)ve & 0xFFu) << (8 * k);
+                oh |= ((unsigned)(vo >> 8) & 0xFFu) << (8 * k);
+                ol |= ((unsigned)vo & 0xFFu) << (8 * k);
+            }
+            Q.she[j] = (int)eh;
+            Q.sle[j] = el;
+            Q.sho[j] = (int)oh;
+            Q.slo[j] = ol;
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+        ssum = sum;
+        __syncthreads();
+    }
+    __device__ static __forceinline__ void terms(const uint32_t (&w)[WPL], const Query &Q,
+                                                 const unsigned char *tab, int lane, float &ip,
+                                                 float &sg) {
+        const uint32_t lane8 = (uint32_t)lane * 8u;
+        unsigned long long acc2 = 0ull;
+        int acc_hi = 0;
+        unsigned acc_lo = 0;
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) {
+            const uint32_t x = w[j];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const unsigned long long cv = *reinterpret_cast<const unsigned long long *>(
+                    tab + __byte_perm(x, lane8, 0x6504u | ((uint32_t)k << 4)));
+                acc2 = ffma2(Q.qr2[4 * j + k], cv, acc2);
+            }
+            const uint32_t be = x & 0x01010101u, bo = (x >> 4) & 0x01010101u;
+            acc_hi = __dp4a((int)be, Q.she[j], acc_hi);
+            acc_lo = __dp4a(be, Q.sle[j], acc_lo);
+            acc_hi = __dp4a((int)bo, Q.sho[j], acc_hi);
+            acc_lo = __dp4a(bo, Q.slo[j], acc_lo);
+        }
+        ip = sum2(acc2);
+        sg = (float)(acc_hi * 256 + (int)acc_lo);  // exact: |.| < 2^22
+    }
+};
+
+template <int PB, int NW, int S>
+constexpr int scant_smem_bytes() {
+    return 65536 + NW * S * (4 * (PB + 12) + 8);
 }
 
-template <int WPL, int NW, int S, bool PACK>
-__global__ void __launch_bounds__(NW * 32, 1) scan8t_kernel(const float *__restrict__ q_rot,
-                                                            const float *__restrict__ s_q,
-                                                            const float *__restrict__ norms,
-                                                            const uint8_t *__restrict__ codes,
-                                                            size_t n, float *__restrict__ out,
-                                                            Params P, DevTables T) {
-    constexpr int D = 128 * WPL;
+template <class U, int NW, int S>
+__global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restrict__ q_rot,
+                                                           const float *__restrict__ s_q,
+                                                           const float *__restrict__ norms,
+                                                           const uint8_t *__restrict__ codes,
+                                                           size_t n, float *__restrict__ out,
+                                                           Params P, DevTables T) {
+    constexpr int WPL = U::kWPL;
+    constexpr int PB = U::PB;                // packed bytes per code (trailer offset)
     static_assert(S >= 2, "the ring needs two stages");
-    constexpr uint32_t GB = 4u * (D + 12);  // bytes per group of 4 codes
-    constexpr int CW = (D + 12) / 4;        // words per code
+    constexpr uint32_t GB = 4u * (PB + 12);  // bytes per group of 4 codes
+    constexpr int CW = (PB + 12) / 4;        // words per code
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ float s_red[NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1361,12 +1476,11 @@ __global__ void __launch_bounds__(NW * 32, 1) scan8t_kernel(const float *__restr
             bulk_load(smem_u32(ring + s * GB), codes + (gw + (size_t)s * TW) * GB, GB, bar);
         }
     }
-    Scan8Query<WPL> Q;
+    typename U::Query Q;
     int ssum;
     float step;
-    scan8_setup<WPL>(q_rot, s_q, tab, T, s_red, Q, ssum, step);
+    U::setup(q_rot, s_q, tab, T, s_red, Q, ssum, step);
     const float qn2 = norms[0], qn = norms[1], sc = P.scale;
-    const uint32_t lane4 = (uint32_t)lane * 4u;
     const bool kind0 = !(lane & 4);                               // holds a centroid dot
     const int ec = 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1);      // code of the group
 
@@ -1382,7 +1496,7 @@ __global__ void __launch_bounds__(NW * 32, 1) scan8t_kernel(const float *__restr
         const size_t ce = 4 * (gw + ke * TW) + ec;
         float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
         if (ev) {
-            const float *tm = reinterpret_cast<const float *>(codes + ce * (D + 12) + D);
+            const float *tm = reinterpret_cast<const float *>(codes + ce * (PB + 12) + PB);
             t0 = __ldg(tm);
             t1 = __ldg(tm + 1);
             t2 = __ldg(tm + 2);
@@ -1402,8 +1516,7 @@ __global__ void __launch_bounds__(NW * 32, 1) scan8t_kernel(const float *__restr
                 for (int j = 0; j < WPL; ++j) w[c][j] = sw[c * CW + lane + 32 * j];
             float v[8];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
-                scan8_terms<WPL, PACK>(w[c], Q, tab, lane4, v[2 * c], v[2 * c + 1]);
+            for (int c = 0; c < 4; ++c) U::terms(w[c], Q, tab, lane, v[2 * c], v[2 * c + 1]);
             const float y = transpose8(v, lane);
             R = ((lane & 3) == i) ? y : R;
             __syncwarp();
@@ -1442,18 +1555,18 @@ __global__ void __launch_bounds__(NW * 32, 1) scan8t_kernel(const float *__restr
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const size_t cc = 4 * G + ((size_t)c < r ? (size_t)c : r - 1);
-            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + cc * (D + 12));
+            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + cc * (PB + 12));
 #pragma unroll
             for (int j = 0; j < WPL; ++j) w[c][j] = __ldg(cw + lane + 32 * j);
         }
         float v[8];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) scan8_terms<WPL, PACK>(w[c], Q, tab, lane4, v[2 * c], v[2 * c + 1]);
+        for (int c = 0; c < 4; ++c) U::terms(w[c], Q, tab, lane, v[2 * c], v[2 * c + 1]);
         const float y = transpose8(v, lane);
         const float sb = __shfl_down_sync(kFull, y, 4);
         if (kind0 && (lane & 3) == 0 && (size_t)ec < r) {
             const size_t ce = 4 * G + ec;
-            const float *tm = reinterpret_cast<const float *>(codes + ce * (D + 12) + D);
+            const float *tm = reinterpret_cast<const float *>(codes + ce * (PB + 12) + PB);
             out[ce] = scan8_distance(y, sb, __ldg(tm), __ldg(tm + 1), __ldg(tm + 2), step, ssum, sc,
                                      qn2, qn);
         }
@@ -1686,13 +1799,13 @@ cudaError_t scan_launch(const Params &P, const DevTables &T, const float *q_rot,
 // 16 warps (4 per scheduler) with ~8 KB rings measured fastest on B200 at
 // 10M x 1036-byte codes (12 warps x 3 stages: 80%, 16 x 2: 85% of the copy
 // bandwidth; 13 or 14 warps are slower than 12).
-template <int WPL, int NW, int S, bool PACK>
-cudaError_t scan8t_launch(const Params &P, const DevTables &T, const float *q_rot,
-                          const float *s_q, const float *norms, const uint8_t *codes, size_t n,
-                          float *out, cudaStream_t st) {
-    auto kern = scan8t_kernel<WPL, NW, S, PACK>;
-    constexpr int smem = scan8t_smem_bytes<WPL, NW, S>();
-    static_assert(smem <= kSmemBudget - 64, "scan8t rings exceed shared memory");
+template <class U, int NW, int S>
+cudaError_t scant_launch(const Params &P, const DevTables &T, const float *q_rot,
+                         const float *s_q, const float *norms, const uint8_t *codes, size_t n,
+                         float *out, cudaStream_t st) {
+    auto kern = scant_kernel<U, NW, S>;
+    constexpr int smem = scant_smem_bytes<U::PB, NW, S>();
+    static_assert(smem <= kSmemBudget - 64, "scan rings exceed shared memory");
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const size_t groups = n / 4;
@@ -1713,7 +1826,7 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
     } else {
         constexpr int WPL = (1 << LOG_D) / 128;
         if (m == 1 && (reinterpret_cast<uintptr_t>(codes) & 15) == 0)
-            return scan8t_launch<WPL, 16, 8400 / (4 * (128 * WPL + 12)), true>(
+            return scant_launch<ByteUnits<WPL>, 16, 8400 / (4 * (128 * WPL + 12))>(
                 P, T, q_rot, s_q, norms, codes, n, out, st);
         auto kern = scan8b_kernel<WPL>;
         const int threads = 256;
@@ -1743,6 +1856,26 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
     }
 }
 
+// The staged 1->N scan of nibble codes at D = 256 .. 2048 (WPL = D / 256
+// words per lane); D = 2048 needs more query registers, so 12 warps.
+template <int LOG_D>
+cudaError_t scan4t_launch(const Params &P, const DevTables &T, const float *q_rot,
+                          const float *s_q, const float *norms, const uint8_t *codes, size_t n,
+                          float *out, cudaStream_t st) {
+    if constexpr (LOG_D < 8 || LOG_D > 11) {
+        return cudaErrorNotSupported;
+    } else {
+        constexpr int WPL = (1 << LOG_D) / 256;
+        constexpr int GB = 4 * (128 * WPL + 12);
+        if constexpr (WPL <= 4)
+            return scant_launch<NibbleUnits<WPL>, 16, 8400 / GB>(P, T, q_rot, s_q, norms, codes, n,
+                                                                 out, st);
+        else
+            return scant_launch<NibbleUnits<WPL>, 12, 12600 / GB>(P, T, q_rot, s_q, norms, codes,
+                                                                  n, out, st);
+    }
+}
+
 template <int LOG_D>
 struct ScanRun {
     static cudaError_t run(const Params &P, const DevTables &T, const float *q_rot,
@@ -1751,6 +1884,9 @@ struct ScanRun {
                            cudaStream_t st) {
         if (!P.nibble && !sym && LOG_D >= 7 && LOG_D <= 10)
             return scan8_launch<LOG_D>(P, T, q_rot, s_q, norms, m, codes, n, out, ldo, st);
+        if (P.nibble && !sym && m == 1 && LOG_D >= 8 && LOG_D <= 11 &&
+            (reinterpret_cast<uintptr_t>(codes) & 15) == 0)
+            return scan4t_launch<LOG_D>(P, T, q_rot, s_q, norms, codes, n, out, st);
         if (P.nibble) {
             return sym ? scan_launch<LOG_D, true, true>(P, T, q_rot, s_q, norms, codes_a, m, codes,
                                                         n, out, ldo, st)
