@@ -630,15 +630,21 @@ __global__ void __launch_bounds__(256) prepare_kernel(const float *__restrict__ 
         for (int i = lane; i < D; i += 32) buf[swz(i)] = (i < P.dim) ? src[i] : 0.0f;
         __syncwarp();
         // |q|^2: the reference's batch drivers evaluate this loop as a plain
-        // sequential sum (:443-445).
+        // sequential sum (:443-445).  Lane 0 keeps the order; the squares of
+        // each run of 32 elements are formed by their lanes and handed over
+        // by shuffles, so the chain waits only on its adds.
         float qn2 = 0.0f;
-        if (lane == 0) {
-            for (int i = 0; i < P.dim; ++i) {
-                const float x = buf[swz(i)];
-                qn2 = __fadd_rn(qn2, __fmul_rn(x, x));
+        for (int i0 = 0; i0 < P.dim; i0 += 32) {
+            const int i = i0 + lane;
+            const float x = (i < P.dim) ? buf[swz(i)] : 0.0f;
+            const float sq = __fmul_rn(x, x);
+            const int cnt = (P.dim - i0 < 32) ? (P.dim - i0) : 32;
+#pragma unroll
+            for (int t = 0; t < 32; ++t) {
+                const float v = __shfl_sync(kFull, sq, t);
+                if (t < cnt) qn2 = __fadd_rn(qn2, v);
             }
         }
-        qn2 = __shfl_sync(kFull, qn2, 0);
         const float qn = __fsqrt_rn(qn2);
         const float qinv = (qn2 > f32_bits(kNormSqFloorBits)) ? __fdiv_rn(1.0f, qn) : 0.0f;
         fwht_from<LOG_D, 0, true>(buf, lane, qinv, s_rot, P.wht_scale);
@@ -832,7 +838,8 @@ __device__ __forceinline__ float sum2(unsigned long long v) {
 }
 
 // ---------------------------------------------------------------------------
-// scan8: the asymmetric scan for byte units (bits >= 5) at D = 128 * WPL.
+// The byte-unit scan arithmetic (bits >= 5, D = 128 * WPL), shared by scan8b
+// and the staged scan (scan8_setup / scan8_terms).
 // A code is read as D/4 32-bit words, word l + 32 j by lane l; each lane owns
 // positions p = 4 (l + 32 j) + b and keeps q_rot[p] in registers.
 //   centroid term: shared memory holds one 256-byte row per unit byte u whose
@@ -847,340 +854,6 @@ __device__ __forceinline__ float sum2(unsigned long long v) {
 //     The fixed-point error enters only the correction term scale*gamma*dot
 //     (space_turbo_quant.h:683), where it is below 1e-6 of the distance's
 //     term scale at the sizes used here.
-// U codes per warp step; the next step's words are loaded before the current
-// step is reduced (transpose reduction: 2U values over 32 lanes).
-// ---------------------------------------------------------------------------
-template <int WPL, int U>
-__global__ void __launch_bounds__(256, 2) scan8_kernel(const float *__restrict__ q_rot,
-                                                       const float *__restrict__ s_q,
-                                                       const float *__restrict__ norms,
-                                                       const uint8_t *__restrict__ codes, size_t n,
-                                                       float *__restrict__ out, size_t ldo, Params P,
-                                                       DevTables T) {
-    static_assert(U == 2, "the transpose reduction below is written for 2 codes");
-    constexpr int D = 128 * WPL;
-    extern __shared__ __align__(16) unsigned char tab[];
-    __shared__ float s_red[8];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const size_t row = blockIdx.y;
-    const float *qr_g = q_rot + row * (size_t)D;
-    const float *sq_g = s_q + row * (size_t)D;
-    for (int i = tid; i < 256 * 32; i += blockDim.x)
-        reinterpret_cast<float *>(tab + (i >> 5) * 256)[i & 31] = T.centroids[(i >> 5) >> 1];
-    // fixed-point scale of s_q: step = max|s_q| / 32767
-    float mx = 0.0f;
-    for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
-    if (lane == 0) s_red[warp] = mx;
-    __syncthreads();
-    mx = s_red[0];
-    for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
-    const float step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
-    const float inv_step = 1.0f / step;
-    unsigned long long qr2[WPL * 2];  // q_rot of positions (4 (lane + 32 j) + 2 h, +1)
-    int shi[WPL];
-    unsigned slo[WPL];
-    int ssum = 0;
-#pragma unroll
-    for (int j = 0; j < WPL; ++j) {
-        unsigned hi = 0, lo = 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int p = 4 * (lane + 32 * j) + b;
-            if (b & 1) qr2[2 * j + (b >> 1)] = pack2(qr_g[p - 1], qr_g[p]);
-            int v = __float2int_rn(sq_g[p] * inv_step);
-            v = max(-32767, min(32767, v));
-            ssum += v;
-            hi |= ((unsigned)(v >> 8) & 0xFFu) << (8 * b);
-            lo |= ((unsigned)v & 0xFFu) << (8 * b);
-        }
-        shi[j] = (int)hi;
-        slo[j] = lo;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) ssum += __shfl_xor_sync(kFull, ssum, off);
-    const float qn2 = norms[2 * row], qn = norms[2 * row + 1];
-    const float sc = P.scale;
-    __syncthreads();
-
-    const uint32_t lane4 = (uint32_t)lane * 4u;
-    const int cs = P.cs;
-    // after the reduction lane 0 finishes code 0 and lane 16 code 1 of a step
-    const int my_u = (lane == 0) ? 0 : ((lane == 16) ? 1 : -1);
-    const size_t stride = (size_t)gridDim.x * nw * U;
-    size_t c0 = ((size_t)blockIdx.x * nw + warp) * U;
-    float *orow = out + row * ldo;
-
-    uint32_t wn[U][WPL];
-    float tn0 = 0.0f, tn1 = 0.0f, tn2 = 0.0f;
-    auto load = [&](size_t base) {
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const size_t c = base + u;
-            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + c * (size_t)cs);
-#pragma unroll
-            for (int j = 0; j < WPL; ++j) wn[u][j] = (c < n) ? __ldg(cw + lane + 32 * j) : 0u;
-        }
-        if (my_u >= 0 && base + my_u < n) {
-            const float *m = reinterpret_cast<const float *>(codes + (base + my_u) * (size_t)cs + D);
-            tn0 = __ldg(m);
-            tn1 = __ldg(m + 1);
-            tn2 = __ldg(m + 2);
-        }
-    };
-    if (c0 < n) load(c0);
-    for (; c0 < n; c0 += stride) {
-        uint32_t w[U][WPL];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int j = 0; j < WPL; ++j) w[u][j] = wn[u][j];
-        const float t0 = tn0, t1 = tn1, t2 = tn2;
-        if (c0 + stride < n) load(c0 + stride);
-
-        float v[2 * U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            unsigned long long acc2 = 0ull;  // (even, odd) position partial sums
-            int acc_hi = 0;
-            unsigned acc_lo = 0;
-#pragma unroll
-            for (int j = 0; j < WPL; ++j) {
-                const uint32_t x = w[u][j];
-                float cv[4];
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const uint32_t a = __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4));
-                    cv[b] = *reinterpret_cast<const float *>(tab + a);
-                }
-                acc2 = ffma2(qr2[2 * j], pack2(cv[0], cv[1]), acc2);
-                acc2 = ffma2(qr2[2 * j + 1], pack2(cv[2], cv[3]), acc2);
-                const uint32_t bits = x & 0x01010101u;
-                acc_hi = __dp4a((int)bits, shi[j], acc_hi);
-                acc_lo = __dp4a(bits, slo[j], acc_lo);
-            }
-            v[2 * u] = sum2(acc2);
-            v[2 * u + 1] = (float)(acc_hi * 256 + (int)acc_lo);  // exact: |.| < 2^21
-        }
-        // transpose reduction of 4 values over 32 lanes (6 shuffles)
-        float w2[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const bool hi = lane & 16;
-            const float send = hi ? v[k] : v[k + 2];
-            const float keep = hi ? v[k + 2] : v[k];
-            w2[k] = keep + __shfl_xor_sync(kFull, send, 16);
-        }
-        float y;
-        {
-            const bool hi = lane & 8;
-            const float send = hi ? w2[0] : w2[1];
-            const float keep = hi ? w2[1] : w2[0];
-            y = keep + __shfl_xor_sync(kFull, send, 8);
-        }
-        y += __shfl_xor_sync(kFull, y, 4);
-        y += __shfl_xor_sync(kFull, y, 2);
-        y += __shfl_xor_sync(kFull, y, 1);
-        // lane holds value ((lane>>4)&1)*2 + ((lane>>3)&1): ip of code u at
-        // lane 16u, its sign sum at lane 16u + 8
-        const float sb = __shfl_down_sync(kFull, y, 8);
-        if (my_u >= 0) {
-            const size_t c = c0 + my_u;
-            if (c < n) {
-                const float dot = __fmul_rn(step, 2.0f * sb - (float)ssum);
-                const float ip_mse = __fmul_rn(y, t2);
-                const float corr = __fmul_rn(__fmul_rn(sc, t1), dot);
-                const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), t0), qn);
-                const float d = __fsub_rn(__fadd_rn(qn2, __fmul_rn(t0, t0)), __fmul_rn(2.0f, ipt));
-                orow[c] = d > 0.0f ? d : 0.0f;
-            }
-        }
-    }
-}
-
-// scan8b: the scan8 arithmetic with the per-code overhead moved out of the
-// step.  A warp owns batches of 16 consecutive codes and runs them as 8 steps
-// of 2 codes; the word registers of the next step are loaded (ping-pong, no
-// copies) before the current step is reduced, and code indices past the end
-// are clamped to the last code, so the loads need no bounds checks.  After
-// each step's transpose reduction the 8-lane group holding a value keeps it in
-// the lane whose (lane & 7) is the step, so after 8 steps lane l holds value
-// kind (l >> 3) & 1 of code 2 (l & 7) + (l >> 4): 16 lanes then finish the 16
-// codes together (trailer loaded at the start of the batch, one store each).
-// Per code this is the same sequence of roundings as scan8.
-// ---------------------------------------------------------------------------
-template <int WPL>
-__global__ void __launch_bounds__(256, 2) scan8b_kernel(const float *__restrict__ q_rot,
-                                                        const float *__restrict__ s_q,
-                                                        const float *__restrict__ norms,
-                                                        const uint8_t *__restrict__ codes, size_t n,
-                                                        float *__restrict__ out, size_t ldo, Params P,
-                                                        DevTables T) {
-    constexpr int D = 128 * WPL;
-    extern __shared__ __align__(16) unsigned char tab[];
-    __shared__ float s_red[8];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const size_t row = blockIdx.y;
-    const float *qr_g = q_rot + row * (size_t)D;
-    const float *sq_g = s_q + row * (size_t)D;
-    for (int i = tid; i < 256 * 32; i += blockDim.x)
-        reinterpret_cast<float *>(tab + (i >> 5) * 256)[i & 31] = T.centroids[(i >> 5) >> 1];
-    float mx = 0.0f;
-    for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
-    if (lane == 0) s_red[warp] = mx;
-    __syncthreads();
-    mx = s_red[0];
-    for (int k = 1; k < nw; ++k) mx = fmaxf(mx, s_red[k]);
-    const float step = (mx > 0.0f) ? mx / 32767.0f : 1.0f;
-    const float inv_step = 1.0f / step;
-    unsigned long long qr2[WPL * 2];
-    int shi[WPL];
-    unsigned slo[WPL];
-    int ssum = 0;
-#pragma unroll
-    for (int j = 0; j < WPL; ++j) {
-        unsigned hi = 0, lo = 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int p = 4 * (lane + 32 * j) + b;
-            if (b & 1) qr2[2 * j + (b >> 1)] = pack2(qr_g[p - 1], qr_g[p]);
-            int v = __float2int_rn(sq_g[p] * inv_step);
-            v = max(-32767, min(32767, v));
-            ssum += v;
-            hi |= ((unsigned)(v >> 8) & 0xFFu) << (8 * b);
-            lo |= ((unsigned)v & 0xFFu) << (8 * b);
-        }
-        shi[j] = (int)hi;
-        slo[j] = lo;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) ssum += __shfl_xor_sync(kFull, ssum, off);
-    const float qn2 = norms[2 * row], qn = norms[2 * row + 1];
-    const float sc = P.scale;
-    __syncthreads();
-
-    const uint32_t lane4 = (uint32_t)lane * 4u;
-    const size_t cs = (size_t)P.cs;
-    const size_t last = n - 1;
-    const size_t nbatch = (n + 15) >> 4;
-    const size_t bstride = (size_t)gridDim.x * nw;
-    size_t bt = (size_t)blockIdx.x * nw + warp;
-    if (bt >= nbatch) return;
-    const int ecode = 2 * (lane & 7) + (lane >> 4);  // the code this lane finishes
-    const bool eowner = !(lane & 8);
-    float *orow = out + row * ldo;
-
-    auto load = [&](uint32_t (&w)[2][WPL], size_t c0) {
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const size_t c = (c0 + u < last) ? c0 + u : last;
-            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + c * cs);
-#pragma unroll
-            for (int j = 0; j < WPL; ++j) w[u][j] = __ldg(cw + lane + 32 * j);
-        }
-    };
-    // one step: 2 codes -> the transpose-reduced value of this lane's group
-    auto reduce_step = [&](const uint32_t (&w)[2][WPL]) -> float {
-        float v[4];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            unsigned long long acc2 = 0ull;
-            int acc_hi = 0;
-            unsigned acc_lo = 0;
-#pragma unroll
-            for (int j = 0; j < WPL; ++j) {
-                const uint32_t x = w[u][j];
-                float cv[4];
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const uint32_t a = __byte_perm(x, lane4, 0x6504u | ((uint32_t)b << 4));
-                    cv[b] = *reinterpret_cast<const float *>(tab + a);
-                }
-                acc2 = ffma2(qr2[2 * j], pack2(cv[0], cv[1]), acc2);
-                acc2 = ffma2(qr2[2 * j + 1], pack2(cv[2], cv[3]), acc2);
-                const uint32_t bits = x & 0x01010101u;
-                acc_hi = __dp4a((int)bits, shi[j], acc_hi);
-                acc_lo = __dp4a(bits, slo[j], acc_lo);
-            }
-            v[2 * u] = sum2(acc2);
-            v[2 * u + 1] = (float)(acc_hi * 256 + (int)acc_lo);
-        }
-        float w2[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const bool hi = lane & 16;
-            const float send = hi ? v[k] : v[k + 2];
-            const float keep = hi ? v[k + 2] : v[k];
-            w2[k] = keep + __shfl_xor_sync(kFull, send, 16);
-        }
-        float y;
-        {
-            const bool hi = lane & 8;
-            const float send = hi ? w2[0] : w2[1];
-            const float keep = hi ? w2[1] : w2[0];
-            y = keep + __shfl_xor_sync(kFull, send, 8);
-        }
-        y += __shfl_xor_sync(kFull, y, 4);
-        y += __shfl_xor_sync(kFull, y, 2);
-        y += __shfl_xor_sync(kFull, y, 1);
-        return y;
-    };
-
-    uint32_t wa[2][WPL], wb[2][WPL];
-    load(wa, bt << 4);
-    for (;;) {
-        const size_t cbase = bt << 4;
-        const size_t next_bt = bt + bstride;
-        // trailer of the code this lane finishes (used after the 8 steps)
-        const size_t ce = cbase + (size_t)ecode;
-        const float *tm = reinterpret_cast<const float *>(codes + (ce < last ? ce : last) * cs + D);
-        const float t0 = __ldg(tm), t1 = __ldg(tm + 1), t2 = __ldg(tm + 2);
-        float R = 0.0f;
-#pragma unroll 1
-        for (int s = 0; s < 8; s += 2) {
-            load(wb, cbase + 2 * s + 2);
-            const float ya = reduce_step(wa);
-            R = ((lane & 7) == s) ? ya : R;
-            load(wa, (s + 2 < 8) ? cbase + 2 * s + 4 : (next_bt << 4));
-            const float yb = reduce_step(wb);
-            R = ((lane & 7) == s + 1) ? yb : R;
-        }
-        const float sb = __shfl_down_sync(kFull, R, 8);
-        if (eowner && ce < n) {
-            const float dot = __fmul_rn(step, 2.0f * sb - (float)ssum);
-            const float ip_mse = __fmul_rn(R, t2);
-            const float corr = __fmul_rn(__fmul_rn(sc, t1), dot);
-            const float ipt = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), t0), qn);
-            const float d = __fsub_rn(__fadd_rn(qn2, __fmul_rn(t0, t0)), __fmul_rn(2.0f, ipt));
-            orow[ce] = d > 0.0f ? d : 0.0f;
-        }
-        bt = next_bt;
-        if (bt >= nbatch) break;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// scan8t: the 1->N byte-unit scan (scan8's arithmetic) fed from shared memory.
-// The corpus is read as groups of 4 consecutive codes: 4 cs bytes, a multiple
-// of 16, so a group is one untiled bulk copy.  Warp w of the grid owns groups
-// w, w + TW, w + 2 TW, ... (TW = warps in the grid) and streams them with
-// cp.async.bulk into a private ring of S stages, one mbarrier per stage; lane
-// 0 refills a stage as soon as the warp has read it.  The bytes in flight per
-// SM are therefore set by the rings (NW x (S - 1) groups), not by registers.
-// Lane l reads word l + 32 j of every code from shared memory: consecutive
-// words, so the reads are conflict-free at any code offset.
-// Each stage gives 8 values (centroid dot and sign sum of 4 codes) that one
-// transpose reduction leaves in the lane groups of 4; across a batch of 4
-// stages lane l keeps the value of stage l & 3, and the 16 lanes with bit 2
-// clear then finish the batch's 16 codes (trailer, distance, store).
-// The last n mod 4 codes are read with plain loads by the warp that would own
-// group n / 4.  The caller guarantees a 16-byte aligned corpus.
-// ---------------------------------------------------------------------------
-constexpr int kErrScanWait = 5;  // status code: a scan stage never arrived
-
 template <int WPL>
 struct Scan8Query {
     unsigned long long qr2[2 * WPL];  // q_rot of positions 4 (lane + 32 j) + {0,1}, {2,3}
@@ -1322,6 +995,129 @@ __device__ __forceinline__ float scan8_distance(float ipr, float sb, float t0, f
     const float d = __fsub_rn(__fadd_rn(qn2, __fmul_rn(t0, t0)), __fmul_rn(2.0f, ipt));
     return d > 0.0f ? d : 0.0f;
 }
+
+// ---------------------------------------------------------------------------
+// scan8b: that arithmetic with registers fed by plain loads (any 4-byte
+// aligned corpus; query rows on grid.y).  A warp owns batches of 16
+// consecutive codes and runs them as 8 steps of 2 codes; the word registers of
+// the next step are loaded (ping-pong, no copies) before the current step is
+// reduced, and code indices past the end are clamped to the last code, so the
+// loads need no bounds checks.  After each step's transpose reduction the
+// 8-lane group holding a value keeps it in the lane whose (lane & 7) is the
+// step, so after 8 steps lane l holds value kind (l >> 3) & 1 of code
+// 2 (l & 7) + (l >> 4): 16 lanes then finish the 16 codes together (trailer
+// loaded at the start of the batch, one store each).  Per code this is the
+// same sequence of roundings as the staged scan's byte units.
+// ---------------------------------------------------------------------------
+template <int WPL>
+__global__ void __launch_bounds__(256, 2) scan8b_kernel(const float *__restrict__ q_rot,
+                                                        const float *__restrict__ s_q,
+                                                        const float *__restrict__ norms,
+                                                        const uint8_t *__restrict__ codes, size_t n,
+                                                        float *__restrict__ out, size_t ldo, Params P,
+                                                        DevTables T) {
+    constexpr int D = 128 * WPL;
+    extern __shared__ __align__(16) unsigned char tab[];
+    __shared__ float s_red[8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const size_t row = blockIdx.y;
+    Scan8Query<WPL> Q;
+    int ssum;
+    float step;
+    scan8_setup<WPL>(q_rot + row * (size_t)D, s_q + row * (size_t)D, tab, T, s_red, Q, ssum, step);
+    const float qn2 = norms[2 * row], qn = norms[2 * row + 1];
+    const float sc = P.scale;
+
+    const uint32_t lane4 = (uint32_t)lane * 4u;
+    const size_t cs = (size_t)P.cs;
+    const size_t last = n - 1;
+    const size_t nbatch = (n + 15) >> 4;
+    const size_t bstride = (size_t)gridDim.x * nw;
+    size_t bt = (size_t)blockIdx.x * nw + warp;
+    if (bt >= nbatch) return;
+    const int ecode = 2 * (lane & 7) + (lane >> 4);  // the code this lane finishes
+    const bool eowner = !(lane & 8);
+    float *orow = out + row * ldo;
+
+    auto load = [&](uint32_t (&w)[2][WPL], size_t c0) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const size_t c = (c0 + u < last) ? c0 + u : last;
+            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + c * cs);
+#pragma unroll
+            for (int j = 0; j < WPL; ++j) w[u][j] = __ldg(cw + lane + 32 * j);
+        }
+    };
+    // one step: 2 codes -> the transpose-reduced value of this lane's group
+    auto reduce_step = [&](const uint32_t (&w)[2][WPL]) -> float {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) scan8_terms<WPL, true>(w[u], Q, tab, lane4, v[2 * u], v[2 * u + 1]);
+        float w2[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const bool hi = lane & 16;
+            const float send = hi ? v[k] : v[k + 2];
+            const float keep = hi ? v[k + 2] : v[k];
+            w2[k] = keep + __shfl_xor_sync(kFull, send, 16);
+        }
+        float y;
+        {
+            const bool hi = lane & 8;
+            const float send = hi ? w2[0] : w2[1];
+            const float keep = hi ? w2[1] : w2[0];
+            y = keep + __shfl_xor_sync(kFull, send, 8);
+        }
+        y += __shfl_xor_sync(kFull, y, 4);
+        y += __shfl_xor_sync(kFull, y, 2);
+        y += __shfl_xor_sync(kFull, y, 1);
+        return y;
+    };
+
+    uint32_t wa[2][WPL], wb[2][WPL];
+    load(wa, bt << 4);
+    for (;;) {
+        const size_t cbase = bt << 4;
+        const size_t next_bt = bt + bstride;
+        // trailer of the code this lane finishes (used after the 8 steps)
+        const size_t ce = cbase + (size_t)ecode;
+        const float *tm = reinterpret_cast<const float *>(codes + (ce < last ? ce : last) * cs + D);
+        const float t0 = __ldg(tm), t1 = __ldg(tm + 1), t2 = __ldg(tm + 2);
+        float R = 0.0f;
+#pragma unroll 1
+        for (int s = 0; s < 8; s += 2) {
+            load(wb, cbase + 2 * s + 2);
+            const float ya = reduce_step(wa);
+            R = ((lane & 7) == s) ? ya : R;
+            load(wa, (s + 2 < 8) ? cbase + 2 * s + 4 : (next_bt << 4));
+            const float yb = reduce_step(wb);
+            R = ((lane & 7) == s + 1) ? yb : R;
+        }
+        const float sb = __shfl_down_sync(kFull, R, 8);
+        if (eowner && ce < n) orow[ce] = scan8_distance(R, sb, t0, t1, t2, step, ssum, sc, qn2, qn);
+        bt = next_bt;
+        if (bt >= nbatch) break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scan8t: the 1->N byte-unit scan (scan8's arithmetic) fed from shared memory.
+// The corpus is read as groups of 4 consecutive codes: 4 cs bytes, a multiple
+// of 16, so a group is one untiled bulk copy.  Warp w of the grid owns groups
+// w, w + TW, w + 2 TW, ... (TW = warps in the grid) and streams them with
+// cp.async.bulk into a private ring of S stages, one mbarrier per stage; lane
+// 0 refills a stage as soon as the warp has read it.  The bytes in flight per
+// SM are therefore set by the rings (NW x (S - 1) groups), not by registers.
+// Lane l reads word l + 32 j of every code from shared memory: consecutive
+// words, so the reads are conflict-free at any code offset.
+// Each stage gives 8 values (centroid dot and sign sum of 4 codes) that one
+// transpose reduction leaves in the lane groups of 4; across a batch of 4
+// stages lane l keeps the value of stage l & 3, and the 16 lanes with bit 2
+// clear then finish the batch's 16 codes (trailer, distance, store).
+// The last n mod 4 codes are read with plain loads by the warp that would own
+// group n / 4.  The caller guarantees a 16-byte aligned corpus.
+// ---------------------------------------------------------------------------
+constexpr int kErrScanWait = 5;  // status code: a scan stage never arrived
 
 // ---------------------------------------------------------------------------
 // Unit policies of the staged scan.  A code's packed part is PB = 128 WPL
