@@ -1,5 +1,5 @@
 """The staged 1->N scan against the oracle: byte units (bits >= 5, D 128 ..
-1024) and nibble units (bits <= 4, D 256 .. 2048).
+1024) and nibble units (bits <= 4, D 128 .. 2048).
 
 distance_1_to_n on a 16-byte aligned device corpus runs the staged kernel:
 groups of 4 codes are bulk-copied into per-warp shared-memory rings and the
@@ -19,9 +19,9 @@ from conftest import asym_term_scale, dist_close
 pytestmark = pytest.mark.gpu
 
 # (dim, bits): D = 128, 256, 512, 1024 with byte units (bits >= 5) and
-# D = 256, 512, 1024, 2048 with nibble units (bits <= 4)
+# D = 128 (a half-warp per code), 256, 512, 1024, 2048 with nibble units
 STAGED = [(128, 8), (200, 5), (500, 9), (768, 8), (1024, 6),
-          (256, 4), (300, 3), (768, 4), (1536, 2), (2048, 4)]
+          (128, 4), (100, 3), (256, 4), (300, 3), (768, 4), (1536, 2), (2048, 4)]
 COUNTS = [1, 2, 3, 4, 5, 7, 63, 1001, 4099]
 
 
@@ -70,7 +70,7 @@ def test_staged_scan_counts_vs_oracle(cuda_ok, dim, bits):
 
 
 @pytest.mark.parametrize("dim,bits,n", [(128, 8, 100003), (768, 8, 50001), (384, 4, 200003),
-                                        (1536, 4, 30001)])
+                                        (1536, 4, 30001), (128, 4, 300001)])
 def test_staged_scan_many_groups_per_warp(cuda_ok, dim, bits, n):
     """Enough codes that every warp wraps its ring several times and runs
     several 16-code batches, with a ragged tail."""

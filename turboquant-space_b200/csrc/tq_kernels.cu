@@ -1131,6 +1131,25 @@ constexpr int kErrScanWait = 5;  // status code: a scan stage never arrived
 //               packed FP32x2 FMA with the query pair (q[2b], q[2b + 1]).
 // Both tables are 256 rows x 256 bytes (64 KB), lane-replicated.
 // ---------------------------------------------------------------------------
+// A group of 4 codes with a whole warp per code (lane l reads words
+// l + 32 j): 8 values (centroid dot, sign sum of each code) reduced by one
+// transpose; value 2 c + kind of code c ends in the lanes with
+// 2 b4 + b3 = c, b2 = kind.  word(c, i) returns word i of code c.
+template <class U, class Word>
+__device__ __forceinline__ float full_warp_group(Word word, const typename U::Query &Q,
+                                                 const unsigned char *tab, int lane) {
+    constexpr int WPL = U::kWPL;
+    uint32_t w[4][WPL];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) w[c][j] = word(c, lane + 32 * j);
+    float v[8];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) U::terms(w[c], Q, tab, lane, v[2 * c], v[2 * c + 1]);
+    return transpose8(v, lane);
+}
+
 template <int WPL>
 struct ByteUnits {
     static constexpr int kWPL = WPL, PB = 128 * WPL;
@@ -1144,6 +1163,14 @@ struct ByteUnits {
                                                  const unsigned char *tab, int lane, float &ip,
                                                  float &sg) {
         scan8_terms<WPL, true>(w, Q, tab, (uint32_t)lane * 4u, ip, sg);
+    }
+    template <class Word>
+    __device__ static __forceinline__ float group(Word word, const Query &Q,
+                                                  const unsigned char *tab, int lane) {
+        return full_warp_group<ByteUnits<WPL>>(word, Q, tab, lane);
+    }
+    __device__ static __forceinline__ int code_of_lane(int lane) {
+        return 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1);
     }
 };
 
@@ -1162,14 +1189,23 @@ struct NibbleUnits {
     __device__ static __forceinline__ void setup(const float *qr_g, const float *sq_g,
                                                  unsigned char *tab, const DevTables &T,
                                                  float *s_red, Query &Q, int &ssum, float &step) {
+        setup_lanes(qr_g, sq_g, tab, T, s_red, Q, ssum, step, D, 31);
+    }
+    // dn: padded dim; lmask: the lane's word column is lane & lmask (31, or 15
+    // when half-warps share positions; then lanes >= 16 add nothing to ssum)
+    __device__ static __forceinline__ void setup_lanes(const float *qr_g, const float *sq_g,
+                                                       unsigned char *tab, const DevTables &T,
+                                                       float *s_red, Query &Q, int &ssum,
+                                                       float &step, int dn, int lmask) {
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+        const int col = lane & lmask;
         for (int i = tid; i < 256 * 64; i += blockDim.x) {
             const int u = i >> 6, half = i & 1;  // row u, float (lane, half) of the row
             const int unit = half ? (u >> 4) : (u & 15);
             reinterpret_cast<float *>(tab + u * 256)[i & 63] = T.centroids[unit >> 1];
         }
         float mx = 0.0f;
-        for (int i = tid; i < D; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
+        for (int i = tid; i < dn; i += blockDim.x) mx = fmaxf(mx, fabsf(sq_g[i]));
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
         if (lane == 0) s_red[warp] = mx;
@@ -1184,7 +1220,7 @@ struct NibbleUnits {
             unsigned eh = 0, el = 0, oh = 0, ol = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int b = 4 * (lane + 32 * j) + k;
+                const int b = 4 * (col + 32 * j) + k;
                 Q.qr2[4 * j + k] = pack2(qr_g[2 * b], qr_g[2 * b + 1]);
                 int ve = __float2int_rn(sq_g[2 * b] * inv_step);
                 int vo = __float2int_rn(sq_g[2 * b + 1] * inv_step);
@@ -1201,6 +1237,7 @@ struct NibbleUnits {
             Q.sho[j] = (int)oh;
             Q.slo[j] = ol;
         }
+        if (lane != col) sum = 0;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
         ssum = sum;
@@ -1231,11 +1268,75 @@ struct NibbleUnits {
         ip = sum2(acc2);
         sg = (float)(acc_hi * 256 + (int)acc_lo);  // exact: |.| < 2^22
     }
+    template <class Word>
+    __device__ static __forceinline__ float group(Word word, const Query &Q,
+                                                  const unsigned char *tab, int lane) {
+        return full_warp_group<NibbleUnits<WPL>>(word, Q, tab, lane);
+    }
+    __device__ static __forceinline__ int code_of_lane(int lane) {
+        return 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1);
+    }
 };
+
+// Nibble units at D = 128: a code is 64 packed bytes, 16 words, so a
+// half-warp takes one code: lane l reads word l & 15 of code 2 r + (l >> 4) of
+// the group (rows r = 0, 1).  The 4 values of a lane (dot and sign sum of its
+// two codes) are reduced within the half-warps; value (row b3, kind b2) of
+// code 2 b3 + b4 ends in the lane groups of 4 as in full_warp_group.
+struct HalfNibbleUnits {
+    static constexpr int kWPL = 1, PB = 64, D = 128;
+    using Query = NibbleQuery<1>;
+    __device__ static __forceinline__ void setup(const float *qr_g, const float *sq_g,
+                                                 unsigned char *tab, const DevTables &T,
+                                                 float *s_red, Query &Q, int &ssum, float &step) {
+        // the half-warps hold the same positions: lane & 15 in NibbleUnits<1>'s
+        // layout, and the sign sum counts each position once
+        NibbleUnits<1>::setup_lanes(qr_g, sq_g, tab, T, s_red, Q, ssum, step, 128, 15);
+    }
+    template <class Word>
+    __device__ static __forceinline__ float group(Word word, const Query &Q,
+                                                  const unsigned char *tab, int lane) {
+        float v[4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const uint32_t w[1] = {word(2 * r + (lane >> 4), lane & 15)};
+            NibbleUnits<1>::terms(w, Q, tab, lane, v[2 * r], v[2 * r + 1]);
+        }
+        float a[2];
+        const bool h8 = lane & 8;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float send = h8 ? v[k] : v[k + 2];
+            const float keep = h8 ? v[k + 2] : v[k];
+            a[k] = keep + __shfl_xor_sync(kFull, send, 8);
+        }
+        const bool h4 = lane & 4;
+        float y = (h4 ? a[1] : a[0]) + __shfl_xor_sync(kFull, h4 ? a[0] : a[1], 4);
+        y += __shfl_xor_sync(kFull, y, 2);
+        y += __shfl_xor_sync(kFull, y, 1);
+        return y;
+    }
+    __device__ static __forceinline__ int code_of_lane(int lane) {
+        return 2 * ((lane >> 3) & 1) + ((lane >> 4) & 1);
+    }
+};
+
+// Groups of 4 codes per ring stage: small codes are fetched several groups
+// at a time so that each bulk copy moves ~2 KB or more.
+template <int PB>
+constexpr int scant_gps() {
+    return (4 * (PB + 12) >= 2048) ? 1 : ((4 * (PB + 12) >= 1024) ? 2 : 4);
+}
+
+// Stages of a warp ring of about `ring` bytes (at least two).
+template <int PB>
+constexpr int scant_stages(int ring) {
+    return ring / (scant_gps<PB>() * 4 * (PB + 12)) < 2 ? 2 : ring / (scant_gps<PB>() * 4 * (PB + 12));
+}
 
 template <int PB, int NW, int S>
 constexpr int scant_smem_bytes() {
-    return 65536 + NW * S * (4 * (PB + 12) + 8);
+    return 65536 + NW * S * (scant_gps<PB>() * 4 * (PB + 12) + 8);
 }
 
 template <class U, int NW, int S>
@@ -1245,31 +1346,34 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
                                                            const uint8_t *__restrict__ codes,
                                                            size_t n, float *__restrict__ out,
                                                            Params P, DevTables T) {
-    constexpr int WPL = U::kWPL;
     constexpr int PB = U::PB;                // packed bytes per code (trailer offset)
     static_assert(S >= 2, "the ring needs two stages");
     constexpr uint32_t GB = 4u * (PB + 12);  // bytes per group of 4 codes
+    constexpr int GPS = scant_gps<PB>();     // groups per stage (a power of two)
+    constexpr uint32_t SB = GPS * GB;        // bytes per stage
     constexpr int CW = (PB + 12) / 4;        // words per code
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ float s_red[NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char *tab = smem;
-    unsigned char *ring = smem + 65536 + (size_t)warp * S * GB;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 65536 + (size_t)NW * S * GB) + warp * S;
+    unsigned char *ring = smem + 65536 + (size_t)warp * S * SB;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 65536 + (size_t)NW * S * SB) + warp * S;
     int *err = T.status;
 
-    const size_t G = n >> 2;
+    // super-group = one stage's GPS groups; warp gw owns super-groups gw, gw + TW, ...
+    const size_t SG = n / (4 * GPS);
     const size_t TW = (size_t)gridDim.x * NW;
     const size_t gw = (size_t)blockIdx.x * NW + warp;
-    const size_t K = gw < G ? (G - gw + TW - 1) / TW : 0;  // groups of this warp
+    const size_t K = gw < SG ? (SG - gw + TW - 1) / TW : 0;  // super-groups of this warp
+    const size_t KG = K * GPS;                               // groups of this warp
     // ring set-up and the first S copies, before the table build
     if (lane == 0) {
         for (int s = 0; s < S; ++s) mbar_init(smem_u32(bars + s), 1);
         mbar_init_fence();
         for (int s = 0; s < S && (size_t)s < K; ++s) {
             const uint32_t bar = smem_u32(bars + s);
-            mbar_expect_tx(bar, GB);
-            bulk_load(smem_u32(ring + s * GB), codes + (gw + (size_t)s * TW) * GB, GB, bar);
+            mbar_expect_tx(bar, SB);
+            bulk_load(smem_u32(ring + s * SB), codes + (gw + (size_t)s * TW) * SB, SB, bar);
         }
     }
     typename U::Query Q;
@@ -1278,18 +1382,19 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
     U::setup(q_rot, s_q, tab, T, s_red, Q, ssum, step);
     const float qn2 = norms[0], qn = norms[1], sc = P.scale;
     const bool kind0 = !(lane & 4);                               // holds a centroid dot
-    const int ec = 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1);      // code of the group
+    const int ec = U::code_of_lane(lane);                         // code of the group
 
-    const size_t src_step = TW * GB;
-    const uint8_t *src_next = codes + (gw + (size_t)S * TW) * GB;  // next group to fetch
+    const size_t src_step = TW * SB;
+    const uint8_t *src_next = codes + (gw + (size_t)S * TW) * SB;  // next super-group to fetch
     int s = 0;
     uint32_t ph = 0;
-    size_t k = 0;
+    size_t kg = 0;
     bool ok = true;
-    for (size_t k0 = 0; k0 < K; k0 += 4) {
+    for (size_t k0 = 0; k0 < KG; k0 += 4) {
+        // trailer of the code this lane finishes (group ke of this warp)
         const size_t ke = k0 + (lane & 3);
-        const bool ev = kind0 && ke < K;
-        const size_t ce = 4 * (gw + ke * TW) + ec;
+        const bool ev = kind0 && ke < KG;
+        const size_t ce = 4 * (GPS * (gw + (ke / GPS) * TW) + (ke % GPS)) + ec;
         float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
         if (ev) {
             const float *tm = reinterpret_cast<const float *>(codes + ce * (PB + 12) + PB);
@@ -1298,33 +1403,30 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
             t2 = __ldg(tm + 2);
         }
         float R = 0.0f;
-        const int nst = (K - k0 < 4) ? (int)(K - k0) : 4;
+        const int nst = (KG - k0 < 4) ? (int)(KG - k0) : 4;
 #pragma unroll 1
-        for (int i = 0; i < nst; ++i, ++k) {
+        for (int i = 0; i < nst; ++i, ++kg) {
+            const int sub = (int)(kg & (GPS - 1));
             const uint32_t bar = smem_u32(bars + s);
-            ok = __all_sync(kFull, mbar_wait(bar, ph, err, kErrScanWait));
-            if (!ok) break;
-            const uint32_t *sw = reinterpret_cast<const uint32_t *>(ring + s * GB);
-            uint32_t w[4][WPL];
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-#pragma unroll
-                for (int j = 0; j < WPL; ++j) w[c][j] = sw[c * CW + lane + 32 * j];
-            float v[8];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) U::terms(w[c], Q, tab, lane, v[2 * c], v[2 * c + 1]);
-            const float y = transpose8(v, lane);
-            R = ((lane & 3) == i) ? y : R;
-            __syncwarp();
-            if (lane == 0 && k + S < K) {
-                fence_proxy_async_smem();
-                mbar_expect_tx(bar, GB);
-                bulk_load(smem_u32(ring + s * GB), src_next, GB, bar);
-                src_next += src_step;
+            if (sub == 0) {
+                ok = __all_sync(kFull, mbar_wait(bar, ph, err, kErrScanWait));
+                if (!ok) break;
             }
-            if (++s == S) {
-                s = 0;
-                ph ^= 1u;
+            const uint32_t *sw = reinterpret_cast<const uint32_t *>(ring + s * SB + sub * GB);
+            const float y = U::group([&](int c, int wi) { return sw[c * CW + wi]; }, Q, tab, lane);
+            R = ((lane & 3) == i) ? y : R;
+            if (sub == GPS - 1) {
+                __syncwarp();
+                if (lane == 0 && kg / GPS + S < K) {
+                    fence_proxy_async_smem();
+                    mbar_expect_tx(bar, SB);
+                    bulk_load(smem_u32(ring + s * SB), src_next, SB, bar);
+                    src_next += src_step;
+                }
+                if (++s == S) {
+                    s = 0;
+                    ph ^= 1u;
+                }
             }
         }
         if (!ok) break;
@@ -1334,6 +1436,7 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
     if (!ok) {
         // wait (bounded) for this warp's copies still in flight, then leave
         if (lane == 0) {
+            const size_t k = kg / GPS;
             for (size_t j = k; j < K && j < k + S; ++j) {
                 mbar_drain(smem_u32(bars + s), ph);
                 if (++s == S) {
@@ -1344,31 +1447,29 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
         }
         return;
     }
-    // the last n mod 4 codes, read straight from global memory
-    const size_t r = n - 4 * G;
-    if (r > 0 && gw == G % TW) {
-        uint32_t w[4][WPL];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const size_t cc = 4 * G + ((size_t)c < r ? (size_t)c : r - 1);
-            const uint32_t *cw = reinterpret_cast<const uint32_t *>(codes + cc * (PB + 12));
-#pragma unroll
-            for (int j = 0; j < WPL; ++j) w[c][j] = __ldg(cw + lane + 32 * j);
-        }
-        float v[8];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) U::terms(w[c], Q, tab, lane, v[2 * c], v[2 * c + 1]);
-        const float y = transpose8(v, lane);
-        const float sb = __shfl_down_sync(kFull, y, 4);
-        if (kind0 && (lane & 3) == 0 && (size_t)ec < r) {
-            const size_t ce = 4 * G + ec;
-            const float *tm = reinterpret_cast<const float *>(codes + ce * (PB + 12) + PB);
-            out[ce] = scan8_distance(y, sb, __ldg(tm), __ldg(tm + 1), __ldg(tm + 2), step, ssum, sc,
-                                     qn2, qn);
+    // the last n mod (4 GPS) codes, read straight from global memory by the
+    // warp that would own super-group SG, one group at a time
+    const size_t c0 = 4 * GPS * SG;
+    if (c0 < n && gw == SG % TW) {
+        const uint32_t *cw0 = reinterpret_cast<const uint32_t *>(codes);
+        for (size_t b = c0; b < n; b += 4) {
+            const size_t r = (n - b < 4) ? (n - b) : 4;
+            const float y = U::group(
+                [&](int c, int wi) {
+                    const size_t cc = b + ((size_t)c < r ? (size_t)c : r - 1);
+                    return __ldg(cw0 + cc * CW + wi);
+                },
+                Q, tab, lane);
+            const float sb = __shfl_down_sync(kFull, y, 4);
+            if (kind0 && (lane & 3) == 0 && (size_t)ec < r) {
+                const size_t ce = b + ec;
+                const float *tm = reinterpret_cast<const float *>(codes + ce * (PB + 12) + PB);
+                out[ce] = scan8_distance(y, sb, __ldg(tm), __ldg(tm + 1), __ldg(tm + 2), step, ssum,
+                                         sc, qn2, qn);
+            }
         }
     }
 }
-
 // Codes whose packed part is narrower than one 32-bit word (D = 4 with
 // nibble packing: 2 bytes) are scanned one thread per code with byte loads.
 template <bool SYM>
@@ -1604,7 +1705,7 @@ cudaError_t scant_launch(const Params &P, const DevTables &T, const float *q_rot
     static_assert(smem <= kSmemBudget - 64, "scan rings exceed shared memory");
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    const size_t groups = n / 4;
+    const size_t groups = n / (4 * scant_gps<U::PB>());
     size_t blocks = (groups + NW - 1) / NW;
     const size_t cap = (size_t)sm_count();
     if (blocks > cap) blocks = cap;
@@ -1622,7 +1723,7 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
     } else {
         constexpr int WPL = (1 << LOG_D) / 128;
         if (m == 1 && (reinterpret_cast<uintptr_t>(codes) & 15) == 0)
-            return scant_launch<ByteUnits<WPL>, 16, 8400 / (4 * (128 * WPL + 12))>(
+            return scant_launch<ByteUnits<WPL>, 16, scant_stages<128 * WPL>(8400)>(
                 P, T, q_rot, s_q, norms, codes, n, out, st);
         auto kern = scan8b_kernel<WPL>;
         const int threads = 256;
@@ -1652,22 +1753,25 @@ cudaError_t scan8_launch(const Params &P, const DevTables &T, const float *q_rot
     }
 }
 
-// The staged 1->N scan of nibble codes at D = 256 .. 2048 (WPL = D / 256
-// words per lane); D = 2048 needs more query registers, so 12 warps.
+// The staged 1->N scan of nibble codes: D = 128 with a half-warp per code,
+// D = 256 .. 2048 with WPL = D / 256 words per lane (D = 2048 needs more query
+// registers, so 12 warps).
 template <int LOG_D>
 cudaError_t scan4t_launch(const Params &P, const DevTables &T, const float *q_rot,
                           const float *s_q, const float *norms, const uint8_t *codes, size_t n,
                           float *out, cudaStream_t st) {
-    if constexpr (LOG_D < 8 || LOG_D > 11) {
+    if constexpr (LOG_D < 7 || LOG_D > 11) {
         return cudaErrorNotSupported;
+    } else if constexpr (LOG_D == 7) {
+        return scant_launch<HalfNibbleUnits, 16, scant_stages<64>(8400)>(P, T, q_rot, s_q, norms, codes, n,
+                                                                 out, st);
     } else {
         constexpr int WPL = (1 << LOG_D) / 256;
-        constexpr int GB = 4 * (128 * WPL + 12);
         if constexpr (WPL <= 4)
-            return scant_launch<NibbleUnits<WPL>, 16, 8400 / GB>(P, T, q_rot, s_q, norms, codes, n,
+            return scant_launch<NibbleUnits<WPL>, 16, scant_stages<128 * WPL>(8400)>(P, T, q_rot, s_q, norms, codes, n,
                                                                  out, st);
         else
-            return scant_launch<NibbleUnits<WPL>, 12, 12600 / GB>(P, T, q_rot, s_q, norms, codes,
+            return scant_launch<NibbleUnits<WPL>, 12, scant_stages<128 * WPL>(12600)>(P, T, q_rot, s_q, norms, codes,
                                                                   n, out, st);
     }
 }
@@ -1680,7 +1784,7 @@ struct ScanRun {
                            cudaStream_t st) {
         if (!P.nibble && !sym && LOG_D >= 7 && LOG_D <= 10)
             return scan8_launch<LOG_D>(P, T, q_rot, s_q, norms, m, codes, n, out, ldo, st);
-        if (P.nibble && !sym && m == 1 && LOG_D >= 8 && LOG_D <= 11 &&
+        if (P.nibble && !sym && m == 1 && LOG_D >= 7 && LOG_D <= 11 &&
             (reinterpret_cast<uintptr_t>(codes) & 15) == 0)
             return scan4t_launch<LOG_D>(P, T, q_rot, s_q, norms, codes, n, out, st);
         if (P.nibble) {
