@@ -7,9 +7,10 @@ the same constructor, method names, keyword names, defaults, output shapes and
 
 Inputs may be any buffer-protocol object (as with the reference's
 ``py::buffer``) -- those run through the synchronous host-pointer entry points
--- or CUDA arrays exposing ``__cuda_array_interface__`` (e.g. torch CUDA
-tensors), which run stream-ordered on torch's current stream and return torch
-CUDA tensors.
+-- or CUDA arrays exposing ``__cuda_array_interface__`` or ``__dlpack__``
+(torch, CuPy, JAX, ...), which run stream-ordered on torch's current stream and
+return torch CUDA tensors.  ``load_codes`` streams a code file (.npy or raw)
+into HBM.
 """
 from __future__ import annotations
 
@@ -21,15 +22,35 @@ import numpy as np
 from . import _capi
 from ._capi import TQError, check, lib
 
-__all__ = ["TurboQuantSpace", "PreparedSymCode", "TQError", "Index", "Server", "BusyError"]
+__all__ = ["TurboQuantSpace", "PreparedSymCode", "TQError", "Index", "Server", "BusyError",
+           "load_codes"]
 __version__ = "0.1.0"
 
 
 # ---------------------------------------------------------------------------
 # argument validation, mirroring bindings.cpp:14-49
 # ---------------------------------------------------------------------------
+def _dlpack_cuda(obj) -> bool:
+    """A DLPack producer (``__dlpack__``) whose memory is on a CUDA device."""
+    if hasattr(obj, "__cuda_array_interface__") or not hasattr(obj, "__dlpack_device__"):
+        return False
+    try:
+        return int(obj.__dlpack_device__()[0]) in (2, 13)  # kDLCUDA, kDLCUDAManaged
+    except Exception:  # a producer that cannot answer is not a device array
+        return False
+
+
 def _is_device(obj) -> bool:
-    return hasattr(obj, "__cuda_array_interface__")
+    return hasattr(obj, "__cuda_array_interface__") or _dlpack_cuda(obj)
+
+
+def _as_cai(obj):
+    """The object itself if it exposes ``__cuda_array_interface__``, else a
+    zero-copy torch view of a CUDA DLPack producer (torch.from_dlpack passes
+    torch's current stream, so the producer's pending work is ordered first)."""
+    if hasattr(obj, "__cuda_array_interface__"):
+        return obj
+    return _torch().utils.dlpack.from_dlpack(obj)
 
 
 def _float_host(buf, expected_last, name, expected_ndim):
@@ -100,7 +121,7 @@ def _torch():
 
 
 def _cai(obj):
-    cai = obj.__cuda_array_interface__
+    cai = _as_cai(obj).__cuda_array_interface__
     shape = tuple(cai["shape"])
     typestr = cai["typestr"]
     strides = cai.get("strides")
@@ -148,7 +169,9 @@ def _codes_dev(obj, cs, bad_type_msg="codes must be uint8"):
 
 def _stream_and_device(obj):
     torch = _torch()
-    dev = obj.device if hasattr(obj, "device") else torch.device("cuda", torch.cuda.current_device())
+    obj = _as_cai(obj)
+    dev = obj.device if isinstance(getattr(obj, "device", None), torch.device) \
+        else torch.device("cuda", torch.cuda.current_device())
     return torch.cuda.current_stream(dev).cuda_stream, dev
 
 
@@ -513,3 +536,4 @@ class TurboQuantSpace:
 
 
 from .serving import BusyError, Index, Server  # noqa: E402
+from .io import load_codes  # noqa: E402

@@ -24,7 +24,9 @@ class BusyError(TQError):
 
 
 def _codes_arg(codes, cs):
-    if hasattr(codes, "__cuda_array_interface__"):
+    from . import _as_cai, _is_device  # the package's CUDA-array helpers (DLPack included)
+    if _is_device(codes):
+        codes = _as_cai(codes)
         cai = codes.__cuda_array_interface__
         total = int(np.prod(cai["shape"]))
         if total % cs:
