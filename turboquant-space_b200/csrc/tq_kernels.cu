@@ -30,6 +30,79 @@ __host__ __device__ __forceinline__ int encode_warp_bytes(int D, int cs) {
 }
 
 // ---------------------------------------------------------------------------
+// Quantizer of CH values held in registers (quantize, space_turbo_quant.h:
+// 332-337), each replaced by its residual x - c[idx] * sigma as one FMA
+// (:366); emit(t, idx) receives the indices.  The table loads of the CH values
+// are independent of one another, so they overlap.
+//   kQuantBucket: the bucket table when every bucket holds at most one
+//                 boundary (qlut_k = 1: b = 6..9), idx = lo + (z > B[lo]);
+//   kQuantRegs:   nb <= 15 boundaries (b = 2..5) held in registers, padded
+//                 with +inf: idx = #{j : z > B[j]} with no table load;
+//   kQuantTable:  anything else, through quantize().
+// ---------------------------------------------------------------------------
+enum { kQuantBucket = 1, kQuantRegs = 2, kQuantTable = 3 };
+
+__device__ __forceinline__ int quant_mode(const Params &P) {
+    if (P.lutq) return P.qlut_k == 1 ? kQuantBucket : kQuantTable;
+    return P.nb <= 15 ? kQuantRegs : kQuantTable;
+}
+
+__device__ __forceinline__ void load_bound_regs(float (&breg)[15], const Params &P,
+                                                const float *s_bnd) {
+#pragma unroll
+    for (int j = 0; j < 15; ++j) breg[j] = (j < P.nb) ? s_bnd[j] : __int_as_float(0x7f800000);
+}
+
+template <int NB, int CH, class Emit>
+__device__ __forceinline__ void quantize_regs_nb(float (&xr)[CH], float isg, float sg,
+                                                 const float (&breg)[15], const float *s_cent,
+                                                 Emit emit) {
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const float z = __fmul_rn(xr[t], isg);
+        int idx = 0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) idx += (z > breg[j]) ? 1 : 0;
+        xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
+        emit(t, idx);
+    }
+}
+
+template <int CH, class Emit>
+__device__ __forceinline__ void quantize_regs(float (&xr)[CH], float isg, float sg, int mode,
+                                              const Params &P, const float (&breg)[15],
+                                              const float *s_bnd, const uint8_t *s_qlut,
+                                              const float *s_cent, Emit emit) {
+    if (mode == kQuantBucket) {
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            const float z = __fmul_rn(xr[t], isg);
+            float y = __fmaf_rn(z, P.qlut_s, P.qlut_c);
+            y = fminf(fmaxf(y, 0.0f), (float)(kQlutBuckets - 1));
+            int idx = s_qlut[(int)y];
+            idx = (idx + ((z > s_bnd[idx]) ? 1 : 0)) & 0xFF;
+            xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
+            emit(t, idx);
+        }
+    } else if (mode == kQuantRegs) {
+        // nb = 2^(b-1) - 1: one compare per boundary, the count fixed at compile time
+        switch (P.nb) {
+            case 1: quantize_regs_nb<1, CH>(xr, isg, sg, breg, s_cent, emit); break;
+            case 3: quantize_regs_nb<3, CH>(xr, isg, sg, breg, s_cent, emit); break;
+            case 7: quantize_regs_nb<7, CH>(xr, isg, sg, breg, s_cent, emit); break;
+            default: quantize_regs_nb<15, CH>(xr, isg, sg, breg, s_cent, emit); break;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            const int idx = quantize(__fmul_rn(xr[t], isg), P, s_bnd, s_qlut);
+            xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
+            emit(t, idx);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // encode: one warp per group of 4 consecutive rows ("quad").
 // ---------------------------------------------------------------------------
 template <int LOG_D>
@@ -112,19 +185,39 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
             inv_sigma = __fdiv_rn(1.0f, sigma);
         }
 
-        // E: quantize + residual (:361-367); the residual is one FMA
+        // E: quantize + residual (:361-367); the residual is one FMA.  The
+        // values are loaded in runs of CH per lane, quantized in registers and
+        // stored afterwards (a store between two loads of the buffer would
+        // order every element's table loads after the previous element's).
+        const int qmode = quant_mode(P);
+        float breg[15];
+        load_bound_regs(breg, P, s_bnd);
 #pragma unroll 1
         for (int v = 0; v < 4; ++v) {
             const float sg = __shfl_sync(kFull, sigma, 8 * v);
             const float isg = __shfl_sync(kFull, inv_sigma, 8 * v);
             float *b = buf + v * VS;
             uint8_t *ib = idxb + v * D;
-            for (int i = lane; i < D; i += 32) {
-                const int p = swz(i);
-                const float x = b[p];
-                const int idx = quantize(__fmul_rn(x, isg), P, s_bnd, s_qlut);
-                b[p] = __fmaf_rn(-s_cent[idx], sg, x);
-                ib[i] = (uint8_t)idx;
+            if constexpr (D >= 32) {
+                constexpr int PER = D / 32, CH = PER < 16 ? PER : 16;
+#pragma unroll 1
+                for (int c0 = 0; c0 < PER; c0 += CH) {
+                    float xr[CH];
+#pragma unroll
+                    for (int t = 0; t < CH; ++t) xr[t] = b[swz(lane + 32 * (c0 + t))];
+                    quantize_regs<CH>(xr, isg, sg, qmode, P, breg, s_bnd, s_qlut, s_cent,
+                                      [&](int t, int idx) { ib[lane + 32 * (c0 + t)] = (uint8_t)idx; });
+#pragma unroll
+                    for (int t = 0; t < CH; ++t) b[swz(lane + 32 * (c0 + t))] = xr[t];
+                }
+            } else {
+                for (int i = lane; i < D; i += 32) {
+                    const int p = swz(i);
+                    const float x = b[p];
+                    const int idx = quantize(__fmul_rn(x, isg), P, s_bnd, s_qlut);
+                    b[p] = __fmaf_rn(-s_cent[idx], sg, x);
+                    ib[i] = (uint8_t)idx;
+                }
             }
         }
         __syncwarp();
@@ -512,9 +605,11 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
         float gamma = 0.0f;
         if (active) {
             // Every Lloyd-Max table of b = 6..9 has at most one boundary per
-            // bucket (qlut_k = 1): idx = lo + (z > B[lo]) with no loop and no
-            // branch, so the unrolled elements' load chains overlap.
-            const bool fastq = P.lutq && P.qlut_k == 1;
+            // bucket (qlut_k = 1), and b = 2..5 have at most 15 boundaries:
+            // either way no loop over a table (quantize_regs).
+            const int qmode = quant_mode(P);
+            float breg[15];
+            load_bound_regs(breg, P, s_bnd);
 #pragma unroll 1
             for (int v = 0; v < 4; ++v) {
                 const float sg = __shfl_sync(kFull, sigma, 8 * v);
@@ -528,25 +623,11 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 uint32_t wq[E / 4];
 #pragma unroll
                 for (int t = 0; t < E; ++t) xr[t] = b[PadLayout<E>::elem(32 * t + lane)];
-                if (fastq) {
-#pragma unroll
-                    for (int t = 0; t < E; ++t) {
-                        const float z = __fmul_rn(xr[t], isg);
-                        float y = __fmaf_rn(z, P.qlut_s, P.qlut_c);
-                        y = fminf(fmaxf(y, 0.0f), (float)(kQlutBuckets - 1));
-                        int idx = s_qlut[(int)y];
-                        idx = (idx + ((z > s_bnd[idx]) ? 1 : 0)) & 0xFF;
-                        xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
-                        wq[t >> 2] = ((t & 3) ? wq[t >> 2] : 0u) | ((uint32_t)idx << (8 * (t & 3)));
-                    }
-                } else {
-#pragma unroll
-                    for (int t = 0; t < E; ++t) {
-                        const int idx = quantize_compact(__fmul_rn(xr[t], isg), P, s_bnd, s_qlut);
-                        xr[t] = __fmaf_rn(-s_cent[idx], sg, xr[t]);
-                        wq[t >> 2] = ((t & 3) ? wq[t >> 2] : 0u) | ((uint32_t)idx << (8 * (t & 3)));
-                    }
-                }
+                quantize_regs<E>(xr, isg, sg, qmode, P, breg, s_bnd, s_qlut, s_cent,
+                                 [&](int t, int idx) {
+                                     wq[t >> 2] = ((t & 3) ? wq[t >> 2] : 0u) |
+                                                  ((uint32_t)idx << (8 * (t & 3)));
+                                 });
 #pragma unroll
                 for (int t = 0; t < E; ++t) b[PadLayout<E>::elem(32 * t + lane)] = xr[t];
 #pragma unroll
