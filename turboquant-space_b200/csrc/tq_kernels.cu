@@ -23,10 +23,10 @@
 namespace tq {
 namespace {
 
-// Per-warp shared bytes of the encode kernel: 4 vectors of D+8 floats, 4 x D
-// quantizer indices, 4 staged codes.
-__host__ __device__ __forceinline__ int encode_warp_bytes(int D, int cs) {
-    return 16 * (D + 8) + 4 * D + align16(4 * cs);
+// Per-warp shared bytes of the encode kernel: vpw vectors of D+8 floats, vpw x D
+// quantizer indices, vpw staged codes.
+__host__ __device__ __forceinline__ int encode_warp_bytes(int D, int cs, int vpw) {
+    return vpw * 4 * (D + 8) + vpw * D + align16(vpw * cs);
 }
 
 // ---------------------------------------------------------------------------
@@ -103,9 +103,12 @@ __device__ __forceinline__ void quantize_regs(float (&xr)[CH], float isg, float 
 }
 
 // ---------------------------------------------------------------------------
-// encode: one warp per group of 4 consecutive rows ("quad").
+// encode: one warp per group of VPW consecutive rows (VPW = 4, or 2 at large
+// D, where four vector buffers per warp would leave room for only 4 warps per
+// SM).  The reduction chains run on 8 lanes per vector; with VPW = 2 the lane
+// groups 2 and 3 repeat the chains of vectors 0 and 1.
 // ---------------------------------------------------------------------------
-template <int LOG_D>
+template <int LOG_D, int VPW>
 __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X, size_t n,
                                                      uint8_t *__restrict__ out, Params P,
                                                      DevTables T) {
@@ -122,23 +125,23 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int cs = P.cs;
-    unsigned char *wbase = smem + kTabBytes + warp * encode_warp_bytes(D, cs);
+    unsigned char *wbase = smem + kTabBytes + warp * encode_warp_bytes(D, cs, VPW);
     float *buf = reinterpret_cast<float *>(wbase);
-    uint8_t *idxb = wbase + 16 * VS;
-    uint8_t *stage = idxb + 4 * D;
+    uint8_t *idxb = wbase + VPW * 4 * VS;
+    uint8_t *stage = idxb + VPW * D;
     const int g = lane >> 3;
-    float *gbuf = buf + g * VS;
+    float *gbuf = buf + (g % VPW) * VS;
     const bool vec4 = ((P.dim & 3) == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
-    const size_t nquads = (n + 3) >> 2;
+    const size_t ngroups = (n + VPW - 1) / VPW;
 
-    for (size_t qd = (size_t)blockIdx.x * nwarps + warp; qd < nquads;
+    for (size_t qd = (size_t)blockIdx.x * nwarps + warp; qd < ngroups;
          qd += (size_t)gridDim.x * nwarps) {
-        const size_t row0 = qd << 2;
-        const int nv = (n - row0 < 4) ? (int)(n - row0) : 4;
+        const size_t row0 = qd * VPW;
+        const int nv = (n - row0 < (size_t)VPW) ? (int)(n - row0) : VPW;
 
         // A: rows -> shared memory, zero padded to D (space_turbo_quant.h:347-350)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
+        for (int v = 0; v < VPW; ++v) {
             float *b = buf + v * VS;
             if (v < nv) {
                 const float *src = X + (row0 + v) * (size_t)P.dim;
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
 
         // C: rotated = RHT_rot(raw * inv_norm) (:349-351)
 #pragma unroll 1
-        for (int v = 0; v < 4; ++v) {
+        for (int v = 0; v < VPW; ++v) {
             const float inv = __shfl_sync(kFull, inv_norm, 8 * v);
             fwht_from<LOG_D, 0, true>(buf + v * VS, lane, inv, s_rot, P.wht_scale);
         }
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
         float breg[15];
         load_bound_regs(breg, P, s_bnd);
 #pragma unroll 1
-        for (int v = 0; v < 4; ++v) {
+        for (int v = 0; v < VPW; ++v) {
             const float sg = __shfl_sync(kFull, sigma, 8 * v);
             const float isg = __shfl_sync(kFull, inv_sigma, 8 * v);
             float *b = buf + v * VS;
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(256) encode_kernel(const float *__restrict__ X
 
         // G: RHT_qjl(residual) (:374)
 #pragma unroll 1
-        for (int v = 0; v < 4; ++v) fwht_from<LOG_D, 0, false>(buf + v * VS, lane, 1.0f, s_qjl, P.wht_scale);
+        for (int v = 0; v < VPW; ++v) fwht_from<LOG_D, 0, false>(buf + v * VS, lane, 1.0f, s_qjl, P.wht_scale);
 
         // H: pack units + trailer into the staging area (:375-395)
         for (int v = 0; v < nv; ++v) {
@@ -1676,26 +1679,26 @@ struct EncodeRun {
         if constexpr (LOG_D >= 8 && LOG_D <= 10)
             return P.nibble ? encode2_launch<LOG_D, true>(P, T, X, n, out, st)
                             : encode2_launch<LOG_D, false>(P, T, X, n, out, st);
+        constexpr int VPW = LOG_D >= 11 ? 2 : 4;
+        auto kern = encode_kernel<LOG_D, VPW>;
         const int D = 1 << LOG_D;
-        const int per_warp = encode_warp_bytes(D, P.cs);
+        const int per_warp = encode_warp_bytes(D, P.cs, VPW);
         int warps = (kSmemBudget - kTabBytes) / per_warp;
         if (warps > 8) warps = 8;
         if (warps < 1) return cudaErrorInvalidConfiguration;
         const size_t smem = (size_t)kTabBytes + (size_t)warps * per_warp;
-        cudaError_t e = cudaFuncSetAttribute(encode_kernel<LOG_D>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel<LOG_D>, 32 * warps,
-                                                          smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
-        const size_t quads = (n + 3) / 4;
-        size_t blocks = (quads + warps - 1) / warps;
+        const size_t groups = (n + VPW - 1) / VPW;
+        size_t blocks = (groups + warps - 1) / warps;
         const size_t cap = (size_t)sm_count() * per_sm;
         if (blocks > cap) blocks = cap;
         if (blocks < 1) blocks = 1;
-        encode_kernel<LOG_D><<<(unsigned)blocks, 32 * warps, smem, st>>>(X, n, out, P, T);
+        kern<<<(unsigned)blocks, 32 * warps, smem, st>>>(X, n, out, P, T);
         return cudaGetLastError();
     }
 };
