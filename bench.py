@@ -167,13 +167,34 @@ def cpu_scan(codes_host, queries, cores, kind_pref="reference"):
     return len(queries) * n / dt / 1e9, kind
 
 
+def code_geometry(dim, bits):
+    """(padded dim D, code bytes) of the reference layout (space_turbo_quant.h:233-266)."""
+    D = 4
+    while D < dim:
+        D *= 2
+    return D, (D // 2 if bits <= 4 else D) + 12
+
+
+def scan_kernel_name(dim, bits):
+    """The staged 1->N scan kernel (tq_kernels.cu) that a dim / bits pair selects."""
+    D, _ = code_geometry(dim, bits)
+    if bits >= 5:
+        return f"scant_kernel<ByteUnits<{D // 128}>,16,S> (staged 1->N scan, byte units)"
+    if D == 128:
+        return "scant_kernel<HalfNibbleUnits,16,S> (staged 1->N scan, half-warp per code)"
+    return f"scant_kernel<NibbleUnits<{D // 256}>,16,S> (staged 1->N scan, nibble units)"
+
+
 def scan_config(n, world):
     """The `config` of the 1->N scan workload, shared by both arms."""
-    return {"workload": "distance_1_to_n x 64 queries over a device-resident corpus of "
-                        "10M codes: dim 768, bits 8 (D 1024, 1036 B/code)",
+    D, cs = code_geometry(DIM, BITS)
+    gb = n * cs / 1e9
+    return {"workload": f"distance_1_to_n x 64 queries over a device-resident corpus of "
+                        f"{n / 1e6:g}M codes: dim {DIM}, bits {BITS} (D {D}, {cs} B/code)",
             "n_codes_per_gpu": n, "queries_per_step": QUERIES, "dim": DIM,
-            "bits_per_coord": BITS, "code_bytes": 1036,
-            "l2": "corpus 10.4 GB per GPU > 126 MB L2: no flush needed",
+            "bits_per_coord": BITS, "code_bytes": cs,
+            "l2": (f"corpus {gb:.2f} GB per GPU > 126 MB L2: no flush needed" if gb > 0.126
+                   else f"corpus {gb:.3f} GB per GPU fits in the 126 MB L2"),
             "parallelism": f"{world} independent shards" if world > 1 else "1 GPU"}
 
 
@@ -210,9 +231,9 @@ def run_reference(args, rank):
         step()
     dt = (time.perf_counter() - t0) / args.steps
     value = q_sample * n_sample / dt / 1e9
-    sample = (f"each step {q_sample} of the 64 queries x {n_sample} of the 10M codes (768-d, "
-              f"8-bit, normalised N(0,1) seed 2), distance_1_to_n, {cores} OpenMP threads; "
-              f"codes/s is independent of the sample size for this per-code loop")
+    sample = (f"each step {q_sample} of the 64 queries x {n_sample} of the corpus's codes "
+              f"({DIM}-d, {BITS}-bit, normalised N(0,1) seed 2), distance_1_to_n, {cores} "
+              f"OpenMP threads; codes/s is independent of the sample size for this per-code loop")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Gcodes/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -543,6 +564,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=10_000_000, help="codes per GPU")
+    ap.add_argument("--dim", type=int, default=768, help="scan: input dimension")
+    ap.add_argument("--bits", type=int, default=8, help="scan: bits per coordinate")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -555,6 +578,8 @@ def main():
                          "distances; serve: the serving loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global DIM, BITS
+    DIM, BITS = args.dim, args.bits
     if args.workload == "serve":
         run_serve(args)
         return
@@ -655,7 +680,7 @@ def main():
     stream.synchronize()
     csample = codes[:2048].cpu().numpy()
     dref = O.OracleSpace(DIM, BITS).distance_1_to_n(Qh[0], csample)
-    meta = np.frombuffer(csample[:, D:D + 4].tobytes(), np.float32).astype(np.float64)
+    meta = np.frombuffer(csample[:, cs - 12:cs - 8].tobytes(), np.float32).astype(np.float64)
     tscale = float(np.sum(Qh[0].astype(np.float64) ** 2)) + meta ** 2
     dist_err = float(np.max(np.abs(out[0, :2048].cpu().numpy() - dref) /
                             np.maximum(np.abs(dref), tscale)))
@@ -744,11 +769,12 @@ def main():
             "config": scan_config(n, world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
-                         "traffic": int(round(SCAN_TRAFFIC_PER_CODE * n)),
+                         "traffic": (int(round(SCAN_TRAFFIC_PER_CODE * n))
+                                     if (DIM, BITS) == (768, 8) else None),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                            "1M-code launch, scaled per code "
                                            "(profiles/scan8t_kernel_1M_768d_b8.md)",
-                         "kernel": "scan8t_kernel<8,16,2,true> (1->N, 16 warps x 2-stage rings)",
+                         "kernel": scan_kernel_name(DIM, BITS),
                          "bytes_per_launch": scan_bytes, "ms_per_launch": round(scan_ms, 4),
                          "peak_kind": peak_kind},
             "encode": {"ms": round(enc_ms, 3), "Mvec_per_s": round(n / enc_ms / 1e3, 2),
