@@ -276,6 +276,32 @@ def test_distance_m_to_n_split_bf16_vs_oracle(cuda_ok, dim, bits):
     assert ok, err.max()
 
 
+@pytest.mark.parametrize("dim,bits", [(768, 4), (1024, 8), (64, 6)])
+def test_split_bf16_exact_sign_degenerate_trailers(cuda_ok, dim, bits):
+    """The split-BF16 asymmetric form divides each code's centroid half by
+    g = scale * gamma and keeps its sign half exact; codes whose g is zero or
+    below 1e-20 keep the plain centroid half and drop the correction term.
+    Zero rows, unnormalised rows and trailers with gamma = 0 or 1e-30 agree
+    with the reference within the distance tolerance."""
+    rng = np.random.default_rng(dim + 7 * bits)
+    X = (rng.standard_normal((300, dim)) * rng.uniform(1e-3, 1e3, (300, 1))).astype(np.float32)
+    X[0] = 0.0
+    Q = rng.standard_normal((130, dim)).astype(np.float32)
+    Q[1] = 0.0
+    s = tq.TurboQuantSpace(dim, bits)
+    cs = s.code_size_bytes()
+    codes = s.encode_batch(X)
+    gam = codes[:, cs - 8:cs - 4].copy().view(np.float32)
+    gam[3:40] = 0.0
+    gam[40:60] = 1e-30
+    codes[:, cs - 8:cs - 4] = gam.view(np.uint8)
+    d = s.distance_m_to_n(Q, codes, precision="split_bf16")
+    ref = O.OracleSpace(dim, bits).distance_m_to_n(Q, codes)
+    err, ok = dist_close(d, ref, asym_term_scale(Q, codes, cs, cs - 12))
+    print(f"split-BF16 asym degenerate {dim}/{bits}: max err {err.max():.2e}")
+    assert ok, err.max()
+
+
 @pytest.mark.parametrize("dim,bits", TC_CASES)
 def test_distance_symmetric_split_bf16_vs_oracle(cuda_ok, dim, bits):
     rng = np.random.default_rng(dim + 5 * bits)

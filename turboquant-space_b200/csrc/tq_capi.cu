@@ -224,8 +224,9 @@ class MtonRunner {
                                               nc_pad, r1_, r2_, c1_, c2_, out + n0, ldo, s),
                         "FP32 GEMM kernel");
             else
-                TQ_CUDA(tq::launch_tc_dist(a0_, a1_, b0_, b1_, K_, m_, m_pad_, nc, nc_pad, r1_, r2_,
-                                           c1_, c2_, out + n0, ldo, err_, s),
+                TQ_CUDA(tq::launch_tc_dist(a0_, a1_, b0_, b1_, K_,
+                                           sym_ ? K_ : tq::asym_lo_width((int)sp_->D), m_, m_pad_,
+                                           nc, nc_pad, r1_, r2_, c1_, c2_, out + n0, ldo, err_, s),
                         "tcgen05 GEMM kernel");
         }
         return TQ_OK;

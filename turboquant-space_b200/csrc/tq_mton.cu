@@ -17,6 +17,14 @@
 // Planes come in two formats: FP32 (the CUDA-core SGEMM below, the drop-in)
 // and a hi/lo BF16 pair, x = hi + lo with hi = bf16(x), lo = bf16(x - hi),
 // for the tcgen05 kernel (tq_tc.cu), which forms hi*hi + hi*lo + lo*hi.
+//
+// Asymmetric BF16 column planes use the exact-sign form: with g_j = scale
+// gamma_j, B[j] = [ sigma_j c[idx_j] / g_j | (+-1)_j ] and c1 = g_j |x|, so
+// the QJL half is exact in BF16 (its lo plane is zero and is not stored: the
+// lo plane has asym_lo_width(D) columns) and the tensor-core kernel needs two
+// products there instead of three.  A code with g_j < 1e-20 (gamma = 0, e.g.
+// a zero row) keeps B[j] = [ sigma_j c[idx_j] | 0 ] and c1 = |x|: its
+// correction term is below 1e-18 of |q| |x| and is left out.
 #include <cuda_bf16.h>
 
 #include "tq_internal.h"
@@ -33,14 +41,19 @@ __device__ __forceinline__ unsigned unit_at(const uint8_t *code, int p, int nibb
     return code[p];
 }
 
-__device__ __forceinline__ void put(void *plane0, void *plane1, size_t idx, float v, int fmt) {
+// Value v at position k of row r: FP32 plane0[r K + k], or BF16 hi at
+// plane0[r K + k] and lo at plane1[r ldl + k] (k < ldl; beyond ldl lo is zero
+// by construction and not stored).
+__device__ __forceinline__ void put(void *plane0, void *plane1, size_t r, int K, int ldl, int k,
+                                    float v, int fmt) {
     if (fmt == kPlaneF32) {
-        static_cast<float *>(plane0)[idx] = v;
+        static_cast<float *>(plane0)[r * K + k] = v;
     } else {
         const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-        static_cast<__nv_bfloat16 *>(plane0)[idx] = hi;
-        static_cast<__nv_bfloat16 *>(plane1)[idx] = lo;
+        static_cast<__nv_bfloat16 *>(plane0)[r * K + k] = hi;
+        if (k < ldl)
+            static_cast<__nv_bfloat16 *>(plane1)[r * ldl + k] =
+                __float2bfloat16_rn(v - __bfloat162float(hi));
     }
 }
 
@@ -48,17 +61,18 @@ __device__ __forceinline__ void put(void *plane0, void *plane1, size_t idx, floa
 // are zero so that padded tiles contribute nothing.
 __global__ void __launch_bounds__(256) planes_from_codes_kernel(
     const uint8_t *__restrict__ codes, size_t rows, size_t rows_pad, Params P, DevTables T,
-    int sym, int fmt, void *plane0, void *plane1, float *__restrict__ s1, float *__restrict__ s2) {
+    int sym, int fmt, int ldl, void *plane0, void *plane1, float *__restrict__ s1,
+    float *__restrict__ s2) {
     const int K = sym ? P.D : 2 * P.D;
+    const bool exact_sign = !sym && fmt == kPlaneBF16;
     const size_t quads_per_row = (size_t)(K / 4);
     const size_t total = rows_pad * quads_per_row;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (size_t)gridDim.x * blockDim.x) {
         const size_t r = t / quads_per_row;
         const int k0 = (int)(t - r * quads_per_row) * 4;
-        const size_t base = r * (size_t)K + k0;
         if (r >= rows) {
-            for (int q = 0; q < 4; ++q) put(plane0, plane1, base + q, 0.0f, fmt);
+            for (int q = 0; q < 4; ++q) put(plane0, plane1, r, K, ldl, k0 + q, 0.0f, fmt);
             if (k0 == 0) {
                 s1[r] = 0.0f;
                 s2[r] = 0.0f;
@@ -73,6 +87,10 @@ __global__ void __launch_bounds__(256) planes_from_codes_kernel(
             meta[q] = __uint_as_float(w);
         }
         const float norm = meta[0], gamma = meta[1], sigma = meta[2];
+        const float sg = __fmul_rn(P.scale, gamma);
+        // exact-sign form: g = scale gamma factored out of the column (see the
+        // file header); !(g >= 1e-20f) also catches a NaN trailer
+        const bool ratio = exact_sign && sg >= 1e-20f && sg <= 3.0e38f;
         for (int q = 0; q < 4; ++q) {
             const int k = k0 + q;
             float v;
@@ -80,14 +98,16 @@ __global__ void __launch_bounds__(256) planes_from_codes_kernel(
                 v = T.centroids[unit_at(code, k, P.nibble) >> 1];
             } else if (k < P.D) {
                 v = __fmul_rn(sigma, T.centroids[unit_at(code, k, P.nibble) >> 1]);
+                if (ratio) v = __fdiv_rn(v, sg);
             } else {
-                const float sg = __fmul_rn(P.scale, gamma);
-                v = (unit_at(code, k - P.D, P.nibble) & 1u) ? sg : -sg;
+                const bool pos = unit_at(code, k - P.D, P.nibble) & 1u;
+                if (!exact_sign) v = pos ? sg : -sg;
+                else v = !ratio ? 0.0f : pos ? 1.0f : -1.0f;
             }
-            put(plane0, plane1, base + q, v, fmt);
+            put(plane0, plane1, r, K, ldl, k, v, fmt);
         }
         if (k0 == 0) {
-            s1[r] = sym ? __fmul_rn(sigma, norm) : norm;
+            s1[r] = sym ? __fmul_rn(sigma, norm) : ratio ? __fmul_rn(sg, norm) : norm;
             s2[r] = __fmul_rn(norm, norm);
         }
     }
@@ -105,7 +125,7 @@ __global__ void __launch_bounds__(256) planes_from_prepared_kernel(
         const int k = (int)(t - r * K);
         float v = 0.0f;
         if (r < rows) v = (k < D) ? q_rot[r * D + k] : s_q[r * D + (k - D)];
-        put(plane0, plane1, t, v, fmt);
+        put(plane0, plane1, r, K, K, k, v, fmt);
         if (k == 0) {
             r1[r] = (r < rows) ? norms[2 * r + 1] : 0.0f;
             r2[r] = (r < rows) ? norms[2 * r] : 0.0f;
@@ -212,8 +232,9 @@ cudaError_t launch_planes_from_codes(const Params &P, const DevTables &T, const 
                                      void *plane1, float *s1, float *s2, cudaStream_t st) {
     if (rows_pad == 0) return cudaSuccess;
     const int K = sym ? P.D : 2 * P.D;
+    const int ldl = (!sym && fmt == kPlaneBF16) ? asym_lo_width(P.D) : K;
     planes_from_codes_kernel<<<grid_for(rows_pad * (K / 4), 256), 256, 0, st>>>(
-        codes, rows, rows_pad, P, T, sym ? 1 : 0, fmt, plane0, plane1, s1, s2);
+        codes, rows, rows_pad, P, T, sym ? 1 : 0, fmt, ldl, plane0, plane1, s1, s2);
     return cudaGetLastError();
 }
 

@@ -10,8 +10,14 @@ constexpr int kPlaneF32 = 0;   // one FP32 plane
 constexpr int kPlaneBF16 = 1;  // hi and lo BF16 planes, x = hi + lo
 constexpr int kPlaneRowAlign = 128;
 
+// Columns of the BF16 lo plane of asymmetric code planes: the QJL half of
+// those planes is exact (+-1, see tq_mton.cu), so lo is stored for the
+// centroid half only, rounded up to a whole 64-wide K block.
+inline int asym_lo_width(int D) { return D % 64 == 0 ? D : 2 * D; }
+
 // Rows [0, rows) of `codes` -> planes of rows_pad x K (K = D symmetric, 2D
 // asymmetric), zero rows beyond `rows`; s1/s2 per-row scalars (rows_pad).
+// BF16 lo planes have K columns, asym_lo_width(D) for asymmetric planes.
 cudaError_t launch_planes_from_codes(const Params &P, const DevTables &T, const uint8_t *codes,
                                      size_t rows, size_t rows_pad, bool sym, int fmt, void *plane0,
                                      void *plane1, float *s1, float *s2, cudaStream_t st);
@@ -29,10 +35,11 @@ cudaError_t launch_sgemm_dist(const float *A, const float *B, int K, size_t m, s
 
 // The same with C = Ah Bh^T + Ah Bl^T + Al Bh^T on tcgen05 tensor cores
 // (FP32 accumulators in tensor memory).  K % 64 == 0, m_pad % 128 == 0,
-// n_pad % 256 == 0.  `err` (device int) is set non-zero if a bounded wait in
-// the kernel gave up.
+// n_pad % 256 == 0.  Bl has k_lo columns (k_lo % 64 == 0, k_lo <= K): B's lo
+// part is zero beyond them, where the Ah Bl^T product is skipped.  `err`
+// (device int) is set non-zero if a bounded wait in the kernel gave up.
 cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const void *Bl, int K,
-                           size_t m, size_t m_pad, size_t n, size_t n_pad, const float *r1,
+                           int k_lo, size_t m, size_t m_pad, size_t n, size_t n_pad, const float *r1,
                            const float *r2, const float *c1, const float *c2, float *out,
                            size_t ldo, int *err, cudaStream_t st);
 
@@ -44,7 +51,8 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
 constexpr int kTopKMax = 16;
 int tc_topk_variants();
 cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
-                           const void *Bh, const void *Bl, size_t n_pad, int K, const int *m_dev,
+                           const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo,
+                           const int *m_dev,
                            size_t n, const float *r1, const float *r2, const float *c1,
                            const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
                            cudaStream_t st);

@@ -42,7 +42,8 @@ struct tq_index {
     tq_space *sp = nullptr;
     size_t n = 0, n_pad = 0;
     int K = 0;
-    void *planes = nullptr;  // hi plane, then lo plane: n_pad x K BF16 each
+    int K_lo = 0;            // columns of the lo plane (tq::asym_lo_width)
+    void *planes = nullptr;  // hi plane n_pad x K, then lo plane n_pad x K_lo, BF16
     float *c1 = nullptr, *c2 = nullptr;
     int device = -1;
 };
@@ -157,8 +158,9 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     if (e != cudaSuccess) return e;
     unsigned char *bh = static_cast<unsigned char *>(ix->planes);
     unsigned char *bl = bh + ix->n_pad * K * 2;
-    e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, sl.d_m, ix->n, sl.d_r1,
-                           sl.d_r2, ix->c1, ix->c2, sv->k, sl.d_pd, sl.d_pi, sl.d_err, sv->grid, st);
+    e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
+                           sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->k, sl.d_pd, sl.d_pi, sl.d_err,
+                           sv->grid, st);
     if (e != cudaSuccess) return e;
     e = tq::launch_topk_merge(sl.d_m, sv->grid, sl.d_pd, sl.d_pi, sv->k, rows_cap, sl.d_od, sl.d_oi, st);
     if (e != cudaSuccess) return e;
@@ -401,17 +403,19 @@ tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n,
     ix->n = n;
     ix->n_pad = round_up(n, 256);
     ix->K = (int)K;
+    ix->K_lo = tq::asym_lo_width((int)sp->D);
     ix->device = sp->device;
-    const size_t plane = ix->n_pad * K * 2;
-    cudaError_t e = cudaMalloc(&ix->planes, 2 * plane + 2 * ix->n_pad * 4 + 256);
+    const size_t plane_hi = ix->n_pad * K * 2, plane_lo = ix->n_pad * (size_t)ix->K_lo * 2;
+    cudaError_t e = cudaMalloc(&ix->planes, plane_hi + plane_lo + 2 * ix->n_pad * 4 + 256);
     if (e != cudaSuccess) {
         delete ix;
         return cuda_fail(e, "cudaMalloc(index planes)");
     }
-    ix->c1 = reinterpret_cast<float *>(static_cast<unsigned char *>(ix->planes) + 2 * plane);
+    ix->c1 = reinterpret_cast<float *>(static_cast<unsigned char *>(ix->planes) + plane_hi +
+                                       plane_lo);
     ix->c2 = ix->c1 + ix->n_pad;
     auto *hi = static_cast<unsigned char *>(ix->planes);
-    auto *lo = hi + plane;
+    auto *lo = hi + plane_hi;
     const size_t chunk = 1 << 20;
     uint8_t *stage = nullptr;
     if (!codes_on_device) {
@@ -433,7 +437,8 @@ tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n,
         if (e == cudaSuccess)
             e = tq::launch_planes_from_codes(sp->P, sp->T, rows ? src : stage ? stage : codes, rows,
                                              rows_pad, false, tq::kPlaneBF16, hi + r0 * K * 2,
-                                             lo + r0 * K * 2, ix->c1 + r0, ix->c2 + r0, nullptr);
+                                             lo + r0 * (size_t)ix->K_lo * 2, ix->c1 + r0,
+                                             ix->c2 + r0, nullptr);
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (stage) cudaFree(stage);

@@ -3,13 +3,17 @@
 //
 // C = Ah Bh^T + Ah Bl^T + Al Bh^T over BF16 hi/lo operand planes (x = hi + lo,
 // see tq_mton.cu), accumulated in FP32 in tensor memory; then
-// d = max(0, r2_i + c2_j - 2 (C_ij r1_i) c1_j) is written to out.
+// d = max(0, r2_i + c2_j - 2 (C_ij r1_i) c1_j) is written to out.  K blocks
+// from kbx on have an exact B (lo = 0: the +-1 QJL half of asymmetric planes):
+// there the Bl tile is not loaded and Ah Bl^T is not issued.
 //
 // Persistent kernel, one CTA per SM, 6 warps:
 //   warp 0      TMA producer: per K block of 64, loads Ah, Al (128 x 64) and
-//               Bh, Bl (256 x 64) tiles, 128-byte swizzled, into a 2-stage ring
+//               Bh, Bl (256 x 64; Bl only below kbx) tiles, 128-byte
+//               swizzled, into a 2-stage ring
 //   warp 1      allocates 512 TMEM columns (two 128 x 256 FP32 accumulators);
 //               one thread issues 3 tcgen05.mma (M128 N256 K16) per K step
+//               (2 from kbx on)
 //               and commits to the stage's "empty" barrier and, after a
 //               tile's last K block, to the accumulator's "full" barrier
 //   warps 2..5  epilogue: tcgen05.ld 32x32b rows of the accumulator, apply the
@@ -113,7 +117,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
     const __grid_constant__ CUtensorMap tm_ah, const __grid_constant__ CUtensorMap tm_al,
     const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl, int K,
-    unsigned num_mb, unsigned num_tiles, size_t m, size_t n, const float *__restrict__ r1,
+    int kbx, unsigned num_mb, unsigned num_tiles, size_t m, size_t n, const float *__restrict__ r1,
     const float *__restrict__ r2, const float *__restrict__ c1, const float *__restrict__ c2,
     float *__restrict__ out, size_t ldo, int *err) {
     extern __shared__ unsigned char smem_raw[];
@@ -164,11 +168,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
                     if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
                     const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
                     const uint32_t fb = full0 + 8 * s;
-                    mbar_expect_tx(fb, TC_STAGE_BYTES);
+                    const bool lo = kb < kbx;
+                    mbar_expect_tx(fb, lo ? TC_STAGE_BYTES : TC_STAGE_BYTES - TC_B_BYTES);
                     tma_load_2d(base, &tm_ah, kb * TC_BK, mb * TC_BM, fb);
                     tma_load_2d(base + TC_A_BYTES, &tm_al, kb * TC_BK, mb * TC_BM, fb);
                     tma_load_2d(base + 2 * TC_A_BYTES, &tm_bh, kb * TC_BK, nb * TC_BN, fb);
-                    tma_load_2d(base + 2 * TC_A_BYTES + TC_B_BYTES, &tm_bl, kb * TC_BK, nb * TC_BN, fb);
+                    if (lo)
+                        tma_load_2d(base + 2 * TC_A_BYTES + TC_B_BYTES, &tm_bl, kb * TC_BK,
+                                    nb * TC_BN, fb);
                 }
             }
             // drain: every stage issued must have landed before the CTA exits
@@ -194,12 +201,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
                     const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
                     const uint32_t ah = base, al = base + TC_A_BYTES;
                     const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TC_B_BYTES;
+                    const bool lo = kb < kbx;
 #pragma unroll
                     for (int kk = 0; kk < TC_BK / 16; ++kk) {
                         const uint32_t koff = kk * 32;  // 16 BF16 along K
                         const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
                         umma(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), acc);
-                        umma(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), 1u);
+                        if (lo) umma(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), 1u);
                         umma(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), 1u);
                     }
                     umma_commit(empty0 + 8 * s);  // smem stage free once these MMAs are done
@@ -288,7 +296,7 @@ template <int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_topk_kernel(
     const __grid_constant__ CUtensorMap tm_ah, const __grid_constant__ CUtensorMap tm_al,
     const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl, int K,
-    const int *__restrict__ m_dev, unsigned nb_tiles, size_t n, const float *__restrict__ r1,
+    int kbx, const int *__restrict__ m_dev, unsigned nb_tiles, size_t n, const float *__restrict__ r1,
     const float *__restrict__ r2, const float *__restrict__ c1, const float *__restrict__ c2, int k,
     float *__restrict__ part_d, int *__restrict__ part_i, int *err) {
     constexpr int B_BYTES = BN * TC_BK * 2;
@@ -351,11 +359,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_topk_kernel(
                     if (!mbar_wait(empty0 + 8 * st, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
                     const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
                     const uint32_t fb = full0 + 8 * st;
-                    mbar_expect_tx(fb, STAGE_BYTES);
+                    const bool lo = kb < kbx;
+                    mbar_expect_tx(fb, lo ? STAGE_BYTES : STAGE_BYTES - B_BYTES);
                     tma_load_2d(base, &tm_ah, kb * TC_BK, mb * TC_BM, fb);
                     tma_load_2d(base + TC_A_BYTES, &tm_al, kb * TC_BK, mb * TC_BM, fb);
                     tma_load_2d(base + 2 * TC_A_BYTES, &tm_bh, kb * TC_BK, nb * BN, fb);
-                    tma_load_2d(base + 2 * TC_A_BYTES + B_BYTES, &tm_bl, kb * TC_BK, nb * BN, fb);
+                    if (lo)
+                        tma_load_2d(base + 2 * TC_A_BYTES + B_BYTES, &tm_bl, kb * TC_BK, nb * BN,
+                                    fb);
                 }
             }
             const uint32_t drain_n = it < (uint32_t)STAGES ? it : (uint32_t)STAGES;
@@ -380,12 +391,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_topk_kernel(
                     const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
                     const uint32_t ah = base, al = base + TC_A_BYTES;
                     const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + B_BYTES;
+                    const bool lo = kb < kbx;
 #pragma unroll
                     for (int kk = 0; kk < TC_BK / 16; ++kk) {
                         const uint32_t koff = kk * 32;
                         const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
                         umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), IDESC, acc);
-                        umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), IDESC, 1u);
+                        if (lo)
+                            umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), IDESC, 1u);
                         umma_i(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), IDESC, 1u);
                     }
                     umma_commit(empty0 + 8 * st);
@@ -603,23 +616,25 @@ bool make_map(CUtensorMap *map, const void *base, int K, size_t rows, int box_ro
 
 template <int BN, int STAGES>
 cudaError_t topk_variant(const void *Ah, const void *Al, size_t rows_pad, const void *Bh,
-                         const void *Bl, size_t n_pad, int K, const int *m_dev, size_t n,
+                         const void *Bl, size_t n_pad, int K, int k_lo, const int *m_dev, size_t n,
                          const float *r1, const float *r2, const float *c1, const float *c2, int k,
                          float *part_d, int *part_i, int *err, int grid, cudaStream_t st) {
-    if (K % TC_BK || rows_pad % TC_BM || n_pad % BN) return cudaErrorInvalidValue;
+    if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || rows_pad % TC_BM || n_pad % BN)
+        return cudaErrorInvalidValue;
     for (const void *p : {Ah, Al, Bh, Bl})
         if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
     alignas(64) CUtensorMap mah, mal, mbh, mbl;
     if (!make_map(&mah, Ah, K, rows_pad, TC_BM) || !make_map(&mal, Al, K, rows_pad, TC_BM) ||
-        !make_map(&mbh, Bh, K, n_pad, BN) || !make_map(&mbl, Bl, K, n_pad, BN))
+        !make_map(&mbh, Bh, K, n_pad, BN) || !make_map(&mbl, Bl, k_lo, n_pad, BN))
         return cudaErrorInvalidValue;
     constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * BN * TC_BK * 2;
     const size_t smem = (size_t)STAGES * STAGE_BYTES + 256 + 1024;
     auto kern = tc_topk_kernel<BN, STAGES>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, m_dev, (unsigned)(n_pad / BN), n, r1,
-                                         r2, c1, c2, k, part_d, part_i, err);
+    kern<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, k_lo / TC_BK, m_dev,
+                                         (unsigned)(n_pad / BN), n, r1, r2, c1, c2, k, part_d,
+                                         part_i, err);
     return cudaGetLastError();
 }
 
@@ -633,16 +648,16 @@ cudaError_t launch_bounded_wait_selftest(int *err, long long budget_cycles, cuda
 }
 
 cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
-                           const void *Bh, const void *Bl, size_t n_pad, int K, const int *m_dev,
-                           size_t n, const float *r1, const float *r2, const float *c1,
-                           const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
-                           cudaStream_t st) {
+                           const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo,
+                           const int *m_dev, size_t n, const float *r1, const float *r2,
+                           const float *c1, const float *c2, int k, float *part_d, int *part_i,
+                           int *err, int grid, cudaStream_t st) {
     if (k < 1 || k > kTopKMax) return cudaErrorInvalidValue;
     if (variant == 1)
-        return topk_variant<128, 3>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, m_dev, n, r1, r2, c1, c2, k,
-                                    part_d, part_i, err, grid, st);
-    return topk_variant<256, 2>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, m_dev, n, r1, r2, c1, c2, k,
-                                part_d, part_i, err, grid, st);
+        return topk_variant<128, 3>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo, m_dev, n, r1, r2, c1,
+                                    c2, k, part_d, part_i, err, grid, st);
+    return topk_variant<256, 2>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo, m_dev, n, r1, r2, c1, c2,
+                                k, part_d, part_i, err, grid, st);
 }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
@@ -656,17 +671,18 @@ cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part
 }
 
 cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const void *Bl, int K,
-                           size_t m, size_t m_pad, size_t n, size_t n_pad, const float *r1,
-                           const float *r2, const float *c1, const float *c2, float *out,
-                           size_t ldo, int *err, cudaStream_t st) {
+                           int k_lo, size_t m, size_t m_pad, size_t n, size_t n_pad,
+                           const float *r1, const float *r2, const float *c1, const float *c2,
+                           float *out, size_t ldo, int *err, cudaStream_t st) {
     if (m == 0 || n == 0) return cudaSuccess;
-    if (K % TC_BK || m_pad % TC_BM || n_pad % TC_BN) return cudaErrorInvalidValue;
+    if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || m_pad % TC_BM || n_pad % TC_BN)
+        return cudaErrorInvalidValue;
     // TMA: 16-byte aligned bases and row strides
     for (const void *p : {Ah, Al, Bh, Bl})
         if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
     alignas(64) CUtensorMap mah, mal, mbh, mbl;
     if (!make_map(&mah, Ah, K, m_pad, TC_BM) || !make_map(&mal, Al, K, m_pad, TC_BM) ||
-        !make_map(&mbh, Bh, K, n_pad, TC_BN) || !make_map(&mbl, Bl, K, n_pad, TC_BN))
+        !make_map(&mbh, Bh, K, n_pad, TC_BN) || !make_map(&mbl, Bl, k_lo, n_pad, TC_BN))
         return cudaErrorInvalidValue;
     const size_t smem = (size_t)TC_STAGES * TC_STAGE_BYTES + 256 + 1024;
     cudaError_t e = cudaFuncSetAttribute(tc_dist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -679,8 +695,9 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned grid = (unsigned)(tiles < (size_t)sms ? tiles : (size_t)sms);
-    tc_dist_kernel<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, num_mb, (unsigned)tiles, m,
-                                                   n, r1, r2, c1, c2, out, ldo, err);
+    tc_dist_kernel<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, k_lo / TC_BK, num_mb,
+                                                   (unsigned)tiles, m, n, r1, r2, c1, c2, out, ldo,
+                                                   err);
     return cudaGetLastError();
 }
 
