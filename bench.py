@@ -376,14 +376,15 @@ def run_symq(args):
     """QJL-corrected symmetric distances (light, full, full-prepared): 2048 row
     codes x 200,000 column codes of a 1024-centre Gaussian mixture at 1536-d
     (padded 2048), 4-bit, device-resident.  Each variant is timed on the GPU
-    (CUDA events) and checked against the FP64 evaluation of its formula on
-    2,000 sampled pairs; the reference's own CPU code (oracle/_ref) is timed
-    on a bounded sample (128 x 512 pairs) on the host cores."""
+    (CUDA events) in both precisions (FP32 CUDA cores, split-TF32 tensor
+    cores) and checked against the FP64 evaluation of its formula on 2,000
+    sampled pairs; the reference's own CPU code (oracle/_ref) is timed on a
+    bounded sample (128 x 512 pairs) on the host cores."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     import turboquant as tq
-    from turboquant._capi import SYM_VARIANT, check, lib
+    from turboquant._capi import PRECISION, SYM_VARIANT, check, lib
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -425,29 +426,31 @@ def run_symq(args):
     res = {}
     for variant in ("light", "full", "full_prepared"):
         v = SYM_VARIANT[variant]
-
-        def call():
-            check(L.tq_distance_m_to_n_symmetric_qjl_device(
-                h, C.c_void_p(acodes.data_ptr()), m, C.c_void_p(codes.data_ptr()), n,
-                C.c_void_p(out.data_ptr()), v, sptr))
-
-        call()
-        stream.synchronize()
-        got = out.view(-1).index_select(0, flat).cpu().numpy().astype(np.float64)
         f64 = np.array([o.distance_symmetric_qjl_f64(ah[k], ch[k], variant) for k in range(2000)])
-        err = float(np.max(np.abs(got - f64) / np.maximum(np.abs(f64), na ** 2 + nb ** 2)))
-        reps = max(1, args.steps // 2)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            call()
-        e1.record(stream)
-        stream.synchronize()
-        ms = e0.elapsed_time(e1) / reps
         k_total = D + (3 * D if variant != "light" else D)
-        r = {"ms": round(ms, 3), "Gdist_s": round(m * n / (ms * 1e-3) / 1e9, 3),
-             "TFLOP_s_issued": round(2.0 * k_total * m * n / (ms * 1e-3) / 1e12, 2),
-             "max_rel_err_vs_fp64": err, "reps": reps}
+        r = {}
+        for prec in ("fp32", "split_tf32"):
+            def call():
+                check(L.tq_distance_m_to_n_symmetric_qjl_device(
+                    h, C.c_void_p(acodes.data_ptr()), m, C.c_void_p(codes.data_ptr()), n,
+                    C.c_void_p(out.data_ptr()), v, PRECISION[prec], sptr))
+
+            call()
+            stream.synchronize()
+            got = out.view(-1).index_select(0, flat).cpu().numpy().astype(np.float64)
+            err = float(np.max(np.abs(got - f64) / np.maximum(np.abs(f64), na ** 2 + nb ** 2)))
+            reps = max(1, args.steps // 2) if prec == "fp32" else max(3, args.steps)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                call()
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            r[prec] = {"ms": round(ms, 3), "Gdist_s": round(m * n / (ms * 1e-3) / 1e9, 3),
+                       "TFLOP_s_algorithmic": round(2.0 * k_total * m * n / (ms * 1e-3) / 1e12, 2),
+                       "max_rel_err_vs_fp64": err, "reps": reps}
+        r["speedup_split_tf32_vs_fp32"] = round(r["fp32"]["ms"] / r["split_tf32"]["ms"], 2)
         if ref_mod is not None:
             rs = ref_mod.TurboQuantSpace(dim, bits, num_threads=cpu_cores())
             fn = getattr(rs, f"distance_m_to_n_symmetric_{variant}")

@@ -48,8 +48,10 @@ typedef enum tq_status {
 
 /* Arithmetic used by the M x N contractions. */
 typedef enum tq_precision {
-    TQ_PRECISION_FP32 = 0,      /* FP32 CUDA-core kernels: the drop-in */
-    TQ_PRECISION_SPLIT_BF16 = 1 /* tcgen05 tensor cores on hi+lo BF16 pairs, FP32 TMEM accumulators */
+    TQ_PRECISION_FP32 = 0,       /* FP32 CUDA-core kernels: the drop-in */
+    TQ_PRECISION_SPLIT_BF16 = 1, /* tcgen05 tensor cores on hi+lo BF16 pairs, FP32 TMEM accumulators */
+    TQ_PRECISION_SPLIT_TF32 = 2  /* tcgen05 tensor cores on hi+lo TF32 pairs, FP32 TMEM accumulators
+                                    (the QJL-corrected symmetric distances only) */
 } tq_precision;
 
 /* The QJL-corrected symmetric distances (space_turbo_quant.h:483-572, 731-945). */
@@ -201,15 +203,20 @@ tq_status tq_rotated_coords_batch_device(const tq_space *sp, const float *X, siz
 /* distanceBatchMToNSymmetric{Light,Full,FullPrepared} (:557-572, 618-647,
  * bindings.cpp:221-266, 312-334): out[m, n] row-major.  Host pointers,
  * synchronous.  Each code is reconstructed and passed through the QJL
- * Hadamard once; the pair terms are two FP32 contractions on the GPU. */
+ * Hadamard once; the pair terms are two contractions on the GPU:
+ * TQ_PRECISION_FP32 on CUDA cores (the drop-in), TQ_PRECISION_SPLIT_TF32 on
+ * tcgen05 tensor cores (hi/lo TF32 operands, FP32 accumulators; padded dims
+ * below 64 stay on CUDA cores).  TQ_PRECISION_SPLIT_BF16 is refused with
+ * TQ_ERR_NOT_SUPPORTED: the operands are values of the small centroid table,
+ * whose BF16-pair rounding errors add up instead of averaging out. */
 tq_status tq_distance_m_to_n_symmetric_qjl(const tq_space *sp, const uint8_t *codes_a, size_t m,
                                            const uint8_t *codes_b, size_t n, float *out,
-                                           tq_sym_variant variant);
+                                           tq_sym_variant variant, tq_precision precision);
 /* The same on device buffers, stream-ordered. */
 tq_status tq_distance_m_to_n_symmetric_qjl_device(const tq_space *sp, const uint8_t *codes_a,
                                                   size_t m, const uint8_t *codes_b, size_t n,
                                                   float *out, tq_sym_variant variant,
-                                                  void *stream);
+                                                  tq_precision precision, void *stream);
 
 /* prepareSymmetricQuery (:499-535; bindings.cpp:276-282) of one code (host
  * pointers): recon_q[padded_dim] = RHT_qjl(c * sigma), sign_q[padded_dim] =

@@ -316,6 +316,38 @@ def test_distance_symmetric_split_bf16_vs_oracle(cuda_ok, dim, bits):
     assert ok, err.max()
 
 
+@pytest.mark.parametrize("dim,bits", [(768, 8), (128, 8), (1536, 4)])
+@pytest.mark.parametrize("precision", ["fp32", "split_bf16"])
+def test_distance_symmetric_self_pairs_vs_fp64(cuda_ok, dim, bits, precision):
+    """Codes against themselves: every term of the contraction is the square
+    of a centroid value, so rounding errors share a sign and add up instead of
+    averaging out.  This is the worst case for the tensor-core form, and for
+    the reference as well: its FP32 sum over 2048 such terms is itself 1.4e-5
+    of the term scale away from FP64 here.  So the bar is 1e-5 of the term
+    scale against the FP64 evaluation; against the reference, the difference
+    is at most 1e-5 plus the reference's own distance from FP64."""
+    rng = np.random.default_rng(dim + 11 * bits)
+    X = rng.standard_normal((260, dim)).astype(np.float32)
+    X /= np.linalg.norm(X, axis=1, keepdims=True)
+    s, o = tq.TurboQuantSpace(dim, bits), O.OracleSpace(dim, bits)
+    codes = s.encode_batch(X)
+    d = s.distance_m_to_n_symmetric(codes[:130], codes, precision=precision)
+    ref = o.distance_m_to_n_symmetric(codes[:130], codes)
+    pairs = [(i, i) for i in range(130)] + [tuple(p) for p in rng.integers(0, [130, 260], (200, 2))]
+    ii, jj = np.array(pairs).T
+    f64 = np.array([o.distance_symmetric_f64(codes[i], codes[j]) for i, j in pairs])
+    cs = s.code_size_bytes()
+    ts = sym_term_scale(codes[:130], codes, cs, cs - 12)[ii, jj]
+    den = np.maximum(np.abs(f64), ts)
+    e64 = np.abs(d[ii, jj] - f64) / den
+    r64 = np.abs(ref[ii, jj] - f64) / den
+    eref = np.abs(d[ii, jj] - ref[ii, jj]) / den
+    print(f"{precision} sym self pairs {dim}/{bits}: vs FP64 max {e64.max():.2e}; "
+          f"reference vs FP64 max {r64.max():.2e}; vs reference max {eref.max():.2e}")
+    assert e64.max() < 1e-5, e64.max()
+    assert np.all(eref <= 1e-5 + r64), (eref - r64).max()
+
+
 def test_split_bf16_error_vs_fp64(cuda_ok):
     """Error of the tensor-core form against the FP64 evaluation, 10,000 sampled pairs."""
     rng = np.random.default_rng(10)

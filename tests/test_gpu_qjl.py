@@ -32,8 +32,8 @@ def _golden(dim, bits):
         return {k: z[k] for k in z.files}
 
 
-def _sym(s, variant, A, B):
-    return getattr(s, f"distance_m_to_n_symmetric_{variant}")(A, B)
+def _sym(s, variant, A, B, precision="fp32"):
+    return getattr(s, f"distance_m_to_n_symmetric_{variant}")(A, B, precision=precision)
 
 
 @pytest.mark.parametrize("dim,bits", QJL_CASES)
@@ -100,6 +100,59 @@ def test_symmetric_qjl_vs_oracle_and_fp64(cuda_ok, dim, bits):
         assert ok64, f"{variant}: max rel err vs FP64 {err64.max():.3e}"
 
 
+@pytest.mark.parametrize("dim,bits", [(3, 2), (64, 4), (128, 8), (200, 5), (1024, 4), (768, 9),
+                                      (1536, 4)])
+def test_symmetric_qjl_split_tf32_vs_oracle_and_fp64(cuda_ok, dim, bits):
+    """The tensor-core form (two TMEM accumulators over hi/lo TF32 planes):
+    two 128-row blocks and three 256-column tiles with ragged edges, every
+    variant within the distance tolerance of the reference and of FP64.
+    Padded dims below 64 (dim 3 here) keep the FP32 kernel."""
+    rng = np.random.default_rng(dim * 7 + bits)
+    X = rng.standard_normal((700, dim)).astype(np.float32)
+    X /= np.linalg.norm(X, axis=1, keepdims=True)
+    X[3] = 0.0
+    s, o = tq.TurboQuantSpace(dim, bits), O.OracleSpace(dim, bits)
+    codes = s.encode_batch(X)
+    A, B = codes[:150], codes[40:]
+    cs = s.code_size_bytes()
+    ts = sym_term_scale(A, B, cs, cs - 12)
+    for variant in ("light", "full", "full_prepared"):
+        got = _sym(s, variant, A, B, "split_tf32")
+        err, ok = dist_close(got, o.distance_m_to_n_symmetric_qjl(A, B, variant), ts)
+        print(f"split-TF32 {variant} {dim}/{bits}: max rel err vs oracle {err.max():.2e}")
+        assert ok, f"{variant}: max rel err vs oracle {err.max():.3e}"
+        pairs = rng.integers(0, [len(A), len(B)], size=(64, 2))
+        d64 = np.array([o.distance_symmetric_qjl_f64(A[i], B[j], variant) for i, j in pairs])
+        err64, ok64 = dist_close(got[pairs[:, 0], pairs[:, 1]], d64,
+                                 ts[pairs[:, 0], pairs[:, 1]])
+        assert ok64, f"{variant}: max rel err vs FP64 {err64.max():.3e}"
+
+
+@pytest.mark.parametrize("dim,bits", QJL_CASES)
+def test_symmetric_qjl_split_tf32_vs_golden(cuda_ok, dim, bits):
+    g, q = load_case(dim, bits), _golden(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    codes = g["codes"]
+    cs = s.code_size_bytes()
+    ts = sym_term_scale(codes[:8], codes, cs, cs - 12)
+    for variant, key in VARIANTS:
+        err, ok = dist_close(_sym(s, variant, codes[:8], codes, "split_tf32"), q[key], ts)
+        assert ok, f"{variant}: max rel err {err.max():.3e}"
+
+
+def test_symmetric_qjl_split_tf32_device_path_equals_host(cuda_ok):
+    import torch
+    X = np.random.default_rng(6).standard_normal((300, 512)).astype(np.float32)
+    s = tq.TurboQuantSpace(512, 4)
+    codes = s.encode_batch(X)
+    cd = torch.from_numpy(codes).cuda()
+    for variant in ("light", "full", "full_prepared"):
+        dv = _sym(s, variant, cd[:130], cd, "split_tf32")
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(dv.cpu().numpy(),
+                                      _sym(s, variant, codes[:130], codes, "split_tf32"))
+
+
 @pytest.mark.parametrize("dim,bits", [(3, 2), (128, 4), (768, 8), (1536, 4)])
 def test_prepare_symmetric_query_bit_exact(cuda_ok, dim, bits):
     X = np.random.default_rng(dim).standard_normal((4, dim)).astype(np.float32)
@@ -142,6 +195,15 @@ def test_symmetric_qjl_device_path_equals_host(cuda_ok):
         dv = _sym(s, variant, cd[:30], cd)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(dv.cpu().numpy(), _sym(s, variant, codes[:30], codes))
+
+
+def test_symmetric_qjl_refuses_split_bf16(cuda_ok):
+    """A BF16 pair is not accurate enough for these contractions (a code
+    against itself reaches 1e-5 of the distance), so it is refused."""
+    s = tq.TurboQuantSpace(256, 8)
+    codes = s.encode_batch(np.random.default_rng(0).standard_normal((5, 256)).astype(np.float32))
+    with pytest.raises(tq.TQError, match="SPLIT_TF32"):
+        s.distance_m_to_n_symmetric_light(codes, codes, precision="split_bf16")
 
 
 def test_symmetric_qjl_shapes_and_errors(cuda_ok):

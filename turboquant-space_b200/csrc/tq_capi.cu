@@ -860,18 +860,31 @@ namespace {
 
 constexpr size_t kSymqChunkBytes = size_t(512) << 20;  // column planes per chunk
 
+size_t sq_round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
 // Row planes built once (from row codes, or from a prepared code), column
-// planes built per chunk; one two-accumulator contraction per chunk.
+// planes built per chunk; one two-accumulator contraction per chunk: the FP32
+// CUDA-core kernel, or (split-TF32) the FP32 planes split into hi/lo TF32
+// planes (K padded to 32, rows to 128 / 256) for the tcgen05 kernel.  Padded
+// dims below 64 keep the FP32 kernel: a tile of so short a reduction is
+// mostly padding.
 struct SymqRunner {
     const tq_space *sp;
     int mode, ldk1, ldk2;
-    size_t m = 0, per = 0;
-    Scratch rows, cols;
+    bool tc;
+    int K1p = 0, K2p = 0;
+    size_t m = 0, m_pad = 0, per = 0;
+    Scratch rows, cols, rows_bf, cols_bf;
     float *P1a = nullptr, *P2a = nullptr, *sa = nullptr;
+    float *A1 = nullptr, *A2 = nullptr;  // hi then lo, m_pad x K1p / K2p each
+    int *err = nullptr;
 
-    SymqRunner(const tq_space *s, int md) : sp(s), mode(md) {
+    SymqRunner(const tq_space *s, int md, bool split_tf32 = false)
+        : sp(s), mode(md), tc(split_tf32 && s->D >= 64) {
         ldk1 = tq::symq_ldk((int)s->D);
         ldk2 = tq::symq_ldk(tq::symq_k2(md, (int)s->D));
+        K1p = (int)sq_round_up((size_t)ldk1, 32);
+        K2p = (int)sq_round_up((size_t)ldk2, 32);
     }
     size_t row_floats() const { return (size_t)ldk1 + ldk2 + 8; }
     tq_status alloc_rows(size_t rows_, cudaStream_t s) {
@@ -887,6 +900,14 @@ struct SymqRunner {
         if (st != TQ_OK) return st;
         TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, A, m, mode, true, P1a, ldk1, P2a, ldk2, sa, s),
                 "symmetric planes kernel");
+        if (!tc) return TQ_OK;
+        m_pad = sq_round_up(m, 128);
+        const size_t e1 = m_pad * K1p, e2 = m_pad * K2p;  // floats per plane
+        TQ_CUDA(rows_bf.alloc(sizeof(float) * 2 * (e1 + e2), s), "cudaMallocAsync(row TF32 planes)");
+        A1 = static_cast<float *>(rows_bf.p);
+        A2 = A1 + 2 * e1;
+        TQ_CUDA(tq::launch_split_tf32(P1a, m, ldk1, m_pad, K1p, A1, A1 + e1, s), "split kernel");
+        TQ_CUDA(tq::launch_split_tf32(P2a, m, ldk2, m_pad, K2p, A2, A2 + e2, s), "split kernel");
         return TQ_OK;
     }
     tq_status prepare_row_from_prepared(const float *recon, const float *sign, const float *sc,
@@ -899,6 +920,7 @@ struct SymqRunner {
     }
     // out[:, 0:n] (leading dimension ldo) for n column codes
     tq_status run_cols(const uint8_t *B, size_t n, float *out, size_t ldo, cudaStream_t s) {
+        if (tc) return run_cols_tc(B, n, out, ldo, s);
         if (!per) {
             per = std::max<size_t>(64, kSymqChunkBytes / (sizeof(float) * row_floats()));
             per = std::min(per, std::max<size_t>(n, 1));
@@ -915,7 +937,56 @@ struct SymqRunner {
         }
         return TQ_OK;
     }
+    tq_status run_cols_tc(const uint8_t *B, size_t n, float *out, size_t ldo, cudaStream_t s) {
+        const size_t f32_row = sizeof(float) * row_floats(), bf_row = (size_t)8 * (K1p + K2p);
+        if (!per) {
+            per = std::max<size_t>(256, (kSymqChunkBytes / (f32_row + bf_row)) & ~size_t(255));
+            per = std::min(per, sq_round_up(n, 256));
+            TQ_CUDA(cols.alloc(f32_row * per, s), "cudaMallocAsync(column planes)");
+            TQ_CUDA(cols_bf.alloc(bf_row * per + 16, s), "cudaMallocAsync(column TF32 planes)");
+            err = reinterpret_cast<int *>(static_cast<unsigned char *>(cols_bf.p) + bf_row * per);
+            TQ_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "memset");
+        }
+        float *P1b = static_cast<float *>(cols.p), *P2b = P1b + per * ldk1, *sb = P2b + per * ldk2;
+        const size_t b1 = per * K1p, b2 = per * K2p;  // floats per plane
+        float *B1 = static_cast<float *>(cols_bf.p), *B2 = B1 + 2 * b1;
+        const size_t a1 = m_pad * K1p, a2 = m_pad * K2p;
+        for (size_t c0 = 0; c0 < n; c0 += per) {
+            const size_t nc = std::min(per, n - c0), nc_pad = sq_round_up(nc, 256);
+            TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, B + c0 * sp->code_size, nc, mode, false, P1b,
+                                           ldk1, P2b, ldk2, sb, s),
+                    "symmetric planes kernel");
+            TQ_CUDA(tq::launch_split_tf32(P1b, nc, ldk1, nc_pad, K1p, B1, B1 + b1, s), "split kernel");
+            TQ_CUDA(tq::launch_split_tf32(P2b, nc, ldk2, nc_pad, K2p, B2, B2 + b2, s), "split kernel");
+            TQ_CUDA(tq::launch_tc_symq(A1, A1 + a1, B1, B1 + b1, K1p, A2, A2 + a2, B2, B2 + b2, K2p,
+                                       mode == tq::SYMQ_LIGHT, m, m_pad, nc, nc_pad, sa, sb, out + c0,
+                                       ldo, err, s),
+                    "tcgen05 symmetric contraction kernel");
+        }
+        return TQ_OK;
+    }
+    // Reports a bounded wait that gave up inside the tensor-core kernel.
+    tq_status finish(cudaStream_t s) {
+        if (!err) return TQ_OK;
+        int h = 0;
+        TQ_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H status");
+        TQ_CUDA(cudaStreamSynchronize(s), "sync");
+        if (h != 0) return fail(TQ_ERR_TIMEOUT, "tensor-core kernel: a pipeline wait timed out (code %d)", h);
+        return TQ_OK;
+    }
 };
+
+// The QJL-corrected symmetric contractions run in FP32 (CUDA cores) or
+// split-TF32 (tensor cores).  A BF16 pair is refused: its planes' rounding
+// errors do not average out (see tc_symq_kernel) and exceed 1e-5.
+tq_status symq_precision_ok(tq_precision p) {
+    if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_TF32) return TQ_OK;
+    if (p == TQ_PRECISION_SPLIT_BF16)
+        return fail(TQ_ERR_NOT_SUPPORTED,
+                    "QJL-corrected symmetric distances take TQ_PRECISION_FP32 or "
+                    "TQ_PRECISION_SPLIT_TF32 (a BF16 pair is not accurate enough here)");
+    return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)p);
+}
 
 int sym_mode(tq_sym_variant v) {
     switch (v) {
@@ -971,29 +1042,33 @@ tq_status tq_rotated_coords_batch(const tq_space *csp, const float *X, size_t n,
 
 tq_status tq_distance_m_to_n_symmetric_qjl_device(const tq_space *sp, const uint8_t *A, size_t m,
                                                   const uint8_t *B, size_t n, float *out,
-                                                  tq_sym_variant variant, void *stream) {
+                                                  tq_sym_variant variant, tq_precision precision,
+                                                  void *stream) {
     tq_status st = need_device(sp);
     if (st != TQ_OK) return st;
     const int mode = sym_mode(variant);
     if (mode < 0) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown symmetric variant %d", (int)variant);
+    if ((st = symq_precision_ok(precision)) != TQ_OK) return st;
     if (m == 0 || n == 0) return TQ_OK;
     DeviceGuard g(sp->device);
     if ((st = check_dev(A, m * sp->code_size, "codes_a")) != TQ_OK) return st;
     if ((st = check_dev(B, n * sp->code_size, "codes_b")) != TQ_OK) return st;
     if ((st = check_dev(out, m * n * 4, "out")) != TQ_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    SymqRunner r(sp, mode);
+    SymqRunner r(sp, mode, precision == TQ_PRECISION_SPLIT_TF32);
     if ((st = r.prepare_rows(A, m, s)) != TQ_OK) return st;
-    return r.run_cols(B, n, out, n, s);
+    if ((st = r.run_cols(B, n, out, n, s)) != TQ_OK) return st;
+    return r.finish(s);
 }
 
 tq_status tq_distance_m_to_n_symmetric_qjl(const tq_space *csp, const uint8_t *codes_a, size_t m,
                                            const uint8_t *codes_b, size_t n, float *out,
-                                           tq_sym_variant variant) {
+                                           tq_sym_variant variant, tq_precision precision) {
     tq_status st = need_device(csp);
     if (st != TQ_OK) return st;
     const int mode = sym_mode(variant);
     if (mode < 0) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown symmetric variant %d", (int)variant);
+    if ((st = symq_precision_ok(precision)) != TQ_OK) return st;
     if (m == 0 || n == 0) return TQ_OK;
     if (!codes_a || !codes_b || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
     auto *sp = const_cast<tq_space *>(csp);
@@ -1005,7 +1080,7 @@ tq_status tq_distance_m_to_n_symmetric_qjl(const tq_space *csp, const uint8_t *c
     Scratch dA;
     TQ_CUDA(dA.alloc(m * cs, s), "cudaMallocAsync(codes_a)");
     TQ_CUDA(cudaMemcpyAsync(dA.p, codes_a, m * cs, cudaMemcpyHostToDevice, s), "H2D codes_a");
-    SymqRunner r(sp, mode);
+    SymqRunner r(sp, mode, precision == TQ_PRECISION_SPLIT_TF32);
     if ((st = r.prepare_rows(static_cast<uint8_t *>(dA.p), m, s)) != TQ_OK) return st;
     size_t per = std::max<size_t>(1, std::min(kChunkBytes / cs, (kChunkBytes * 2) / (4 * m)));
     per = std::min(per, n);
@@ -1022,7 +1097,7 @@ tq_status tq_distance_m_to_n_symmetric_qjl(const tq_space *csp, const uint8_t *c
                 "D2H distances");
     }
     TQ_CUDA(cudaStreamSynchronize(s), "distance_m_to_n_symmetric (QJL)");
-    return TQ_OK;
+    return r.finish(s);
 }
 
 tq_status tq_prepare_symmetric_query(const tq_space *csp, const uint8_t *code, float *recon_q,

@@ -86,5 +86,10 @@ cudaError_t launch_symq_prepared_row(const float *recon, const float *sign, cons
 cudaError_t launch_symq_gemm(const float *P1a, const float *P2a, const float *sa, size_t m,
                              const float *P1b, const float *P2b, const float *sb, size_t n,
                              int ldk1, int ldk2, float *out, size_t ldo, cudaStream_t st);
+// FP32 plane (rows x lds) -> TF32 hi/lo planes in FP32 containers (rows_pad x
+// K, x = hi + lo to about 2^-22), zero past `rows` and past `lds`.
+// lds % 4 == 0, K % 4 == 0, lds <= K.
+cudaError_t launch_split_tf32(const float *src, size_t rows, int lds, size_t rows_pad, int K,
+                              float *hi, float *lo, cudaStream_t st);
 
 }  // namespace tq

@@ -60,6 +60,19 @@ cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part
                               const int *part_i, int k, size_t max_rows, float *out_d,
                               long long *out_i, cudaStream_t st);
 
+// The two contractions of the QJL-corrected symmetric distances on tcgen05
+// tensor cores: C1 = A1 B1^T (K1) and C2 = A2 B2^T (K2) over hi/lo TF32 planes
+// (FP32 containers, launch_split_tf32), then out[i, j] = max(0, na^2 + nb^2 -
+// 2 (C1 s1a s1b + clamp(C2 s2a s2b, +-|C1 s1a s1b|)) na nb) with the 8-float
+// row scalars sa / sb of tq_symq.cu.  exact2: both K2 planes are +-1 (lo
+// zero), one product per K step there.  K1, K2 % 32 == 0, m_pad % 128 == 0,
+// n_pad % 256 == 0.
+cudaError_t launch_tc_symq(const void *A1h, const void *A1l, const void *B1h, const void *B1l,
+                           int K1, const void *A2h, const void *A2l, const void *B2h,
+                           const void *B2l, int K2, bool exact2, size_t m, size_t m_pad, size_t n,
+                           size_t n_pad, const float *sa, const float *sb, float *out, size_t ldo,
+                           int *err, cudaStream_t st);
+
 // One thread waits on an mbarrier nothing arrives at; after budget_cycles the
 // wait gives up and writes a non-zero code to *err (the failure path of every
 // bounded wait in the tensor-core kernels).

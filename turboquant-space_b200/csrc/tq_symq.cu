@@ -269,6 +269,39 @@ __global__ void __launch_bounds__(256) symq_gemm_kernel(
     }
 }
 
+// x rounded to TF32 (10 fraction bits), nearest-even, kept in an FP32
+// container with the low 13 bits clear (finite x).
+__device__ __forceinline__ float round_tf32(float x) {
+    const uint32_t b = __float_as_uint(x);
+    return __uint_as_float((b + 0xFFFu + ((b >> 13) & 1u)) & ~0x1FFFu);
+}
+
+// FP32 plane -> hi/lo TF32 planes (x = hi + lo, hi = tf32(x),
+// lo = tf32(x - hi)), four columns per thread.
+__global__ void __launch_bounds__(256) split_tf32_kernel(const float *__restrict__ src, size_t rows,
+                                                         int lds, size_t rows_pad, int K,
+                                                         float *__restrict__ hi,
+                                                         float *__restrict__ lo) {
+    const size_t quads = (size_t)(K / 4), total = rows_pad * quads;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = t / quads;
+        const int k = (int)(t - r * quads) * 4;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (r < rows && k < lds) v = *reinterpret_cast<const float4 *>(src + r * (size_t)lds + k);
+        const float x[4] = {v.x, v.y, v.z, v.w};
+        float h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            h[i] = round_tf32(x[i]);
+            l[i] = round_tf32(__fsub_rn(x[i], h[i]));
+        }
+        const size_t o = r * (size_t)K + k;
+        *reinterpret_cast<float4 *>(hi + o) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4 *>(lo + o) = make_float4(l[0], l[1], l[2], l[3]);
+    }
+}
+
 template <template <int> class F, typename... Args>
 cudaError_t dispatch_logd_sq(int log2D, Args &&...args) {
     switch (log2D) {
@@ -367,6 +400,20 @@ cudaError_t launch_symq_prepared_row(const float *recon, const float *sign, cons
                                      float *P1, int ldk1, float *P2, int ldk2, float *scal,
                                      cudaStream_t st) {
     symq_prepared_row_kernel<<<1, 256, 0, st>>>(recon, sign, sc, D, P1, ldk1, P2, ldk2, scal);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_tf32(const float *src, size_t rows, int lds, size_t rows_pad, int K,
+                              float *hi, float *lo, cudaStream_t st) {
+    if (rows_pad == 0) return cudaSuccess;
+    if (lds % 4 || K % 4 || lds > K) return cudaErrorInvalidValue;
+    for (const void *p : {(const void *)src, (const void *)hi, (const void *)lo})
+        if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
+    size_t blocks = (rows_pad * (size_t)(K / 4) + 255) / 256;
+    const size_t cap = (size_t)sq_sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    split_tf32_kernel<<<(unsigned)(blocks ? blocks : 1), 256, 0, st>>>(src, rows, lds, rows_pad, K,
+                                                                       hi, lo);
     return cudaGetLastError();
 }
 

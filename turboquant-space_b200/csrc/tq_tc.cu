@@ -1,27 +1,42 @@
-// tq_tc.cu -- split-BF16 tensor-core contraction of the M x N distances on
-// sm_100a (tcgen05 + TMA), with the distance epilogue fused.
+// tq_tc.cu -- the tensor-core contractions of the M x N distances on sm_100a
+// (tcgen05 + TMA), with their epilogues fused: the split-BF16 asymmetric and
+// symmetric distances (tc_dist), their per-row top-k over a device-resident
+// index (tc_topk, the serving kernel) and the split-TF32 QJL-corrected
+// symmetric distances (tc_symq).
 //
-// C = Ah Bh^T + Ah Bl^T + Al Bh^T over BF16 hi/lo operand planes (x = hi + lo,
-// see tq_mton.cu), accumulated in FP32 in tensor memory; then
-// d = max(0, r2_i + c2_j - 2 (C_ij r1_i) c1_j) is written to out.  K blocks
-// from kbx on have an exact B (lo = 0: the +-1 QJL half of asymmetric planes):
-// there the Bl tile is not loaded and Ah Bl^T is not issued.
+// C = Ah Bh^T + Ah Bl^T + Al Bh^T over hi/lo operand planes (x = hi + lo,
+// see tq_mton.cu and tq_symq.cu), accumulated in FP32 in tensor memory.  A
+// product is skipped where its lo operand is zero by construction: B's lo
+// from K block kbx on (the +-1 QJL half of asymmetric planes), A's lo in a
+// segment marked a_exact (the +-1 signs of the light variant).
 //
-// Persistent kernel, one CTA per SM, 6 warps:
-//   warp 0      TMA producer: per K block of 64, loads Ah, Al (128 x 64) and
-//               Bh, Bl (256 x 64; Bl only below kbx) tiles, 128-byte
-//               swizzled, into a 2-stage ring
-//   warp 1      allocates 512 TMEM columns (two 128 x 256 FP32 accumulators);
-//               one thread issues 3 tcgen05.mma (M128 N256 K16) per K step
-//               (2 from kbx on)
-//               and commits to the stage's "empty" barrier and, after a
-//               tile's last K block, to the accumulator's "full" barrier
-//   warps 2..5  epilogue: tcgen05.ld 32x32b rows of the accumulator, apply the
-//               distance formula, store; then release the accumulator
-// Tiles are visited with the A-block index fastest so that CTAs running at the
-// same time share the B tile in L2.  Every mbarrier wait is bounded: after
-// ~2 s it records an error code in *err and the CTA winds down (frees its
-// tensor memory) instead of waiting forever.
+// Accumulation with promotion.  The tensor core's FP32 accumulation loses
+// low bits of what it adds to a large running sum, always toward zero, so a
+// reduction whose terms share a sign (a code against itself: squares of
+// centroid values) drifted by 1.3e-5 of the result at K = 2048 (measured).
+// Here the MMAs of a chunk of CH K blocks accumulate from zero into one of two
+// chunk buffers X0 / X1 in tensor memory; the epilogue warps add each chunk
+// into a running sum Y (one per K segment, also in tensor memory) with IEEE
+// FP32 adds while the MMAs fill the other buffer.  In each K step the small
+// products (hi x lo, lo x hi) are issued before hi x hi.  The drift is then
+// that of one chunk (CH = 2 K blocks) at any K.
+//
+// Persistent kernel, one CTA per SM, 6 warps, 128 x 128 tiles:
+//   warp 0      TMA producer: per K block (128 bytes of K: 64 BF16 or 32
+//               TF32 values) loads the Ah, Al, Bh, Bl tiles it needs,
+//               128-byte swizzled, into a ring of STAGES stages
+//   warp 1      allocates 512 tensor-memory columns (X0, X1, Y0, Y1, 128
+//               each); one thread issues the tcgen05.mma of each K block as
+//               its stage lands, into the current chunk's buffer, and commits
+//               the stage's "empty" barrier and, per chunk, the buffer's
+//               "full" barrier
+//   warps 2..5  epilogue: per chunk, tcgen05.ld the buffer, add it into the
+//               running sum Y with tcgen05.ld / st, release the buffer; per
+//               tile, the policy's epilogue (distances, top-k or the
+//               QJL-corrected distances) reads Y
+// Every mbarrier wait is bounded: after ~2 s it records an error code in
+// *err and the CTA winds down (frees its tensor memory) instead of waiting
+// forever.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -35,10 +50,12 @@
 namespace tq {
 namespace {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 64, TC_STAGES = 2;
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;   // 16 KB
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;   // 32 KB
-constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // 96 KB
+constexpr int TC_BM = 128, TC_BN = 128;
+constexpr int TC_BK = 64;    // BF16 values per K block (128 bytes)
+constexpr int SQ_TBK = 32;   // TF32 values per K block (128 bytes)
+constexpr int TC_A_BYTES = TC_BM * 128;  // 16 KB
+constexpr int TC_B_BYTES = TC_BN * 128;  // 16 KB
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // 64 KB
 constexpr int TC_TMEM_COLS = 512;
 constexpr int TC_THREADS = 192;
 // error codes written to *err
@@ -54,7 +71,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
 }
 
 // Shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile whose
-// rows are 128 bytes (64 BF16) and whose 8-row groups are 1024 bytes apart.
+// rows are 128 bytes and whose 8-row groups are 1024 bytes apart.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFFu);  // start address
@@ -65,27 +82,30 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
     return d;
 }
 
-// Instruction descriptor: kind::f16, BF16 x BF16 -> FP32, both K-major, M128 N256.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                            ((uint32_t)(TC_BM >> 4) << 24);
-
-__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
-        : "memory");
+// Instruction descriptor: FP32 accumulator, A and B of format `fmt` (1 =
+// BF16 for kind::f16, 2 = TF32 for kind::tf32), both K-major, M128 N128.
+constexpr uint32_t tc_idesc(uint32_t fmt) {
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+           ((uint32_t)(TC_BM >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_i(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
-                                       uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
+template <bool TF32>
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+    if constexpr (TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(tc_idesc(2)), "r"(acc)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(tc_idesc(1)), "r"(acc)
+            : "memory");
+    }
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -98,6 +118,25 @@ __device__ __forceinline__ void tc_fence_before() {
 }
 __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 32 consecutive 32-bit columns of this warp's 32 tensor-memory lanes; the
+// _nw form leaves the wait (tcgen05.wait::ld) to the caller.
+__device__ __forceinline__ void tmem_ld32_nw(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
@@ -114,31 +153,64 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
-    const __grid_constant__ CUtensorMap tm_ah, const __grid_constant__ CUtensorMap tm_al,
-    const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl, int K,
-    int kbx, unsigned num_mb, unsigned num_tiles, size_t m, size_t n, const float *__restrict__ r1,
-    const float *__restrict__ r2, const float *__restrict__ c1, const float *__restrict__ c2,
-    float *__restrict__ out, size_t ldo, int *err) {
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+        "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+        "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+        "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+        "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() {
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// The tensor maps of up to two K segments: [segment][Ah, Al, Bh, Bl].
+struct TcMaps {
+    CUtensorMap m[2][4];
+};
+
+// K blocks of each segment, the first block whose B lo is zero (kbx = KB: none)
+// and whether the segment's A lo is zero.
+struct TcShape {
+    int nseg;
+    int KB[2], kbx[2], a_exact[2];
+};
+
+// ---------------------------------------------------------------------------
+// The pipeline.  Epi supplies the tile schedule (tiles(), tile_at()) and the
+// epilogue State (tile() reads the running sums Y0 / Y1 of a finished tile,
+// finish() runs once after the last tile).
+// ---------------------------------------------------------------------------
+template <bool TF32, int STAGES, int CH, class Epi>
+__global__ void __launch_bounds__(TC_THREADS, 1) tcp_kernel(const __grid_constant__ TcMaps maps,
+                                                            const TcShape sh,
+                                                            const typename Epi::Params ep,
+                                                            int *err) {
+    constexpr int KBLK = TF32 ? SQ_TBK : TC_BK;  // values per K block
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles
     unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TC_STAGES * TC_STAGE_BYTES);
-    // bars: full[2], empty[2], tfull[2], tempty[2], drain; then the TMEM address slot
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 9);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * TC_STAGE_BYTES);
+    // bars: full[STAGES], empty[STAGES], xfull[2], xempty[2], drain; then the TMEM slot
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + 2);
-    const uint32_t tfull0 = smem_u32(bars + 4), tempty0 = smem_u32(bars + 6);
-    const uint32_t drain = smem_u32(bars + 8);
-
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
+    const uint32_t xfull0 = smem_u32(bars + 2 * STAGES), xempty0 = smem_u32(bars + 2 * STAGES + 2);
+    const uint32_t drain = smem_u32(bars + 2 * STAGES + 4);
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; ++s) {
+        for (int s = 0; s < STAGES; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
         }
         for (int b = 0; b < 2; ++b) {
-            mbar_init(tfull0 + 8 * b, 1);
-            mbar_init(tempty0 + 8 * b, 128);
+            mbar_init(xfull0 + 8 * b, 1);
+            mbar_init(xempty0 + 8 * b, 128);
         }
         mbar_init(drain, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -154,104 +226,201 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int KB = K / TC_BK;
+    const int ntiles = Epi::tiles(ep);
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
-            for (unsigned tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
-                const int mb = (int)(tile % num_mb), nb = (int)(tile / num_mb);
-                for (int kb = 0; kb < KB; ++kb, ++it) {
-                    const uint32_t s = it % TC_STAGES, ph = (it / TC_STAGES) & 1u;
-                    if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
-                    const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
-                    const uint32_t fb = full0 + 8 * s;
-                    const bool lo = kb < kbx;
-                    mbar_expect_tx(fb, lo ? TC_STAGE_BYTES : TC_STAGE_BYTES - TC_B_BYTES);
-                    tma_load_2d(base, &tm_ah, kb * TC_BK, mb * TC_BM, fb);
-                    tma_load_2d(base + TC_A_BYTES, &tm_al, kb * TC_BK, mb * TC_BM, fb);
-                    tma_load_2d(base + 2 * TC_A_BYTES, &tm_bh, kb * TC_BK, nb * TC_BN, fb);
-                    if (lo)
-                        tma_load_2d(base + 2 * TC_A_BYTES + TC_B_BYTES, &tm_bl, kb * TC_BK,
-                                    nb * TC_BN, fb);
+            for (int t = 0; t < ntiles && ok; ++t) {
+                int mb, nb;
+                Epi::tile_at(ep, t, mb, nb);
+                for (int sg = 0; sg < sh.nseg && ok; ++sg) {
+                    const CUtensorMap *mp = maps.m[sg];
+                    const bool alo = !sh.a_exact[sg];
+                    for (int kb = 0; kb < sh.KB[sg]; ++kb, ++it) {
+                        const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+                        if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
+                        const bool blo = kb < sh.kbx[sg];
+                        const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
+                        const uint32_t fb = full0 + 8 * s;
+                        mbar_expect_tx(fb, (alo ? 2 : 1) * TC_A_BYTES + (blo ? 2 : 1) * TC_B_BYTES);
+                        const int kx = kb * KBLK;
+                        tma_load_2d(base, &mp[0], kx, mb * TC_BM, fb);
+                        if (alo) tma_load_2d(base + TC_A_BYTES, &mp[1], kx, mb * TC_BM, fb);
+                        tma_load_2d(base + 2 * TC_A_BYTES, &mp[2], kx, nb * TC_BN, fb);
+                        if (blo) tma_load_2d(base + 2 * TC_A_BYTES + TC_B_BYTES, &mp[3], kx, nb * TC_BN, fb);
+                    }
                 }
             }
-            // drain: every stage issued must have landed before the CTA exits
-            for (uint32_t k = 0; k < TC_STAGES && k < it; ++k) {
+            // every stage issued must have landed before the CTA exits
+            for (uint32_t k = 0; k < (uint32_t)STAGES && k < it; ++k) {
                 const uint32_t j = it - 1 - k;
-                mbar_wait(full0 + 8 * (j % TC_STAGES), (j / TC_STAGES) & 1u, err, kErrFull);
+                mbar_drain(full0 + 8 * (j % STAGES), (j / STAGES) & 1u);
             }
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            uint32_t it = 0, t = 0;
+            uint32_t it = 0, gc = 0;
             bool ok = true;
-            for (unsigned tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++t) {
-                const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
-                if (!mbar_wait(tempty0 + 8 * b, tph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
-                tc_fence_after();
-                const uint32_t d_tmem = tmem_base + b * TC_BN;
-                for (int kb = 0; kb < KB; ++kb, ++it) {
-                    const uint32_t s = it % TC_STAGES, ph = (it / TC_STAGES) & 1u;
-                    if (!mbar_wait(full0 + 8 * s, ph, err, kErrFull)) { ok = false; break; }
-                    tc_fence_after();
-                    const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
-                    const uint32_t ah = base, al = base + TC_A_BYTES;
-                    const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TC_B_BYTES;
-                    const bool lo = kb < kbx;
+            for (int t = 0; t < ntiles && ok; ++t) {
+                for (int sg = 0; sg < sh.nseg && ok; ++sg) {
+                    const bool alo = !sh.a_exact[sg];
+                    for (int c0 = 0; c0 < sh.KB[sg] && ok; c0 += CH, ++gc) {
+                        const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
+                        if (!mbar_wait(xempty0 + 8 * b, xph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t d_tmem = tmem_base + b * TC_BN;
+                        const int c1 = c0 + CH < sh.KB[sg] ? c0 + CH : sh.KB[sg];
+                        uint32_t acc = 0u;
+                        for (int kb = c0; kb < c1; ++kb, ++it) {
+                            const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+                            if (!mbar_wait(full0 + 8 * s, ph, err, kErrFull)) { ok = false; break; }
+                            tc_fence_after();
+                            const bool blo = kb < sh.kbx[sg];
+                            const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
+                            const uint32_t ah = base, al = base + TC_A_BYTES;
+                            const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TC_B_BYTES;
 #pragma unroll
-                    for (int kk = 0; kk < TC_BK / 16; ++kk) {
-                        const uint32_t koff = kk * 32;  // 16 BF16 along K
-                        const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
-                        umma(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), acc);
-                        if (lo) umma(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), 1u);
-                        umma(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), 1u);
+                            for (int kk = 0; kk < 4; ++kk) {
+                                const uint32_t koff = kk * 32;  // one MMA's K: 32 bytes
+                                // the small products first, while the sum is smaller
+                                if (blo) {
+                                    umma<TF32>(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), acc);
+                                    acc = 1u;
+                                }
+                                if (alo) {
+                                    umma<TF32>(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), acc);
+                                    acc = 1u;
+                                }
+                                umma<TF32>(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), acc);
+                                acc = 1u;
+                            }
+                            umma_commit(empty0 + 8 * s);  // stage free once these MMAs are done
+                        }
+                        if (ok) umma_commit(xfull0 + 8 * b);  // chunk sum ready
                     }
-                    umma_commit(empty0 + 8 * s);  // smem stage free once these MMAs are done
                 }
-                if (ok) umma_commit(tfull0 + 8 * b);  // accumulator ready
             }
             // every MMA issued must be complete before the tensor memory is freed
             umma_commit(drain);
-            mbar_wait(drain, 0, err, kErrFull);
+            mbar_drain(drain, 0);
         }
     } else {
         // ---------------- epilogue (warps 2..5, 128 threads) ----------------
-        const int q = warp & 3;           // TMEM lane quadrant this warp may access
-        const int row_in_tile = 32 * q + lane;
-        uint32_t t = 0;
-        for (unsigned tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++t) {
-            const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
-            if (!mbar_wait(tfull0 + 8 * b, tph, err, kErrTmemFull)) break;
-            tc_fence_after();
-            const int mb = (int)(tile % num_mb), nb = (int)(tile / num_mb);
-            const size_t row = (size_t)mb * TC_BM + row_in_tile;
-            const bool row_ok = row < m;
-            const float rr1 = row_ok ? __ldg(r1 + row) : 0.0f;
-            const float rr2 = row_ok ? __ldg(r2 + row) : 0.0f;
-            float *orow = out + row * ldo;
-            const bool vec = ((ldo & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+        const int q = warp & 3;  // the tensor-memory lane quadrant this warp may access
+        const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16);
+        typename Epi::State st(ep, 32 * q + lane);
+        uint32_t gc = 0;
+        bool ok = true;
+        for (int t = 0; t < ntiles && ok; ++t) {
+            int mb, nb;
+            Epi::tile_at(ep, t, mb, nb);
+            for (int sg = 0; sg < sh.nseg && ok; ++sg) {
+                const uint32_t Y = lanes + (2 + sg) * TC_BN;
+                for (int c0 = 0; c0 < sh.KB[sg]; c0 += CH, ++gc) {
+                    const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
+                    if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t X = lanes + b * TC_BN;
+#pragma unroll 1
+                    for (int p = 0; p < TC_BN / 32; ++p) {
+                        uint32_t x[32], y[32];
+                        __syncwarp();
+                        tmem_ld32_nw(X + 32 * p, x);
+                        if (c0 != 0) tmem_ld32_nw(Y + 32 * p, y);
+                        tmem_wait_ld();
+                        if (c0 != 0) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                x[j] = __float_as_uint(__fadd_rn(__uint_as_float(y[j]), __uint_as_float(x[j])));
+                        }
+                        tmem_st32(Y + 32 * p, x);
+                    }
+                    tmem_wait_st();
+                    __syncwarp();
+                    tc_fence_before();
+                    mbar_arrive(xempty0 + 8 * b);
+                }
+            }
+            if (ok) st.tile(ep, mb, nb, lanes + 2 * TC_BN, lanes + 3 * TC_BN);
+        }
+        if (ok) st.finish(ep);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// Reads 32 columns of a running sum as floats.
+__device__ __forceinline__ void ld_sum32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    __syncwarp();
+    tmem_ld32(taddr, r);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// ---- epilogue policies --------------------------------------------------------
+// Tiles of an m_pad x n_pad output visited with the row-block index fastest,
+// so that CTAs running at the same time share the B tile in L2.
+struct GridTiles {
+    unsigned num_mb, num_tiles;
+    __device__ static int count(unsigned num_tiles) {
+        return blockIdx.x < num_tiles ? (int)((num_tiles - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+    }
+    __device__ void at(int t, int &mb, int &nb) const {
+        const unsigned tile = blockIdx.x + (unsigned)t * gridDim.x;
+        mb = (int)(tile % num_mb);
+        nb = (int)(tile / num_mb);
+    }
+};
+
+// d = max(0, r2_i + c2_j - 2 (C_ij r1_i) c1_j), stored to out[i * ldo + j].
+struct DistEpi {
+    struct Params {
+        GridTiles g;
+        size_t m, n;
+        const float *r1, *r2, *c1, *c2;
+        float *out;
+        size_t ldo;
+    };
+    __device__ static int tiles(const Params &p) { return GridTiles::count(p.g.num_tiles); }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) { p.g.at(t, mb, nb); }
+    struct State {
+        int rit;
+        bool vec;
+        __device__ State(const Params &p, int row_in_tile)
+            : rit(row_in_tile),
+              vec(((p.ldo & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.out) & 15) == 0)) {}
+        __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
+            const size_t row = (size_t)mb * TC_BM + rit;
+            const bool row_ok = row < p.m;
+            const float rr1 = row_ok ? __ldg(p.r1 + row) : 0.0f;
+            const float rr2 = row_ok ? __ldg(p.r2 + row) : 0.0f;
+            float *orow = p.out + row * p.ldo;
 #pragma unroll 1
             for (int ch = 0; ch < TC_BN / 32; ++ch) {
-                uint32_t r[32];
-                __syncwarp();
-                tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + b * TC_BN + ch * 32, r);
+                float c[32];
+                ld_sum32(y0 + 32 * ch, c);
                 const size_t col0 = (size_t)nb * TC_BN + ch * 32;
-                if (row_ok && col0 < n) {
+                if (!row_ok || col0 >= p.n) continue;
                 float dv[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const size_t col = col0 + j;
-                    const float cc1 = (col < n) ? __ldg(c1 + col) : 0.0f;
-                    const float cc2 = (col < n) ? __ldg(c2 + col) : 0.0f;
-                    const float ipt = __fmul_rn(__fmul_rn(__uint_as_float(r[j]), rr1), cc1);
-                    const float d = __fsub_rn(__fadd_rn(rr2, cc2), __fmul_rn(2.0f, ipt));
+                    const size_t col = col0 + j < p.n ? col0 + j : p.n - 1;
+                    const float ipt = __fmul_rn(__fmul_rn(c[j], rr1), __ldg(p.c1 + col));
+                    const float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
                     dv[j] = d > 0.0f ? d : 0.0f;
                 }
-                if (vec && col0 + 32 <= n) {
+                if (vec && col0 + 32 <= p.n) {
                     float4 *o4 = reinterpret_cast<float4 *>(orow + col0);
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
@@ -259,239 +428,205 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_dist_kernel(
                 } else {
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
-                        if (col0 + j < n) orow[col0 + j] = dv[j];
-                }
+                        if (col0 + j < p.n) orow[col0 + j] = dv[j];
                 }
             }
-            __syncwarp();
-            tc_fence_before();
-            mbar_arrive(tempty0 + 8 * b);
         }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 1) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"(TC_TMEM_COLS)
-                     : "memory");
-    }
-}
+        __device__ void finish(const Params &) {}
+    };
+};
 
-// ---------------------------------------------------------------------------
-// tc_topk_kernel: the same contraction over a device-resident index, with the
-// distances reduced to a per-row top-k instead of being stored.  The number of
-// query rows m is read from device memory (so that one captured launch serves
-// batches of any size up to the buffers' capacity).  CTA c takes row block
-// c / S and the contiguous slice c % S of the column tiles, S = grid / row
-// blocks; each epilogue thread keeps its row's best k (distance, index) pairs,
-// ties broken by the smaller index, and writes them to the partial buffers
-// part_d / part_i [(block * S + slice) * 128 + row][kTopKMax].
-// ---------------------------------------------------------------------------
 __device__ __forceinline__ bool better(float d, int i, float bd, int bi) {
     return d < bd || (d == bd && i < bi);
 }
 
-template <int BN, int STAGES>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_topk_kernel(
-    const __grid_constant__ CUtensorMap tm_ah, const __grid_constant__ CUtensorMap tm_al,
-    const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl, int K,
-    int kbx, const int *__restrict__ m_dev, unsigned nb_tiles, size_t n, const float *__restrict__ r1,
-    const float *__restrict__ r2, const float *__restrict__ c1, const float *__restrict__ c2, int k,
-    float *__restrict__ part_d, int *__restrict__ part_i, int *err) {
-    constexpr int B_BYTES = BN * TC_BK * 2;
-    constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * B_BYTES;
-    constexpr int TMEM_COLS = 2 * BN;
-    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                               ((uint32_t)(TC_BM >> 4) << 24);
-    const int m = *m_dev;
-    const int num_mb = (m + TC_BM - 1) / TC_BM;
-    if (num_mb <= 0 || num_mb > (int)gridDim.x) return;
-    const int S = (int)gridDim.x / num_mb;
-    if ((int)blockIdx.x >= num_mb * S) return;  // uniform over the CTA
-    const int mb = (int)blockIdx.x / S, slice = (int)blockIdx.x % S;
-    const unsigned nb0 = (unsigned)(((size_t)nb_tiles * slice) / S);
-    const unsigned nb1 = (unsigned)(((size_t)nb_tiles * (slice + 1)) / S);
-    const unsigned ntiles = nb1 - nb0;
-
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
-    // bars: full[STAGES], empty[STAGES], tfull[2], tempty[2], drain; then the TMEM slot
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
-    const uint32_t tfull0 = smem_u32(bars + 2 * STAGES), tempty0 = smem_u32(bars + 2 * STAGES + 2);
-    const uint32_t drain = smem_u32(bars + 2 * STAGES + 4);
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < STAGES; ++st) {
-            mbar_init(full0 + 8 * st, 1);
-            mbar_init(empty0 + 8 * st, 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(tfull0 + 8 * b, 1);
-            mbar_init(tempty0 + 8 * b, 128);
-        }
-        mbar_init(drain, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+// Per-row top-k over a device-resident index.  The number of query rows m is
+// read from device memory (so that one captured launch serves batches of any
+// size up to the buffers' capacity).  CTA c takes row block c / S and the
+// contiguous slice c % S of the column tiles, S = grid / row blocks; each
+// epilogue thread keeps its row's best k (distance, index) pairs, ties broken
+// by the smaller index, and writes them to the partial buffers
+// part_d / part_i [(block * S + slice) * 128 + row][kTopKMax].
+struct TopkEpi {
+    struct Params {
+        const int *m_dev;
+        unsigned nb_tiles;
+        size_t n;
+        const float *r1, *r2, *c1, *c2;
+        int k;
+        float *part_d;
+        int *part_i;
+    };
+    // this CTA's row block, column-tile range; false when it has no slice
+    __device__ static bool slice(const Params &p, int &mb, unsigned &nb0, unsigned &nb1) {
+        const int m = *p.m_dev;
+        const int num_mb = (m + TC_BM - 1) / TC_BM;
+        if (num_mb <= 0 || num_mb > (int)gridDim.x) return false;
+        const int S = (int)gridDim.x / num_mb;
+        if ((int)blockIdx.x >= num_mb * S) return false;
+        mb = (int)blockIdx.x / S;
+        const int sl = (int)blockIdx.x % S;
+        nb0 = (unsigned)(((size_t)p.nb_tiles * sl) / S);
+        nb1 = (unsigned)(((size_t)p.nb_tiles * (sl + 1)) / S);
+        return true;
     }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    __device__ static int tiles(const Params &p) {
+        int mb;
+        unsigned nb0, nb1;
+        return slice(p, mb, nb0, nb1) ? (int)(nb1 - nb0) : 0;
     }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem_base = *tmem_slot;
-    const int KB = K / TC_BK;
-
-    if (warp == 0) {
-        if (lane == 0) {
-            uint32_t it = 0;
-            bool ok = true;
-            for (unsigned t = 0; t < ntiles && ok; ++t) {
-                const int nb = (int)(nb0 + t);
-                for (int kb = 0; kb < KB; ++kb, ++it) {
-                    const uint32_t st = it % STAGES, ph = (it / STAGES) & 1u;
-                    if (!mbar_wait(empty0 + 8 * st, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
-                    const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
-                    const uint32_t fb = full0 + 8 * st;
-                    const bool lo = kb < kbx;
-                    mbar_expect_tx(fb, lo ? STAGE_BYTES : STAGE_BYTES - B_BYTES);
-                    tma_load_2d(base, &tm_ah, kb * TC_BK, mb * TC_BM, fb);
-                    tma_load_2d(base + TC_A_BYTES, &tm_al, kb * TC_BK, mb * TC_BM, fb);
-                    tma_load_2d(base + 2 * TC_A_BYTES, &tm_bh, kb * TC_BK, nb * BN, fb);
-                    if (lo)
-                        tma_load_2d(base + 2 * TC_A_BYTES + B_BYTES, &tm_bl, kb * TC_BK, nb * BN,
-                                    fb);
-                }
-            }
-            const uint32_t drain_n = it < (uint32_t)STAGES ? it : (uint32_t)STAGES;
-            for (uint32_t q = 0; q < drain_n; ++q) {
-                const uint32_t j = it - 1 - q;
-                mbar_wait(full0 + 8 * (j % STAGES), (j / STAGES) & 1u, err, kErrFull);
-            }
-        }
-    } else if (warp == 1) {
-        if (lane == 0) {
-            uint32_t it = 0;
-            bool ok = true;
-            for (unsigned t = 0; t < ntiles && ok; ++t) {
-                const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
-                if (!mbar_wait(tempty0 + 8 * b, tph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
-                tc_fence_after();
-                const uint32_t d_tmem = tmem_base + b * BN;
-                for (int kb = 0; kb < KB; ++kb, ++it) {
-                    const uint32_t st = it % STAGES, ph = (it / STAGES) & 1u;
-                    if (!mbar_wait(full0 + 8 * st, ph, err, kErrFull)) { ok = false; break; }
-                    tc_fence_after();
-                    const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
-                    const uint32_t ah = base, al = base + TC_A_BYTES;
-                    const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + B_BYTES;
-                    const bool lo = kb < kbx;
-#pragma unroll
-                    for (int kk = 0; kk < TC_BK / 16; ++kk) {
-                        const uint32_t koff = kk * 32;
-                        const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
-                        umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), IDESC, acc);
-                        if (lo)
-                            umma_i(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), IDESC, 1u);
-                        umma_i(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), IDESC, 1u);
-                    }
-                    umma_commit(empty0 + 8 * st);
-                }
-                if (ok) umma_commit(tfull0 + 8 * b);
-            }
-            umma_commit(drain);
-            mbar_wait(drain, 0, err, kErrFull);
-        }
-    } else {
-        const int q = warp & 3;
-        const int row_in_tile = 32 * q + lane;
-        const int row = mb * TC_BM + row_in_tile;
-        const bool row_ok = row < m;
-        const float rr1 = row_ok ? __ldg(r1 + row) : 0.0f;
-        const float rr2 = row_ok ? __ldg(r2 + row) : 0.0f;
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) {
+        unsigned nb0, nb1;
+        slice(p, mb, nb0, nb1);
+        nb = (int)nb0 + t;
+    }
+    struct State {
+        int rit, m;
+        bool valid;
+        float rr1 = 0.0f, rr2 = 0.0f;
         float bd[kTopKMax];
         int bi[kTopKMax];
-#pragma unroll
-        for (int t = 0; t < kTopKMax; ++t) {
-            bd[t] = INFINITY;
-            bi[t] = 0x7fffffff;
-        }
         float thr_d = INFINITY;
         int thr_i = 0x7fffffff;
-        for (unsigned t = 0; t < ntiles; ++t) {
-            const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
-            if (!mbar_wait(tfull0 + 8 * b, tph, err, kErrTmemFull)) break;
-            tc_fence_after();
-            const size_t colbase = (size_t)(nb0 + t) * BN;
+        __device__ State(const Params &p, int row_in_tile) : rit(row_in_tile) {
+            int mb;
+            unsigned nb0, nb1;
+            m = *p.m_dev;
+            valid = slice(p, mb, nb0, nb1);
+            const int row = valid ? mb * TC_BM + rit : 0;
+            if (valid && row < m) {
+                rr1 = __ldg(p.r1 + row);
+                rr2 = __ldg(p.r2 + row);
+            }
+#pragma unroll
+            for (int t = 0; t < kTopKMax; ++t) {
+                bd[t] = INFINITY;
+                bi[t] = 0x7fffffff;
+            }
+        }
+        __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
+            const bool row_ok = mb * TC_BM + rit < m;
+            const size_t colbase = (size_t)nb * TC_BN;
 #pragma unroll 1
-            for (int ch = 0; ch < BN / 32; ++ch) {
-                uint32_t r[32];
-                __syncwarp();
-                tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + b * BN + ch * 32, r);
+            for (int ch = 0; ch < TC_BN / 32; ++ch) {
+                float c[32];
+                ld_sum32(y0 + 32 * ch, c);
+                if (!row_ok) continue;
                 const size_t col0 = colbase + ch * 32;
-                if (row_ok) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const size_t col = col0 + j;
-                        if (col >= n) break;
-                        const float ipt = __fmul_rn(__fmul_rn(__uint_as_float(r[j]), rr1), __ldg(c1 + col));
-                        float d = __fsub_rn(__fadd_rn(rr2, __ldg(c2 + col)), __fmul_rn(2.0f, ipt));
-                        d = d > 0.0f ? d : 0.0f;
-                        const int ci = (int)col;
-                        if (better(d, ci, thr_d, thr_i)) {
-                            float cd = d;
-                            int cx = ci;
+                for (int j = 0; j < 32; ++j) {
+                    const size_t col = col0 + j;
+                    if (col >= p.n) break;
+                    const float ipt = __fmul_rn(__fmul_rn(c[j], rr1), __ldg(p.c1 + col));
+                    float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
+                    d = d > 0.0f ? d : 0.0f;
+                    const int ci = (int)col;
+                    if (better(d, ci, thr_d, thr_i)) {
+                        float cd = d;
+                        int cx = ci;
 #pragma unroll
-                            for (int u = 0; u < kTopKMax; ++u) {
-                                if (u < k) {
-                                    const bool sw = better(cd, cx, bd[u], bi[u]);
-                                    const float td = bd[u];
-                                    const int ti = bi[u];
-                                    bd[u] = sw ? cd : td;
-                                    bi[u] = sw ? cx : ti;
-                                    cd = sw ? td : cd;
-                                    cx = sw ? ti : cx;
-                                }
+                        for (int u = 0; u < kTopKMax; ++u) {
+                            if (u < p.k) {
+                                const bool sw = better(cd, cx, bd[u], bi[u]);
+                                const float td = bd[u];
+                                const int ti = bi[u];
+                                bd[u] = sw ? cd : td;
+                                bi[u] = sw ? cx : ti;
+                                cd = sw ? td : cd;
+                                cx = sw ? ti : cx;
                             }
-#pragma unroll
-                            for (int u = 0; u < kTopKMax; ++u)
-                                if (u == k - 1) {
-                                    thr_d = bd[u];
-                                    thr_i = bi[u];
-                                }
                         }
+#pragma unroll
+                        for (int u = 0; u < kTopKMax; ++u)
+                            if (u == p.k - 1) {
+                                thr_d = bd[u];
+                                thr_i = bi[u];
+                            }
                     }
                 }
             }
-            __syncwarp();
-            tc_fence_before();
-            mbar_arrive(tempty0 + 8 * b);
         }
-        if (row_ok) {
-            const size_t o = ((size_t)blockIdx.x * TC_BM + row_in_tile) * kTopKMax;
+        __device__ void finish(const Params &p) {
+            if (!valid) return;
+            int mb;
+            unsigned nb0, nb1;
+            slice(p, mb, nb0, nb1);
+            if (mb * TC_BM + rit >= m) return;
+            const size_t o = ((size_t)blockIdx.x * TC_BM + rit) * kTopKMax;
 #pragma unroll
             for (int u = 0; u < kTopKMax; ++u)
-                if (u < k) {
-                    part_d[o + u] = bd[u];
-                    part_i[o + u] = bi[u];
+                if (u < p.k) {
+                    p.part_d[o + u] = bd[u];
+                    p.part_i[o + u] = bi[u];
                 }
         }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 1) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"(TMEM_COLS)
-                     : "memory");
-    }
-}
+    };
+};
+
+// The QJL-corrected symmetric distances (tq_symq.cu): Y0 = C1, Y1 = C2,
+// ip_mse = C1 s1a s1b, corr = clamp(C2 s2a s2b, +-|ip_mse|),
+// ip = (ip_mse + corr) na nb, d = max(0, na^2 + nb^2 - 2 ip), with the
+// per-row scalars s = [s1, norm, s2, ...] (8 floats per row).
+struct SymqEpi {
+    struct Params {
+        GridTiles g;
+        size_t m, n;
+        const float *sa, *sb;
+        float *out;
+        size_t ldo;
+    };
+    __device__ static int tiles(const Params &p) { return GridTiles::count(p.g.num_tiles); }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) { p.g.at(t, mb, nb); }
+    struct State {
+        int rit;
+        bool vec;
+        __device__ State(const Params &p, int row_in_tile)
+            : rit(row_in_tile),
+              vec(((p.ldo & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.out) & 15) == 0)) {}
+        __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t y1) {
+            const size_t row = (size_t)mb * TC_BM + rit;
+            const bool row_ok = row < p.m;
+            const float s1a = row_ok ? __ldg(p.sa + 8 * row) : 0.0f;
+            const float na = row_ok ? __ldg(p.sa + 8 * row + 1) : 0.0f;
+            const float s2a = row_ok ? __ldg(p.sa + 8 * row + 2) : 0.0f;
+            const float na2 = __fmul_rn(na, na);
+            float *orow = p.out + row * p.ldo;
+#pragma unroll 1
+            for (int ch = 0; ch < TC_BN / 32; ++ch) {
+                float c1[32], c2[32];
+                ld_sum32(y0 + 32 * ch, c1);
+                ld_sum32(y1 + 32 * ch, c2);
+                const size_t col0 = (size_t)nb * TC_BN + ch * 32;
+                if (!row_ok || col0 >= p.n) continue;
+                float dv[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const size_t col = col0 + j < p.n ? col0 + j : p.n - 1;
+                    const float s1b = __ldg(p.sb + 8 * col), nb_ = __ldg(p.sb + 8 * col + 1);
+                    const float s2b = __ldg(p.sb + 8 * col + 2);
+                    const float ip_mse = __fmul_rn(__fmul_rn(c1[j], s1a), s1b);
+                    const float lim = fabsf(ip_mse);
+                    float corr = __fmul_rn(__fmul_rn(c2[j], s2a), s2b);
+                    corr = fmaxf(-lim, fminf(lim, corr));
+                    const float ip = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), na), nb_);
+                    const float d = __fsub_rn(__fadd_rn(na2, __fmul_rn(nb_, nb_)), __fmul_rn(2.0f, ip));
+                    dv[j] = d > 0.0f ? d : 0.0f;
+                }
+                if (vec && col0 + 32 <= p.n) {
+                    float4 *o4 = reinterpret_cast<float4 *>(orow + col0);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        o4[j] = make_float4(dv[4 * j], dv[4 * j + 1], dv[4 * j + 2], dv[4 * j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (col0 + j < p.n) orow[col0 + j] = dv[j];
+                }
+            }
+        }
+        __device__ void finish(const Params &) {}
+    };
+};
 
 // Merge of the per-slice candidates: one warp per query row.  Each lane keeps
 // the best k of its slices, then k rounds of a warp arg-min on (d, index)
@@ -614,28 +749,55 @@ bool make_map(CUtensorMap *map, const void *base, int K, size_t rows, int box_ro
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int BN, int STAGES>
-cudaError_t topk_variant(const void *Ah, const void *Al, size_t rows_pad, const void *Bh,
-                         const void *Bl, size_t n_pad, int K, int k_lo, const int *m_dev, size_t n,
-                         const float *r1, const float *r2, const float *c1, const float *c2, int k,
-                         float *part_d, int *part_i, int *err, int grid, cudaStream_t st) {
-    if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || rows_pad % TC_BM || n_pad % BN)
-        return cudaErrorInvalidValue;
-    for (const void *p : {Ah, Al, Bh, Bl})
-        if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
-    alignas(64) CUtensorMap mah, mal, mbh, mbl;
-    if (!make_map(&mah, Ah, K, rows_pad, TC_BM) || !make_map(&mal, Al, K, rows_pad, TC_BM) ||
-        !make_map(&mbh, Bh, K, n_pad, BN) || !make_map(&mbl, Bl, k_lo, n_pad, BN))
-        return cudaErrorInvalidValue;
-    constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * BN * TC_BK * 2;
-    const size_t smem = (size_t)STAGES * STAGE_BYTES + 256 + 1024;
-    auto kern = tc_topk_kernel<BN, STAGES>;
+// FP32 planes (TF32 operands): K x rows, 32-value (128-byte) boxes, 128-byte swizzle.
+bool make_map_f32(CUtensorMap *map, const void *base, int K, size_t rows, int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)K * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)SQ_TBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// CH: K blocks per promoted chunk.
+template <bool TF32, int STAGES, int CH, class Epi>
+cudaError_t tcp_launch(const TcMaps &maps, const TcShape &sh, const typename Epi::Params &ep,
+                       int *err, unsigned grid, cudaStream_t st) {
+    static_assert(CH >= 1, "a chunk holds at least one K block");
+    const size_t smem = (size_t)STAGES * TC_STAGE_BYTES + 256 + 1024;
+    auto kern = tcp_kernel<TF32, STAGES, CH, Epi>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, k_lo / TC_BK, m_dev,
-                                         (unsigned)(n_pad / BN), n, r1, r2, c1, c2, k, part_d,
-                                         part_i, err);
+    kern<<<grid, TC_THREADS, smem, st>>>(maps, sh, ep, err);
     return cudaGetLastError();
+}
+
+bool aligned16(std::initializer_list<const void *> ps) {
+    for (const void *p : ps)
+        if (reinterpret_cast<uintptr_t>(p) & 15) return false;
+    return true;
+}
+
+unsigned sm_grid(size_t tiles) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (unsigned)(tiles < (size_t)sms ? tiles : (size_t)sms);
+}
+
+// BF16 planes of one K segment: A (K x m_pad), B hi (K x n_pad), B lo (k_lo x n_pad).
+bool bf16_maps(TcMaps &mp, TcShape &sh, const void *Ah, const void *Al, size_t m_pad,
+               const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo) {
+    sh = TcShape{};
+    sh.nseg = 1;
+    sh.KB[0] = K / TC_BK;
+    sh.kbx[0] = k_lo / TC_BK;
+    sh.a_exact[0] = 0;
+    return make_map(&mp.m[0][0], Ah, K, m_pad, TC_BM) && make_map(&mp.m[0][1], Al, K, m_pad, TC_BM) &&
+           make_map(&mp.m[0][2], Bh, K, n_pad, TC_BN) && make_map(&mp.m[0][3], Bl, k_lo, n_pad, TC_BN);
 }
 
 }  // namespace
@@ -652,12 +814,16 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
                            const int *m_dev, size_t n, const float *r1, const float *r2,
                            const float *c1, const float *c2, int k, float *part_d, int *part_i,
                            int *err, int grid, cudaStream_t st) {
-    if (k < 1 || k > kTopKMax) return cudaErrorInvalidValue;
-    if (variant == 1)
-        return topk_variant<128, 3>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo, m_dev, n, r1, r2, c1,
-                                    c2, k, part_d, part_i, err, grid, st);
-    return topk_variant<256, 2>(Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo, m_dev, n, r1, r2, c1, c2,
-                                k, part_d, part_i, err, grid, st);
+    if (k < 1 || k > kTopKMax || grid < 1) return cudaErrorInvalidValue;
+    if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || rows_pad % TC_BM || n_pad % TC_BN)
+        return cudaErrorInvalidValue;
+    if (!aligned16({Ah, Al, Bh, Bl})) return cudaErrorMisalignedAddress;
+    alignas(64) TcMaps mp;
+    TcShape sh;
+    if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
+    const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+    if (variant == 1) return tcp_launch<false, 2, 2, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    return tcp_launch<false, 3, 2, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
 }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
@@ -675,30 +841,50 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
                            const float *r1, const float *r2, const float *c1, const float *c2,
                            float *out, size_t ldo, int *err, cudaStream_t st) {
     if (m == 0 || n == 0) return cudaSuccess;
-    if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || m_pad % TC_BM || n_pad % TC_BN)
+    if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || m_pad % TC_BM || n_pad % TC_BN ||
+        m > m_pad || n > n_pad)
         return cudaErrorInvalidValue;
-    // TMA: 16-byte aligned bases and row strides
-    for (const void *p : {Ah, Al, Bh, Bl})
-        if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
-    alignas(64) CUtensorMap mah, mal, mbh, mbl;
-    if (!make_map(&mah, Ah, K, m_pad, TC_BM) || !make_map(&mal, Al, K, m_pad, TC_BM) ||
-        !make_map(&mbh, Bh, K, n_pad, TC_BN) || !make_map(&mbl, Bl, k_lo, n_pad, TC_BN))
-        return cudaErrorInvalidValue;
-    const size_t smem = (size_t)TC_STAGES * TC_STAGE_BYTES + 256 + 1024;
-    cudaError_t e = cudaFuncSetAttribute(tc_dist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
+    if (!aligned16({Ah, Al, Bh, Bl})) return cudaErrorMisalignedAddress;
+    alignas(64) TcMaps mp;
+    TcShape sh;
+    if (!bf16_maps(mp, sh, Ah, Al, m_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
     const unsigned num_mb = (unsigned)(m_pad / TC_BM);
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
-    if (tiles > 0xFFFFFFFFull) return cudaErrorInvalidValue;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned grid = (unsigned)(tiles < (size_t)sms ? tiles : (size_t)sms);
-    tc_dist_kernel<<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, K, k_lo / TC_BK, num_mb,
-                                                   (unsigned)tiles, m, n, r1, r2, c1, c2, out, ldo,
-                                                   err);
-    return cudaGetLastError();
+    if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    const DistEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, r1, r2, c1, c2, out, ldo};
+    return tcp_launch<false, 3, 2, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
+}
+
+cudaError_t launch_tc_symq(const void *A1h, const void *A1l, const void *B1h, const void *B1l,
+                           int K1, const void *A2h, const void *A2l, const void *B2h,
+                           const void *B2l, int K2, bool exact2, size_t m, size_t m_pad, size_t n,
+                           size_t n_pad, const float *sa, const float *sb, float *out, size_t ldo,
+                           int *err, cudaStream_t st) {
+    if (m == 0 || n == 0) return cudaSuccess;
+    if (K1 <= 0 || K2 <= 0 || K1 % SQ_TBK || K2 % SQ_TBK || m_pad % TC_BM || n_pad % TC_BN ||
+        m > m_pad || n > n_pad)
+        return cudaErrorInvalidValue;
+    if (!aligned16({A1h, A1l, B1h, B1l, A2h, A2l, B2h, B2l})) return cudaErrorMisalignedAddress;
+    alignas(64) TcMaps mp;
+    const void *pl[2][4] = {{A1h, A1l, B1h, B1l}, {A2h, A2l, B2h, B2l}};
+    const int Ks[2] = {K1, K2};
+    for (int sg = 0; sg < 2; ++sg)
+        for (int o = 0; o < 4; ++o)
+            if (!make_map_f32(&mp.m[sg][o], pl[sg][o], Ks[sg], o < 2 ? m_pad : n_pad, o < 2 ? TC_BM : TC_BN))
+                return cudaErrorInvalidValue;
+    TcShape sh{};
+    sh.nseg = 2;
+    sh.KB[0] = K1 / SQ_TBK;
+    sh.KB[1] = K2 / SQ_TBK;
+    sh.kbx[0] = sh.KB[0];
+    sh.kbx[1] = exact2 ? 0 : sh.KB[1];
+    sh.a_exact[0] = 0;
+    sh.a_exact[1] = exact2 ? 1 : 0;
+    const unsigned num_mb = (unsigned)(m_pad / TC_BM);
+    const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
+    if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    const SymqEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, sa, sb, out, ldo};
+    return tcp_launch<true, 3, 2, SymqEpi>(mp, sh, ep, err, sm_grid(tiles), st);
 }
 
 }  // namespace tq

@@ -444,9 +444,10 @@ class TurboQuantSpace:
         return out
 
     # -- QJL-corrected symmetric distances (bindings.cpp:221-334) --------------
-    def _symmetric_qjl(self, codes_a, codes_b, variant):
+    def _symmetric_qjl(self, codes_a, codes_b, variant, precision):
         cs = self.code_size_bytes()
         v = _capi.SYM_VARIANT[variant]
+        prec = _capi.PRECISION[precision]
         if _is_device(codes_a) or _is_device(codes_b):
             aptr, m = _codes_dev(codes_a, cs)
             bptr, n = _codes_dev(codes_b, cs)
@@ -455,7 +456,7 @@ class TurboQuantSpace:
             out = torch.empty((m, n), dtype=torch.float32, device=dev)
             check(lib().tq_distance_m_to_n_symmetric_qjl_device(
                 self._h, C.c_void_p(aptr), m, C.c_void_p(bptr), n, C.c_void_p(out.data_ptr()), v,
-                C.c_void_p(stream)))
+                prec, C.c_void_p(stream)))
             return out
         mva, mvb = memoryview(codes_a), memoryview(codes_b)
         if mva.itemsize != 1 or mvb.itemsize != 1:
@@ -465,20 +466,23 @@ class TurboQuantSpace:
         a, m = _codes_host(codes_a, cs)
         b, n = _codes_host(codes_b, cs)
         out = np.empty((m, n), np.float32)
-        check(lib().tq_distance_m_to_n_symmetric_qjl(self._h, _ptr(a), m, _ptr(b), n, _ptr(out), v))
+        check(lib().tq_distance_m_to_n_symmetric_qjl(self._h, _ptr(a), m, _ptr(b), n, _ptr(out), v,
+                                                     prec))
         return out
 
-    def distance_m_to_n_symmetric_full(self, codes_a, codes_b):
+    # precision="fp32" is the drop-in (CUDA cores); "split_tf32" runs the two
+    # contractions on tcgen05 tensor cores (hi/lo TF32 operands, FP32 sums).
+    def distance_m_to_n_symmetric_full(self, codes_a, codes_b, precision="fp32"):
         """distanceBatchMToNSymmetricFull: MSE + all four QJL terms (:618-631, 731-800)."""
-        return self._symmetric_qjl(codes_a, codes_b, "full")
+        return self._symmetric_qjl(codes_a, codes_b, "full", precision)
 
-    def distance_m_to_n_symmetric_light(self, codes_a, codes_b):
+    def distance_m_to_n_symmetric_light(self, codes_a, codes_b, precision="fp32"):
         """distanceBatchMToNSymmetricLight: MSE + the sign-agreement term (:634-647, 902-945)."""
-        return self._symmetric_qjl(codes_a, codes_b, "light")
+        return self._symmetric_qjl(codes_a, codes_b, "light", precision)
 
-    def distance_m_to_n_symmetric_full_prepared(self, codes_a, codes_b):
+    def distance_m_to_n_symmetric_full_prepared(self, codes_a, codes_b, precision="fp32"):
         """distanceBatchMToNSymmetricFullPrepared: row codes prepared once (:557-572, 808-878)."""
-        return self._symmetric_qjl(codes_a, codes_b, "full_prepared")
+        return self._symmetric_qjl(codes_a, codes_b, "full_prepared", precision)
 
     def prepare_symmetric_query(self, code):
         """prepareSymmetricQuery (:499-535) of one code: a PreparedSymCode."""

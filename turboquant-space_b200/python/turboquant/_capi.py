@@ -21,7 +21,7 @@ TQ_ERR_TIMEOUT = 5
 TQ_ERR_BUSY = 6
 TQ_ERR_NOT_SUPPORTED = 7
 
-PRECISION = {"fp32": 0, "split_bf16": 1}
+PRECISION = {"fp32": 0, "split_bf16": 1, "split_tf32": 2}
 
 # Every symbol include/turboquant_b200.h declares.
 EXPORTS = (
@@ -146,9 +146,10 @@ def lib() -> C.CDLL:
     L.tq_rotated_coords_batch_device.restype = st
     L.tq_rotated_coords_batch_device.argtypes = [vp, fp, sz, fp, vp]
     L.tq_distance_m_to_n_symmetric_qjl.restype = st
-    L.tq_distance_m_to_n_symmetric_qjl.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int]
+    L.tq_distance_m_to_n_symmetric_qjl.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int, C.c_int]
     L.tq_distance_m_to_n_symmetric_qjl_device.restype = st
-    L.tq_distance_m_to_n_symmetric_qjl_device.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int, vp]
+    L.tq_distance_m_to_n_symmetric_qjl_device.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int,
+                                                          C.c_int, vp]
     L.tq_prepare_symmetric_query.restype = st
     L.tq_prepare_symmetric_query.argtypes = [vp, u8p, fp, fp, fp]
     L.tq_distance_1_to_n_symmetric_full.restype = st
