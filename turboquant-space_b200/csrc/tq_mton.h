@@ -34,8 +34,8 @@ cudaError_t launch_sgemm_dist(const float *A, const float *B, int K, size_t m, s
                               cudaStream_t st);
 
 // The same with C = Ah Bh^T + Ah Bl^T + Al Bh^T on tcgen05 tensor cores
-// (FP32 accumulators in tensor memory).  K % 64 == 0, m_pad % 128 == 0,
-// n_pad % 256 == 0.  Bl has k_lo columns (k_lo % 64 == 0, k_lo <= K): B's lo
+// (FP32 accumulators in tensor memory, promoted to an IEEE FP32 running sum
+// every few K blocks).  K % 64 == 0, m_pad % 128 == 0, n_pad % 128 == 0.  Bl has k_lo columns (k_lo % 64 == 0, k_lo <= K): B's lo
 // part is zero beyond them, where the Ah Bl^T product is skipped.  `err`
 // (device int) is set non-zero if a bounded wait in the kernel gave up.
 cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const void *Bl, int K,
@@ -47,7 +47,8 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
 // k (<= 16) smallest (distance, index) pairs, ties to the smaller index.
 // The row count is read from m_dev; `grid` CTAs split the rows into 128-row
 // blocks and the columns into slices; partials hold grid * 128 * 16 entries.
-// Variant 0: 128 x 256 tiles, 2 stages; variant 1: 128 x 128 tiles, 3 stages.
+// 128 x 128 tiles; variant 0: 3 stages, 4-block promoted chunks; variant 1:
+// 2 stages, 2-block chunks.
 constexpr int kTopKMax = 16;
 int tc_topk_variants();
 cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,

@@ -21,7 +21,7 @@
 // products (hi x lo, lo x hi) are issued before hi x hi.  The drift is then
 // that of one chunk (CH = 2 K blocks) at any K.
 //
-// Persistent kernel, one CTA per SM, 6 warps, 128 x 128 tiles:
+// Persistent kernel, one CTA per SM, 10 warps (6 for two K segments), 128 x 128 tiles:
 //   warp 0      TMA producer: per K block (128 bytes of K: 64 BF16 or 32
 //               TF32 values) loads the Ah, Al, Bh, Bl tiles it needs,
 //               128-byte swizzled, into a ring of STAGES stages
@@ -30,10 +30,12 @@
 //               its stage lands, into the current chunk's buffer, and commits
 //               the stage's "empty" barrier and, per chunk, the buffer's
 //               "full" barrier
-//   warps 2..5  epilogue: per chunk, tcgen05.ld the buffer, add it into the
-//               running sum Y with tcgen05.ld / st, release the buffer; per
-//               tile, the policy's epilogue (distances, top-k or the
-//               QJL-corrected distances) reads Y
+//   warps 2..5  promotion: per chunk, tcgen05.ld the buffer, add it into the
+//               running sum Y with tcgen05.ld / st, release the buffer
+//   warps 6..9  per tile, the policy's epilogue (distances, top-k) reads Y,
+//               double-buffered over tiles; with two K segments (the
+//               QJL-corrected distances, Y0 and Y1 per tile) warps 2..5 run
+//               it themselves after the tile's promotions
 // Every mbarrier wait is bounded: after ~2 s it records an error code in
 // *err and the CTA winds down (frees its tensor memory) instead of waiting
 // forever.
@@ -57,7 +59,9 @@ constexpr int TC_A_BYTES = TC_BM * 128;  // 16 KB
 constexpr int TC_B_BYTES = TC_BN * 128;  // 16 KB
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // 64 KB
 constexpr int TC_TMEM_COLS = 512;
-constexpr int TC_THREADS = 192;
+// threads: producer, MMA and 4 epilogue warps; plus 4 finalize warps when the
+// running sum is double-buffered (one K segment)
+constexpr int tc_threads(bool split) { return split ? 320 : 192; }
 // error codes written to *err
 constexpr int kErrFull = 1, kErrEmpty = 2, kErrTmemFull = 3, kErrTmemEmpty = 4;
 
@@ -186,23 +190,30 @@ struct TcShape {
 // The pipeline.  Epi supplies the tile schedule (tiles(), tile_at()) and the
 // epilogue State (tile() reads the running sums Y0 / Y1 of a finished tile,
 // finish() runs once after the last tile).
+// SPLIT (one K segment): the running sum is double-buffered over tiles (tile t
+// in Y[t & 1]) and 4 more warps (6..9) run the tile epilogue, so that it
+// overlaps the next tile's MMAs and promotions; the promotion warps then wait
+// for Y[t & 1] to be read ("yempty") and signal it complete ("yfull").
+// Otherwise (two segments, Y0 and Y1 per tile) warps 2..5 do both.
 // ---------------------------------------------------------------------------
-template <bool TF32, int STAGES, int CH, class Epi>
-__global__ void __launch_bounds__(TC_THREADS, 1) tcp_kernel(const __grid_constant__ TcMaps maps,
-                                                            const TcShape sh,
-                                                            const typename Epi::Params ep,
-                                                            int *err) {
+template <bool TF32, int STAGES, int CH, bool SPLIT, class Epi>
+__global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_constant__ TcMaps maps,
+                                                                   const TcShape sh,
+                                                                   const typename Epi::Params ep,
+                                                                   int *err) {
     constexpr int KBLK = TF32 ? SQ_TBK : TC_BK;  // values per K block
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles
     unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * TC_STAGE_BYTES);
-    // bars: full[STAGES], empty[STAGES], xfull[2], xempty[2], drain; then the TMEM slot
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
+    // bars: full[STAGES], empty[STAGES], xfull[2], xempty[2], drain, yfull[2],
+    // yempty[2]; then the TMEM slot
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 9);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
     const uint32_t xfull0 = smem_u32(bars + 2 * STAGES), xempty0 = smem_u32(bars + 2 * STAGES + 2);
     const uint32_t drain = smem_u32(bars + 2 * STAGES + 4);
+    const uint32_t yfull0 = smem_u32(bars + 2 * STAGES + 5), yempty0 = smem_u32(bars + 2 * STAGES + 7);
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(full0 + 8 * s, 1);
@@ -211,6 +222,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tcp_kernel(const __grid_constan
         for (int b = 0; b < 2; ++b) {
             mbar_init(xfull0 + 8 * b, 1);
             mbar_init(xempty0 + 8 * b, 128);
+            mbar_init(yfull0 + 8 * b, 128);
+            mbar_init(yempty0 + 8 * b, 128);
         }
         mbar_init(drain, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -308,18 +321,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tcp_kernel(const __grid_constan
             umma_commit(drain);
             mbar_drain(drain, 0);
         }
-    } else {
-        // ---------------- epilogue (warps 2..5, 128 threads) ----------------
+    } else if (!SPLIT || warp < 6) {
+        // ---------------- promotion (warps 2..5, 128 threads) ----------------
+        // (without SPLIT these warps also run the tile epilogue)
         const int q = warp & 3;  // the tensor-memory lane quadrant this warp may access
         const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16);
         typename Epi::State st(ep, 32 * q + lane);
         uint32_t gc = 0;
         bool ok = true;
         for (int t = 0; t < ntiles && ok; ++t) {
-            int mb, nb;
-            Epi::tile_at(ep, t, mb, nb);
+            const uint32_t yb = (uint32_t)t & 1u, yph = ((uint32_t)t >> 1) & 1u;
+            if constexpr (SPLIT) {
+                if (!mbar_wait(yempty0 + 8 * yb, yph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
+                tc_fence_after();
+            }
             for (int sg = 0; sg < sh.nseg && ok; ++sg) {
-                const uint32_t Y = lanes + (2 + sg) * TC_BN;
+                const uint32_t Y = lanes + (2 + (SPLIT ? yb : (uint32_t)sg)) * TC_BN;
                 for (int c0 = 0; c0 < sh.KB[sg]; c0 += CH, ++gc) {
                     const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
                     if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
@@ -345,7 +362,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tcp_kernel(const __grid_constan
                     mbar_arrive(xempty0 + 8 * b);
                 }
             }
-            if (ok) st.tile(ep, mb, nb, lanes + 2 * TC_BN, lanes + 3 * TC_BN);
+            if (!ok) break;
+            if constexpr (SPLIT) {
+                mbar_arrive(yfull0 + 8 * yb);  // Y[yb] complete (its stores were waited for)
+            } else {
+                int mb, nb;
+                Epi::tile_at(ep, t, mb, nb);
+                st.tile(ep, mb, nb, lanes + 2 * TC_BN, lanes + 3 * TC_BN);
+            }
+        }
+        if constexpr (!SPLIT) {
+            if (ok) st.finish(ep);
+        }
+    } else {
+        // ---------------- tile epilogue (warps 6..9, SPLIT only) ----------------
+        const int q = warp & 3;
+        const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16);
+        typename Epi::State st(ep, 32 * q + lane);
+        bool ok = true;
+        for (int t = 0; t < ntiles; ++t) {
+            const uint32_t yb = (uint32_t)t & 1u, yph = ((uint32_t)t >> 1) & 1u;
+            if (!mbar_wait(yfull0 + 8 * yb, yph, err, kErrTmemFull)) { ok = false; break; }
+            tc_fence_after();
+            int mb, nb;
+            Epi::tile_at(ep, t, mb, nb);
+            st.tile(ep, mb, nb, lanes + (2 + yb) * TC_BN, 0u);
+            __syncwarp();
+            tc_fence_before();
+            mbar_arrive(yempty0 + 8 * yb);
         }
         if (ok) st.finish(ep);
     }
@@ -507,6 +551,16 @@ struct TopkEpi {
         __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
             const bool row_ok = mb * TC_BM + rit < m;
             const size_t colbase = (size_t)nb * TC_BN;
+            // the list in registers for the tile (the State itself may live in local memory)
+            float d_[kTopKMax];
+            int i_[kTopKMax];
+#pragma unroll
+            for (int u = 0; u < kTopKMax; ++u) {
+                d_[u] = bd[u];
+                i_[u] = bi[u];
+            }
+            float td = thr_d;
+            int ti = thr_i;
 #pragma unroll 1
             for (int ch = 0; ch < TC_BN / 32; ++ch) {
                 float c[32];
@@ -521,30 +575,37 @@ struct TopkEpi {
                     float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
                     d = d > 0.0f ? d : 0.0f;
                     const int ci = (int)col;
-                    if (better(d, ci, thr_d, thr_i)) {
+                    if (better(d, ci, td, ti)) {
                         float cd = d;
                         int cx = ci;
 #pragma unroll
                         for (int u = 0; u < kTopKMax; ++u) {
                             if (u < p.k) {
-                                const bool sw = better(cd, cx, bd[u], bi[u]);
-                                const float td = bd[u];
-                                const int ti = bi[u];
-                                bd[u] = sw ? cd : td;
-                                bi[u] = sw ? cx : ti;
-                                cd = sw ? td : cd;
-                                cx = sw ? ti : cx;
+                                const bool sw = better(cd, cx, d_[u], i_[u]);
+                                const float od = d_[u];
+                                const int ox = i_[u];
+                                d_[u] = sw ? cd : od;
+                                i_[u] = sw ? cx : ox;
+                                cd = sw ? od : cd;
+                                cx = sw ? ox : cx;
                             }
                         }
 #pragma unroll
                         for (int u = 0; u < kTopKMax; ++u)
                             if (u == p.k - 1) {
-                                thr_d = bd[u];
-                                thr_i = bi[u];
+                                td = d_[u];
+                                ti = i_[u];
                             }
                     }
                 }
             }
+#pragma unroll
+            for (int u = 0; u < kTopKMax; ++u) {
+                bd[u] = d_[u];
+                bi[u] = i_[u];
+            }
+            thr_d = td;
+            thr_i = ti;
         }
         __device__ void finish(const Params &p) {
             if (!valid) return;
@@ -763,15 +824,16 @@ bool make_map_f32(CUtensorMap *map, const void *base, int K, size_t rows, int bo
 }
 
 // CH: K blocks per promoted chunk.
-template <bool TF32, int STAGES, int CH, class Epi>
+template <bool TF32, int STAGES, int CH, bool SPLIT, class Epi>
 cudaError_t tcp_launch(const TcMaps &maps, const TcShape &sh, const typename Epi::Params &ep,
                        int *err, unsigned grid, cudaStream_t st) {
     static_assert(CH >= 1, "a chunk holds at least one K block");
+    if (SPLIT && sh.nseg != 1) return cudaErrorInvalidValue;  // Y[t & 1] needs the second Y
     const size_t smem = (size_t)STAGES * TC_STAGE_BYTES + 256 + 1024;
-    auto kern = tcp_kernel<TF32, STAGES, CH, Epi>;
+    auto kern = tcp_kernel<TF32, STAGES, CH, SPLIT, Epi>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, TC_THREADS, smem, st>>>(maps, sh, ep, err);
+    kern<<<grid, tc_threads(SPLIT), smem, st>>>(maps, sh, ep, err);
     return cudaGetLastError();
 }
 
@@ -822,8 +884,8 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
     TcShape sh;
     if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
     const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
-    if (variant == 1) return tcp_launch<false, 2, 2, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
-    return tcp_launch<false, 3, 2, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    if (variant == 1) return tcp_launch<false, 2, 2, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    return tcp_launch<false, 3, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
 }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
@@ -852,7 +914,7 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
     if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
     const DistEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, r1, r2, c1, c2, out, ldo};
-    return tcp_launch<false, 3, 2, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
+    return tcp_launch<false, 3, 4, true, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
 }
 
 cudaError_t launch_tc_symq(const void *A1h, const void *A1l, const void *B1h, const void *B1l,
@@ -884,7 +946,7 @@ cudaError_t launch_tc_symq(const void *A1h, const void *A1l, const void *B1h, co
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
     if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
     const SymqEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, sa, sb, out, ldo};
-    return tcp_launch<true, 3, 2, SymqEpi>(mp, sh, ep, err, sm_grid(tiles), st);
+    return tcp_launch<true, 3, 4, false, SymqEpi>(mp, sh, ep, err, sm_grid(tiles), st);
 }
 
 }  // namespace tq
