@@ -139,6 +139,19 @@ __device__ __forceinline__ void tmem_ld32_nw(uint32_t taddr, uint32_t (&r)[32]) 
         : "r"(taddr)
         : "memory");
 }
+// 16 consecutive 32-bit columns of this warp's lanes; the caller waits
+// (tcgen05.wait::ld) before reading them.
+__device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -479,6 +492,220 @@ struct DistEpi {
         __device__ void finish(const Params &) {}
     };
 };
+
+// ---------------------------------------------------------------------------
+// tcw_dist_kernel: the M x N distances with 128 x 256 tiles.  A 128 x 128 tile
+// with three operand reads per K step needs more shared-memory bandwidth than
+// the SM has once the TMA writes are counted (128 B/clk of MMA operands + 85
+// B/clk of copies), which held tcp_kernel near half of the tensor cycles; a
+// 256-wide tile needs 96 + 62.5 B/clk.  The two 256-column chunk buffers then
+// fill the tensor memory, so the running sum lives in registers: 8 epilogue
+// warps, two per lane quadrant, each thread one row and 128 of the columns.
+// The promotion loads a chunk in 16-column pieces, the next piece in flight
+// while the current one is added, so that the MMAs seldom wait for a chunk
+// buffer; the distances are written from the registers.  Otherwise as
+// tcp_kernel (promoted chunks of CH K blocks, bounded waits).
+// ---------------------------------------------------------------------------
+constexpr int TW_BN = 256;
+constexpr int TW_B_BYTES = TW_BN * 128;                           // 32 KB
+constexpr int TW_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TW_B_BYTES;  // 96 KB
+constexpr int TW_EPI_WARPS = 8, TW_COLS = TW_BN * 4 / TW_EPI_WARPS;  // 128 columns per thread
+constexpr int TW_THREADS = 32 * (2 + TW_EPI_WARPS);
+constexpr uint32_t kIdescW = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TW_BN >> 3) << 17) |
+                             ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_w(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdescW), "r"(acc)
+        : "memory");
+}
+
+template <int STAGES, int CH>
+__global__ void __launch_bounds__(TW_THREADS, 1) tcw_dist_kernel(const __grid_constant__ TcMaps maps,
+                                                                 const TcShape sh,
+                                                                 const DistEpi::Params ep,
+                                                                 int *err) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * TW_STAGE_BYTES);
+    // bars: full[STAGES], empty[STAGES], xfull[2], xempty[2], drain; then the TMEM slot
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
+    const uint32_t xfull0 = smem_u32(bars + 2 * STAGES), xempty0 = smem_u32(bars + 2 * STAGES + 2);
+    const uint32_t drain = smem_u32(bars + 2 * STAGES + 4);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(xfull0 + 8 * b, 1);
+            mbar_init(xempty0 + 8 * b, 32 * TW_EPI_WARPS);
+        }
+        mbar_init(drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int ntiles = GridTiles::count(ep.g.num_tiles);
+    const int KB = sh.KB[0], kbx = sh.kbx[0];
+    const CUtensorMap *mp = maps.m[0];
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = 0; t < ntiles && ok; ++t) {
+                int mb, nb;
+                ep.g.at(t, mb, nb);
+                for (int kb = 0; kb < KB; ++kb, ++it) {
+                    const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+                    if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
+                    const bool blo = kb < kbx;
+                    const uint32_t base = smem_u32(smem + s * TW_STAGE_BYTES);
+                    const uint32_t fb = full0 + 8 * s;
+                    mbar_expect_tx(fb, 2 * TC_A_BYTES + (blo ? 2 : 1) * TW_B_BYTES);
+                    const int kx = kb * TC_BK;
+                    tma_load_2d(base, &mp[0], kx, mb * TC_BM, fb);
+                    tma_load_2d(base + TC_A_BYTES, &mp[1], kx, mb * TC_BM, fb);
+                    tma_load_2d(base + 2 * TC_A_BYTES, &mp[2], kx, nb * TW_BN, fb);
+                    if (blo) tma_load_2d(base + 2 * TC_A_BYTES + TW_B_BYTES, &mp[3], kx, nb * TW_BN, fb);
+                }
+            }
+            for (uint32_t k = 0; k < (uint32_t)STAGES && k < it; ++k) {
+                const uint32_t j = it - 1 - k;
+                mbar_drain(full0 + 8 * (j % STAGES), (j / STAGES) & 1u);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            uint32_t it = 0, gc = 0;
+            bool ok = true;
+            for (int t = 0; t < ntiles && ok; ++t) {
+                for (int c0 = 0; c0 < KB && ok; c0 += CH, ++gc) {
+                    const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
+                    if (!mbar_wait(xempty0 + 8 * b, xph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t d_tmem = tmem_base + b * TW_BN;
+                    const int c1 = c0 + CH < KB ? c0 + CH : KB;
+                    uint32_t acc = 0u;
+                    for (int kb = c0; kb < c1; ++kb, ++it) {
+                        const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+                        if (!mbar_wait(full0 + 8 * s, ph, err, kErrFull)) { ok = false; break; }
+                        tc_fence_after();
+                        const bool blo = kb < kbx;
+                        const uint32_t base = smem_u32(smem + s * TW_STAGE_BYTES);
+                        const uint32_t ah = base, al = base + TC_A_BYTES;
+                        const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TW_B_BYTES;
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            const uint32_t koff = kk * 32;
+                            if (blo) {
+                                umma_w(d_tmem, sw128_desc(ah + koff), sw128_desc(bl + koff), acc);
+                                acc = 1u;
+                            }
+                            umma_w(d_tmem, sw128_desc(al + koff), sw128_desc(bh + koff), acc);
+                            umma_w(d_tmem, sw128_desc(ah + koff), sw128_desc(bh + koff), 1u);
+                            acc = 1u;
+                        }
+                        umma_commit(empty0 + 8 * s);
+                    }
+                    if (ok) umma_commit(xfull0 + 8 * b);
+                }
+            }
+            umma_commit(drain);
+            mbar_drain(drain, 0);
+        }
+    } else {
+        // ---------------- epilogue (warps 2..9, 256 threads) ----------------
+        const int q = warp & 3, h = (warp - 2) >> 2;  // lane quadrant, column half
+        const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(TW_COLS * h);
+        const int rit = 32 * q + lane;
+        const bool vec = ((ep.ldo & 3) == 0) && ((reinterpret_cast<uintptr_t>(ep.out) & 15) == 0);
+        float y[TW_COLS];
+        uint32_t gc = 0;
+        bool ok = true;
+        for (int t = 0; t < ntiles && ok; ++t) {
+            int mb, nb;
+            ep.g.at(t, mb, nb);
+            for (int c0 = 0; c0 < KB; c0 += CH, ++gc) {
+                const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
+                if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t X = lanes + b * TW_BN;
+                uint32_t xa[16], xb[16];
+                __syncwarp();
+                tmem_ld16_nw(X, xa);
+                tmem_wait_ld();
+#pragma unroll
+                for (int p = 0; p < TW_COLS / 16; ++p) {
+                    uint32_t(&cur)[16] = (p & 1) ? xb : xa;
+                    uint32_t(&nxt)[16] = (p & 1) ? xa : xb;
+                    if (p + 1 < TW_COLS / 16) tmem_ld16_nw(X + 16 * (p + 1), nxt);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const float a = __uint_as_float(cur[j]);
+                        y[16 * p + j] = c0 == 0 ? a : __fadd_rn(y[16 * p + j], a);
+                    }
+                    tmem_wait_ld();
+                }
+                __syncwarp();
+                tc_fence_before();
+                mbar_arrive(xempty0 + 8 * b);
+            }
+            if (!ok) break;
+            // d = max(0, r2 + c2 - 2 (C r1) c1) from the registers
+            const size_t row = (size_t)mb * TC_BM + rit;
+            if (row >= ep.m) continue;
+            const float rr1 = __ldg(ep.r1 + row), rr2 = __ldg(ep.r2 + row);
+            float *orow = ep.out + row * ep.ldo;
+            const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
+#pragma unroll
+            for (int g = 0; g < TW_COLS / 4; ++g) {  // groups of 4 columns
+                const size_t col0 = cbase + 4 * g;
+                if (col0 >= ep.n) break;
+                float dv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const size_t col = col0 + u < ep.n ? col0 + u : ep.n - 1;
+                    const float ipt = __fmul_rn(__fmul_rn(y[4 * g + u], rr1), __ldg(ep.c1 + col));
+                    const float d = __fsub_rn(__fadd_rn(rr2, __ldg(ep.c2 + col)), __fmul_rn(2.0f, ipt));
+                    dv[u] = d > 0.0f ? d : 0.0f;
+                }
+                if (vec && col0 + 4 <= ep.n) {
+                    *reinterpret_cast<float4 *>(orow + col0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (col0 + u < ep.n) orow[col0 + u] = dv[u];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
 
 __device__ __forceinline__ bool better(float d, int i, float bd, int bi) {
     return d < bd || (d == bd && i < bi);
@@ -913,6 +1140,20 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
     const unsigned num_mb = (unsigned)(m_pad / TC_BM);
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
     if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    if (n_pad % TW_BN == 0) {
+        // 128 x 256 tiles (tcw_dist_kernel): B maps with 256-row boxes
+        if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
+            return cudaErrorInvalidValue;
+        const size_t wtiles = (size_t)num_mb * (n_pad / TW_BN);
+        const DistEpi::Params ep{GridTiles{num_mb, (unsigned)wtiles}, m, n, r1, r2, c1, c2, out, ldo};
+        constexpr int STAGES = 2;
+        const size_t smem = (size_t)STAGES * TW_STAGE_BYTES + 256 + 1024;
+        auto kern = tcw_dist_kernel<STAGES, 4>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<sm_grid(wtiles), TW_THREADS, smem, st>>>(mp, sh, ep, err);
+        return cudaGetLastError();
+    }
     const DistEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, r1, r2, c1, c2, out, ldo};
     return tcp_launch<false, 3, 4, true, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
 }
