@@ -274,7 +274,8 @@ void tq_index_destroy(tq_index *ix);
 /* A server answering top-k (k <= 16) for requests of up to max_rows queries
  * (a multiple of 128).  `slots` batches may be in flight at once (fewer if
  * they do not fit in half of the free device memory); kernel_variant -1
- * autotunes the contraction's tile shape per batch-size bucket; queue_rows
+ * autotunes the contraction's tile shape per batch-size bucket, 0..2 fixes it
+ * (0: 128 x 256 tiles; 1, 2: 128 x 128 tiles with 3 or 2 stages); queue_rows
  * bounds the queued query rows (0: 16 x max_rows), beyond which submit
  * returns TQ_ERR_BUSY. */
 tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int kernel_variant,

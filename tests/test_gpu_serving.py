@@ -68,7 +68,7 @@ def test_index_search_exact_topk(corpus):
     assert exact >= 270
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_kernel_variants_agree(corpus, variant):
     space, codes, Q, ref, index = corpus
     with index.serve(k=10, max_rows=256, slots=1, kernel_variant=variant) as sv:
@@ -132,7 +132,7 @@ def test_autotuner_reports_each_bucket(corpus):
     with index.serve(k=10, max_rows=512, slots=1) as sv:
         t = sv.tuning()
     assert [b["bucket_rows"] for b in t] == [128, 256, 512]
-    assert all(b["variant"] in (0, 1) and b["ms"] > 0 for b in t)
+    assert all(b["variant"] in (0, 1, 2) and b["ms"] > 0 for b in t)
 
 
 def test_fewer_codes_than_k(cuda_ok):

@@ -47,17 +47,21 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
 // k (<= 16) smallest (distance, index) pairs, ties to the smaller index.
 // The row count is read from m_dev; `grid` CTAs split the rows into 128-row
 // blocks and the columns into slices; partials hold grid * 128 * 16 entries.
-// 128 x 128 tiles; variant 0: 3 stages, 4-block promoted chunks; variant 1:
-// 2 stages, 2-block chunks.
+// Variant 0: 128 x 256 tiles (n_pad % 256 == 0), two partial lists per (row,
+// slice); variant 1: 128 x 128 tiles, 3 stages, 4-block promoted chunks;
+// variant 2: 128 x 128 tiles, 2 stages, 2-block chunks.  The partial buffers
+// hold grid * 128 * tc_topk_lists(variant) * kTopKMax entries.
 constexpr int kTopKMax = 16;
+constexpr int kTopKListsMax = 2;
 int tc_topk_variants();
+int tc_topk_lists(int variant);
 cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
                            const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo,
                            const int *m_dev,
                            size_t n, const float *r1, const float *r2, const float *c1,
                            const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
                            cudaStream_t st);
-cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
+cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,
                               const int *part_i, int k, size_t max_rows, float *out_d,
                               long long *out_i, cudaStream_t st);
 

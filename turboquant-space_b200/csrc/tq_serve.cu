@@ -162,7 +162,8 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
                            sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->k, sl.d_pd, sl.d_pi, sl.d_err,
                            sv->grid, st);
     if (e != cudaSuccess) return e;
-    e = tq::launch_topk_merge(sl.d_m, sv->grid, sl.d_pd, sl.d_pi, sv->k, rows_cap, sl.d_od, sl.d_oi, st);
+    e = tq::launch_topk_merge(sl.d_m, sv->grid, tq::tc_topk_lists(var), sl.d_pd, sl.d_pi, sv->k,
+                              rows_cap, sl.d_od, sl.d_oi, st);
     if (e != cudaSuccess) return e;
     if (copies) {
         e = cudaMemcpyAsync(sl.h_d, sl.d_od, (size_t)rows_cap * sv->k * 4, cudaMemcpyDeviceToHost, st);
@@ -196,7 +197,7 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     };
     const size_t o_q = take(R * sp->dim * 4), o_m = take(16), o_prep = take(R * (2 * D + 2) * 4);
     const size_t o_ap = take(R * K * 4), o_r1 = take(R * 4), o_r2 = take(R * 4);
-    const size_t parts = (size_t)sv->grid * 128 * tq::kTopKMax;
+    const size_t parts = (size_t)sv->grid * 128 * tq::kTopKListsMax * tq::kTopKMax;
     const size_t o_pd = take(parts * 4), o_pi = take(parts * 4), o_od = take(R * k * 4);
     const size_t o_oi = take(R * k * 8), o_err = take(16);
     TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
@@ -481,7 +482,7 @@ tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int ker
     cudaMemGetInfo(&free_b, &total_b);
     const size_t D = ix->sp->D, K = (size_t)ix->K, R = (size_t)max_rows;
     const size_t slot_bytes = R * (ix->sp->dim * 4 + (2 * D + 2) * 4 + K * 4 + 8 + (size_t)k * 12) +
-                              (size_t)sms * 128 * tq::kTopKMax * 8 + 4096;
+                              (size_t)sms * 128 * tq::kTopKListsMax * tq::kTopKMax * 8 + 4096;
     const size_t fit = std::max<size_t>(1, (free_b / 2) / slot_bytes);
     slots = (int)std::min<size_t>((size_t)slots, fit);
     sv->slots.resize(slots);

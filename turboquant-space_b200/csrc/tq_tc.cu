@@ -494,7 +494,8 @@ struct DistEpi {
 };
 
 // ---------------------------------------------------------------------------
-// tcw_dist_kernel: the M x N distances with 128 x 256 tiles.  A 128 x 128 tile
+// tcw_kernel: the M x N distances and the serving top-k with 128 x 256 tiles
+// (epilogue policies WDist, WTopk).  A 128 x 128 tile
 // with three operand reads per K step needs more shared-memory bandwidth than
 // the SM has once the TMA writes are counted (128 B/clk of MMA operands + 85
 // B/clk of copies), which held tcp_kernel near half of the tensor cycles; a
@@ -523,11 +524,10 @@ __device__ __forceinline__ void umma_w(uint32_t d_tmem, uint64_t a, uint64_t b, 
         : "memory");
 }
 
-template <int STAGES, int CH>
-__global__ void __launch_bounds__(TW_THREADS, 1) tcw_dist_kernel(const __grid_constant__ TcMaps maps,
-                                                                 const TcShape sh,
-                                                                 const DistEpi::Params ep,
-                                                                 int *err) {
+template <int STAGES, int CH, class W>
+__global__ void __launch_bounds__(TW_THREADS, 1) tcw_kernel(const __grid_constant__ TcMaps maps,
+                                                            const TcShape sh,
+                                                            const typename W::Params ep, int *err) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * TW_STAGE_BYTES);
@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tcw_dist_kernel(const __grid_co
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int ntiles = GridTiles::count(ep.g.num_tiles);
+    const int ntiles = W::tiles(ep);
     const int KB = sh.KB[0], kbx = sh.kbx[0];
     const CUtensorMap *mp = maps.m[0];
 
@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tcw_dist_kernel(const __grid_co
             bool ok = true;
             for (int t = 0; t < ntiles && ok; ++t) {
                 int mb, nb;
-                ep.g.at(t, mb, nb);
+                W::tile_at(ep, t, mb, nb);
                 for (int kb = 0; kb < KB; ++kb, ++it) {
                     const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
                     if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
@@ -635,14 +635,13 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tcw_dist_kernel(const __grid_co
         // ---------------- epilogue (warps 2..9, 256 threads) ----------------
         const int q = warp & 3, h = (warp - 2) >> 2;  // lane quadrant, column half
         const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(TW_COLS * h);
-        const int rit = 32 * q + lane;
-        const bool vec = ((ep.ldo & 3) == 0) && ((reinterpret_cast<uintptr_t>(ep.out) & 15) == 0);
+        typename W::State st(ep, 32 * q + lane, h);
         float y[TW_COLS];
         uint32_t gc = 0;
         bool ok = true;
         for (int t = 0; t < ntiles && ok; ++t) {
             int mb, nb;
-            ep.g.at(t, mb, nb);
+            W::tile_at(ep, t, mb, nb);
             for (int c0 = 0; c0 < KB; c0 += CH, ++gc) {
                 const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
                 if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
@@ -669,33 +668,9 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tcw_dist_kernel(const __grid_co
                 mbar_arrive(xempty0 + 8 * b);
             }
             if (!ok) break;
-            // d = max(0, r2 + c2 - 2 (C r1) c1) from the registers
-            const size_t row = (size_t)mb * TC_BM + rit;
-            if (row >= ep.m) continue;
-            const float rr1 = __ldg(ep.r1 + row), rr2 = __ldg(ep.r2 + row);
-            float *orow = ep.out + row * ep.ldo;
-            const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
-#pragma unroll
-            for (int g = 0; g < TW_COLS / 4; ++g) {  // groups of 4 columns
-                const size_t col0 = cbase + 4 * g;
-                if (col0 >= ep.n) break;
-                float dv[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const size_t col = col0 + u < ep.n ? col0 + u : ep.n - 1;
-                    const float ipt = __fmul_rn(__fmul_rn(y[4 * g + u], rr1), __ldg(ep.c1 + col));
-                    const float d = __fsub_rn(__fadd_rn(rr2, __ldg(ep.c2 + col)), __fmul_rn(2.0f, ipt));
-                    dv[u] = d > 0.0f ? d : 0.0f;
-                }
-                if (vec && col0 + 4 <= ep.n) {
-                    *reinterpret_cast<float4 *>(orow + col0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                } else {
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (col0 + u < ep.n) orow[col0 + u] = dv[u];
-                }
-            }
+            st.tile(ep, mb, nb, y);
         }
+        if (ok) st.finish(ep);
     }
     tc_fence_before();
     __syncthreads();
@@ -851,6 +826,137 @@ struct TopkEpi {
     };
 };
 
+// ---- epilogue policies of tcw_kernel: each thread holds one row's running
+// sums of TW_COLS columns (half h of the 256-column tile) in registers.
+struct WDist {
+    using Params = DistEpi::Params;
+    __device__ static int tiles(const Params &p) { return GridTiles::count(p.g.num_tiles); }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) { p.g.at(t, mb, nb); }
+    struct State {
+        int rit, h;
+        bool vec;
+        __device__ State(const Params &p, int row_in_tile, int half)
+            : rit(row_in_tile), h(half),
+              vec(((p.ldo & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.out) & 15) == 0)) {}
+        // d = max(0, r2 + c2 - 2 (C r1) c1) from the registers
+        __device__ void tile(const Params &p, int mb, int nb, const float (&y)[TW_COLS]) {
+            const size_t row = (size_t)mb * TC_BM + rit;
+            if (row >= p.m) return;
+            const float rr1 = __ldg(p.r1 + row), rr2 = __ldg(p.r2 + row);
+            float *orow = p.out + row * p.ldo;
+            const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
+#pragma unroll
+            for (int g = 0; g < TW_COLS / 4; ++g) {  // groups of 4 columns
+                const size_t col0 = cbase + 4 * g;
+                if (col0 >= p.n) break;
+                float dv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const size_t col = col0 + u < p.n ? col0 + u : p.n - 1;
+                    const float ipt = __fmul_rn(__fmul_rn(y[4 * g + u], rr1), __ldg(p.c1 + col));
+                    const float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
+                    dv[u] = d > 0.0f ? d : 0.0f;
+                }
+                if (vec && col0 + 4 <= p.n) {
+                    *reinterpret_cast<float4 *>(orow + col0) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (col0 + u < p.n) orow[col0 + u] = dv[u];
+                }
+            }
+        }
+        __device__ void finish(const Params &) {}
+    };
+};
+
+// The top-k over 256-wide column tiles: each thread keeps the best k of its
+// half of the columns, so a (row, slice) has two partial lists, written to
+// part_d / part_i [((cta * 128 + row) * 2 + half)][kTopKMax].  The list lives
+// in the thread's local frame and is touched only on an insertion; the
+// per-column test reads the k-th entry kept in registers.
+struct WTopk {
+    using Params = TopkEpi::Params;  // nb_tiles counts 256-wide tiles
+    __device__ static int tiles(const Params &p) { return TopkEpi::tiles(p); }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) {
+        TopkEpi::tile_at(p, t, mb, nb);
+    }
+    struct State {
+        int rit, h, m;
+        bool valid;
+        float rr1 = 0.0f, rr2 = 0.0f;
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+        float thr_d = INFINITY;
+        int thr_i = 0x7fffffff;
+        __device__ State(const Params &p, int row_in_tile, int half) : rit(row_in_tile), h(half) {
+            int mb;
+            unsigned nb0, nb1;
+            m = *p.m_dev;
+            valid = TopkEpi::slice(p, mb, nb0, nb1);
+            const int row = valid ? mb * TC_BM + rit : 0;
+            if (valid && row < m) {
+                rr1 = __ldg(p.r1 + row);
+                rr2 = __ldg(p.r2 + row);
+            }
+#pragma unroll
+            for (int t = 0; t < kTopKMax; ++t) {
+                bd[t] = INFINITY;
+                bi[t] = 0x7fffffff;
+            }
+        }
+        __device__ void tile(const Params &p, int mb, int nb, const float (&y)[TW_COLS]) {
+            if (mb * TC_BM + rit >= m) return;
+            const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
+            float td = thr_d;
+            int ti = thr_i;
+#pragma unroll
+            for (int j = 0; j < TW_COLS; ++j) {
+                const size_t col = cbase + j;
+                if (col >= p.n) break;
+                const float ipt = __fmul_rn(__fmul_rn(y[j], rr1), __ldg(p.c1 + col));
+                float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
+                d = d > 0.0f ? d : 0.0f;
+                const int ci = (int)col;
+                if (better(d, ci, td, ti)) {
+                    float cd = d;
+                    int cx = ci;
+#pragma unroll
+                    for (int u = 0; u < kTopKMax; ++u) {
+                        if (u < p.k) {
+                            const bool sw = better(cd, cx, bd[u], bi[u]);
+                            const float od = bd[u];
+                            const int ox = bi[u];
+                            bd[u] = sw ? cd : od;
+                            bi[u] = sw ? cx : ox;
+                            cd = sw ? od : cd;
+                            cx = sw ? ox : cx;
+                        }
+                    }
+                    td = bd[p.k - 1];
+                    ti = bi[p.k - 1];
+                }
+            }
+            thr_d = td;
+            thr_i = ti;
+        }
+        __device__ void finish(const Params &p) {
+            if (!valid) return;
+            int mb;
+            unsigned nb0, nb1;
+            TopkEpi::slice(p, mb, nb0, nb1);
+            if (mb * TC_BM + rit >= m) return;
+            const size_t o = (((size_t)blockIdx.x * TC_BM + rit) * 2 + h) * kTopKMax;
+#pragma unroll
+            for (int u = 0; u < kTopKMax; ++u)
+                if (u < p.k) {
+                    p.part_d[o + u] = bd[u];
+                    p.part_i[o + u] = bi[u];
+                }
+        }
+    };
+};
+
 // The QJL-corrected symmetric distances (tq_symq.cu): Y0 = C1, Y1 = C2,
 // ip_mse = C1 s1a s1b, corr = clamp(C2 s2a s2b, +-|ip_mse|),
 // ip = (ip_mse + corr) na nb, d = max(0, na^2 + nb^2 - 2 ip), with the
@@ -919,7 +1025,7 @@ struct SymqEpi {
 // Merge of the per-slice candidates: one warp per query row.  Each lane keeps
 // the best k of its slices, then k rounds of a warp arg-min on (d, index)
 // produce the sorted top-k.
-__global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__ m_dev, int slices_cap,
+__global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__ m_dev, int lists,
                                                          int grid_ctas, const float *__restrict__ part_d,
                                                          const int *__restrict__ part_i, int k,
                                                          float *__restrict__ out_d,
@@ -928,7 +1034,6 @@ __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__
     const int num_mb = (m + TC_BM - 1) / TC_BM;
     if (num_mb <= 0 || num_mb > grid_ctas) return;
     const int S = grid_ctas / num_mb;
-    (void)slices_cap;
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < m; row += gridDim.x * wpb) {
@@ -940,8 +1045,9 @@ __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__
             bd[t] = INFINITY;
             bi[t] = 0x7fffffff;
         }
-        for (int sl = lane; sl < S; sl += 32) {
-            const size_t o = ((size_t)(mb * S + sl) * TC_BM + rit) * kTopKMax;
+        for (int sl = lane; sl < S * lists; sl += 32) {
+            const size_t cta = (size_t)mb * S + sl / lists;
+            const size_t o = ((cta * TC_BM + rit) * lists + sl % lists) * kTopKMax;
             for (int u = 0; u < k; ++u) {
                 float cd = part_d[o + u];
                 int cx = part_i[o + u];
@@ -1064,6 +1170,19 @@ cudaError_t tcp_launch(const TcMaps &maps, const TcShape &sh, const typename Epi
     return cudaGetLastError();
 }
 
+template <class W>
+cudaError_t tcw_launch(const TcMaps &maps, const TcShape &sh, const typename W::Params &ep, int *err,
+                       unsigned grid, cudaStream_t st) {
+    if (sh.nseg != 1) return cudaErrorInvalidValue;
+    constexpr int STAGES = 2;
+    const size_t smem = (size_t)STAGES * TW_STAGE_BYTES + 256 + 1024;
+    auto kern = tcw_kernel<STAGES, 4, W>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, TW_THREADS, smem, st>>>(maps, sh, ep, err);
+    return cudaGetLastError();
+}
+
 bool aligned16(std::initializer_list<const void *> ps) {
     for (const void *p : ps)
         if (reinterpret_cast<uintptr_t>(p) & 15) return false;
@@ -1091,7 +1210,8 @@ bool bf16_maps(TcMaps &mp, TcShape &sh, const void *Ah, const void *Al, size_t m
 
 }  // namespace
 
-int tc_topk_variants() { return 2; }
+int tc_topk_variants() { return 3; }
+int tc_topk_lists(int variant) { return variant == 0 ? 2 : 1; }
 
 cudaError_t launch_bounded_wait_selftest(int *err, long long budget_cycles, cudaStream_t st) {
     bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(err, budget_cycles);
@@ -1103,24 +1223,34 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
                            const int *m_dev, size_t n, const float *r1, const float *r2,
                            const float *c1, const float *c2, int k, float *part_d, int *part_i,
                            int *err, int grid, cudaStream_t st) {
-    if (k < 1 || k > kTopKMax || grid < 1) return cudaErrorInvalidValue;
+    if (k < 1 || k > kTopKMax || grid < 1 || variant < 0 || variant >= tc_topk_variants())
+        return cudaErrorInvalidValue;
     if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || rows_pad % TC_BM || n_pad % TC_BN)
         return cudaErrorInvalidValue;
     if (!aligned16({Ah, Al, Bh, Bl})) return cudaErrorMisalignedAddress;
     alignas(64) TcMaps mp;
     TcShape sh;
     if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
+    if (variant == 0) {
+        // 128 x 256 tiles (tcw_kernel), two partial lists per (row, slice)
+        if (n_pad % TW_BN) return cudaErrorInvalidValue;
+        if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
+            return cudaErrorInvalidValue;
+        const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TW_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+        return tcw_launch<WTopk>(mp, sh, ep, err, (unsigned)grid, st);
+    }
     const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
-    if (variant == 1) return tcp_launch<false, 2, 2, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    if (variant == 2) return tcp_launch<false, 2, 2, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
     return tcp_launch<false, 3, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
 }
 
-cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, const float *part_d,
+cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,
                               const int *part_i, int k, size_t max_rows, float *out_d,
                               long long *out_i, cudaStream_t st) {
+    if (lists < 1 || lists > 2) return cudaErrorInvalidValue;
     const int wpb = 8;
     const unsigned blocks = (unsigned)((max_rows + wpb - 1) / wpb);
-    topk_merge_kernel<<<blocks ? blocks : 1, 32 * wpb, 0, st>>>(m_dev, grid_ctas, grid_ctas, part_d,
+    topk_merge_kernel<<<blocks ? blocks : 1, 32 * wpb, 0, st>>>(m_dev, lists, grid_ctas, part_d,
                                                                 part_i, k, out_d, out_i);
     return cudaGetLastError();
 }
@@ -1141,18 +1271,12 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
     if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
     if (n_pad % TW_BN == 0) {
-        // 128 x 256 tiles (tcw_dist_kernel): B maps with 256-row boxes
+        // 128 x 256 tiles (tcw_kernel): B maps with 256-row boxes
         if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
             return cudaErrorInvalidValue;
         const size_t wtiles = (size_t)num_mb * (n_pad / TW_BN);
         const DistEpi::Params ep{GridTiles{num_mb, (unsigned)wtiles}, m, n, r1, r2, c1, c2, out, ldo};
-        constexpr int STAGES = 2;
-        const size_t smem = (size_t)STAGES * TW_STAGE_BYTES + 256 + 1024;
-        auto kern = tcw_dist_kernel<STAGES, 4>;
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        kern<<<sm_grid(wtiles), TW_THREADS, smem, st>>>(mp, sh, ep, err);
-        return cudaGetLastError();
+        return tcw_launch<WDist>(mp, sh, ep, err, sm_grid(wtiles), st);
     }
     const DistEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, r1, r2, c1, c2, out, ldo};
     return tcp_launch<false, 3, 4, true, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
