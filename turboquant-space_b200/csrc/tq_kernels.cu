@@ -1475,17 +1475,11 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
     size_t kg = 0;
     bool ok = true;
     for (size_t k0 = 0; k0 < KG; k0 += 4) {
-        // trailer of the code this lane finishes (group ke of this warp)
+        // the code this lane finishes: code ec of group ke of this warp
         const size_t ke = k0 + (lane & 3);
         const bool ev = kind0 && ke < KG;
         const size_t ce = 4 * (GPS * (gw + (ke / GPS) * TW) + (ke % GPS)) + ec;
-        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
-        if (ev) {
-            const float *tm = reinterpret_cast<const float *>(codes + ce * (PB + 12) + PB);
-            t0 = __ldg(tm);
-            t1 = __ldg(tm + 1);
-            t2 = __ldg(tm + 2);
-        }
+        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;  // its trailer, read from the stage below
         float R = 0.0f;
         const int nst = (KG - k0 < 4) ? (int)(KG - k0) : 4;
 #pragma unroll 1
@@ -1499,6 +1493,15 @@ __global__ void __launch_bounds__(NW * 32, 1) scant_kernel(const float *__restri
             const uint32_t *sw = reinterpret_cast<const uint32_t *>(ring + s * SB + sub * GB);
             const float y = U::group([&](int c, int wi) { return sw[c * CW + wi]; }, Q, tab, lane);
             R = ((lane & 3) == i) ? y : R;
+            if (kind0 && (lane & 3) == i) {
+                // the trailer of the code this lane finishes, from the stage (three
+                // conflict-free words for the 4 lanes; from global memory these
+                // touched 16 lines per load)
+                const float *tw = reinterpret_cast<const float *>(sw + ec * CW) + PB / 4;
+                t0 = tw[0];
+                t1 = tw[1];
+                t2 = tw[2];
+            }
             if (sub == GPS - 1) {
                 __syncwarp();
                 if (lane == 0 && kg / GPS + S < K) {
