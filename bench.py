@@ -37,9 +37,9 @@ sys.path.insert(0, os.path.join(ROOT, "turboquant-space_b200", "python"))
 METRIC = "distance Gcodes/s vs plain FP32 kernel at ≤1e-5 rel err; serving p99 ms at QPS"
 DIM, BITS, QUERIES = 768, 8, 64
 # DRAM bytes (read + write) per code of one scan launch, from the ncu capture of
-# a 1M-code launch of the 768-d 8-bit corpus: 1.036052 GB read + 6.99 MB
+# a 1M-code launch of the 768-d 8-bit corpus: 1.036057 GB read + 7.84 MB
 # written.  Traffic grows with the code count, so the bench scales it per code.
-SCAN_TRAFFIC_PER_CODE = (1.036052e9 + 6.991e6) / 1e6
+SCAN_TRAFFIC_PER_CODE = (1.036057e9 + 7.835e6) / 1e6
 
 
 def peaks():
@@ -776,7 +776,7 @@ def main():
                                      if (DIM, BITS) == (768, 8) else None),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                            "1M-code launch, scaled per code "
-                                           "(profiles/scan8t_kernel_1M_768d_b8.md)",
+                                           "(profiles/scant_kernel_1M_768d_b8.md)",
                          "kernel": scan_kernel_name(DIM, BITS),
                          "bytes_per_launch": scan_bytes, "ms_per_launch": round(scan_ms, 4),
                          "peak_kind": peak_kind},
