@@ -623,14 +623,11 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 // between two of its loads would order every element's chain
                 // of table loads after the previous one's.
                 float xr[E];
-                uint32_t wq[E / 4];
+                uint32_t wq[E / 4] = {};
 #pragma unroll
                 for (int t = 0; t < E; ++t) xr[t] = b[PadLayout<E>::elem(32 * t + lane)];
                 quantize_regs<E>(xr, isg, sg, qmode, P, breg, s_bnd, s_qlut, s_cent,
-                                 [&](int t, int idx) {
-                                     wq[t >> 2] = ((t & 3) ? wq[t >> 2] : 0u) |
-                                                  ((uint32_t)idx << (8 * (t & 3)));
-                                 });
+                                 [&](int t, int idx) { wq[t >> 2] |= (uint32_t)idx << (8 * (t & 3)); });
 #pragma unroll
                 for (int t = 0; t < E; ++t) b[PadLayout<E>::elem(32 * t + lane)] = xr[t];
 #pragma unroll
