@@ -1170,13 +1170,13 @@ cudaError_t tcp_launch(const TcMaps &maps, const TcShape &sh, const typename Epi
     return cudaGetLastError();
 }
 
-template <class W>
+template <class W, int CH = 4>
 cudaError_t tcw_launch(const TcMaps &maps, const TcShape &sh, const typename W::Params &ep, int *err,
                        unsigned grid, cudaStream_t st) {
     if (sh.nseg != 1) return cudaErrorInvalidValue;
     constexpr int STAGES = 2;
     const size_t smem = (size_t)STAGES * TW_STAGE_BYTES + 256 + 1024;
-    auto kern = tcw_kernel<STAGES, 4, W>;
+    auto kern = tcw_kernel<STAGES, CH, W>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, TW_THREADS, smem, st>>>(maps, sh, ep, err);
@@ -1276,7 +1276,12 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
             return cudaErrorInvalidValue;
         const size_t wtiles = (size_t)num_mb * (n_pad / TW_BN);
         const DistEpi::Params ep{GridTiles{num_mb, (unsigned)wtiles}, m, n, r1, r2, c1, c2, out, ldo};
-        return tcw_launch<WDist>(mp, sh, ep, err, sm_grid(wtiles), st);
+        // Chunk length: asymmetric planes (B lo narrower than K: a query against
+        // codes) take 8 K blocks per chunk; symmetric planes, whose code-against-
+        // itself terms are squares of centroid values, 4 (their drift per chunk
+        // is larger against a BF16-pair floor of 5-7e-6).
+        if (k_lo < K) return tcw_launch<WDist, 8>(mp, sh, ep, err, sm_grid(wtiles), st);
+        return tcw_launch<WDist, 4>(mp, sh, ep, err, sm_grid(wtiles), st);
     }
     const DistEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, n, r1, r2, c1, c2, out, ldo};
     return tcp_launch<false, 3, 4, true, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
