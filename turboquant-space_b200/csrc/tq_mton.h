@@ -48,8 +48,8 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
 // The row count is read from m_dev; `grid` CTAs split the rows into 128-row
 // blocks and the columns into slices; partials hold grid * 128 * 16 entries.
 // Variant 0: 128 x 256 tiles (n_pad % 256 == 0), two partial lists per (row,
-// slice); variant 1: 128 x 128 tiles, 3 stages, 4-block promoted chunks;
-// variant 2: 128 x 128 tiles, 2 stages, 2-block chunks.  The partial buffers
+// slice); variant 1: 128 x 128 tiles, 3 stages, 8-block promoted chunks;
+// variant 2: 128 x 128 tiles, 2 stages, 4-block chunks.  The partial buffers
 // hold grid * 128 * tc_topk_lists(variant) * kTopKMax entries.
 constexpr int kTopKMax = 16;
 constexpr int kTopKListsMax = 2;

@@ -1237,11 +1237,12 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
         if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
             return cudaErrorInvalidValue;
         const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TW_BN), n, r1, r2, c1, c2, k, part_d, part_i};
-        return tcw_launch<WTopk>(mp, sh, ep, err, (unsigned)grid, st);
+        return tcw_launch<WTopk, 8>(mp, sh, ep, err, (unsigned)grid, st);
     }
     const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
-    if (variant == 2) return tcp_launch<false, 2, 2, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
-    return tcp_launch<false, 3, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    // asymmetric planes: 8-block chunks (see launch_tc_dist)
+    if (variant == 2) return tcp_launch<false, 2, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    return tcp_launch<false, 3, 8, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
 }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,
