@@ -316,6 +316,28 @@ def test_distance_symmetric_split_bf16_vs_oracle(cuda_ok, dim, bits):
     assert ok, err.max()
 
 
+def test_split_bf16_edge_shapes(cuda_ok):
+    """One query row, one code, and a padded dim of 32: the asymmetric K (64)
+    is a single K block with no sign-only blocks; the symmetric K (32) is not
+    a whole K block and is refused with TQ_ERR_NOT_SUPPORTED."""
+    from turboquant import _capi
+    rng = np.random.default_rng(77)
+    for dim, bits in [(32, 4), (768, 8)]:
+        s, o = tq.TurboQuantSpace(dim, bits), O.OracleSpace(dim, bits)
+        X = rng.standard_normal((300, dim)).astype(np.float32)
+        codes = s.encode_batch(X)
+        cs = s.code_size_bytes()
+        for Q, C in [(X[:1], codes), (X[:130], codes[:1]), (X[:1], codes[:1])]:
+            d = s.distance_m_to_n(Q, C, precision="split_bf16")
+            err, ok = dist_close(d, o.distance_m_to_n(Q, C), asym_term_scale(Q, C, cs, cs - 12))
+            assert d.shape == (len(Q), len(C)) and ok, (dim, d.shape, err.max())
+    s = tq.TurboQuantSpace(32, 4)
+    codes = s.encode_batch(rng.standard_normal((10, 32)).astype(np.float32))
+    with pytest.raises(tq.TQError) as e:
+        s.distance_m_to_n_symmetric(codes, codes, precision="split_bf16")
+    assert e.value.status == _capi.TQ_ERR_NOT_SUPPORTED
+
+
 @pytest.mark.parametrize("dim,bits", [(768, 8), (384, 4), (1536, 4), (64, 6)])
 def test_distance_split_bf16_query_is_a_row(cuda_ok, dim, bits):
     """Queries equal to encoded rows: the nearest-neighbour case, where the
