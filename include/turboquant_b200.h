@@ -266,7 +266,9 @@ typedef struct tq_server_stats {
 } tq_server_stats;
 
 /* Decode n codes (host or device memory) once into the index's BF16 operand
- * planes (4 * 2 * padded_dim bytes per code) in HBM. */
+ * planes in HBM: the hi plane of 2 * padded_dim values and the lo plane of the
+ * padded_dim centroid values (the sign half is exact), 6 * padded_dim + 8
+ * bytes per code. */
 tq_status tq_index_create(const tq_space *sp, const uint8_t *codes, size_t n, int codes_on_device,
                           tq_index **out);
 void tq_index_destroy(tq_index *ix);
