@@ -137,18 +137,24 @@ __global__ void __launch_bounds__(256) planes_from_prepared_kernel(
 // FP32 CUDA-core GEMM with the distance epilogue: 128 x 128 tile, K step 16,
 // 256 threads, 8 x 8 outputs per thread (two 4 x 4 quadrants 64 apart),
 // double-buffered shared tiles stored K-major-transposed for float4 reads.
+// The tile column is XOR-swizzled with bit 3 of k (sw_col), which keeps each
+// float4 group intact and makes the transposed stores conflict-free.  Row
+// blocks are blockIdx.x (fastest), so CTAs running together share the B tile
+// in L2; two CTAs per SM.
 // A: rows_pad(m) x K, B: rows_pad(n) x K, both multiples of 128 rows, K % 16 == 0.
 // ---------------------------------------------------------------------------
 constexpr int SG_BM = 128, SG_BN = 128, SG_BK = 16, SG_PAD = 4;
 
-__global__ void __launch_bounds__(256) sgemm_dist_kernel(
+__device__ __forceinline__ int sw_col(int k, int col) { return col ^ (((k >> 3) & 1) << 3); }
+
+__global__ void __launch_bounds__(256, 2) sgemm_dist_kernel(
     const float *__restrict__ A, const float *__restrict__ B, int K, size_t m, size_t n,
     const float *__restrict__ r1, const float *__restrict__ r2, const float *__restrict__ c1,
     const float *__restrict__ c2, float *__restrict__ out, size_t ldo) {
     __shared__ __align__(16) float As[2][SG_BK][SG_BM + SG_PAD];
     __shared__ __align__(16) float Bs[2][SG_BK][SG_BN + SG_PAD];
     const int tid = threadIdx.x;
-    const size_t m0 = (size_t)blockIdx.y * SG_BM, n0 = (size_t)blockIdx.x * SG_BN;
+    const size_t m0 = (size_t)blockIdx.x * SG_BM, n0 = (size_t)blockIdx.y * SG_BN;
     const int lrow = tid >> 2, lk = (tid & 3) * 4;
     const float *Ag = A + (m0 + lrow) * (size_t)K + lk;
     const float *Bg = B + (n0 + lrow) * (size_t)K + lk;
@@ -161,15 +167,17 @@ __global__ void __launch_bounds__(256) sgemm_dist_kernel(
         rb0 = __ldg(reinterpret_cast<const float4 *>(Bg + o));
         rb1 = __ldg(reinterpret_cast<const float4 *>(Bg + half + o));
     };
+    // lk + q has the same bit 3 for q < 4, so one swizzled column per thread
+    const int r0s = sw_col(lk, lrow), r1s = sw_col(lk, lrow + 64);
     auto sstore = [&](int buf) {
-        As[buf][lk + 0][lrow] = ra0.x; As[buf][lk + 1][lrow] = ra0.y;
-        As[buf][lk + 2][lrow] = ra0.z; As[buf][lk + 3][lrow] = ra0.w;
-        As[buf][lk + 0][lrow + 64] = ra1.x; As[buf][lk + 1][lrow + 64] = ra1.y;
-        As[buf][lk + 2][lrow + 64] = ra1.z; As[buf][lk + 3][lrow + 64] = ra1.w;
-        Bs[buf][lk + 0][lrow] = rb0.x; Bs[buf][lk + 1][lrow] = rb0.y;
-        Bs[buf][lk + 2][lrow] = rb0.z; Bs[buf][lk + 3][lrow] = rb0.w;
-        Bs[buf][lk + 0][lrow + 64] = rb1.x; Bs[buf][lk + 1][lrow + 64] = rb1.y;
-        Bs[buf][lk + 2][lrow + 64] = rb1.z; Bs[buf][lk + 3][lrow + 64] = rb1.w;
+        As[buf][lk + 0][r0s] = ra0.x; As[buf][lk + 1][r0s] = ra0.y;
+        As[buf][lk + 2][r0s] = ra0.z; As[buf][lk + 3][r0s] = ra0.w;
+        As[buf][lk + 0][r1s] = ra1.x; As[buf][lk + 1][r1s] = ra1.y;
+        As[buf][lk + 2][r1s] = ra1.z; As[buf][lk + 3][r1s] = ra1.w;
+        Bs[buf][lk + 0][r0s] = rb0.x; Bs[buf][lk + 1][r0s] = rb0.y;
+        Bs[buf][lk + 2][r0s] = rb0.z; Bs[buf][lk + 3][r0s] = rb0.w;
+        Bs[buf][lk + 0][r1s] = rb1.x; Bs[buf][lk + 1][r1s] = rb1.y;
+        Bs[buf][lk + 2][r1s] = rb1.z; Bs[buf][lk + 3][r1s] = rb1.w;
     };
     const int tx = tid & 15, ty = tid >> 4;
     float acc[8][8];
@@ -186,10 +194,10 @@ __global__ void __launch_bounds__(256) sgemm_dist_kernel(
         if (kt + 1 < KT) gload(kt + 1);
 #pragma unroll
         for (int kk = 0; kk < SG_BK; ++kk) {
-            const float4 a0 = *reinterpret_cast<const float4 *>(&As[buf][kk][ty * 4]);
-            const float4 a1 = *reinterpret_cast<const float4 *>(&As[buf][kk][ty * 4 + 64]);
-            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][tx * 4]);
-            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][tx * 4 + 64]);
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[buf][kk][sw_col(kk, ty * 4)]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[buf][kk][sw_col(kk, ty * 4 + 64)]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][sw_col(kk, tx * 4)]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][sw_col(kk, tx * 4 + 64)]);
             const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
             const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
@@ -253,11 +261,13 @@ cudaError_t launch_sgemm_dist(const float *A, const float *B, int K, size_t m, s
                               cudaStream_t st) {
     if (m == 0 || n == 0) return cudaSuccess;
     if (K % SG_BK || m_pad % SG_BM || n_pad % SG_BN) return cudaErrorInvalidValue;
-    for (size_t mb = 0; mb < m_pad; mb += (size_t)SG_BM * 65535) {
-        const size_t rows = (m_pad - mb < (size_t)SG_BM * 65535) ? (m_pad - mb) : (size_t)SG_BM * 65535;
-        dim3 grid((unsigned)(n_pad / SG_BN), (unsigned)(rows / SG_BM));
-        sgemm_dist_kernel<<<grid, 256, 0, st>>>(A + mb * (size_t)K, B, K, m > mb ? m - mb : 0, n,
-                                               r1 + mb, r2 + mb, c1, c2, out + mb * ldo, ldo);
+    if (m_pad / SG_BM > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    // row blocks on grid.x (up to 2^31 - 1), column blocks on grid.y in chunks of 65535
+    for (size_t nb = 0; nb < n_pad; nb += (size_t)SG_BN * 65535) {
+        const size_t cols = (n_pad - nb < (size_t)SG_BN * 65535) ? (n_pad - nb) : (size_t)SG_BN * 65535;
+        dim3 grid((unsigned)(m_pad / SG_BM), (unsigned)(cols / SG_BN));
+        sgemm_dist_kernel<<<grid, 256, 0, st>>>(A, B + nb * (size_t)K, K, m, n > nb ? n - nb : 0,
+                                               r1, r2, c1 + nb, c2 + nb, out + nb, ldo);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
