@@ -9,7 +9,8 @@
 //                          centroid values, the +-1 QJL signs and, for the
 //                          full variants, the reconstruction passed through
 //                          the QJL Hadamard (randomizedHadamard of c * sigma).
-//   symq_gemm_kernel       two FP32 contractions per tile (the MSE term and the
+//   symq_gemm_wide_kernel  two FP32 contractions per tile (the MSE term and the
+//   / symq_gemm_kernel
 //                          correction) with the reference's distance epilogue
 //                          fused: corr = clamp(corr, +-|ip_mse|),
 //                          ip = (ip_mse + corr) |a| |b|, d = max(0, ...).
@@ -302,6 +303,121 @@ __global__ void __launch_bounds__(256) split_tf32_kernel(const float *__restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same two contractions with 128 x 128 tiles and 8 x 8 outputs per thread
+// (half the shared-memory reads per FMA of the 64 x 64 kernel, which is bound
+// by them): C1 is accumulated first and parked in shared memory (64 floats
+// per thread, 64 KB), then C2 in the same registers; the epilogue combines
+// them as above.  K step 16, double-buffered transposed tiles whose columns
+// are XOR-swizzled with bit 3 of k (conflict-free stores); rows past m or n
+// load as zeros.  128 registers, two CTAs per SM.
+// ---------------------------------------------------------------------------
+constexpr int SQW_BM = 128, SQW_BK = 16, SQW_PAD = 4;
+constexpr size_t kSqwStashBytes = (size_t)64 * 256 * 4;
+
+__device__ __forceinline__ int sqw_col(int k, int col) { return col ^ (((k >> 3) & 1) << 3); }
+
+__device__ __forceinline__ void sqw_accumulate(float (&acc)[8][8], const float *__restrict__ Pa,
+                                               const float *__restrict__ Pb, size_t m, size_t n,
+                                               size_t r0, size_t c0, int ldk,
+                                               float (*As)[SQW_BK][SQW_BM + SQW_PAD],
+                                               float (*Bs)[SQW_BK][SQW_BM + SQW_PAD], int tid) {
+    const int lrow = tid >> 2, lk = (tid & 3) * 4, tx = tid & 15, ty = tid >> 4;
+    const bool a0ok = r0 + lrow < m, a1ok = r0 + lrow + 64 < m;
+    const bool b0ok = c0 + lrow < n, b1ok = c0 + lrow + 64 < n;
+    const float *Ag0 = Pa + (a0ok ? (r0 + lrow) * (size_t)ldk : 0) + lk;
+    const float *Ag1 = Pa + (a1ok ? (r0 + lrow + 64) * (size_t)ldk : 0) + lk;
+    const float *Bg0 = Pb + (b0ok ? (c0 + lrow) * (size_t)ldk : 0) + lk;
+    const float *Bg1 = Pb + (b1ok ? (c0 + lrow + 64) * (size_t)ldk : 0) + lk;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 ra0, ra1, rb0, rb1;
+    auto gload = [&](int kt) {
+        const size_t o = (size_t)kt * SQW_BK;
+        ra0 = a0ok ? __ldg(reinterpret_cast<const float4 *>(Ag0 + o)) : z;
+        ra1 = a1ok ? __ldg(reinterpret_cast<const float4 *>(Ag1 + o)) : z;
+        rb0 = b0ok ? __ldg(reinterpret_cast<const float4 *>(Bg0 + o)) : z;
+        rb1 = b1ok ? __ldg(reinterpret_cast<const float4 *>(Bg1 + o)) : z;
+    };
+    const int s0 = sqw_col(lk, lrow), s1 = sqw_col(lk, lrow + 64);
+    auto sstore = [&](int buf) {
+        As[buf][lk + 0][s0] = ra0.x; As[buf][lk + 1][s0] = ra0.y;
+        As[buf][lk + 2][s0] = ra0.z; As[buf][lk + 3][s0] = ra0.w;
+        As[buf][lk + 0][s1] = ra1.x; As[buf][lk + 1][s1] = ra1.y;
+        As[buf][lk + 2][s1] = ra1.z; As[buf][lk + 3][s1] = ra1.w;
+        Bs[buf][lk + 0][s0] = rb0.x; Bs[buf][lk + 1][s0] = rb0.y;
+        Bs[buf][lk + 2][s0] = rb0.z; Bs[buf][lk + 3][s0] = rb0.w;
+        Bs[buf][lk + 0][s1] = rb1.x; Bs[buf][lk + 1][s1] = rb1.y;
+        Bs[buf][lk + 2][s1] = rb1.z; Bs[buf][lk + 3][s1] = rb1.w;
+    };
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    const int KT = ldk / SQW_BK;
+    gload(0);
+    sstore(0);
+    __syncthreads();
+    for (int kt = 0; kt < KT; ++kt) {
+        const int buf = kt & 1;
+        if (kt + 1 < KT) gload(kt + 1);
+#pragma unroll
+        for (int kk = 0; kk < SQW_BK; ++kk) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[buf][kk][sqw_col(kk, ty * 4)]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[buf][kk][sqw_col(kk, ty * 4 + 64)]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][sqw_col(kk, tx * 4)]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][sqw_col(kk, tx * 4 + 64)]);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
+        }
+        if (kt + 1 < KT) sstore(buf ^ 1);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256, 2) symq_gemm_wide_kernel(
+    const float *__restrict__ P1a, const float *__restrict__ P2a, const float *__restrict__ sa,
+    size_t m, const float *__restrict__ P1b, const float *__restrict__ P2b,
+    const float *__restrict__ sb, size_t n, int ldk1, int ldk2, float *__restrict__ out,
+    size_t ldo) {
+    __shared__ __align__(16) float As[2][SQW_BK][SQW_BM + SQW_PAD];
+    __shared__ __align__(16) float Bs[2][SQW_BK][SQW_BM + SQW_PAD];
+    extern __shared__ float stash[];  // [64][256]: value i * 8 + j of thread tid at [(i * 8 + j) * 256 + tid]
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    // row blocks on grid.x (fastest): CTAs running together share the column tile in L2
+    const size_t r0 = (size_t)blockIdx.x * SQW_BM, c0 = (size_t)blockIdx.y * SQW_BM;
+    float acc[8][8];
+    sqw_accumulate(acc, P1a, P1b, m, n, r0, c0, ldk1, As, Bs, tid);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) stash[(i * 8 + j) * 256 + tid] = acc[i][j];
+    sqw_accumulate(acc, P2a, P2b, m, n, r0, c0, ldk2, As, Bs, tid);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const size_t r = r0 + ty * 4 + (i & 3) + (i >> 2) * 64;
+        if (r >= m) continue;
+        const float s1a = sa[8 * r], na = sa[8 * r + 1], s2a = sa[8 * r + 2];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const size_t c = c0 + tx * 4 + (j & 3) + (j >> 2) * 64;
+            if (c >= n) continue;
+            const float s1b = sb[8 * c], nb = sb[8 * c + 1], s2b = sb[8 * c + 2];
+            const float ip_mse = __fmul_rn(__fmul_rn(stash[(i * 8 + j) * 256 + tid], s1a), s1b);
+            const float lim = fabsf(ip_mse);
+            float corr = __fmul_rn(__fmul_rn(acc[i][j], s2a), s2b);
+            corr = fmaxf(-lim, fminf(lim, corr));
+            const float ip = __fmul_rn(__fmul_rn(__fadd_rn(ip_mse, corr), na), nb);
+            const float d = __fsub_rn(__fadd_rn(__fmul_rn(na, na), __fmul_rn(nb, nb)),
+                                      __fmul_rn(2.0f, ip));
+            out[r * ldo + c] = d > 0.0f ? d : 0.0f;
+        }
+    }
+}
+
 template <template <int> class F, typename... Args>
 cudaError_t dispatch_logd_sq(int log2D, Args &&...args) {
     switch (log2D) {
@@ -421,6 +537,27 @@ cudaError_t launch_symq_gemm(const float *P1a, const float *P2a, const float *sa
                              const float *P1b, const float *P2b, const float *sb, size_t n,
                              int ldk1, int ldk2, float *out, size_t ldo, cudaStream_t st) {
     if (m == 0 || n == 0) return cudaSuccess;
+    if (ldk1 % SQW_BK || ldk2 % SQW_BK) return cudaErrorInvalidValue;
+    if (m >= 64) {
+        // 128 x 128 tiles: row blocks on grid.x, column blocks on grid.y in chunks of 65535
+        cudaError_t e = cudaFuncSetAttribute(symq_gemm_wide_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSqwStashBytes);
+        if (e != cudaSuccess) return e;
+        const size_t gx = (m + SQW_BM - 1) / SQW_BM;
+        if (gx > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+        const size_t nblk = (n + SQW_BM - 1) / SQW_BM;
+        for (size_t y0 = 0; y0 < nblk; y0 += 65535) {
+            const size_t gy = (nblk - y0 < 65535) ? nblk - y0 : 65535;
+            const size_t cc = y0 * SQW_BM;
+            symq_gemm_wide_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, kSqwStashBytes, st>>>(
+                P1a, P2a, sa, m, P1b + cc * (size_t)ldk1, P2b + cc * (size_t)ldk2, sb + 8 * cc,
+                n - cc, ldk1, ldk2, out + cc, ldo);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
     const size_t gx = (n + SQ_BN - 1) / SQ_BN;
     for (size_t y0 = 0; y0 < (m + SQ_BM - 1) / SQ_BM; y0 += 65535) {
         const size_t gy = ((m + SQ_BM - 1) / SQ_BM - y0 < 65535) ? (m + SQ_BM - 1) / SQ_BM - y0 : 65535;
