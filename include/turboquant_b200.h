@@ -139,6 +139,11 @@ tq_status tq_encode_batch_device(const tq_space *sp, const float *X, size_t n, u
  * m x padded_dim, norms is m x 2 = (|q|^2, |q|). */
 tq_status tq_prepare_queries_device(const tq_space *sp, const float *queries, size_t m,
                                     float *q_rot, float *s_q, float *norms, void *stream);
+/* TurboQuantSpace::prepareQuery (:439-460; bindings.cpp:268-273) of one query
+ * on host pointers, synchronous: q_rot[padded_dim], s_q[padded_dim],
+ * norms[2] = (|q|^2, |q|), bit-identical to the reference. */
+tq_status tq_prepare_query(const tq_space *sp, const float *query, float *q_rot, float *s_q,
+                           float *norms);
 
 /* distanceBatch1ToN on device buffers.  Scratch for the prepared query is
  * taken from the stream-ordered pool of the device (cudaMallocAsync). */

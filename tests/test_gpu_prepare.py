@@ -38,3 +38,22 @@ def test_prepare_queries_bit_exact(cuda_ok, dim, bits):
         np.testing.assert_array_equal(qr[i].cpu().numpy(), q_rot)
         np.testing.assert_array_equal(sq[i].cpu().numpy(), s_q)
         np.testing.assert_array_equal(nm[i].cpu().numpy(), norms)
+
+
+@pytest.mark.parametrize("dim,bits", [(3, 4), (128, 4), (768, 8), (1536, 4)])
+def test_prepare_query_host_bit_exact(cuda_ok, dim, bits):
+    """TurboQuantSpace.prepare_query (bindings.cpp:268-273) through the host
+    entry point tq_prepare_query: the PreparedQuery's fields equal the oracle's
+    bit for bit; its input checks are the reference's."""
+    rng = np.random.default_rng(dim * 3 + bits)
+    s, o = tq.TurboQuantSpace(dim, bits), O.OracleSpace(dim, bits)
+    for q in (rng.standard_normal(dim).astype(np.float32), np.zeros(dim, np.float32)):
+        pq = s.prepare_query(q)
+        q_rot, s_q, norms = o.prepare_query(q)
+        np.testing.assert_array_equal(pq.q_rot, q_rot)
+        np.testing.assert_array_equal(pq.s_q, s_q)
+        assert (np.float32(pq.q_norm_sq), np.float32(pq.q_norm)) == (norms[0], norms[1])
+    with pytest.raises(ValueError, match="query: wrong length"):
+        s.prepare_query(np.zeros(dim + 1, np.float32))
+    with pytest.raises(ValueError):
+        s.prepare_query(np.zeros(dim, np.float64))

@@ -491,6 +491,29 @@ tq_status tq_prepare_queries_device(const tq_space *sp, const float *Q, size_t m
     return TQ_OK;
 }
 
+tq_status tq_prepare_query(const tq_space *csp, const float *query, float *q_rot, float *s_q,
+                           float *norms) {
+    tq_status st = need_device(csp);
+    if (st != TQ_OK) return st;
+    if (!query || !q_rot || !s_q || !norms) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    auto *sp = const_cast<tq_space *>(csp);
+    std::lock_guard<std::mutex> lock(sp->host_mu);
+    DeviceGuard g(sp->device);
+    if ((st = ensure_host_streams(sp)) != TQ_OK) return st;
+    cudaStream_t s = sp->host_stream[0];
+    const size_t D = sp->D, dim = sp->dim;
+    Scratch buf;
+    TQ_CUDA(buf.alloc(sizeof(float) * (dim + 2 * D + 2), s), "cudaMallocAsync(prepare)");
+    float *dq = static_cast<float *>(buf.p), *dr = dq + dim, *ds = dr + D, *dn = ds + D;
+    TQ_CUDA(cudaMemcpyAsync(dq, query, dim * 4, cudaMemcpyHostToDevice, s), "H2D query");
+    TQ_CUDA(tq::launch_prepare(sp->P, sp->T, dq, 1, dr, ds, dn, s), "prepare kernel");
+    TQ_CUDA(cudaMemcpyAsync(q_rot, dr, D * 4, cudaMemcpyDeviceToHost, s), "D2H q_rot");
+    TQ_CUDA(cudaMemcpyAsync(s_q, ds, D * 4, cudaMemcpyDeviceToHost, s), "D2H s_q");
+    TQ_CUDA(cudaMemcpyAsync(norms, dn, 8, cudaMemcpyDeviceToHost, s), "D2H norms");
+    TQ_CUDA(cudaStreamSynchronize(s), "prepare_query");
+    return TQ_OK;
+}
+
 tq_status tq_distance_1_to_n_device(const tq_space *sp, const float *query,
                                     const uint8_t *codes, size_t n, float *out, void *stream) {
     tq_status st = need_device(sp);

@@ -22,8 +22,8 @@ import numpy as np
 from . import _capi
 from ._capi import TQError, check, lib
 
-__all__ = ["TurboQuantSpace", "PreparedSymCode", "TQError", "Index", "Server", "BusyError",
-           "load_codes"]
+__all__ = ["TurboQuantSpace", "PreparedQuery", "PreparedSymCode", "TQError", "Index", "Server",
+           "BusyError", "load_codes"]
 __version__ = "0.1.0"
 
 
@@ -173,6 +173,21 @@ def _stream_and_device(obj):
     dev = obj.device if isinstance(getattr(obj, "device", None), torch.device) \
         else torch.device("cuda", torch.cuda.current_device())
     return torch.cuda.current_stream(dev).cuda_stream, dev
+
+
+class PreparedQuery:
+    """TurboQuantPreparedQuery (space_turbo_quant.h:138-144): a query rotated
+    once (q_rot = RHT_rot(q / |q|)), its QJL image (s_q = RHT_qjl(q_rot)) and
+    its norms, held on the host as float32.  The reference binds it as an
+    opaque object (bindings.cpp:56); its fields are exposed here."""
+
+    __slots__ = ("q_rot", "s_q", "q_norm_sq", "q_norm")
+
+    def __init__(self, q_rot, s_q, q_norm_sq, q_norm):
+        self.q_rot = np.ascontiguousarray(q_rot, dtype=np.float32)
+        self.s_q = np.ascontiguousarray(s_q, dtype=np.float32)
+        self.q_norm_sq = float(q_norm_sq)
+        self.q_norm = float(q_norm)
 
 
 class PreparedSymCode:
@@ -483,6 +498,16 @@ class TurboQuantSpace:
     def distance_m_to_n_symmetric_full_prepared(self, codes_a, codes_b, precision="fp32"):
         """distanceBatchMToNSymmetricFullPrepared: row codes prepared once (:557-572, 808-878)."""
         return self._symmetric_qjl(codes_a, codes_b, "full_prepared", precision)
+
+    def prepare_query(self, query):
+        """prepareQuery (:439-460; bindings.cpp:268-273) of one query: a PreparedQuery."""
+        q = _float_host(query, self.dim(), "query", 1)
+        D = self.padded_dim()
+        q_rot = np.empty(D, np.float32)
+        s_q = np.empty(D, np.float32)
+        norms = np.empty(2, np.float32)
+        check(lib().tq_prepare_query(self._h, _ptr(q), _ptr(q_rot), _ptr(s_q), _ptr(norms)))
+        return PreparedQuery(q_rot, s_q, norms[0], norms[1])
 
     def prepare_symmetric_query(self, code):
         """prepareSymmetricQuery (:499-535) of one code: a PreparedSymCode."""

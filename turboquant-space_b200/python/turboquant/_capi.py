@@ -27,7 +27,7 @@ PRECISION = {"fp32": 0, "split_bf16": 1, "split_tf32": 2}
 EXPORTS = (
     "tq_last_error", "tq_version", "tq_space_create", "tq_space_destroy", "tq_space_get_info",
     "tq_space_tables", "tq_space_quantize", "tq_encode_batch", "tq_distance_1_to_n", "tq_distance_m_to_n",
-    "tq_distance_m_to_n_symmetric", "tq_encode_batch_device", "tq_prepare_queries_device",
+    "tq_distance_m_to_n_symmetric", "tq_encode_batch_device", "tq_prepare_queries_device", "tq_prepare_query",
     "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device",
     "tq_distance_1_to_n_device_noalloc", "tq_distance_m_to_n_device",
     "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
@@ -107,6 +107,8 @@ def lib() -> C.CDLL:
     L.tq_encode_batch_device.argtypes = [vp, fp, sz, u8p, vp]
     L.tq_prepare_queries_device.restype = st
     L.tq_prepare_queries_device.argtypes = [vp, fp, sz, fp, fp, fp, vp]
+    L.tq_prepare_query.restype = st
+    L.tq_prepare_query.argtypes = [vp, fp, fp, fp, fp]
     L.tq_distance_1_to_n_device.restype = st
     L.tq_distance_1_to_n_device.argtypes = [vp, fp, u8p, sz, fp, vp]
     L.tq_distance_1_to_n_prepared_device.restype = st
