@@ -686,6 +686,33 @@ __device__ __forceinline__ bool better(float d, int i, float bd, int bi) {
     return d < bd || (d == bd && i < bi);
 }
 
+struct TopkEntry {
+    float d;
+    int i;
+};
+
+// Inserts (d, ci) into the ascending list (bd, bi) of k >= 1 entries, ties
+// broken by the smaller index, and returns its new k-th entry.  Out of line
+// and rolled: few columns pass a row's threshold, and a sorted insert inlined
+// into every column of the unrolled epilogue loops made their code many times
+// larger than the instruction cache.
+__device__ __noinline__ TopkEntry topk_insert(float *bd, int *bi, int k, float d, int ci) {
+    float cd = d;
+    int cx = ci;
+#pragma unroll 1
+    for (int u = 0; u < k; ++u) {
+        if (better(cd, cx, bd[u], bi[u])) {
+            const float od = bd[u];
+            const int ox = bi[u];
+            bd[u] = cd;
+            bi[u] = cx;
+            cd = od;
+            cx = ox;
+        }
+    }
+    return TopkEntry{bd[k - 1], bi[k - 1]};
+}
+
 // Per-row top-k over a device-resident index.  The number of query rows m is
 // read from device memory (so that one captured launch serves batches of any
 // size up to the buffers' capacity).  CTA c takes row block c / S and the
@@ -753,14 +780,6 @@ struct TopkEpi {
         __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
             const bool row_ok = mb * TC_BM + rit < m;
             const size_t colbase = (size_t)nb * TC_BN;
-            // the list in registers for the tile (the State itself may live in local memory)
-            float d_[kTopKMax];
-            int i_[kTopKMax];
-#pragma unroll
-            for (int u = 0; u < kTopKMax; ++u) {
-                d_[u] = bd[u];
-                i_[u] = bi[u];
-            }
             float td = thr_d;
             int ti = thr_i;
 #pragma unroll 1
@@ -778,33 +797,11 @@ struct TopkEpi {
                     d = d > 0.0f ? d : 0.0f;
                     const int ci = (int)col;
                     if (better(d, ci, td, ti)) {
-                        float cd = d;
-                        int cx = ci;
-#pragma unroll
-                        for (int u = 0; u < kTopKMax; ++u) {
-                            if (u < p.k) {
-                                const bool sw = better(cd, cx, d_[u], i_[u]);
-                                const float od = d_[u];
-                                const int ox = i_[u];
-                                d_[u] = sw ? cd : od;
-                                i_[u] = sw ? cx : ox;
-                                cd = sw ? od : cd;
-                                cx = sw ? ox : cx;
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < kTopKMax; ++u)
-                            if (u == p.k - 1) {
-                                td = d_[u];
-                                ti = i_[u];
-                            }
+                        const TopkEntry e = topk_insert(bd, bi, p.k, d, ci);
+                        td = e.d;
+                        ti = e.i;
                     }
                 }
-            }
-#pragma unroll
-            for (int u = 0; u < kTopKMax; ++u) {
-                bd[u] = d_[u];
-                bi[u] = i_[u];
             }
             thr_d = td;
             thr_i = ti;
@@ -919,22 +916,9 @@ struct WTopk {
                 d = d > 0.0f ? d : 0.0f;
                 const int ci = (int)col;
                 if (better(d, ci, td, ti)) {
-                    float cd = d;
-                    int cx = ci;
-#pragma unroll
-                    for (int u = 0; u < kTopKMax; ++u) {
-                        if (u < p.k) {
-                            const bool sw = better(cd, cx, bd[u], bi[u]);
-                            const float od = bd[u];
-                            const int ox = bi[u];
-                            bd[u] = sw ? cd : od;
-                            bi[u] = sw ? cx : ox;
-                            cd = sw ? od : cd;
-                            cx = sw ? ox : cx;
-                        }
-                    }
-                    td = bd[p.k - 1];
-                    ti = bi[p.k - 1];
+                    const TopkEntry e = topk_insert(bd, bi, p.k, d, ci);
+                    td = e.d;
+                    ti = e.i;
                 }
             }
             thr_d = td;
