@@ -572,7 +572,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--rates", default="5,20,40,60,1000,50000",
+    ap.add_argument("--rates", default="5,20,40,60,100,150,1000,50000",
                     help="serve: request rates (req/s) to sweep")
     ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
     ap.add_argument("--workload", choices=("scan", "mton", "sym", "symq", "serve"), default="scan",

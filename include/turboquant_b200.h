@@ -298,7 +298,8 @@ void tq_request_release(tq_request *r);
 tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latencies, size_t cap,
                           size_t *n_latencies);
 tq_status tq_server_reset_stats(tq_server *sv);
-/* The autotuner's choice per bucket: rows, kernel variant, measured ms. */
+/* The autotuner's choice per bucket: rows, kernel variant, and its measured ms
+   per batch (two slots' launches overlapped, as the server runs them). */
 tq_status tq_server_tuning(tq_server *sv, int *bucket_rows, int *variant, float *ms, int cap,
                            int *n);
 void tq_server_destroy(tq_server *sv);
