@@ -504,7 +504,7 @@ def run_serve(args):
     build_s = time.perf_counter() - t0
     del codes
     torch.cuda.empty_cache()
-    server = index.serve(k=10, max_rows=1024, slots=2)
+    server = index.serve(k=10, max_rows=1024, slots=2, kernel_variant=args.kernel_variant)
     tuning = server.tuning()
     rates = [float(r) for r in args.rates.split(",")]
     rng = np.random.default_rng(9)
@@ -554,6 +554,7 @@ def run_serve(args):
         "config": {"dim": dim, "padded_dim": space.padded_dim(), "bits_per_coord": bits,
                    "n_codes": n, "k": 10, "request_rows": "U{1..256}", "arrivals": "Poisson",
                    "window_s": args.window, "max_batch_rows": 1024, "slots": 2,
+                   "kernel_variant": "autotuned" if args.kernel_variant < 0 else args.kernel_variant,
                    "data": "1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 8/9)"},
         "index_build_s": round(build_s, 2), "tuning": tuning, "results": results,
     }), flush=True)
@@ -575,6 +576,9 @@ def main():
     ap.add_argument("--rates", default="5,20,40,60,100,150,1000,50000",
                     help="serve: request rates (req/s) to sweep")
     ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
+    ap.add_argument("--kernel-variant", type=int, default=-1,
+                    help="serve: top-k kernel variant (-1: autotuned per batch bucket; 0: 128 x 256 "
+                         "tiles; 1, 2: 128 x 128 tiles)")
     ap.add_argument("--workload", choices=("scan", "mton", "sym", "symq", "serve"), default="scan",
                     help="scan (default): the 1->N scan benchmark; mton/sym: the dense M x N "
                          "contractions, FP32 vs split-BF16; symq: the QJL-corrected symmetric "
