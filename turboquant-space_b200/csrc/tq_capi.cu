@@ -881,7 +881,8 @@ tq_status tq_distance_m_to_n_symmetric(const tq_space *csp, const uint8_t *codes
 // ---- rotated coordinates and QJL-corrected symmetric distances -------------
 namespace {
 
-constexpr size_t kSymqChunkBytes = size_t(512) << 20;  // column planes per chunk
+constexpr size_t kSymqChunkBytes = size_t(512) << 20;     // FP32 column planes per chunk
+constexpr size_t kSymqTcChunkBytes = size_t(2048) << 20;  // TF32 pairs: fewer, longer launches
 
 size_t sq_round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -919,20 +920,30 @@ struct SymqRunner {
         return TQ_OK;
     }
     tq_status prepare_rows(const uint8_t *A, size_t rows_, cudaStream_t s) {
+        if (tc) return prepare_rows_tc(A, rows_, s);
         tq_status st = alloc_rows(rows_, s);
         if (st != TQ_OK) return st;
         TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, A, m, mode, true, P1a, ldk1, P2a, ldk2, sa, s),
                 "symmetric planes kernel");
-        if (!tc) return TQ_OK;
+        return TQ_OK;
+    }
+    // The row planes straight into hi/lo TF32 pairs (m_pad x K1p, m_pad x
+    // K2p); the light variant's sign plane is exact and has no lo plane.
+    tq_status prepare_rows_tc(const uint8_t *A, size_t rows_, cudaStream_t s) {
+        m = rows_;
+        TQ_CUDA(rows.alloc(sizeof(float) * 8 * m, s), "cudaMallocAsync(row scalars)");
+        sa = static_cast<float *>(rows.p);
         m_pad = sq_round_up(m, 128);
         const size_t e1 = m_pad * K1p, e2 = m_pad * K2p;  // floats per plane
         TQ_CUDA(rows_bf.alloc(sizeof(float) * 2 * (e1 + e2), s), "cudaMallocAsync(row TF32 planes)");
         A1 = static_cast<float *>(rows_bf.p);
         A2 = A1 + 2 * e1;
-        TQ_CUDA(tq::launch_split_tf32(P1a, m, ldk1, m_pad, K1p, A1, A1 + e1, s), "split kernel");
-        TQ_CUDA(tq::launch_split_tf32(P2a, m, ldk2, m_pad, K2p, A2, A2 + e2, s), "split kernel");
+        TQ_CUDA(tq::launch_symq_planes_tf32(sp->P, sp->T, A, m, m_pad, mode, true, A1, A1 + e1, K1p, A2,
+                                            light() ? nullptr : A2 + e2, K2p, sa, s),
+                "symmetric TF32 planes kernel");
         return TQ_OK;
     }
+    bool light() const { return mode == tq::SYMQ_LIGHT; }
     tq_status prepare_row_from_prepared(const float *recon, const float *sign, const float *sc,
                                         cudaStream_t s) {
         tq_status st = alloc_rows(1, s);
@@ -961,29 +972,27 @@ struct SymqRunner {
         return TQ_OK;
     }
     tq_status run_cols_tc(const uint8_t *B, size_t n, float *out, size_t ldo, cudaStream_t s) {
-        const size_t f32_row = sizeof(float) * row_floats(), bf_row = (size_t)8 * (K1p + K2p);
+        const size_t bf_row = (size_t)8 * (K1p + K2p);  // hi + lo floats of both planes
         if (!per) {
-            per = std::max<size_t>(256, (kSymqChunkBytes / (f32_row + bf_row)) & ~size_t(255));
+            per = std::max<size_t>(256, (kSymqTcChunkBytes / (bf_row + 32)) & ~size_t(255));
             per = std::min(per, sq_round_up(n, 256));
-            TQ_CUDA(cols.alloc(f32_row * per, s), "cudaMallocAsync(column planes)");
+            TQ_CUDA(cols.alloc(sizeof(float) * 8 * per, s), "cudaMallocAsync(column scalars)");
             TQ_CUDA(cols_bf.alloc(bf_row * per + 16, s), "cudaMallocAsync(column TF32 planes)");
             err = reinterpret_cast<int *>(static_cast<unsigned char *>(cols_bf.p) + bf_row * per);
             TQ_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "memset");
         }
-        float *P1b = static_cast<float *>(cols.p), *P2b = P1b + per * ldk1, *sb = P2b + per * ldk2;
+        float *sb = static_cast<float *>(cols.p);
         const size_t b1 = per * K1p, b2 = per * K2p;  // floats per plane
         float *B1 = static_cast<float *>(cols_bf.p), *B2 = B1 + 2 * b1;
         const size_t a1 = m_pad * K1p, a2 = m_pad * K2p;
         for (size_t c0 = 0; c0 < n; c0 += per) {
             const size_t nc = std::min(per, n - c0), nc_pad = sq_round_up(nc, 256);
-            TQ_CUDA(tq::launch_symq_planes(sp->P, sp->T, B + c0 * sp->code_size, nc, mode, false, P1b,
-                                           ldk1, P2b, ldk2, sb, s),
-                    "symmetric planes kernel");
-            TQ_CUDA(tq::launch_split_tf32(P1b, nc, ldk1, nc_pad, K1p, B1, B1 + b1, s), "split kernel");
-            TQ_CUDA(tq::launch_split_tf32(P2b, nc, ldk2, nc_pad, K2p, B2, B2 + b2, s), "split kernel");
+            TQ_CUDA(tq::launch_symq_planes_tf32(sp->P, sp->T, B + c0 * sp->code_size, nc, nc_pad, mode,
+                                                false, B1, B1 + b1, K1p, B2, light() ? nullptr : B2 + b2,
+                                                K2p, sb, s),
+                    "symmetric TF32 planes kernel");
             TQ_CUDA(tq::launch_tc_symq(A1, A1 + a1, B1, B1 + b1, K1p, A2, A2 + a2, B2, B2 + b2, K2p,
-                                       mode == tq::SYMQ_LIGHT, m, m_pad, nc, nc_pad, sa, sb, out + c0,
-                                       ldo, err, s),
+                                       light(), m, m_pad, nc, nc_pad, sa, sb, out + c0, ldo, err, s),
                     "tcgen05 symmetric contraction kernel");
         }
         return TQ_OK;

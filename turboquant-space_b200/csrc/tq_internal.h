@@ -80,16 +80,19 @@ int symq_k2(int mode, int D);   // columns of the correction plane
 cudaError_t launch_symq_planes(const Params &P, const DevTables &T, const uint8_t *codes,
                                size_t rows, int mode, bool row_side, float *P1, int ldk1,
                                float *P2, int ldk2, float *scal, cudaStream_t st);
+// The same planes as hi/lo TF32 pairs in FP32 containers (hi = tf32(v),
+// lo = tf32(v - hi)): H1/L1 rows_pad x K1, H2/L2 rows_pad x K2, zero past the
+// planes' columns and past `rows`; L2 may be null for the light variant
+// (exact +-1 signs, lo = 0).  Scalars for the first `rows` rows.
+cudaError_t launch_symq_planes_tf32(const Params &P, const DevTables &T, const uint8_t *codes,
+                                    size_t rows, size_t rows_pad, int mode, bool row_side,
+                                    float *H1, float *L1, int K1, float *H2, float *L2, int K2,
+                                    float *scal, cudaStream_t st);
 cudaError_t launch_symq_prepared_row(const float *recon, const float *sign, const float *sc, int D,
                                      float *P1, int ldk1, float *P2, int ldk2, float *scal,
                                      cudaStream_t st);
 cudaError_t launch_symq_gemm(const float *P1a, const float *P2a, const float *sa, size_t m,
                              const float *P1b, const float *P2b, const float *sb, size_t n,
                              int ldk1, int ldk2, float *out, size_t ldo, cudaStream_t st);
-// FP32 plane (rows x lds) -> TF32 hi/lo planes in FP32 containers (rows_pad x
-// K, x = hi + lo to about 2^-22), zero past `rows` and past `lds`.
-// lds % 4 == 0, K % 4 == 0, lds <= K.
-cudaError_t launch_split_tf32(const float *src, size_t rows, int lds, size_t rows_pad, int K,
-                              float *hi, float *lo, cudaStream_t st);
 
 }  // namespace tq

@@ -67,7 +67,7 @@ cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const 
 
 // The two contractions of the QJL-corrected symmetric distances on tcgen05
 // tensor cores: C1 = A1 B1^T (K1) and C2 = A2 B2^T (K2) over hi/lo TF32 planes
-// (FP32 containers, launch_split_tf32), then out[i, j] = max(0, na^2 + nb^2 -
+// (FP32 containers, launch_symq_planes_tf32), then out[i, j] = max(0, na^2 + nb^2 -
 // 2 (C1 s1a s1b + clamp(C2 s2a s2b, +-|C1 s1a s1b|)) na nb) with the 8-float
 // row scalars sa / sb of tq_symq.cu.  exact2: both K2 planes are +-1 (lo
 // zero), one product per K step there.  K1, K2 % 32 == 0, m_pad % 128 == 0,

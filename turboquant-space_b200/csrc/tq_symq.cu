@@ -70,18 +70,31 @@ __global__ void __launch_bounds__(256) rotated_coords_kernel(const float *__rest
     }
 }
 
+// x rounded to TF32 (10 fraction bits), nearest-even, kept in an FP32
+// container with the low 13 bits clear (finite x).
+__device__ __forceinline__ float round_tf32(float x) {
+    const uint32_t b = __float_as_uint(x);
+    return __uint_as_float((b + 0xFFFu + ((b >> 13) & 1u)) & ~0x1FFFu);
+}
+
 // ---------------------------------------------------------------------------
 // Operand planes: one warp per code.  P1 (ldk1 columns), P2 (ldk2 columns)
 // and 8 scalars per row: [s1, norm, s2, gamma, sigma, scale * gamma,
 // (pi / 2D) * gamma, 0].  The GEMM uses s1, norm and s2:
 //   ip_mse = C1 s1_a s1_b, corr = clamp(C2 s2_a s2_b, +-|ip_mse|).
 // Columns past K are written as zeros.
+// TF32: each value v is written as the pair hi = tf32(v) (P1 / P2) and
+// lo = tf32(v - hi) (L1 / L2; L2 may be null when the second plane holds
+// exact values, the light variant's +-1), and rows [rows, rows_pad) are
+// zero rows (no scalars).
 // ---------------------------------------------------------------------------
-template <int LOG_D>
+template <int LOG_D, bool TF32>
 __global__ void __launch_bounds__(256) symq_planes_kernel(const uint8_t *__restrict__ codes,
-                                                          size_t rows, int mode, int row_side,
-                                                          float *__restrict__ P1, int ldk1,
-                                                          float *__restrict__ P2, int ldk2,
+                                                          size_t rows, size_t rows_pad, int mode,
+                                                          int row_side, float *__restrict__ P1,
+                                                          float *__restrict__ L1, int ldk1,
+                                                          float *__restrict__ P2,
+                                                          float *__restrict__ L2, int ldk2,
                                                           float *__restrict__ scal, Params P,
                                                           DevTables T) {
     constexpr int D = 1 << LOG_D;
@@ -95,7 +108,34 @@ __global__ void __launch_bounds__(256) symq_planes_kernel(const uint8_t *__restr
     float *buf = reinterpret_cast<float *>(smem + kTabBytes) + warp * VS;
     const bool recon = mode != SYMQ_LIGHT;
     const float p2d = __fdiv_rn(kPi, __fmul_rn(2.0f, (float)D));  // (float)M_PI / (2.0f * d)
-    for (size_t r = (size_t)blockIdx.x * nw + warp; r < rows; r += (size_t)gridDim.x * nw) {
+    for (size_t r = (size_t)blockIdx.x * nw + warp; r < rows_pad; r += (size_t)gridDim.x * nw) {
+        float *p1 = P1 + r * (size_t)ldk1;
+        float *p2 = P2 + r * (size_t)ldk2;
+        float *l1 = TF32 ? L1 + r * (size_t)ldk1 : nullptr;
+        float *l2 = (TF32 && L2) ? L2 + r * (size_t)ldk2 : nullptr;
+        auto put1 = [&](int i, float v) {
+            if constexpr (TF32) {
+                const float h = round_tf32(v);
+                p1[i] = h;
+                l1[i] = round_tf32(__fsub_rn(v, h));
+            } else {
+                p1[i] = v;
+            }
+        };
+        auto put2 = [&](int i, float v) {
+            if constexpr (TF32) {
+                const float h = round_tf32(v);
+                p2[i] = h;
+                if (l2) l2[i] = round_tf32(__fsub_rn(v, h));
+            } else {
+                p2[i] = v;
+            }
+        };
+        if (r >= rows) {  // TF32 padding row
+            for (int i = lane; i < ldk1; i += 32) put1(i, 0.0f);
+            for (int i = lane; i < ldk2; i += 32) put2(i, 0.0f);
+            continue;
+        }
         const uint8_t *c = codes + r * (size_t)P.cs;
         float meta[3];  // the trailer may be unaligned (D = 4 nibble codes: pb = 2)
 #pragma unroll
@@ -107,8 +147,6 @@ __global__ void __launch_bounds__(256) symq_planes_kernel(const uint8_t *__restr
         const float norm = meta[0], gamma = meta[1], sigma = meta[2];
         const float sg = __fmul_rn(P.scale, gamma);
         const float pg = __fmul_rn(p2d, gamma);
-        float *p1 = P1 + r * (size_t)ldk1;
-        float *p2 = P2 + r * (size_t)ldk2;
         // pass 1: units -> centroid values and signs
         for (int i = lane; i < D; i += 32) {
             unsigned u;
@@ -122,21 +160,21 @@ __global__ void __launch_bounds__(256) symq_planes_kernel(const uint8_t *__restr
             const float sgn = (u & 1u) ? 1.0f : -1.0f;
             if (recon) buf[swz(i)] = __fmul_rn(cv, sigma);
             if (mode == SYMQ_LIGHT) {
-                p1[i] = cv;
-                p2[i] = sgn;
+                put1(i, cv);
+                put2(i, sgn);
             } else if (mode == SYMQ_FULL) {
-                p1[i] = cv;
+                put1(i, cv);
             }
             if (mode == SYMQ_FULL || mode == SYMQ_FULL_PREPARED) {
                 if (row_side) {
-                    p2[D + i] = sgn * sg;
-                    p2[2 * D + i] = sgn * pg;
+                    put2(D + i, sgn * sg);
+                    put2(2 * D + i, sgn * pg);
                 } else {
-                    p2[i] = sgn * sg;
-                    p2[2 * D + i] = sgn * gamma;
+                    put2(i, sgn * sg);
+                    put2(2 * D + i, sgn * gamma);
                 }
             } else if (mode == SYMQ_PREPARE) {
-                p2[i] = sgn;
+                put2(i, sgn);
             }
         }
         // pass 2: recon = RHT_qjl(c * sigma)
@@ -145,14 +183,14 @@ __global__ void __launch_bounds__(256) symq_planes_kernel(const uint8_t *__restr
             fwht_from<LOG_D, 0, false>(buf, lane, 1.0f, s_qjl, P.wht_scale);
             for (int i = lane; i < D; i += 32) {
                 const float x = buf[swz(i)];
-                if (mode != SYMQ_FULL) p1[i] = x;
-                if (mode == SYMQ_FULL || mode == SYMQ_FULL_PREPARED) p2[(row_side ? 0 : D) + i] = x;
+                if (mode != SYMQ_FULL) put1(i, x);
+                if (mode == SYMQ_FULL || mode == SYMQ_FULL_PREPARED) put2((row_side ? 0 : D) + i, x);
             }
             __syncwarp();
         }
         const int k2 = (mode == SYMQ_FULL || mode == SYMQ_FULL_PREPARED) ? 3 * D : D;
-        for (int i = D + lane; i < ldk1; i += 32) p1[i] = 0.0f;
-        for (int i = k2 + lane; i < ldk2; i += 32) p2[i] = 0.0f;
+        for (int i = D + lane; i < ldk1; i += 32) put1(i, 0.0f);
+        for (int i = k2 + lane; i < ldk2; i += 32) put2(i, 0.0f);
         if (lane == 0) {
             float *s = scal + 8 * r;
             s[0] = (mode == SYMQ_LIGHT || mode == SYMQ_FULL) ? sigma : 1.0f;
@@ -267,39 +305,6 @@ __global__ void __launch_bounds__(256) symq_gemm_kernel(
                                       __fmul_rn(2.0f, ip));
             out[r * ldo + c] = d > 0.0f ? d : 0.0f;
         }
-    }
-}
-
-// x rounded to TF32 (10 fraction bits), nearest-even, kept in an FP32
-// container with the low 13 bits clear (finite x).
-__device__ __forceinline__ float round_tf32(float x) {
-    const uint32_t b = __float_as_uint(x);
-    return __uint_as_float((b + 0xFFFu + ((b >> 13) & 1u)) & ~0x1FFFu);
-}
-
-// FP32 plane -> hi/lo TF32 planes (x = hi + lo, hi = tf32(x),
-// lo = tf32(x - hi)), four columns per thread.
-__global__ void __launch_bounds__(256) split_tf32_kernel(const float *__restrict__ src, size_t rows,
-                                                         int lds, size_t rows_pad, int K,
-                                                         float *__restrict__ hi,
-                                                         float *__restrict__ lo) {
-    const size_t quads = (size_t)(K / 4), total = rows_pad * quads;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (size_t)gridDim.x * blockDim.x) {
-        const size_t r = t / quads;
-        const int k = (int)(t - r * quads) * 4;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (r < rows && k < lds) v = *reinterpret_cast<const float4 *>(src + r * (size_t)lds + k);
-        const float x[4] = {v.x, v.y, v.z, v.w};
-        float h[4], l[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            h[i] = round_tf32(x[i]);
-            l[i] = round_tf32(__fsub_rn(x[i], h[i]));
-        }
-        const size_t o = r * (size_t)K + k;
-        *reinterpret_cast<float4 *>(hi + o) = make_float4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<float4 *>(lo + o) = make_float4(l[0], l[1], l[2], l[3]);
     }
 }
 
@@ -473,20 +478,29 @@ struct RotRun {
 
 template <int LOG_D>
 struct PlanesRun {
-    static cudaError_t run(const Params &P, const DevTables &T, const uint8_t *codes, size_t rows,
-                           int mode, int row_side, float *P1, int ldk1, float *P2, int ldk2,
-                           float *scal, cudaStream_t st) {
+    template <bool TF32>
+    static cudaError_t go(const Params &P, const DevTables &T, const uint8_t *codes, size_t rows,
+                          size_t rows_pad, int mode, int row_side, float *P1, float *L1, int ldk1,
+                          float *P2, float *L2, int ldk2, float *scal, cudaStream_t st) {
         const int D = 1 << LOG_D, w = sq_warps(D);
         const size_t smem = (size_t)kTabBytes + (size_t)w * 4 * (D + 8);
-        cudaError_t e = cudaFuncSetAttribute(symq_planes_kernel<LOG_D>,
+        cudaError_t e = cudaFuncSetAttribute(symq_planes_kernel<LOG_D, TF32>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        size_t blocks = (rows + w - 1) / w;
+        size_t blocks = (rows_pad + w - 1) / w;
         const size_t cap = (size_t)sq_sm_count() * 8;
         if (blocks > cap) blocks = cap;
-        symq_planes_kernel<LOG_D><<<(unsigned)blocks, 32 * w, smem, st>>>(
-            codes, rows, mode, row_side, P1, ldk1, P2, ldk2, scal, P, T);
+        symq_planes_kernel<LOG_D, TF32><<<(unsigned)blocks, 32 * w, smem, st>>>(
+            codes, rows, rows_pad, mode, row_side, P1, L1, ldk1, P2, L2, ldk2, scal, P, T);
         return cudaGetLastError();
+    }
+    static cudaError_t run(const Params &P, const DevTables &T, const uint8_t *codes, size_t rows,
+                           size_t rows_pad, int mode, int row_side, float *P1, float *L1, int ldk1,
+                           float *P2, float *L2, int ldk2, float *scal, cudaStream_t st) {
+        if (L1) return go<true>(P, T, codes, rows, rows_pad, mode, row_side, P1, L1, ldk1, P2, L2, ldk2,
+                                scal, st);
+        return go<false>(P, T, codes, rows, rows, mode, row_side, P1, nullptr, ldk1, P2, nullptr, ldk2,
+                         scal, st);
     }
 };
 
@@ -508,28 +522,26 @@ cudaError_t launch_symq_planes(const Params &P, const DevTables &T, const uint8_
                                size_t rows, int mode, bool row_side, float *P1, int ldk1,
                                float *P2, int ldk2, float *scal, cudaStream_t st) {
     if (rows == 0) return cudaSuccess;
-    return dispatch_logd_sq<PlanesRun>(P.log2D, P, T, codes, rows, mode, (int)row_side, P1, ldk1,
-                                       P2, ldk2, scal, st);
+    return dispatch_logd_sq<PlanesRun>(P.log2D, P, T, codes, rows, rows, mode, (int)row_side, P1,
+                                       (float *)nullptr, ldk1, P2, (float *)nullptr, ldk2, scal, st);
+}
+
+cudaError_t launch_symq_planes_tf32(const Params &P, const DevTables &T, const uint8_t *codes,
+                                    size_t rows, size_t rows_pad, int mode, bool row_side,
+                                    float *H1, float *L1, int K1, float *H2, float *L2, int K2,
+                                    float *scal, cudaStream_t st) {
+    if (rows_pad == 0) return cudaSuccess;
+    if (!H1 || !L1 || !H2 || rows > rows_pad || K1 < (1 << P.log2D) ||
+        K2 < symq_k2(mode, 1 << P.log2D))
+        return cudaErrorInvalidValue;
+    return dispatch_logd_sq<PlanesRun>(P.log2D, P, T, codes, rows, rows_pad, mode, (int)row_side, H1,
+                                       L1, K1, H2, L2, K2, scal, st);
 }
 
 cudaError_t launch_symq_prepared_row(const float *recon, const float *sign, const float *sc, int D,
                                      float *P1, int ldk1, float *P2, int ldk2, float *scal,
                                      cudaStream_t st) {
     symq_prepared_row_kernel<<<1, 256, 0, st>>>(recon, sign, sc, D, P1, ldk1, P2, ldk2, scal);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_split_tf32(const float *src, size_t rows, int lds, size_t rows_pad, int K,
-                              float *hi, float *lo, cudaStream_t st) {
-    if (rows_pad == 0) return cudaSuccess;
-    if (lds % 4 || K % 4 || lds > K) return cudaErrorInvalidValue;
-    for (const void *p : {(const void *)src, (const void *)hi, (const void *)lo})
-        if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorMisalignedAddress;
-    size_t blocks = (rows_pad * (size_t)(K / 4) + 255) / 256;
-    const size_t cap = (size_t)sq_sm_count() * 16;
-    if (blocks > cap) blocks = cap;
-    split_tf32_kernel<<<(unsigned)(blocks ? blocks : 1), 256, 0, st>>>(src, rows, lds, rows_pad, K,
-                                                                       hi, lo);
     return cudaGetLastError();
 }
 

@@ -192,11 +192,14 @@ struct TcMaps {
     CUtensorMap m[2][4];
 };
 
-// K blocks of each segment, the first block whose B lo is zero (kbx = KB: none)
-// and whether the segment's A lo is zero.
+// K blocks of each segment, the first block whose B lo is zero (kbx = KB: none),
+// whether the segment's A lo is zero, and whether its sums are exact in one
+// accumulator (whole: products of +-1 by +-1, integer partial sums of
+// magnitude <= K < 2^24, which FP32 accumulation holds exactly; the segment
+// is then one chunk with no promotion).
 struct TcShape {
     int nseg;
-    int KB[2], kbx[2], a_exact[2];
+    int KB[2], kbx[2], a_exact[2], whole[2];
 };
 
 // ---------------------------------------------------------------------------
@@ -294,12 +297,13 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
             for (int t = 0; t < ntiles && ok; ++t) {
                 for (int sg = 0; sg < sh.nseg && ok; ++sg) {
                     const bool alo = !sh.a_exact[sg];
-                    for (int c0 = 0; c0 < sh.KB[sg] && ok; c0 += CH, ++gc) {
+                    const int chl = sh.whole[sg] ? sh.KB[sg] : CH;
+                    for (int c0 = 0; c0 < sh.KB[sg] && ok; c0 += chl, ++gc) {
                         const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
                         if (!mbar_wait(xempty0 + 8 * b, xph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
                         tc_fence_after();
                         const uint32_t d_tmem = tmem_base + b * TC_BN;
-                        const int c1 = c0 + CH < sh.KB[sg] ? c0 + CH : sh.KB[sg];
+                        const int c1 = c0 + chl < sh.KB[sg] ? c0 + chl : sh.KB[sg];
                         uint32_t acc = 0u;
                         for (int kb = c0; kb < c1; ++kb, ++it) {
                             const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
@@ -350,7 +354,8 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
             }
             for (int sg = 0; sg < sh.nseg && ok; ++sg) {
                 const uint32_t Y = lanes + (2 + (SPLIT ? yb : (uint32_t)sg)) * TC_BN;
-                for (int c0 = 0; c0 < sh.KB[sg]; c0 += CH, ++gc) {
+                const int chl = sh.whole[sg] ? sh.KB[sg] : CH;
+                for (int c0 = 0; c0 < sh.KB[sg]; c0 += chl, ++gc) {
                     const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
                     if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
                     tc_fence_after();
@@ -1213,7 +1218,7 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
         return cudaErrorInvalidValue;
     if (!aligned16({Ah, Al, Bh, Bl})) return cudaErrorMisalignedAddress;
     alignas(64) TcMaps mp;
-    TcShape sh;
+    TcShape sh{};
     if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
     if (variant == 0) {
         // 128 x 256 tiles (tcw_kernel), two partial lists per (row, slice)
@@ -1250,7 +1255,7 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
         return cudaErrorInvalidValue;
     if (!aligned16({Ah, Al, Bh, Bl})) return cudaErrorMisalignedAddress;
     alignas(64) TcMaps mp;
-    TcShape sh;
+    TcShape sh{};
     if (!bf16_maps(mp, sh, Ah, Al, m_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
     const unsigned num_mb = (unsigned)(m_pad / TC_BM);
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
@@ -1297,6 +1302,7 @@ cudaError_t launch_tc_symq(const void *A1h, const void *A1l, const void *B1h, co
     sh.kbx[1] = exact2 ? 0 : sh.KB[1];
     sh.a_exact[0] = 0;
     sh.a_exact[1] = exact2 ? 1 : 0;
+    sh.whole[1] = exact2 ? 1 : 0;
     const unsigned num_mb = (unsigned)(m_pad / TC_BM);
     const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
     if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
