@@ -143,3 +143,23 @@ def test_fewer_codes_than_k(cuda_ok):
     D, I = ix.search(rng.standard_normal((3, DIM)).astype(np.float32), k=8)
     assert np.all(I[:, 5:] == -1) and np.all(np.sort(I[:, :5], axis=1) == np.arange(5))
     ix.close()
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_every_column_inserts(corpus, variant):
+    """Worst case for the per-row lists: the index holds the codes in order of
+    descending distance to the first query, so every column of every slice
+    beats that row's current k-th entry and goes through the sorted insert."""
+    space, codes, Q, ref, _ = corpus
+    perm = np.argsort(-ref[0].astype(np.float64), kind="stable")
+    index = space.index(np.ascontiguousarray(codes[perm]))
+    try:
+        ref_p = ref[:64][:, perm]
+        qn2 = np.sum(Q[:64].astype(np.float64) ** 2, axis=1)
+        for k in (1, 10, 16):
+            with index.serve(k=k, max_rows=128, slots=1, kernel_variant=variant) as sv:
+                D, I = sv.submit(Q[:64]).wait()
+            assert D.shape == (64, k)
+            assert _check_topk(D, I, ref_p, k, qn2) >= 58
+    finally:
+        index.close()
