@@ -779,8 +779,7 @@ def main():
                          "traffic": (int(round(SCAN_TRAFFIC_PER_CODE * n))
                                      if (DIM, BITS) == (768, 8) else None),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                           "1M-code launch, scaled per code "
-                                           "(profiles/scant_kernel_1M_768d_b8.md)",
+                                           "1M-code launch, scaled per code",
                          "kernel": scan_kernel_name(DIM, BITS),
                          "bytes_per_launch": scan_bytes, "ms_per_launch": round(scan_ms, 4),
                          "peak_kind": peak_kind},

@@ -174,7 +174,10 @@ tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_
  * with TQ_ERR_INVALID_ARGUMENT.  No call allocates or frees device memory.
  *
  * The first call on a device looks up that device's copy of the array
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress) and keeps its address for the life of the process;
+ * make that first call before any stream capture.  A device reset
+ * (cudaDeviceReset) may move the array, so this entry point must not be
+ * called on a device after that device was reset.
  * All calls on a device share the one array, and it keeps the last call's
  * contents; each call rewrites every value it reads before reading it, so
  * nothing needs clearing.  Calls whose work overlaps on the GPU (different
