@@ -282,22 +282,150 @@ static inline void code_meta(const tqo_space *sp, const uint8_t *code, float m[3
     memcpy(m, code + sp->packed_bytes, 12);
 }
 
-/* distSearchScalar / distSearchScalarB4: space_turbo_quant.h:659-686, 951-983 */
-static float dist_search(const tqo_space *sp, const float *q_rot, const float *s_q,
-                         const float *norms, const uint8_t *code) {
+/* ---- asymmetric distance as the pinned build computes it --------------------
+ * The reference picks distSearchAVX (space_turbo_quant.h:1457-1539) for bits >= 5
+ * and distSearchScalarB4 (:951-983) for bits <= 4 on x86 (:280-302).  Under
+ * -O3 -ffast-math -march=x86-64-v3 the compiler re-associates both loops; the
+ * order below is the one read from the x86 assembly of that build (the
+ * assembly of code compiled here from the reference's sources).  Every
+ * operation is a single IEEE FP32 rounding (this file is compiled without
+ * contraction; fmaf is a fused multiply-add). */
+
+/* A __m256 reduced to a scalar the way both functions end:
+ * ((v0 + v4) + (v2 + v6)) + ((v1 + v5) + (v3 + v7)). */
+static float hsum8(const float v[8]) {
+    float w0 = v[0] + v[4], w1 = v[1] + v[5], w2 = v[2] + v[6], w3 = v[3] + v[7];
+    return (w0 + w2) + (w1 + w3);
+}
+
+/* A __m128 reduced to a scalar: (u0 + u2) + (u1 + u3). */
+static float hsum4(const float u[4]) { return (u[0] + u[2]) + (u[1] + u[3]); }
+
+static inline float signed_s(float s, unsigned bit) { return bit ? s : -s; }
+
+/* distSearchScalarB4 (:951-983), nibble codes.  Byte b holds coordinates 2b
+ * (low nibble) and 2b+1 (high nibble).  Per byte the two MSE terms fuse as
+ * fma(q[2b], c_lo, q[2b+1] * c_hi) and the two QJL terms add as e_lo + e_hi.
+ *  - D >= 64: 32 running sums, byte b into sum b mod 32, in byte order; then
+ *    V_j = (A_{16+j} + A_{24+j}) + (A_j + A_{8+j}) and hsum8(V).
+ *  - D == 32 (16 bytes left): one 4-lane step whose tree is written out below.
+ *  - D <= 16: a sequential loop over bytes.
+ * Epilogue: ip = fma(ip_sum, sigma, (scale * gamma) * dot) * |x|, then
+ * d = fma(-ip, 2|q|, fma(|x|, |x|, |q|^2)), clamped at 0. */
+static float dist_search_b4(const tqo_space *sp, const float *q, const float *s,
+                            const float *norms, const uint8_t *code) {
+    const size_t D = sp->D, nb = sp->packed_bytes;
+    const float *c = sp->centroids;
     float m[3];
     code_meta(sp, code, m);
-    float ip_mse = 0.0f, dot_qjl = 0.0f;
-    for (size_t i = 0; i < sp->D; ++i) {
-        unsigned u = code_unit(code, i, sp->bits);
-        ip_mse = ip_mse + q_rot[i] * sp->centroids[u >> 1];
-        dot_qjl = dot_qjl + s_q[i] * ((u & 1) ? 1.0f : -1.0f);
+    /* the reference reads q[2b + 1] of the last byte even at D == 1; it is
+     * past the end of its prepared query there, zero here */
+    #define QAT(i) ((i) < D ? q[(i)] : 0.0f)
+    #define SAT(i) ((i) < D ? s[(i)] : 0.0f)
+    float ip = 0.0f, dot = 0.0f;
+    size_t b = 0;
+    if (D >= 63) {
+        float A[32], S[32];
+        for (int t = 0; t < 32; ++t) A[t] = S[t] = 0.0f;
+        const size_t nb32 = nb & ~(size_t)31;
+        for (; b < nb32; b += 32)
+            for (int t = 0; t < 32; ++t) {
+                const size_t k = b + (size_t)t;
+                const unsigned lo = code[k] & 15u, hi = code[k] >> 4;
+                const float ph = q[2 * k + 1] * c[hi >> 1];
+                A[t] = A[t] + fmaf(q[2 * k], c[lo >> 1], ph);
+                S[t] = S[t] + (signed_s(s[2 * k], lo & 1u) + signed_s(s[2 * k + 1], hi & 1u));
+            }
+        float V[8], W[8];
+        for (int j = 0; j < 8; ++j) {
+            V[j] = (A[16 + j] + A[24 + j]) + (A[j] + A[8 + j]);
+            W[j] = (S[16 + j] + S[24 + j]) + (S[j] + S[8 + j]);
+        }
+        ip = hsum8(V);
+        dot = hsum8(W);
     }
-    ip_mse = ip_mse * m[2];
-    float correction = sp->scale * m[1] * dot_qjl;
-    float ip = (ip_mse + correction) * m[0] * norms[1];
-    float d = norms[0] + m[0] * m[0] - 2.0f * ip;
-    return d > 0.0f ? d : 0.0f;
+    if (nb - b >= 16) {
+        /* bytes b .. b+15 as four groups g of four lanes j: byte b + 4g + j */
+        float L[4][4], H[4][4], El[4][4], Eh[4][4];
+        for (int g = 0; g < 4; ++g)
+            for (int j = 0; j < 4; ++j) {
+                const size_t k = b + (size_t)(4 * g + j);
+                const unsigned lo = code[k] & 15u, hi = code[k] >> 4;
+                L[g][j] = c[lo >> 1];
+                H[g][j] = c[hi >> 1];
+                El[g][j] = signed_s(SAT(2 * k), lo & 1u);
+                Eh[g][j] = signed_s(SAT(2 * k + 1), hi & 1u);
+            }
+        float U[4], Q4[4];
+        for (int j = 0; j < 4; ++j) {
+            const size_t k0 = b + (size_t)j, k1 = k0 + 4, k2 = k0 + 8, k3 = k0 + 12;
+            const float t1 = fmaf(L[2][j], QAT(2 * k2), QAT(2 * k3) * L[3][j]);
+            const float t2 = fmaf(QAT(2 * k0), L[0][j], L[1][j] * QAT(2 * k1));
+            const float t3 = fmaf(QAT(2 * k2 + 1), H[2][j], QAT(2 * k3 + 1) * H[3][j]);
+            const float t4 = fmaf(QAT(2 * k0 + 1), H[0][j], H[1][j] * QAT(2 * k1 + 1));
+            U[j] = ((t4 + t3) + t2) + t1;
+            const float p1 = El[0][j] + El[1][j], p2 = El[2][j] + El[3][j];
+            const float q1 = Eh[0][j] + Eh[1][j], q3 = Eh[2][j] + Eh[3][j];
+            Q4[j] = q3 + (q1 + (p2 + p1));
+        }
+        ip = ip + hsum4(U);
+        dot = dot + hsum4(Q4);
+        b += 16;
+    }
+    for (; b < nb; ++b) {
+        const unsigned lo = code[b] & 15u, hi = code[b] >> 4;
+        const float ph = c[hi >> 1] * QAT(2 * b + 1);
+        ip = ip + fmaf(QAT(2 * b), c[lo >> 1], ph);
+        dot = dot + (signed_s(SAT(2 * b + 1), hi & 1u) + signed_s(SAT(2 * b), lo & 1u));
+    }
+    #undef QAT
+    #undef SAT
+    float t = (sp->scale * m[1]) * dot;
+    t = fmaf(ip, m[2], t) * m[0];
+    const float d = fmaf(-t, norms[1] + norms[1], fmaf(m[0], m[0], norms[0]));
+    return 0.0f < d ? d : 0.0f;
+}
+
+/* distSearchAVX (:1457-1539), byte codes.  D >= 8: eight running sums,
+ * coordinate i into sum i mod 8, as fma(c[u >> 1], q[i], sum) and sum + (+-s[i]);
+ * ip = hsum8 * sigma, dot = hsum8.  D < 8: a sequential loop of
+ * (sigma * q[i]) * c[u >> 1] and +-s[i].  Epilogue:
+ * ip = fma(gamma * scale, dot, ip) * |x|, then
+ * d = fma(-ip, 2|q|, fma(|x|, |x|, |q|^2)), clamped at 0. */
+static float dist_search_b8(const tqo_space *sp, const float *q, const float *s,
+                            const float *norms, const uint8_t *code) {
+    const size_t D = sp->D;
+    const float *c = sp->centroids;
+    float m[3];
+    code_meta(sp, code, m);
+    float ip = 0.0f, dot = 0.0f;
+    size_t i = 0;
+    if (D >= 8) {
+        float A[8], S[8];
+        for (int j = 0; j < 8; ++j) A[j] = S[j] = 0.0f;
+        for (; i + 8 <= D; i += 8)
+            for (int j = 0; j < 8; ++j) {
+                const unsigned u = code[i + (size_t)j];
+                A[j] = fmaf(c[u >> 1], q[i + (size_t)j], A[j]);
+                S[j] = S[j] + signed_s(s[i + (size_t)j], u & 1u);
+            }
+        ip = hsum8(A) * m[2];
+        dot = hsum8(S);
+    }
+    for (; i < D; ++i) {
+        const unsigned u = code[i];
+        ip = ip + (m[2] * q[i]) * c[u >> 1];
+        dot = dot + signed_s(s[i], u & 1u);
+    }
+    float t = fmaf(m[1] * sp->scale, dot, ip) * m[0];
+    const float d = fmaf(-t, norms[1] + norms[1], fmaf(m[0], m[0], norms[0]));
+    return 0.0f < d ? d : 0.0f;
+}
+
+static float dist_search(const tqo_space *sp, const float *q_rot, const float *s_q,
+                         const float *norms, const uint8_t *code) {
+    return sp->bits <= 4 ? dist_search_b4(sp, q_rot, s_q, norms, code)
+                         : dist_search_b8(sp, q_rot, s_q, norms, code);
 }
 
 /* distBuildScalar / distBuildScalarB4: space_turbo_quant.h:688-714, 985-1019 */

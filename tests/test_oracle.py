@@ -42,12 +42,11 @@ def test_oracle_distances_vs_golden(dim, bits):
     o = O.OracleSpace(dim, bits)
     cs, pb = o.cs, o.cs - 12
     codes = g["codes"]
-    d1 = o.distance_1_to_n(g["q"], codes)
-    err, ok = dist_close(d1, g["d1n"], asym_term_scale(g["q"], codes, cs, pb)[0])
-    assert ok, err.max()
-    dm = o.distance_m_to_n(g["Q"], codes)
-    err, ok = dist_close(dm, g["dmn"], asym_term_scale(g["Q"], codes, cs, pb))
-    assert ok, err.max()
+    # asymmetric distances: the pinned build's summation order, bit for bit
+    np.testing.assert_array_equal(o.distance_1_to_n(g["q"], codes).view(np.uint32),
+                                  g["d1n"].view(np.uint32))
+    np.testing.assert_array_equal(o.distance_m_to_n(g["Q"], codes).view(np.uint32),
+                                  g["dmn"].view(np.uint32))
     ds = o.distance_m_to_n_symmetric(codes[:8], codes)
     err, ok = dist_close(ds, g["dsym"], sym_term_scale(codes[:8], codes, cs, pb))
     assert ok, err.max()
@@ -109,6 +108,25 @@ def test_oracle_vs_reference_live(dim, bits):
     q = rng.standard_normal(dim).astype(np.float32)
     for a, b in zip(o.prepare_query(q), r.prepare_query(q)):
         np.testing.assert_array_equal(a, b)
+    codes = r.encode_batch(X)
+    for qq in (q, np.zeros(dim, np.float32), (q * 1e-3).astype(np.float32)):
+        np.testing.assert_array_equal(o.distance_1_to_n(qq, codes).view(np.uint32),
+                                      r.distance_1_to_n(qq, codes).view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("bits", [2, 3, 4, 5, 8, 9])
+def test_oracle_asym_distances_bit_exact_every_dim(bits):
+    """Every padded dim 4 .. 4096: the three nibble loop shapes (D <= 16, D == 32,
+    D >= 64) and the two byte shapes (D < 8, D >= 8) of the pinned build."""
+    for dim in (1, 3, 5, 9, 17, 33, 64, 100, 256, 384, 768, 1024, 2048, 4096):
+        rng = np.random.default_rng(dim * 7 + bits)
+        X = rng.standard_normal((200, dim)).astype(np.float32)
+        Q = rng.standard_normal((3, dim)).astype(np.float32)
+        o, r = O.OracleSpace(dim, bits), O.RefSpace(dim, bits)
+        codes = r.encode_batch(X)
+        np.testing.assert_array_equal(o.distance_m_to_n(Q, codes).view(np.uint32),
+                                      r.distance_m_to_n(Q, codes).view(np.uint32))
 
 
 @needs_ref
