@@ -50,8 +50,11 @@ typedef enum tq_status {
 typedef enum tq_precision {
     TQ_PRECISION_FP32 = 0,       /* FP32 CUDA-core kernels: the drop-in */
     TQ_PRECISION_SPLIT_BF16 = 1, /* tcgen05 tensor cores on hi+lo BF16 pairs, FP32 TMEM accumulators */
-    TQ_PRECISION_SPLIT_TF32 = 2  /* tcgen05 tensor cores on hi+lo TF32 pairs, FP32 TMEM accumulators
+    TQ_PRECISION_SPLIT_TF32 = 2, /* tcgen05 tensor cores on hi+lo TF32 pairs, FP32 TMEM accumulators
                                     (the QJL-corrected symmetric distances only) */
+    TQ_PRECISION_REFERENCE = 3   /* the reference's own FP32 arithmetic in its Release build's
+                                    summation order, one code per thread: bit-identical to
+                                    distSearchScalarB4 / distSearchAVX (asymmetric M x N only) */
 } tq_precision;
 
 /* The QJL-corrected symmetric distances (space_turbo_quant.h:483-572, 731-945). */
@@ -260,9 +263,12 @@ tq_status tq_selftest_bounded_wait(int device, int budget_ms);
 
 /* ---- serving: device-resident index + continuous-batching top-k server ---
  * The reference has no index or serving loop (README.md:81-83); these entry
- * points serve exact top-k asymmetric search (distSearch, space_turbo_quant.h
- * :659-686) over a corpus kept in HBM.  Results are ascending by distance,
- * ties broken by the smaller code index (a stable argsort). */
+ * points serve exact top-k asymmetric search over a corpus kept in HBM.  The
+ * results are the stable argsort of the reference's own distances
+ * (distSearchScalarB4 / distSearchAVX, space_turbo_quant.h:951-983 and
+ * :1457-1539, in its Release build's summation order): ascending distance,
+ * ties broken by the smaller code index, bit-identical distances, the same
+ * whatever batch a request shares. */
 typedef struct tq_index tq_index;
 typedef struct tq_server tq_server;
 typedef struct tq_request tq_request;
@@ -271,23 +277,41 @@ typedef struct tq_server_stats {
     uint64_t submitted, rejected, completed, batches, rows;
     size_t queued_rows;
     int slots, max_rows;
+    int candidates;              /* tensor-pass candidates per query row */
+    uint64_t fallback_rows;      /* rows the certificate left open, answered by a full exact pass */
+    uint64_t bound_violations;   /* candidates whose two distances differed by more than the bound */
 } tq_server_stats;
 
-/* Decode n codes (host or device memory) once into the index's BF16 operand
- * planes in HBM: the hi plane of 2 * padded_dim values and the lo plane of the
- * padded_dim centroid values (the sign half is exact), 6 * padded_dim + 8
- * bytes per code. */
+/* Keep n codes (host or device memory) resident in HBM, with their BF16
+ * tensor-core operand planes: the hi plane of 2 * padded_dim values and the
+ * lo plane of the padded_dim centroid values (the sign half is exact), so
+ * code_size + 6 * padded_dim + 8 bytes per code. */
 tq_status tq_index_create(const tq_space *sp, const uint8_t *codes, size_t n, int codes_on_device,
                           tq_index **out);
 void tq_index_destroy(tq_index *ix);
 
-/* A server answering top-k (k <= 16) for requests of up to max_rows queries
- * (a multiple of 128).  `slots` batches may be in flight at once (fewer if
- * they do not fit in half of the free device memory); kernel_variant -1
- * autotunes the contraction's tile shape per batch-size bucket, 0..2 fixes it
- * (0: 128 x 256 tiles; 1, 2: 128 x 128 tiles with 3 or 2 stages); queue_rows
- * bounds the queued query rows (0: 16 x max_rows), beyond which submit
- * returns TQ_ERR_BUSY. */
+typedef struct tq_server_params {
+    int k;              /* results per query row, 1..16 */
+    int max_rows;       /* query rows per batch, a positive multiple of 128 */
+    int slots;          /* batches in flight, 1..8 (fewer if they do not fit in half of the
+                           free device memory) */
+    int kernel_variant; /* -1: autotune the contraction per batch-size bucket; 0..2 fixed
+                           (0: 128 x 256 tiles; 1, 2: 128 x 128 tiles with 3 or 2 stages) */
+    size_t queue_rows;  /* queued query rows beyond which submit returns TQ_ERR_BUSY
+                           (0: 16 x max_rows) */
+    int candidates;     /* tensor-pass candidates per row that the exact stage rescores,
+                           k..32 (0: min(32, k + 16)) */
+    float bound_scale;  /* multiplier on the certificate's error bound (0: 1); a larger
+                           value sends more rows to the exact full pass */
+} tq_server_params;
+
+/* A server answering exact top-k for requests of up to max_rows queries:
+ * a tcgen05 split-BF16 pass keeps `candidates` per row, a rescoring kernel
+ * recomputes them with the reference's arithmetic and certifies the top-k
+ * against the pass's error bound, and rows it cannot certify get an exact
+ * full pass over the codes. */
+tq_status tq_server_create_ex(tq_index *ix, const tq_server_params *params, tq_server **out);
+/* tq_server_create_ex with candidates = 0 and bound_scale = 0. */
 tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int kernel_variant,
                            size_t queue_rows, tq_server **out);
 /* Queue m query rows (m x dim float32, copied); non-blocking. */

@@ -427,3 +427,46 @@ def test_bounded_wait_reports_timeout_and_context_survives(cuda_ok):
     g = load_case(128, 4)
     s = tq.TurboQuantSpace(128, 4)
     np.testing.assert_array_equal(s.encode_batch(g["X"]), g["codes"])
+
+
+# ---- reference-order arithmetic (TQ_PRECISION_REFERENCE) -------------------
+# The same FP32 operations in the same order as the reference's Release build
+# (distSearchScalarB4 / distSearchAVX as compiled), so the distances are
+# bit-identical to the reference's, not merely within the tolerance.
+
+@pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
+def test_reference_precision_bit_identical_to_golden(cuda_ok, dim, bits):
+    g = load_case(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    got = s.distance_m_to_n(g["Q"], g["codes"], precision="reference")
+    np.testing.assert_array_equal(got.view(np.uint32), g["dmn"].view(np.uint32))
+
+
+@pytest.mark.parametrize("dim,bits", [(3, 4), (17, 3), (31, 2), (33, 4), (100, 4), (384, 4),
+                                      (768, 4), (1536, 4), (5, 8), (9, 5), (200, 8), (768, 8),
+                                      (2048, 9), (4096, 7)])
+def test_reference_precision_bit_identical_to_oracle(cuda_ok, dim, bits):
+    """Every loop shape of both reference functions: nibble D <= 16, D == 32,
+    D >= 64; byte D < 8, D >= 8; zero and tiny rows; the device path too."""
+    import torch
+    rng = np.random.default_rng(dim * 5 + bits)
+    X = (rng.standard_normal((700, dim)) * rng.uniform(1e-3, 1e3, (700, 1))).astype(np.float32)
+    X[0] = 0.0
+    Q = rng.standard_normal((9, dim)).astype(np.float32)
+    Q[0] = 0.0
+    s = tq.TurboQuantSpace(dim, bits)
+    codes = s.encode_batch(X)
+    want = O.OracleSpace(dim, bits).distance_m_to_n(Q, codes)
+    got = s.distance_m_to_n(Q, codes, precision="reference")
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    dev = s.distance_m_to_n(torch.from_numpy(Q).cuda(), torch.from_numpy(codes).cuda(),
+                            precision="reference")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dev.cpu().numpy().view(np.uint32), want.view(np.uint32))
+
+
+def test_reference_precision_refused_for_symmetric(cuda_ok):
+    s = tq.TurboQuantSpace(64, 4)
+    codes = s.encode_batch(np.ones((3, 64), np.float32))
+    with pytest.raises(tq.TQError):
+        s.distance_m_to_n_symmetric(codes, codes, precision="reference")

@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "tq_exact.h"
 #include "tq_host.h"
 #include "tq_internal.h"
 #include "tq_mton.h"
@@ -122,11 +123,24 @@ tq_status ensure_host_streams(tq_space *sp) {
     return TQ_OK;
 }
 
+// Precisions of the M x N entry points: FP32 and split-BF16 for both forms;
+// the reference-order arithmetic for the asymmetric form only (the symmetric
+// distBuild order is not restated).
+tq_status mton_precision_ok(tq_precision p, bool sym) {
+    if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_BF16) return TQ_OK;
+    if (p == TQ_PRECISION_REFERENCE && !sym) return TQ_OK;
+    if (p == TQ_PRECISION_REFERENCE || p == TQ_PRECISION_SPLIT_TF32)
+        return fail(TQ_ERR_NOT_SUPPORTED, "precision %d is not available for %s distances", (int)p,
+                    sym ? "symmetric" : "asymmetric");
+    return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)p);
+}
+
 // M x N driver.  The row side (m queries, or m codes for the symmetric form)
 // is prepared once; the column side is decoded and contracted in chunks:
 //   FP32, m < kScanRows:  the HBM-bound scan kernel per row (no planes);
 //   FP32 otherwise:       FP32 planes + CUDA-core SGEMM;
-//   SPLIT_BF16:           hi/lo BF16 planes + tcgen05 GEMM.
+//   SPLIT_BF16:           hi/lo BF16 planes + tcgen05 GEMM;
+//   REFERENCE:            the reference build's own arithmetic, one code per thread.
 // Every distance ends in the same epilogue d = max(0, r2 + c2 - 2 C r1 c1).
 class MtonRunner {
   public:
@@ -145,7 +159,7 @@ class MtonRunner {
         : sp_(sp), sym_(sym), prec_(prec), m_(m) {
         K_ = sym ? (int)sp->D : 2 * (int)sp->D;
         fmt_ = prec == TQ_PRECISION_SPLIT_BF16 ? tq::kPlaneBF16 : tq::kPlaneF32;
-        planes_ = prec == TQ_PRECISION_SPLIT_BF16 || m >= kScanRows;
+        planes_ = prec != TQ_PRECISION_REFERENCE && (prec == TQ_PRECISION_SPLIT_BF16 || m >= kScanRows);
         m_pad_ = round_up(m, tq::kPlaneRowAlign);
         const size_t col_align = prec == TQ_PRECISION_SPLIT_BF16 ? 256 : 128;
         nc_max_ = std::max(col_align, ((kColPlaneBytes / ((size_t)K_ * 4)) / col_align) * col_align);
@@ -190,7 +204,11 @@ class MtonRunner {
     // columns [0, n) of device codes -> out[i * ldo + j]
     tq_status run_cols(const uint8_t *codes, size_t n, float *out, size_t ldo, cudaStream_t s) {
         if (!planes_) {
-            if (!sym_)
+            if (!sym_ && prec_ == TQ_PRECISION_REFERENCE)
+                TQ_CUDA(tq::launch_exact_mton(sp_->P, sp_->T.centroids, q_rot_, s_q_, norms_, m_, codes,
+                                              n, out, ldo, s),
+                        "reference-order m_to_n kernel");
+            else if (!sym_)
                 TQ_CUDA(tq::launch_mton_fp32(sp_->P, sp_->T, q_rot_, s_q_, norms_, m_, codes, n, out,
                                              ldo, s),
                         "m_to_n scan kernel");
@@ -630,8 +648,7 @@ tq_status tq_distance_m_to_n_device(const tq_space *sp, const float *queries, si
                                     tq_precision precision, void *stream) {
     tq_status st = need_device(sp);
     if (st != TQ_OK) return st;
-    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if ((st = mton_precision_ok(precision, false)) != TQ_OK) return st;
     if (m == 0 || n == 0) return TQ_OK;
     DeviceGuard g(sp->device);
     if ((st = check_dev(queries, m * sp->dim * 4, "queries")) != TQ_OK) return st;
@@ -655,8 +672,7 @@ tq_status tq_distance_m_to_n_symmetric_device(const tq_space *sp, const uint8_t 
                                               tq_precision precision, void *stream) {
     tq_status st = need_device(sp);
     if (st != TQ_OK) return st;
-    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if ((st = mton_precision_ok(precision, true)) != TQ_OK) return st;
     if (m == 0 || n == 0) return TQ_OK;
     DeviceGuard g(sp->device);
     if ((st = check_dev(A, m * sp->code_size, "codes_a")) != TQ_OK) return st;
@@ -849,8 +865,7 @@ tq_status tq_distance_m_to_n(const tq_space *csp, const float *queries, size_t m
                              const uint8_t *codes, size_t n, float *out, tq_precision precision) {
     tq_status st = need_device(csp);
     if (st != TQ_OK) return st;
-    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if ((st = mton_precision_ok(precision, false)) != TQ_OK) return st;
     if (m == 0 || n == 0) return TQ_OK;
     if (!queries || !codes || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
     auto *sp = const_cast<tq_space *>(csp);
@@ -865,8 +880,7 @@ tq_status tq_distance_m_to_n_symmetric(const tq_space *csp, const uint8_t *codes
                                        tq_precision precision) {
     tq_status st = need_device(csp);
     if (st != TQ_OK) return st;
-    if (precision != TQ_PRECISION_FP32 && precision != TQ_PRECISION_SPLIT_BF16)
-        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)precision);
+    if ((st = mton_precision_ok(precision, true)) != TQ_OK) return st;
     if (m == 0 || n == 0) return TQ_OK;
     if (!codes_a || !codes_b || !out) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL buffer");
     auto *sp = const_cast<tq_space *>(csp);
@@ -1013,7 +1027,7 @@ struct SymqRunner {
 // errors do not average out (see tc_symq_kernel) and exceed 1e-5.
 tq_status symq_precision_ok(tq_precision p) {
     if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_TF32) return TQ_OK;
-    if (p == TQ_PRECISION_SPLIT_BF16)
+    if (p == TQ_PRECISION_SPLIT_BF16 || p == TQ_PRECISION_REFERENCE)
         return fail(TQ_ERR_NOT_SUPPORTED,
                     "QJL-corrected symmetric distances take TQ_PRECISION_FP32 or "
                     "TQ_PRECISION_SPLIT_TF32 (a BF16 pair is not accurate enough here)");

@@ -1,0 +1,609 @@
+// tq_exact.cu -- the reference's asymmetric distance replayed on the GPU in the
+// summation order of the reference's own Release build, and the serving
+// path's exact top-k stages built on it.
+//
+// The reference evaluates distSearchScalarB4 (space_turbo_quant.h:951-983) for
+// bits <= 4 and distSearchAVX (:1457-1539) for bits >= 5 on x86 (:280-302).
+// Compiled with its Release flags (-O3 -ffast-math -march=x86-64-v3), both
+// loops are re-associated by the compiler; the orders below are the ones that
+// build executes (read from its x86 assembly, and pinned bit for bit against
+// it on every padded dim by the CPU checker's tests):
+//
+//   nibble codes, byte b = coordinates 2b (low nibble) and 2b+1 (high):
+//     pair_b = fma(q[2b], c[lo >> 1], q[2b+1] * c[hi >> 1]),
+//     sign_b = (+-s[2b]) + (+-s[2b+1]);
+//     D >= 64: 32 running sums, byte b into sum b mod 32 in byte order, then
+//              V_j = (A_{16+j} + A_{24+j}) + (A_j + A_{8+j}), hsum8(V);
+//     D == 32: one 16-byte step with the tree written out in exact_b4;
+//     D <= 16: a sequential loop;
+//     ip = fma(sum, sigma, (scale * gamma) * dot) * |x|.
+//   byte codes: D >= 8: 8 running sums, coordinate i into sum i mod 8 as
+//     fma(c[u >> 1], q[i], sum); ip = hsum8 * sigma, dot = hsum8;
+//     D < 8: a sequential loop of (sigma * q[i]) * c[u >> 1];
+//     ip = fma(gamma * scale, dot, ip) * |x|.
+//   both: d = max(0, fma(-ip, 2|q|, fma(|x|, |x|, |q|^2))),
+//   hsum8(v) = ((v0 + v4) + (v2 + v6)) + ((v1 + v5) + (v3 + v7)).
+//
+// Every operation below is one IEEE FP32 rounding (explicit _rn intrinsics:
+// nvcc would otherwise contract a multiply and an add into an FMA).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+
+#include "tq_exact.h"
+#include "tq_mton.h"
+
+namespace tq {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kNoIdx = INT_MAX;
+
+// Relative error bound of the split-BF16 tensor pass (and of the reference's
+// own FP32 sums) against the terms' absolute sum; derivation in
+// rescore_kernel.
+constexpr float kKappa = 2.5e-4f;
+constexpr float kKappaEpi = 1e-6f;
+constexpr float kDegenerateG = 1e-20f;
+
+__device__ __forceinline__ float sgn_s(float s, unsigned bit) { return bit ? s : -s; }
+
+__device__ __forceinline__ uint32_t ld_u32(const uint8_t *p, bool al4) {
+    if (al4) return __ldg(reinterpret_cast<const unsigned int *>(p));
+    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+
+__device__ __forceinline__ float ld_f32(const uint8_t *p, bool al4) { return __uint_as_float(ld_u32(p, al4)); }
+
+__device__ __forceinline__ float hsum8(const float (&v)[8]) {
+    const float w0 = __fadd_rn(v[0], v[4]), w1 = __fadd_rn(v[1], v[5]);
+    const float w2 = __fadd_rn(v[2], v[6]), w3 = __fadd_rn(v[3], v[7]);
+    return __fadd_rn(__fadd_rn(w0, w2), __fadd_rn(w1, w3));
+}
+
+__device__ __forceinline__ float hsum4(const float (&u)[4]) {
+    return __fadd_rn(__fadd_rn(u[0], u[2]), __fadd_rn(u[1], u[3]));
+}
+
+__device__ __forceinline__ float finish_dist(float t, float xn, float qn2, float qn) {
+    const float d = __fmaf_rn(-t, __fadd_rn(qn, qn), __fmaf_rn(xn, xn, qn2));
+    return 0.0f < d ? d : 0.0f;
+}
+
+// distSearchScalarB4 in the reference build's order (nibble codes, pb = D/2).
+__device__ float exact_b4(const float *__restrict__ c, const float *__restrict__ q,
+                          const float *__restrict__ s, float qn2, float qn, float scale, int D,
+                          int nb, const uint8_t *__restrict__ code, bool al4) {
+    float ip = 0.0f, dot = 0.0f;
+    int b = 0;
+    if (D >= 63) {
+        float A[32], S[32];
+#pragma unroll
+        for (int t = 0; t < 32; ++t) A[t] = S[t] = 0.0f;
+        const int nb32 = nb & ~31;
+#pragma unroll 1
+        for (; b < nb32; b += 32) {
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                const uint32_t x = ld_u32(code + b + 4 * w, al4);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int t = 4 * w + e, k = b + t;
+                    const unsigned lo = (x >> (8 * e)) & 15u, hi = (x >> (8 * e + 4)) & 15u;
+                    const float2 qq = __ldg(reinterpret_cast<const float2 *>(q) + k);
+                    const float2 ss = __ldg(reinterpret_cast<const float2 *>(s) + k);
+                    const float ph = __fmul_rn(qq.y, c[hi >> 1]);
+                    A[t] = __fadd_rn(A[t], __fmaf_rn(qq.x, c[lo >> 1], ph));
+                    S[t] = __fadd_rn(S[t], __fadd_rn(sgn_s(ss.x, lo & 1u), sgn_s(ss.y, hi & 1u)));
+                }
+            }
+        }
+        float V[8], W[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            V[j] = __fadd_rn(__fadd_rn(A[16 + j], A[24 + j]), __fadd_rn(A[j], A[8 + j]));
+            W[j] = __fadd_rn(__fadd_rn(S[16 + j], S[24 + j]), __fadd_rn(S[j], S[8 + j]));
+        }
+        ip = hsum8(V);
+        dot = hsum8(W);
+    }
+    if (nb - b >= 16) {
+        // bytes b .. b+15 as four groups g of four lanes j: byte b + 4g + j
+        float L[16], H[16], El[16], Eh[16], Qe[16], Qo[16];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const uint32_t x = ld_u32(code + b + 4 * w, al4);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int t = 4 * w + e, k = b + t;
+                const unsigned lo = (x >> (8 * e)) & 15u, hi = (x >> (8 * e + 4)) & 15u;
+                const float2 qq = __ldg(reinterpret_cast<const float2 *>(q) + k);
+                const float2 ss = __ldg(reinterpret_cast<const float2 *>(s) + k);
+                L[t] = c[lo >> 1];
+                H[t] = c[hi >> 1];
+                El[t] = sgn_s(ss.x, lo & 1u);
+                Eh[t] = sgn_s(ss.y, hi & 1u);
+                Qe[t] = qq.x;
+                Qo[t] = qq.y;
+            }
+        }
+        float U[4], Q4[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k0 = j, k1 = 4 + j, k2 = 8 + j, k3 = 12 + j;
+            const float t1 = __fmaf_rn(L[k2], Qe[k2], __fmul_rn(Qe[k3], L[k3]));
+            const float t2 = __fmaf_rn(Qe[k0], L[k0], __fmul_rn(L[k1], Qe[k1]));
+            const float t3 = __fmaf_rn(Qo[k2], H[k2], __fmul_rn(Qo[k3], H[k3]));
+            const float t4 = __fmaf_rn(Qo[k0], H[k0], __fmul_rn(H[k1], Qo[k1]));
+            U[j] = __fadd_rn(__fadd_rn(__fadd_rn(t4, t3), t2), t1);
+            const float p1 = __fadd_rn(El[k0], El[k1]), p2 = __fadd_rn(El[k2], El[k3]);
+            const float q1 = __fadd_rn(Eh[k0], Eh[k1]), q3 = __fadd_rn(Eh[k2], Eh[k3]);
+            Q4[j] = __fadd_rn(q3, __fadd_rn(q1, __fadd_rn(p2, p1)));
+        }
+        ip = __fadd_rn(ip, hsum4(U));
+        dot = __fadd_rn(dot, hsum4(Q4));
+        b += 16;
+    }
+#pragma unroll 1
+    for (; b < nb; ++b) {
+        const unsigned byte = code[b], lo = byte & 15u, hi = byte >> 4;
+        const float ph = __fmul_rn(c[hi >> 1], q[2 * b + 1]);
+        ip = __fadd_rn(ip, __fmaf_rn(q[2 * b], c[lo >> 1], ph));
+        dot = __fadd_rn(dot, __fadd_rn(sgn_s(s[2 * b + 1], hi & 1u), sgn_s(s[2 * b], lo & 1u)));
+    }
+    const float xn = ld_f32(code + nb, al4), g = ld_f32(code + nb + 4, al4);
+    const float sig = ld_f32(code + nb + 8, al4);
+    float t = __fmul_rn(__fmul_rn(scale, g), dot);
+    t = __fmul_rn(__fmaf_rn(ip, sig, t), xn);
+    return finish_dist(t, xn, qn2, qn);
+}
+
+// distSearchAVX in the reference build's order (byte codes, pb = D).
+__device__ float exact_b8(const float *__restrict__ c, const float *__restrict__ q,
+                          const float *__restrict__ s, float qn2, float qn, float scale, int D,
+                          const uint8_t *__restrict__ code, bool al4) {
+    const float xn = ld_f32(code + D, al4), g = ld_f32(code + D + 4, al4);
+    const float sig = ld_f32(code + D + 8, al4);
+    float ip = 0.0f, dot = 0.0f;
+    int i = 0;
+    if (D >= 8) {
+        float A[8], S[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) A[j] = S[j] = 0.0f;
+#pragma unroll 1
+        for (; i + 8 <= D; i += 8) {
+            const uint32_t x0 = ld_u32(code + i, al4), x1 = ld_u32(code + i + 4, al4);
+            const float4 q0 = __ldg(reinterpret_cast<const float4 *>(q + i));
+            const float4 q1 = __ldg(reinterpret_cast<const float4 *>(q + i) + 1);
+            const float4 s0 = __ldg(reinterpret_cast<const float4 *>(s + i));
+            const float4 s1 = __ldg(reinterpret_cast<const float4 *>(s + i) + 1);
+            const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            const float sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const unsigned u = ((j < 4 ? x0 : x1) >> (8 * (j & 3))) & 255u;
+                A[j] = __fmaf_rn(c[u >> 1], qv[j], A[j]);
+                S[j] = __fadd_rn(S[j], sgn_s(sv[j], u & 1u));
+            }
+        }
+        ip = __fmul_rn(hsum8(A), sig);
+        dot = hsum8(S);
+    }
+#pragma unroll 1
+    for (; i < D; ++i) {
+        const unsigned u = code[i];
+        ip = __fadd_rn(ip, __fmul_rn(__fmul_rn(sig, q[i]), c[u >> 1]));
+        dot = __fadd_rn(dot, sgn_s(s[i], u & 1u));
+    }
+    const float t = __fmul_rn(__fmaf_rn(__fmul_rn(g, scale), dot, ip), xn);
+    return finish_dist(t, xn, qn2, qn);
+}
+
+template <bool NIBBLE>
+__device__ __forceinline__ float exact_dist(const Params &P, const float *c, const float *q,
+                                            const float *s, float qn2, float qn, const uint8_t *code,
+                                            bool al4) {
+    if (NIBBLE) return exact_b4(c, q, s, qn2, qn, P.scale, P.D, P.pb, code, al4);
+    return exact_b8(c, q, s, qn2, qn, P.scale, P.D, code, al4);
+}
+
+__device__ __forceinline__ bool better(float d, int i, float bd, int bi) {
+    return d < bd || (d == bd && i < bi);
+}
+
+// Sorted insert of (d, i) into the ascending list of k entries; returns the
+// new k-th entry through kd / ki.  Out of line: few candidates pass a
+// thread's threshold.
+__device__ __noinline__ void list_insert(float *bd, int *bi, int k, float d, int i, float *kd,
+                                         int *ki) {
+    float cd = d;
+    int cx = i;
+#pragma unroll 1
+    for (int u = 0; u < k; ++u) {
+        if (better(cd, cx, bd[u], bi[u])) {
+            const float od = bd[u];
+            const int ox = bi[u];
+            bd[u] = cd;
+            bi[u] = cx;
+            cd = od;
+            cx = ox;
+        }
+    }
+    *kd = bd[k - 1];
+    *ki = bi[k - 1];
+}
+
+// k rounds of a warp arg-min over the lanes' ascending lists (each of k
+// entries): lane u receives the u-th smallest (distance, index) of the warp;
+// lanes u >= k receive (+inf, no index).
+__device__ void warp_merge(const float *bd, const int *bi, int k, int lane, float &my_d, int &my_i) {
+    int head = 0;
+    my_d = INFINITY;
+    my_i = kNoIdx;
+#pragma unroll 1
+    for (int u = 0; u < k; ++u) {
+        const float hd = head < k ? bd[head] : INFINITY;
+        const int hx = head < k ? bi[head] : kNoIdx;
+        float wd = hd;
+        int wx = hx;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float od = __shfl_xor_sync(kFull, wd, off);
+            const int ox = __shfl_xor_sync(kFull, wx, off);
+            if (better(od, ox, wd, wx)) {
+                wd = od;
+                wx = ox;
+            }
+        }
+        if (hx == wx && hd == wd && wx != kNoIdx) ++head;  // the winning lane pops its head
+        if (lane == u) {
+            my_d = wd;
+            my_i = wx;
+        }
+    }
+}
+
+__device__ __forceinline__ void load_centroids(float *sc, const float *centroids, int levels) {
+    for (int i = threadIdx.x; i < levels; i += blockDim.x) sc[i] = centroids[i];
+    __syncthreads();
+}
+
+struct RescoreArgs {
+    Params P;
+    const float *centroids;
+    float cmax;
+    const int *m_dev;
+    int kc, k;
+    const float *cand_d;
+    const long long *cand_i;
+    const float *q_rot, *s_q, *norms;
+    const uint8_t *codes;
+    size_t n;
+    bool al4;
+    const float *bound;
+    float bound_scale;
+    float *out_d;
+    long long *out_i;
+    int *fail_rows, *counters;
+};
+
+// One warp per query row, lane l on candidate l.
+//
+// The certificate.  Let d'_j be the tensor pass's distance of code j and d_j
+// the reference's.  If |d'_j - d_j| <= eps for every j, a code outside the kc
+// candidates has d_j >= d'_j - eps >= d'_(kc) - eps (the candidates are the kc
+// smallest d'), so when the k-th exact distance among the candidates is below
+// d'_(kc) - eps no excluded code can enter the top-k, ties included.
+//
+// eps.  The tensor pass forms ip = sum_i a_i b_i from hi + lo BF16 pairs:
+// a_i = q_rot_i, b_i = sigma c_i / g (the centroid half; g = scale gamma) and
+// a_i = s_q_i, b_i = +-1 (the sign half), scaled by g |x| |q|.  Per term, the
+// dropped lo*lo product and the pairs' residuals are below 3 * 2^-16 |a_i b_i|;
+// each 16-deep MMA step is assumed to add at most 2^-20 (|acc| + sum |p|), and
+// a chunk of at most 8 K blocks issues at most 96 MMAs into one accumulator
+// from zero (96 * 2^-20 of the chunk's |terms|); promotions, the planes' FP32
+// roundings and the reference's own FP32 sums (chains of at most D/64 + 8
+// adds) add a few 1e-7.  Their sum, 1.4e-4, is taken as kKappa = 2.5e-4 of
+// sum_i |terms|, and
+//   sum_i |terms| <= |q| (cmax sigma_j |x_j| sum|q_rot| + scale gamma_j |x_j| sum|s_q|),
+// bounded with the index-wide maxima of sigma |x| and scale gamma |x|.  The
+// distance epilogues of both sides add kKappaEpi (|q|^2 + max |x|^2), and a
+// code with g < 1e-20 (whose sign half the tensor pass drops) at most
+// 2 |q| sum|s_q| 1e-20 max|x|.  Each candidate is checked against the same
+// eps; a candidate outside it is counted and fails its row.
+template <bool NIBBLE>
+__global__ void __launch_bounds__(256) rescore_kernel(RescoreArgs a) {
+    __shared__ float sc[kMaxLevels];
+    load_centroids(sc, a.centroids, a.P.levels);
+    const int m = *a.m_dev;
+    const int D = a.P.D, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < m; row += gridDim.x * wpb) {
+        const float *q = a.q_rot + (size_t)row * D, *s = a.s_q + (size_t)row * D;
+        const float qn2 = a.norms[2 * row], qn = a.norms[2 * row + 1];
+        float ad = INFINITY, ed = INFINITY;
+        int ci = kNoIdx;
+        if (lane < a.kc) {
+            const long long id = a.cand_i[(size_t)row * a.kc + lane];
+            if (id >= 0 && (size_t)id < a.n) {
+                ci = (int)id;
+                ad = a.cand_d[(size_t)row * a.kc + lane];
+                ed = exact_dist<NIBBLE>(a.P, sc, q, s, qn2, qn, a.codes + (size_t)ci * a.P.cs, a.al4);
+            }
+        }
+        float sq = 0.0f, ss = 0.0f;
+        for (int i = lane; i < D; i += 32) {
+            sq += fabsf(q[i]);
+            ss += fabsf(s[i]);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            sq += __shfl_xor_sync(kFull, sq, off);
+            ss += __shfl_xor_sync(kFull, ss, off);
+        }
+        const float eps =
+            a.bound_scale * (2.0f * qn * (kKappa * (a.cmax * a.bound[0] * sq + a.bound[1] * ss) +
+                                          kDegenerateG * ss * a.bound[3]) +
+                             kKappaEpi * (qn2 + a.bound[2]));
+        const bool viol = ci != kNoIdx && !(fabsf(ad - ed) <= eps);
+        const unsigned viol_mask = __ballot_sync(kFull, viol);
+        const float ad_last = __shfl_sync(kFull, ad, a.kc - 1);
+        const int ci_last = __shfl_sync(kFull, ci, a.kc - 1);
+        // ascending bitonic sort of the 32 (exact distance, index) pairs
+        float d = ed;
+        int ix = ci;
+#pragma unroll
+        for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                const float od = __shfl_xor_sync(kFull, d, stride);
+                const int ox = __shfl_xor_sync(kFull, ix, stride);
+                const bool keep_min = (((lane & size) == 0) == ((lane & stride) == 0));
+                const bool take = keep_min ? better(od, ox, d, ix) : better(d, ix, od, ox);
+                if (take) {
+                    d = od;
+                    ix = ox;
+                }
+            }
+        }
+        const float ek = __shfl_sync(kFull, d, a.k - 1);
+        // fewer than kc codes in the corpus: every code is a candidate
+        const bool all_in = ci_last == kNoIdx;
+        const bool certified = viol_mask == 0u && (all_in || ek < ad_last - eps);
+        if (certified) {
+            if (lane < a.k) {
+                a.out_d[(size_t)row * a.k + lane] = d;
+                a.out_i[(size_t)row * a.k + lane] = ix == kNoIdx ? -1 : (long long)ix;
+            }
+        } else if (lane == 0) {
+            const int pos = atomicAdd(&a.counters[kCntFallbackRows], 1);
+            a.fail_rows[pos] = row;
+            if (viol_mask) atomicAdd(&a.counters[kCntBoundViolations], __popc(viol_mask));
+        }
+    }
+}
+
+struct FallbackArgs {
+    Params P;
+    const float *centroids;
+    int k;
+    const float *q_rot, *s_q, *norms;
+    const uint8_t *codes;
+    size_t n;
+    bool al4;
+    const int *fail_rows, *counters;
+    float *part_d;
+    int *part_i;
+    float *out_d;
+    long long *out_i;
+};
+
+// Exact top-k by a full pass over the codes for each row the certificate did
+// not settle: each thread keeps a sorted list of its codes, the warps merge
+// their lanes' lists and warp 0 merges the block's into part[row][cta].
+template <bool NIBBLE>
+__global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a) {
+    const int nf = a.counters[kCntFallbackRows];
+    if (nf == 0) return;
+    __shared__ float sc[kMaxLevels];
+    __shared__ float wd[8][kTopKMax];
+    __shared__ int wi[8][kTopKMax];
+    load_centroids(sc, a.centroids, a.P.levels);
+    const int D = a.P.D, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int k = a.k;
+    for (int f = 0; f < nf; ++f) {
+        const int row = a.fail_rows[f];
+        const float *q = a.q_rot + (size_t)row * D, *s = a.s_q + (size_t)row * D;
+        const float qn2 = a.norms[2 * row], qn = a.norms[2 * row + 1];
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+#pragma unroll
+        for (int u = 0; u < kTopKMax; ++u) {
+            bd[u] = INFINITY;
+            bi[u] = kNoIdx;
+        }
+        float td = INFINITY;
+        int ti = kNoIdx;
+        for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.n;
+             j += (size_t)gridDim.x * blockDim.x) {
+            const float d = exact_dist<NIBBLE>(a.P, sc, q, s, qn2, qn, a.codes + j * a.P.cs, a.al4);
+            if (better(d, (int)j, td, ti)) list_insert(bd, bi, k, d, (int)j, &td, &ti);
+        }
+        float md;
+        int mi;
+        warp_merge(bd, bi, k, lane, md, mi);
+        if (lane < k) {
+            wd[warp][lane] = md;
+            wi[warp][lane] = mi;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            float ld[kTopKMax];
+            int li[kTopKMax];
+#pragma unroll
+            for (int u = 0; u < kTopKMax; ++u) {
+                ld[u] = (lane < nw && u < k) ? wd[lane][u] : INFINITY;
+                li[u] = (lane < nw && u < k) ? wi[lane][u] : kNoIdx;
+            }
+            warp_merge(ld, li, k, lane, md, mi);
+            if (lane < k) {
+                const size_t o = ((size_t)f * gridDim.x + blockIdx.x) * k + lane;
+                a.part_d[o] = md;
+                a.part_i[o] = mi;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One warp per fallback row: merge the CTAs' lists into the row's output.
+__global__ void __launch_bounds__(256) fallback_merge_kernel(const int *__restrict__ counters,
+                                                             const int *__restrict__ fail_rows,
+                                                             int ctas, int k,
+                                                             const float *__restrict__ part_d,
+                                                             const int *__restrict__ part_i,
+                                                             float *__restrict__ out_d,
+                                                             long long *__restrict__ out_i) {
+    const int nf = counters[kCntFallbackRows];
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < nf; f += gridDim.x * wpb) {
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+#pragma unroll
+        for (int u = 0; u < kTopKMax; ++u) {
+            bd[u] = INFINITY;
+            bi[u] = kNoIdx;
+        }
+        float td = INFINITY;
+        int ti = kNoIdx;
+        for (int c = lane; c < ctas; c += 32)
+            for (int u = 0; u < k; ++u) {
+                const size_t o = ((size_t)f * ctas + c) * k + u;
+                const float d = part_d[o];
+                const int i = part_i[o];
+                if (i != kNoIdx && better(d, i, td, ti)) list_insert(bd, bi, k, d, i, &td, &ti);
+            }
+        float md;
+        int mi;
+        warp_merge(bd, bi, k, lane, md, mi);
+        const int row = fail_rows[f];
+        if (lane < k) {
+            out_d[(size_t)row * k + lane] = md;
+            out_i[(size_t)row * k + lane] = mi == kNoIdx ? -1 : (long long)mi;
+        }
+    }
+}
+
+template <bool NIBBLE>
+__global__ void __launch_bounds__(256) exact_mton_kernel(Params P, const float *centroids,
+                                                         const float *q_rot, const float *s_q,
+                                                         const float *norms, size_t m,
+                                                         const uint8_t *codes, size_t n, bool al4,
+                                                         float *out, size_t ldo) {
+    __shared__ float sc[kMaxLevels];
+    load_centroids(sc, centroids, P.levels);
+    const size_t total = m * n;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = t / n, j = t % n;
+        out[r * ldo + j] = exact_dist<NIBBLE>(P, sc, q_rot + r * P.D, s_q + r * P.D, norms[2 * r],
+                                    norms[2 * r + 1], codes + j * P.cs, al4);
+    }
+}
+
+// Index-wide maxima of sigma |x|, scale gamma |x|, |x|^2 and |x| (bound must
+// be zeroed; non-negative floats order like their bit patterns, NaN counts as
+// +inf).
+__global__ void __launch_bounds__(256) index_bound_kernel(Params P, const uint8_t *codes, size_t n,
+                                                          float *bound) {
+    float v[kBoundFloats] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (size_t)gridDim.x * blockDim.x) {
+        const uint8_t *t = codes + j * P.cs + P.pb;
+        const bool al4 = ((reinterpret_cast<uintptr_t>(t) & 3) == 0);
+        const float xn = fabsf(ld_f32(t, al4)), g = fabsf(ld_f32(t + 4, al4));
+        const float sig = fabsf(ld_f32(t + 8, al4));
+        const float w[kBoundFloats] = {sig * xn, P.scale * g * xn, xn * xn, xn};
+#pragma unroll
+        for (int i = 0; i < kBoundFloats; ++i) v[i] = (w[i] != w[i]) ? INFINITY : fmaxf(v[i], w[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < kBoundFloats; ++i) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[i] = fmaxf(v[i], __shfl_xor_sync(kFull, v[i], off));
+        if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(bound) + i, __float_as_int(v[i]));
+    }
+}
+
+bool codes_al4(const Params &P, const uint8_t *codes) {
+    return (P.cs % 4 == 0) && ((reinterpret_cast<uintptr_t>(codes) & 3) == 0);
+}
+
+}  // namespace
+
+cudaError_t launch_index_bound(const Params &P, const uint8_t *codes, size_t n, float *bound,
+                               cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(bound, 0, kBoundFloats * sizeof(float), st);
+    if (e != cudaSuccess || n == 0) return e;
+    const size_t blocks = std::min<size_t>((n + 255) / 256, 4096);
+    index_bound_kernel<<<(unsigned)blocks, 256, 0, st>>>(P, codes, n, bound);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, const int *m_dev,
+                           int kc, int k, const float *cand_d, const long long *cand_i,
+                           const float *q_rot, const float *s_q, const float *norms,
+                           const uint8_t *codes, size_t n, const float *bound, float bound_scale,
+                           float *out_d, long long *out_i, int *fail_rows, int *counters,
+                           int max_rows, cudaStream_t st) {
+    if (kc < 1 || kc > 32 || k < 1 || k > kc || k > kTopKMax || max_rows < 1)
+        return cudaErrorInvalidValue;
+    const RescoreArgs a{P,     centroids, cmax,  m_dev,     kc,          k,     cand_d,
+                        cand_i, q_rot,    s_q,   norms,     codes,       n,     codes_al4(P, codes),
+                        bound, bound_scale, out_d, out_i, fail_rows, counters};
+    const unsigned blocks = (unsigned)((max_rows + 7) / 8);
+    if (P.nibble)
+        rescore_kernel<true><<<blocks, 256, 0, st>>>(a);
+    else
+        rescore_kernel<false><<<blocks, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+int fallback_ctas(int sms) { return 2 * (sms > 0 ? sms : 148); }
+
+cudaError_t launch_fallback(const Params &P, const float *centroids, int k, const float *q_rot,
+                            const float *s_q, const float *norms, const uint8_t *codes, size_t n,
+                            const int *fail_rows, const int *counters, int fb_ctas, float *part_d,
+                            int *part_i, float *out_d, long long *out_i, int max_rows,
+                            cudaStream_t st) {
+    if (k < 1 || k > kTopKMax || fb_ctas < 1 || max_rows < 1) return cudaErrorInvalidValue;
+    const FallbackArgs a{P,     centroids, k,         q_rot,    s_q,    norms,  codes, n,
+                         codes_al4(P, codes), fail_rows, counters, part_d, part_i, out_d, out_i};
+    if (P.nibble)
+        fallback_scan_kernel<true><<<fb_ctas, 256, 0, st>>>(a);
+    else
+        fallback_scan_kernel<false><<<fb_ctas, 256, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    fallback_merge_kernel<<<(unsigned)((max_rows + 7) / 8), 256, 0, st>>>(
+        counters, fail_rows, fb_ctas, k, part_d, part_i, out_d, out_i);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact_mton(const Params &P, const float *centroids, const float *q_rot,
+                              const float *s_q, const float *norms, size_t m, const uint8_t *codes,
+                              size_t n, float *out, size_t ldo, cudaStream_t st) {
+    if (m == 0 || n == 0) return cudaSuccess;
+    const size_t total = m * n;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+    if (P.nibble)
+        exact_mton_kernel<true><<<blocks, 256, 0, st>>>(P, centroids, q_rot, s_q, norms, m, codes, n,
+                                                        codes_al4(P, codes), out, ldo);
+    else
+        exact_mton_kernel<false><<<blocks, 256, 0, st>>>(P, centroids, q_rot, s_q, norms, m, codes, n,
+                                                         codes_al4(P, codes), out, ldo);
+    return cudaGetLastError();
+}
+
+}  // namespace tq

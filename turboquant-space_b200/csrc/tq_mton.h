@@ -44,14 +44,15 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
                            size_t ldo, int *err, cudaStream_t st);
 
 // Top-k over a device-resident index: C = A B^T as above, reduced per row to the
-// k (<= 16) smallest (distance, index) pairs, ties to the smaller index.
+// k (<= kCandMax) smallest (distance, index) pairs, ties to the smaller index.
 // The row count is read from m_dev; `grid` CTAs split the rows into 128-row
-// blocks and the columns into slices; partials hold grid * 128 * 16 entries.
+// blocks and the columns into slices.
 // Variant 0: 128 x 256 tiles (n_pad % 256 == 0), two partial lists per (row,
 // slice); variant 1: 128 x 128 tiles, 3 stages, 8-block promoted chunks;
 // variant 2: 128 x 128 tiles, 2 stages, 4-block chunks.  The partial buffers
-// hold grid * 128 * tc_topk_lists(variant) * kTopKMax entries.
-constexpr int kTopKMax = 16;
+// hold grid * 128 * tc_topk_lists(variant) * kCandMax entries.
+constexpr int kTopKMax = 16;   // results per row (k) of the serving path
+constexpr int kCandMax = 32;   // list length of the tensor-core top-k (candidates per row)
 constexpr int kTopKListsMax = 2;
 int tc_topk_variants();
 int tc_topk_lists(int variant);

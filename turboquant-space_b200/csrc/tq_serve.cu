@@ -23,10 +23,18 @@
 //              queue capacity.
 //   autotune   per bucket, each kernel variant (tile shape x stage depth) is
 //              timed on the index and the fastest is captured into the graph.
+//   exact      the tensor-core pass keeps `kc` candidates per row; the
+//              rescoring kernel recomputes them with the reference's own
+//              arithmetic (tq_exact.cu) and certifies the row's top-k with the
+//              pass's error bound; rows it cannot certify are answered by an
+//              exact full pass over the codes.  Results are therefore the
+//              stable argsort of the reference's distances, whatever the
+//              batch they ran in.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -35,6 +43,7 @@
 #include <thread>
 #include <vector>
 
+#include "tq_exact.h"
 #include "tq_host.h"
 #include "tq_mton.h"
 
@@ -45,6 +54,9 @@ struct tq_index {
     int K_lo = 0;            // columns of the lo plane (tq::asym_lo_width)
     void *planes = nullptr;  // hi plane n_pad x K, then lo plane n_pad x K_lo, BF16
     float *c1 = nullptr, *c2 = nullptr;
+    uint8_t *codes = nullptr;  // the corpus itself (n x code_size), for the exact stages
+    float *bound = nullptr;    // kBoundFloats index-wide maxima of the error bound
+    float cmax = 0.0f;         // max |centroid|
     int device = -1;
 };
 
@@ -90,8 +102,11 @@ struct Slot {
     long long *h_i = nullptr;
     void *d_block = nullptr;  // one device allocation for all buffers below
     float *d_q = nullptr, *d_prep = nullptr, *d_r1 = nullptr, *d_r2 = nullptr, *d_pd = nullptr,
-          *d_od = nullptr;
-    int *d_m = nullptr, *d_pi = nullptr, *d_err = nullptr;
+          *d_od = nullptr, *d_cd = nullptr, *d_fpd = nullptr;
+    int *d_m = nullptr, *d_pi = nullptr, *d_err = nullptr, *d_fail = nullptr, *d_cnt = nullptr,
+        *d_fpi = nullptr;
+    long long *d_ci = nullptr;
+    int *h_cnt = nullptr;  // pinned copy of d_cnt after each batch
     void *d_ap = nullptr;  // query planes: max_rows x K x 2 BF16 planes
     long long *d_oi = nullptr;
     std::vector<int> bucket_rows;
@@ -106,6 +121,9 @@ struct Slot {
 struct tq_server {
     tq_index *index = nullptr;
     int k = 10;
+    int kc = 26;              // tensor-pass candidates per row
+    float bound_scale = 1.0f; // multiplier on the certificate's error bound
+    int fb_ctas = 296;        // CTAs of the exact fallback pass
     int grid = 148;
     int max_rows = 1024;
     size_t queue_rows_cap = 0;
@@ -120,6 +138,7 @@ struct tq_server {
     bool stop = false;
     // stats
     uint64_t submitted = 0, rejected = 0, completed = 0, batches = 0, rows_done = 0;
+    uint64_t fallback_rows = 0, bound_violations = 0;
     std::vector<float> latencies_ms;  // ring of the most recent completions
     size_t lat_pos = 0;
     double busy_ms = 0;
@@ -158,18 +177,33 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     if (e != cudaSuccess) return e;
     unsigned char *bh = static_cast<unsigned char *>(ix->planes);
     unsigned char *bl = bh + ix->n_pad * K * 2;
+    // tensor-core pass: each row's kc best candidates by approximate distance
     e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
-                           sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->k, sl.d_pd, sl.d_pi, sl.d_err,
+                           sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
                            sv->grid, st);
     if (e != cudaSuccess) return e;
-    e = tq::launch_topk_merge(sl.d_m, sv->grid, tq::tc_topk_lists(var), sl.d_pd, sl.d_pi, sv->k,
-                              rows_cap, sl.d_od, sl.d_oi, st);
+    e = tq::launch_topk_merge(sl.d_m, sv->grid, tq::tc_topk_lists(var), sl.d_pd, sl.d_pi, sv->kc,
+                              rows_cap, sl.d_cd, sl.d_ci, st);
+    if (e != cudaSuccess) return e;
+    // exact stages: rescoring + certificate, then the full pass for the rows
+    // the certificate leaves open
+    e = cudaMemsetAsync(sl.d_cnt, 0, tq::kCntWords * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    e = tq::launch_rescore(sp->P, sp->T.centroids, ix->cmax, sl.d_m, sv->kc, sv->k, sl.d_cd, sl.d_ci,
+                           q_rot, s_q, norms, ix->codes, ix->n, ix->bound, sv->bound_scale, sl.d_od,
+                           sl.d_oi, sl.d_fail, sl.d_cnt, rows_cap, st);
+    if (e != cudaSuccess) return e;
+    e = tq::launch_fallback(sp->P, sp->T.centroids, sv->k, q_rot, s_q, norms, ix->codes, ix->n,
+                            sl.d_fail, sl.d_cnt, sv->fb_ctas, sl.d_fpd, sl.d_fpi, sl.d_od, sl.d_oi,
+                            rows_cap, st);
     if (e != cudaSuccess) return e;
     if (copies) {
         e = cudaMemcpyAsync(sl.h_d, sl.d_od, (size_t)rows_cap * sv->k * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(sl.h_i, sl.d_oi, (size_t)rows_cap * sv->k * 8, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_err, sl.d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(sl.h_cnt, sl.d_cnt, tq::kCntWords * sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     return e;
 }
@@ -187,6 +221,8 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     *sl.h_err = 0;
     TQ_CUDA(cudaMallocHost(&sl.h_d, R * k * 4), "cudaMallocHost(dist)");
     TQ_CUDA(cudaMallocHost(&sl.h_i, R * k * 8), "cudaMallocHost(idx)");
+    TQ_CUDA(cudaMallocHost(&sl.h_cnt, tq::kCntWords * sizeof(int)), "cudaMallocHost(counters)");
+    std::memset(sl.h_cnt, 0, tq::kCntWords * sizeof(int));
     std::memset(sl.h_q, 0, R * sp->dim * 4);
     // device block layout (each part 256-byte aligned)
     size_t off = 0;
@@ -197,9 +233,12 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     };
     const size_t o_q = take(R * sp->dim * 4), o_m = take(16), o_prep = take(R * (2 * D + 2) * 4);
     const size_t o_ap = take(R * K * 4), o_r1 = take(R * 4), o_r2 = take(R * 4);
-    const size_t parts = (size_t)sv->grid * 128 * tq::kTopKListsMax * tq::kTopKMax;
+    const size_t parts = (size_t)sv->grid * 128 * tq::kTopKListsMax * tq::kCandMax;
     const size_t o_pd = take(parts * 4), o_pi = take(parts * 4), o_od = take(R * k * 4);
     const size_t o_oi = take(R * k * 8), o_err = take(16);
+    const size_t kc = (size_t)sv->kc, fparts = R * (size_t)sv->fb_ctas * k;
+    const size_t o_cd = take(R * kc * 4), o_ci = take(R * kc * 8), o_fail = take(R * 4);
+    const size_t o_cnt = take(tq::kCntWords * 4), o_fpd = take(fparts * 4), o_fpi = take(fparts * 4);
     TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
     TQ_CUDA(cudaMemset(sl.d_block, 0, off), "cudaMemset(slot)");
     auto *base = static_cast<unsigned char *>(sl.d_block);
@@ -214,6 +253,12 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     sl.d_od = reinterpret_cast<float *>(base + o_od);
     sl.d_oi = reinterpret_cast<long long *>(base + o_oi);
     sl.d_err = reinterpret_cast<int *>(base + o_err);
+    sl.d_cd = reinterpret_cast<float *>(base + o_cd);
+    sl.d_ci = reinterpret_cast<long long *>(base + o_ci);
+    sl.d_fail = reinterpret_cast<int *>(base + o_fail);
+    sl.d_cnt = reinterpret_cast<int *>(base + o_cnt);
+    sl.d_fpd = reinterpret_cast<float *>(base + o_fpd);
+    sl.d_fpi = reinterpret_cast<int *>(base + o_fpi);
     for (int b = 128; b < sv->max_rows; b *= 2) sl.bucket_rows.push_back(b);
     sl.bucket_rows.push_back(sv->max_rows);
     return TQ_OK;
@@ -230,6 +275,7 @@ void slot_free(Slot &sl) {
     if (sl.h_err) cudaFreeHost(sl.h_err);
     if (sl.h_d) cudaFreeHost(sl.h_d);
     if (sl.h_i) cudaFreeHost(sl.h_i);
+    if (sl.h_cnt) cudaFreeHost(sl.h_cnt);
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.stream) cudaStreamDestroy(sl.stream);
     sl = Slot();
@@ -363,6 +409,10 @@ void worker_loop(tq_server *sv) {
             }
             const double t = now_ms();
             const int herr = (q == cudaSuccess) ? *sl.h_err : 0;
+            if (q == cudaSuccess) {
+                sv->fallback_rows += (uint64_t)sl.h_cnt[tq::kCntFallbackRows];
+                sv->bound_violations += (uint64_t)sl.h_cnt[tq::kCntBoundViolations];
+            }
             size_t row = 0;
             for (tq_request *r : sl.batch) {
                 if (q != cudaSuccess || herr) {
@@ -444,43 +494,36 @@ tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n,
     ix->K = (int)K;
     ix->K_lo = tq::asym_lo_width((int)sp->D);
     ix->device = sp->device;
+    for (float c : sp->centroids) ix->cmax = std::max(ix->cmax, std::fabs(c));
     const size_t plane_hi = ix->n_pad * K * 2, plane_lo = ix->n_pad * (size_t)ix->K_lo * 2;
-    cudaError_t e = cudaMalloc(&ix->planes, plane_hi + plane_lo + 2 * ix->n_pad * 4 + 256);
+    const size_t code_bytes = round_up(n * sp->code_size, 256);
+    cudaError_t e = cudaMalloc(&ix->planes, plane_hi + plane_lo + 2 * ix->n_pad * 4 + code_bytes +
+                                                tq::kBoundFloats * 4 + 256);
     if (e != cudaSuccess) {
         delete ix;
-        return cuda_fail(e, "cudaMalloc(index planes)");
+        return cuda_fail(e, "cudaMalloc(index)");
     }
-    ix->c1 = reinterpret_cast<float *>(static_cast<unsigned char *>(ix->planes) + plane_hi +
-                                       plane_lo);
-    ix->c2 = ix->c1 + ix->n_pad;
     auto *hi = static_cast<unsigned char *>(ix->planes);
     auto *lo = hi + plane_hi;
+    ix->c1 = reinterpret_cast<float *>(lo + plane_lo);
+    ix->c2 = ix->c1 + ix->n_pad;
+    ix->codes = reinterpret_cast<uint8_t *>(ix->c2 + ix->n_pad);
+    ix->bound = reinterpret_cast<float *>(ix->codes + code_bytes);
+    // the corpus itself stays resident (the exact stages read it); the planes
+    // are decoded from that copy
+    e = cudaMemcpy(ix->codes, codes, n * sp->code_size,
+                   codes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
     const size_t chunk = 1 << 20;
-    uint8_t *stage = nullptr;
-    if (!codes_on_device) {
-        e = cudaMalloc(&stage, std::min(chunk, n) * sp->code_size + 16);
-        if (e != cudaSuccess) {
-            cudaFree(ix->planes);
-            delete ix;
-            return cuda_fail(e, "cudaMalloc(index staging)");
-        }
-    }
     for (size_t r0 = 0; r0 < ix->n_pad && e == cudaSuccess; r0 += chunk) {
         const size_t rows_pad = std::min(chunk, ix->n_pad - r0);
         const size_t rows = r0 < n ? std::min(rows_pad, n - r0) : 0;
-        const uint8_t *src = codes + r0 * sp->code_size;
-        if (!codes_on_device && rows) {
-            e = cudaMemcpy(stage, src, rows * sp->code_size, cudaMemcpyHostToDevice);
-            src = stage;
-        }
-        if (e == cudaSuccess)
-            e = tq::launch_planes_from_codes(sp->P, sp->T, rows ? src : stage ? stage : codes, rows,
-                                             rows_pad, false, tq::kPlaneBF16, hi + r0 * K * 2,
-                                             lo + r0 * (size_t)ix->K_lo * 2, ix->c1 + r0,
-                                             ix->c2 + r0, nullptr);
+        e = tq::launch_planes_from_codes(sp->P, sp->T, ix->codes + std::min(r0, n - 1) * sp->code_size,
+                                         rows, rows_pad, false, tq::kPlaneBF16, hi + r0 * K * 2,
+                                         lo + r0 * (size_t)ix->K_lo * 2, ix->c1 + r0, ix->c2 + r0,
+                                         nullptr);
     }
+    if (e == cudaSuccess) e = tq::launch_index_bound(sp->P, ix->codes, n, ix->bound, nullptr);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (stage) cudaFree(stage);
     if (e != cudaSuccess) {
         cudaFree(ix->planes);
         delete ix;
@@ -497,11 +540,16 @@ void tq_index_destroy(tq_index *ix) {
     delete ix;
 }
 
-tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int kernel_variant,
-                           size_t queue_rows, tq_server **out) {
-    if (!out || !ix) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL argument");
+tq_status tq_server_create_ex(tq_index *ix, const tq_server_params *prm, tq_server **out) {
+    if (!out || !ix || !prm) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL argument");
     *out = nullptr;
+    const int k = prm->k, max_rows = prm->max_rows, kernel_variant = prm->kernel_variant;
+    int slots = prm->slots;
     if (k < 1 || k > tq::kTopKMax) return fail(TQ_ERR_INVALID_ARGUMENT, "k must be in 1..%d", tq::kTopKMax);
+    const int kc = prm->candidates ? prm->candidates : std::min(tq::kCandMax, k + 16);
+    if (kc < k || kc > tq::kCandMax)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "candidates must be in k..%d", tq::kCandMax);
+    if (!(prm->bound_scale >= 0.0f)) return fail(TQ_ERR_INVALID_ARGUMENT, "bound_scale must be >= 0");
     if (max_rows < 128 || max_rows % 128) return fail(TQ_ERR_INVALID_ARGUMENT, "max_rows must be a positive multiple of 128");
     if (slots < 1 || slots > 8) return fail(TQ_ERR_INVALID_ARGUMENT, "slots must be in 1..8");
     if (kernel_variant >= tq::tc_topk_variants()) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown kernel variant");
@@ -512,15 +560,20 @@ tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int ker
     auto *sv = new tq_server();
     sv->index = ix;
     sv->k = k;
+    sv->kc = kc;
+    sv->bound_scale = prm->bound_scale > 0.0f ? prm->bound_scale : 1.0f;
     sv->grid = sms;
+    sv->fb_ctas = tq::fallback_ctas(sms);
     sv->max_rows = max_rows;
-    sv->queue_rows_cap = queue_rows ? queue_rows : (size_t)16 * max_rows;
+    sv->queue_rows_cap = prm->queue_rows ? prm->queue_rows : (size_t)16 * max_rows;
     // admission by free device memory: no more slots than fit in half the free memory
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     const size_t D = ix->sp->D, K = (size_t)ix->K, R = (size_t)max_rows;
-    const size_t slot_bytes = R * (ix->sp->dim * 4 + (2 * D + 2) * 4 + K * 4 + 8 + (size_t)k * 12) +
-                              (size_t)sms * 128 * tq::kTopKListsMax * tq::kTopKMax * 8 + 4096;
+    const size_t slot_bytes =
+        R * (ix->sp->dim * 4 + (2 * D + 2) * 4 + K * 4 + 8 + (size_t)k * 12 + (size_t)kc * 12 + 4 +
+             (size_t)sv->fb_ctas * k * 8) +
+        (size_t)sms * 128 * tq::kTopKListsMax * tq::kCandMax * 8 + 8192;
     const size_t fit = std::max<size_t>(1, (free_b / 2) / slot_bytes);
     slots = (int)std::min<size_t>((size_t)slots, fit);
     sv->slots.resize(slots);
@@ -540,6 +593,17 @@ tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int ker
     sv->worker = std::thread(worker_loop, sv);
     *out = sv;
     return TQ_OK;
+}
+
+tq_status tq_server_create(tq_index *ix, int k, int max_rows, int slots, int kernel_variant,
+                           size_t queue_rows, tq_server **out) {
+    tq_server_params p{};
+    p.k = k;
+    p.max_rows = max_rows;
+    p.slots = slots;
+    p.kernel_variant = kernel_variant;
+    p.queue_rows = queue_rows;
+    return tq_server_create_ex(ix, &p, out);
 }
 
 tq_status tq_server_submit(tq_server *sv, const float *queries, size_t m, tq_request **out) {
@@ -614,6 +678,9 @@ tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latenc
     out->queued_rows = sv->pending_rows;
     out->slots = (int)sv->slots.size();
     out->max_rows = sv->max_rows;
+    out->candidates = sv->kc;
+    out->fallback_rows = sv->fallback_rows;
+    out->bound_violations = sv->bound_violations;
     size_t nl = std::min(cap, sv->latencies_ms.size());
     if (latencies && nl) std::memcpy(latencies, sv->latencies_ms.data(), nl * sizeof(float));
     if (n_lat) *n_lat = latencies ? nl : sv->latencies_ms.size();
@@ -624,6 +691,7 @@ tq_status tq_server_reset_stats(tq_server *sv) {
     if (!sv) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL server");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->submitted = sv->rejected = sv->completed = sv->batches = sv->rows_done = 0;
+    sv->fallback_rows = sv->bound_violations = 0;
     sv->latencies_ms.clear();
     sv->lat_pos = 0;
     return TQ_OK;

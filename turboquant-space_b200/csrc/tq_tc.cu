@@ -724,7 +724,7 @@ __device__ __noinline__ TopkEntry topk_insert(float *bd, int *bi, int k, float d
 // contiguous slice c % S of the column tiles, S = grid / row blocks; each
 // epilogue thread keeps its row's best k (distance, index) pairs, ties broken
 // by the smaller index, and writes them to the partial buffers
-// part_d / part_i [(block * S + slice) * 128 + row][kTopKMax].
+// part_d / part_i [(block * S + slice) * 128 + row][kCandMax].
 struct TopkEpi {
     struct Params {
         const int *m_dev;
@@ -762,8 +762,8 @@ struct TopkEpi {
         int rit, m;
         bool valid;
         float rr1 = 0.0f, rr2 = 0.0f;
-        float bd[kTopKMax];
-        int bi[kTopKMax];
+        float bd[kCandMax];
+        int bi[kCandMax];
         float thr_d = INFINITY;
         int thr_i = 0x7fffffff;
         __device__ State(const Params &p, int row_in_tile) : rit(row_in_tile) {
@@ -777,7 +777,7 @@ struct TopkEpi {
                 rr2 = __ldg(p.r2 + row);
             }
 #pragma unroll
-            for (int t = 0; t < kTopKMax; ++t) {
+            for (int t = 0; t < kCandMax; ++t) {
                 bd[t] = INFINITY;
                 bi[t] = 0x7fffffff;
             }
@@ -817,9 +817,9 @@ struct TopkEpi {
             unsigned nb0, nb1;
             slice(p, mb, nb0, nb1);
             if (mb * TC_BM + rit >= m) return;
-            const size_t o = ((size_t)blockIdx.x * TC_BM + rit) * kTopKMax;
+            const size_t o = ((size_t)blockIdx.x * TC_BM + rit) * kCandMax;
 #pragma unroll
-            for (int u = 0; u < kTopKMax; ++u)
+            for (int u = 0; u < kCandMax; ++u)
                 if (u < p.k) {
                     p.part_d[o + u] = bd[u];
                     p.part_i[o + u] = bi[u];
@@ -874,7 +874,7 @@ struct WDist {
 
 // The top-k over 256-wide column tiles: each thread keeps the best k of its
 // half of the columns, so a (row, slice) has two partial lists, written to
-// part_d / part_i [((cta * 128 + row) * 2 + half)][kTopKMax].  The list lives
+// part_d / part_i [((cta * 128 + row) * 2 + half)][kCandMax].  The list lives
 // in the thread's local frame and is touched only on an insertion; the
 // per-column test reads the k-th entry kept in registers.
 struct WTopk {
@@ -887,8 +887,8 @@ struct WTopk {
         int rit, h, m;
         bool valid;
         float rr1 = 0.0f, rr2 = 0.0f;
-        float bd[kTopKMax];
-        int bi[kTopKMax];
+        float bd[kCandMax];
+        int bi[kCandMax];
         float thr_d = INFINITY;
         int thr_i = 0x7fffffff;
         __device__ State(const Params &p, int row_in_tile, int half) : rit(row_in_tile), h(half) {
@@ -902,7 +902,7 @@ struct WTopk {
                 rr2 = __ldg(p.r2 + row);
             }
 #pragma unroll
-            for (int t = 0; t < kTopKMax; ++t) {
+            for (int t = 0; t < kCandMax; ++t) {
                 bd[t] = INFINITY;
                 bi[t] = 0x7fffffff;
             }
@@ -935,9 +935,9 @@ struct WTopk {
             unsigned nb0, nb1;
             TopkEpi::slice(p, mb, nb0, nb1);
             if (mb * TC_BM + rit >= m) return;
-            const size_t o = (((size_t)blockIdx.x * TC_BM + rit) * 2 + h) * kTopKMax;
+            const size_t o = (((size_t)blockIdx.x * TC_BM + rit) * 2 + h) * kCandMax;
 #pragma unroll
-            for (int u = 0; u < kTopKMax; ++u)
+            for (int u = 0; u < kCandMax; ++u)
                 if (u < p.k) {
                     p.part_d[o + u] = bd[u];
                     p.part_i[o + u] = bi[u];
@@ -1027,21 +1027,21 @@ __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__
     const int wpb = blockDim.x >> 5;
     for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < m; row += gridDim.x * wpb) {
         const int mb = row / TC_BM, rit = row % TC_BM;
-        float bd[kTopKMax];
-        int bi[kTopKMax];
+        float bd[kCandMax];
+        int bi[kCandMax];
 #pragma unroll
-        for (int t = 0; t < kTopKMax; ++t) {
+        for (int t = 0; t < kCandMax; ++t) {
             bd[t] = INFINITY;
             bi[t] = 0x7fffffff;
         }
         for (int sl = lane; sl < S * lists; sl += 32) {
             const size_t cta = (size_t)mb * S + sl / lists;
-            const size_t o = ((cta * TC_BM + rit) * lists + sl % lists) * kTopKMax;
+            const size_t o = ((cta * TC_BM + rit) * lists + sl % lists) * kCandMax;
             for (int u = 0; u < k; ++u) {
                 float cd = part_d[o + u];
                 int cx = part_i[o + u];
 #pragma unroll
-                for (int v = 0; v < kTopKMax; ++v) {
+                for (int v = 0; v < kCandMax; ++v) {
                     if (v < k) {
                         const bool sw = better(cd, cx, bd[v], bi[v]);
                         const float td = bd[v];
@@ -1060,7 +1060,7 @@ __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__
             float hd = INFINITY;
             int hx = 0x7fffffff;
 #pragma unroll
-            for (int v = 0; v < kTopKMax; ++v)
+            for (int v = 0; v < kCandMax; ++v)
                 if (v == head) {
                     hd = bd[v];
                     hx = bi[v];
@@ -1212,7 +1212,7 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
                            const int *m_dev, size_t n, const float *r1, const float *r2,
                            const float *c1, const float *c2, int k, float *part_d, int *part_i,
                            int *err, int grid, cudaStream_t st) {
-    if (k < 1 || k > kTopKMax || grid < 1 || variant < 0 || variant >= tc_topk_variants())
+    if (k < 1 || k > kCandMax || grid < 1 || variant < 0 || variant >= tc_topk_variants())
         return cudaErrorInvalidValue;
     if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || rows_pad % TC_BM || n_pad % TC_BN)
         return cudaErrorInvalidValue;

@@ -21,7 +21,7 @@ TQ_ERR_TIMEOUT = 5
 TQ_ERR_BUSY = 6
 TQ_ERR_NOT_SUPPORTED = 7
 
-PRECISION = {"fp32": 0, "split_bf16": 1, "split_tf32": 2}
+PRECISION = {"fp32": 0, "split_bf16": 1, "split_tf32": 2, "reference": 3}
 
 # Every symbol include/turboquant_b200.h declares.
 EXPORTS = (
@@ -31,7 +31,7 @@ EXPORTS = (
     "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device",
     "tq_distance_1_to_n_device_noalloc", "tq_distance_m_to_n_device",
     "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
-    "tq_server_create", "tq_server_submit", "tq_request_wait", "tq_request_done",
+    "tq_server_create", "tq_server_create_ex", "tq_server_submit", "tq_request_wait", "tq_request_done",
     "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning",
     "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status",
     "tq_rotated_coords_batch", "tq_rotated_coords_batch_device",
@@ -47,7 +47,15 @@ class ServerStats(C.Structure):
     _fields_ = [
         ("submitted", C.c_uint64), ("rejected", C.c_uint64), ("completed", C.c_uint64),
         ("batches", C.c_uint64), ("rows", C.c_uint64), ("queued_rows", C.c_size_t),
-        ("slots", C.c_int), ("max_rows", C.c_int),
+        ("slots", C.c_int), ("max_rows", C.c_int), ("candidates", C.c_int),
+        ("fallback_rows", C.c_uint64), ("bound_violations", C.c_uint64),
+    ]
+
+
+class ServerParams(C.Structure):
+    _fields_ = [
+        ("k", C.c_int), ("max_rows", C.c_int), ("slots", C.c_int), ("kernel_variant", C.c_int),
+        ("queue_rows", C.c_size_t), ("candidates", C.c_int), ("bound_scale", C.c_float),
     ]
 
 
@@ -123,6 +131,8 @@ def lib() -> C.CDLL:
     L.tq_index_create.argtypes = [vp, u8p, sz, C.c_int, C.POINTER(vp)]
     L.tq_index_destroy.restype = None
     L.tq_index_destroy.argtypes = [vp]
+    L.tq_server_create_ex.restype = st
+    L.tq_server_create_ex.argtypes = [vp, C.POINTER(ServerParams), C.POINTER(vp)]
     L.tq_server_create.restype = st
     L.tq_server_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, sz, C.POINTER(vp)]
     L.tq_server_submit.restype = st

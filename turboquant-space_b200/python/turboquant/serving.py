@@ -4,7 +4,8 @@ The reference has no index or serving loop (its README.md:81-83); this wraps
 the C ABI's tq_index_* / tq_server_* entry points:
 
     index = Index(space, codes)              # codes: host uint8 or CUDA uint8
-    D, I = index.search(queries, k=10)       # exact top-k, ascending, ties by index
+    D, I = index.search(queries, k=10)       # exact top-k: the stable argsort of the
+                                             # reference's distances, bit-identical
     with index.serve(k=10) as server:        # continuous batching
         req = server.submit(queries)         # non-blocking; BusyError if refused
         D, I = req.wait()
@@ -69,12 +70,21 @@ class Request:
 
 
 class Server:
-    def __init__(self, index, k=10, max_rows=1024, slots=2, kernel_variant=-1, queue_rows=0):
+    """Continuous-batching exact top-k server over an Index.
+
+    candidates: rows kept by the tensor-core pass for exact rescoring (0: k + 16,
+    at most 32); bound_scale: multiplier on the certificate's error bound (rows
+    it cannot certify are answered by an exact full pass over the codes)."""
+
+    def __init__(self, index, k=10, max_rows=1024, slots=2, kernel_variant=-1, queue_rows=0,
+                 candidates=0, bound_scale=0.0):
         self.index = index
         self.k = int(k)
+        p = _capi.ServerParams(k=self.k, max_rows=int(max_rows), slots=int(slots),
+                               kernel_variant=int(kernel_variant), queue_rows=int(queue_rows),
+                               candidates=int(candidates), bound_scale=float(bound_scale))
         h = C.c_void_p()
-        check(lib().tq_server_create(index._h, self.k, int(max_rows), int(slots), int(kernel_variant),
-                                     int(queue_rows), C.byref(h)))
+        check(lib().tq_server_create_ex(index._h, C.byref(p), C.byref(h)))
         self._h = h
 
     def submit(self, queries):
@@ -130,7 +140,7 @@ class Server:
 
 
 class Index:
-    """A corpus of codes decoded once into HBM-resident tensor-core operands."""
+    """A corpus of codes kept in HBM with its tensor-core operand planes."""
 
     def __init__(self, space, codes):
         self.space = space
@@ -141,8 +151,9 @@ class Index:
         self.n = n
         self._search_server = None
 
-    def serve(self, k=10, max_rows=1024, slots=2, kernel_variant=-1, queue_rows=0):
-        return Server(self, k, max_rows, slots, kernel_variant, queue_rows)
+    def serve(self, k=10, max_rows=1024, slots=2, kernel_variant=-1, queue_rows=0, candidates=0,
+              bound_scale=0.0):
+        return Server(self, k, max_rows, slots, kernel_variant, queue_rows, candidates, bound_scale)
 
     def search(self, queries, k=10):
         """Exact top-k (ascending distance, ties to the smaller index) for each query row."""
