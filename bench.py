@@ -14,7 +14,15 @@ same metric through the public Python API with the corpus, the queries and the
 distances in pinned host memory (copies inside the timed region);
 `roofline` is the scan kernel's achieved HBM bandwidth against the measured
 copy peak; `cpu_baseline` is the reference library (compiled from its own
-sources into oracle/_ref) timed on this host's cores on a bounded sample.
+sources into oracle/_ref, the x86-64-v4 build on an AVX-512 host) timed on
+this host's cores on a bounded sample.
+
+The same line carries the metric's other halves, each measured on its own
+workload after the scan (skip with --no-extras): `cfg1` (100k x 128 4-bit
+encode + distance_1_to_n), `mton` (4096 x 1M 768-d 4-bit, FP32 vs split-BF16),
+`sym` (2048 x 2M 1536-d 4-bit symmetric, FP32 vs split-BF16) and `serve`
+(20M x 384-d 4-bit corpus, exact top-10, p50/p99 and goodput at a few request
+rates), each with its reference CPU slice and the clocks seen.
 
 Under torchrun each rank scans its own 10M-code shard (weak scaling, no data
 exchange); timing is on the device, max over ranks.
@@ -138,33 +146,76 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
+REF_FLAGS = "-O3 -ffast-math -fno-finite-math-only -march={} -fopenmp"
+_REF_MOD = None
+
+
+def host_has_avx512():
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = set()
+            for ln in f:
+                if ln.startswith("flags"):
+                    flags = set(ln.split(":", 1)[1].split())
+                    break
+        return {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags
+    except OSError:
+        return False
+
+
 def reference_module():
-    ref_dir = os.path.join(ROOT, "oracle", "_ref")
-    if ref_dir not in sys.path:
-        sys.path.insert(0, ref_dir)
-    import _turboquant  # the reference's own pybind11 module, built from its sources
-    return _turboquant
+    """The reference's own pybind11 module, built from its sources (oracle/Makefile):
+    the x86-64-v4 build on an AVX-512 host (the fixed stand-in for its default
+    -march=native), else the x86-64-v3 wheel build.  Returns (module, flags)."""
+    global _REF_MOD
+    if _REF_MOD is None:
+        import glob
+        import importlib.util
+        ref_dir = os.path.join(ROOT, "oracle", "_ref")
+        cands = []
+        if host_has_avx512():
+            cands.append((os.path.join(ref_dir, "v4"), "x86-64-v4"))
+        cands.append((ref_dir, "x86-64-v3"))
+        last = None
+        for d, arch in cands:
+            so = sorted(glob.glob(os.path.join(d, "_turboquant*.so")))
+            if not so:
+                continue
+            try:
+                spec = importlib.util.spec_from_file_location("_turboquant", so[0])
+                mod = importlib.util.module_from_spec(spec)
+                spec.loader.exec_module(mod)
+                _REF_MOD = (mod, REF_FLAGS.format(arch))
+                break
+            except Exception as e:  # e.g. an ISA the host lacks
+                last = e
+        if _REF_MOD is None:
+            raise ImportError(f"reference build not found under oracle/_ref ({last})")
+    return _REF_MOD
+
+
+def cpu_space(dim, bits, cores):
+    """(space, kind, build flags): the reference module, or without it the restatement."""
+    try:
+        mod, flags = reference_module()
+        return mod.TurboQuantSpace(dim, bits_per_coord=bits, num_threads=cores), "reference", flags
+    except Exception:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        return O.OracleSpace(dim, bits, num_threads=cores), "port", "restatement (tq_oracle.c)"
 
 
 def cpu_scan(codes_host, queries, cores, kind_pref="reference"):
     """Time distance_1_to_n of the reference (or, without its build, the
     restatement) over `codes_host` for each query; returns (Gcodes/s, kind)."""
     n = codes_host.shape[0]
-    try:
-        mod = reference_module()
-        sp = mod.TurboQuantSpace(DIM, bits_per_coord=BITS, num_threads=cores)
-        kind = "reference"
-    except Exception:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        sp = O.OracleSpace(DIM, BITS, num_threads=cores)
-        kind = "port"
+    sp, kind, flags = cpu_space(DIM, BITS, cores)
     sp.distance_1_to_n(queries[0], codes_host[: min(n, 10000)])  # warm the threads
     t0 = time.perf_counter()
     for q in queries:
         sp.distance_1_to_n(q, codes_host)
     dt = time.perf_counter() - t0
-    return len(queries) * n / dt / 1e9, kind
+    return len(queries) * n / dt / 1e9, kind, flags
 
 
 def code_geometry(dim, bits):
@@ -208,15 +259,7 @@ def run_reference(args, rank):
     X = np.concatenate([l2n(rng.standard_normal((250_000, DIM)).astype(np.float32))
                         for _ in range(n_sample // 250_000)])
     Q = l2n(np.random.default_rng(3).standard_normal((QUERIES, DIM)).astype(np.float32))[:q_sample]
-    try:
-        mod = reference_module()
-        sp = mod.TurboQuantSpace(DIM, bits_per_coord=BITS, num_threads=cores)
-        kind = "reference"
-    except Exception:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        sp = O.OracleSpace(DIM, BITS, num_threads=cores)
-        kind = "port"
+    sp, kind, flags = cpu_space(DIM, BITS, cores)
     codes = sp.encode_batch(X)
     del X
 
@@ -241,7 +284,7 @@ def run_reference(args, rank):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": scan_config(args.n, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": round(value, 6), "unit": "Gcodes/s", "cores": cores,
-                         "kind": kind, "sample": sample},
+                         "kind": kind, "build": flags, "sample": sample},
         "e2e": {"value": round(value, 6), "unit": "Gcodes/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -273,13 +316,26 @@ def normal_rows(torch, gen, dev, n, dim, chunk=1 << 20):
     return out
 
 
-def run_mton(args, sym):
+def bf16_peaks():
+    """(burst, sustained) dense BF16 TFLOP/s of MEASURED_PEAKS.json, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["bf16_tflops"]), float(p["bf16_tflops_sustained"]), "measured"
+    except Exception:
+        return 1590.0, 1400.0, "fallback"
+
+
+def mton_result(args, sym, steps=10, cpu=True):
     """Dense M x N contractions, FP32 CUDA cores vs split-BF16 tcgen05.
 
     mton: 1,000,000 codes of normalised N(0,1) 768-d rows (4-bit), 4096
           normalised queries -> 4096 x 1,000,000 asymmetric distances.
     sym:  2048 x 2,000,000 codes of a 1024-centre Gaussian mixture at 1536-d
-          (padded to 2048), 4-bit -> symmetric distances."""
+          (padded to 2048), 4-bit -> symmetric distances.
+    Both forms are timed with CUDA events on their stream; the error of each is
+    taken against the FP64 evaluation of the formula on 10,000 sampled pairs;
+    the reference's CPU code is timed on a 128-row slice against 100,000 codes."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -292,15 +348,16 @@ def run_mton(args, sym):
     stream = torch.cuda.Stream(dev)
     sptr = C.c_void_p(stream.cuda_stream)
     gen = torch.Generator(device=dev)
+    full_n = args.n == 10_000_000
     if sym:
-        dim, bits, m, n = 1536, 4, 2048, args.n if args.n != 10_000_000 else 2_000_000
+        dim, bits, m, n = 1536, 4, 2048, 2_000_000 if full_n else args.n
         gen.manual_seed(6)
         centres = torch.randn((1024, dim), generator=gen, device=dev)
         Arows = mixture_rows(torch, gen, dev, m, dim, centres)
         gen.manual_seed(7)
         Brows = mixture_rows(torch, gen, dev, n, dim, centres)
     else:
-        dim, bits, m, n = 768, 4, 4096, args.n if args.n != 10_000_000 else 1_000_000
+        dim, bits, m, n = 768, 4, 4096, 1_000_000 if full_n else args.n
         gen.manual_seed(4)
         Brows = normal_rows(torch, gen, dev, n, dim)
         gen.manual_seed(5)
@@ -345,11 +402,13 @@ def run_mton(args, sym):
     mb = np.frombuffer(ch[:, cs - 12:cs - 8].tobytes(), np.float32).astype(np.float64)
     tscale = np.maximum(np.abs(f64), ma ** 2 + mb ** 2)
     flat = torch.from_numpy(ii * n + jj).to(dev)
-    for name, prec, reps in (("fp32", 0, max(1, args.steps // 5)), ("split_bf16", 1, args.steps)):
+    burst, sustained, pkind = bf16_peaks()
+    for name, prec, reps in (("fp32", 0, max(1, steps // 5)), ("split_bf16", 1, max(3, steps))):
         call(prec)
         stream.synchronize()
         got = out.view(-1).index_select(0, flat).cpu().numpy().astype(np.float64)
         err = float(np.max(np.abs(got - f64) / tscale))
+        plain = float(np.max(np.abs(got - f64) / np.maximum(np.abs(f64), 1e-30)))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
@@ -357,19 +416,59 @@ def run_mton(args, sym):
         e1.record(stream)
         stream.synchronize()
         ms = e0.elapsed_time(e1) / reps
-        res[name] = {"ms": round(ms, 3), "TFLOP_s": round(flops / (ms * 1e-3) / 1e12, 2),
-                     "Gdist_s": round(m * n / (ms * 1e-3) / 1e9, 3),
-                     "max_rel_err_vs_fp64": err, "reps": reps}
-    print(json.dumps({
-        "metric": METRIC, "workload": "sym" if sym else "mton",
+        tf = flops / (ms * 1e-3) / 1e12
+        r = {"ms": round(ms, 3), "TFLOP_s_algorithmic": round(tf, 2),
+             "Gdist_s": round(m * n / (ms * 1e-3) / 1e9, 3),
+             "max_rel_err_vs_fp64": err, "max_plain_rel_err_vs_fp64": plain, "reps": reps}
+        if name == "split_bf16":
+            # issued tensor work: exact-sign asymmetric planes take 3 products over
+            # the D centroid columns and 2 over the D sign columns; symmetric 3 over D
+            issued = float(m) * n * 2 * (5 * D if not sym else 3 * D)
+            r["TFLOP_s_issued"] = round(issued / (ms * 1e-3) / 1e12, 2)
+            r["frac_issued_of_bf16_sustained"] = round(issued / (ms * 1e-3) / 1e12 / sustained, 4)
+            r["frac_algorithmic_of_bf16_sustained"] = round(tf / sustained, 4)
+            r["peak_bf16_sustained_tflops"] = sustained
+            r["peak_kind"] = pkind
+        res[name] = r
+    del out
+    cpu_base = None
+    if cpu:
+        cores = cpu_cores()
+        sp, kind, rflags = cpu_space(dim, bits, cores)
+        cb = codes[:100_000].cpu().numpy()
+        if sym:
+            ca = acodes[:128].cpu().numpy()
+            sp.distance_m_to_n_symmetric(ca[:8], cb[:1000])
+            t0 = time.perf_counter()
+            sp.distance_m_to_n_symmetric(ca, cb)
+        else:
+            qa = np.ascontiguousarray(Qh[:128])
+            sp.distance_m_to_n(qa[:8], cb[:1000])
+            t0 = time.perf_counter()
+            sp.distance_m_to_n(qa, cb)
+        dt = time.perf_counter() - t0
+        gd = 128 * 100_000 / dt / 1e9
+        cpu_base = {"value": round(gd, 6), "unit": "Gdist/s", "cores": cores, "kind": kind,
+                    "build": rflags, "full_config_s_extrapolated": round(m * n / (gd * 1e9), 1),
+                    "sample": f"128 rows x 100,000 codes of this corpus, "
+                              f"distance_m_to_n{'_symmetric' if sym else ''}"}
+    return {
         "config": {"dim": dim, "padded_dim": D, "bits_per_coord": bits, "m": m, "n": n,
                    "flops_per_pair": 2 * D if sym else 4 * D,
-                   "data": ("1024-centre Gaussian mixture, std 0.3, rows L2-normalised"
-                            if sym else "N(0,1) rows L2-normalised"),
-                   "error_sample": "10,000 (i, j) pairs, seed 10, vs the FP64 evaluation"},
+                   "data": ("1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 6/7)"
+                            if sym else "N(0,1) rows L2-normalised (seeds 4/5)"),
+                   "error_sample": "10,000 (i, j) pairs, seed 10, vs the FP64 evaluation "
+                                   "(max_rel_err: relative to max(|d|, |a|^2 + |b|^2))"},
         "results": res,
         "speedup_split_bf16_vs_fp32": round(res["fp32"]["ms"] / res["split_bf16"]["ms"], 2),
-    }), flush=True)
+        "target_speedup": 4.0,
+        "cpu_baseline": cpu_base,
+    }
+
+
+def run_mton(args, sym):
+    r = mton_result(args, sym, steps=args.steps, cpu=not args.no_cpu_baseline)
+    print(json.dumps({"metric": METRIC, "workload": "sym" if sym else "mton", **r}), flush=True)
 
 
 def run_symq(args):
@@ -419,7 +518,7 @@ def run_symq(args):
     flat = torch.from_numpy(ii * n + jj).to(dev)
     ref_mod = None
     try:
-        ref_mod = O.import_ref_module()
+        ref_mod = reference_module()[0]
     except Exception:  # the reference build is optional
         ref_mod = None
     a_cpu, b_cpu = acodes[:128].cpu().numpy(), codes[:512].cpu().numpy()
@@ -470,20 +569,21 @@ def run_symq(args):
     }), flush=True)
 
 
-def run_serve(args):
+def serve_result(args, rates, window, cpu=True):
     """Serving over a device-resident corpus: 20,000,000 codes of a 1024-centre
     Gaussian mixture at dim 384 (padded 512), 4-bit; requests of m ~ U{1..256}
     queries from the same mixture ask for exact top-10; Poisson arrivals at each
     swept rate for one window; p50/p99 request latency (submit -> result on the
-    host) and goodput (completed requests / window) per rate."""
-    import threading
+    host) and goodput (completed requests / window) per rate.  The CPU figure is
+    the reference's distance_m_to_n + a stable argsort top-10 on a 128-row x
+    100,000-code slice, as query rows per second over the whole corpus."""
     import torch
     import turboquant as tq
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     dim, bits = 384, 4
-    n = args.n if args.n != 10_000_000 else 20_000_000
+    n = 20_000_000 if args.n == 10_000_000 else args.n
     gen = torch.Generator(device=dev)
     gen.manual_seed(8)
     centres = torch.randn((1024, dim), generator=gen, device=dev)
@@ -498,15 +598,17 @@ def run_serve(args):
     del X
     gen.manual_seed(9)
     pool = mixture_rows(torch, gen, dev, 262_144, dim, centres).cpu().numpy()
+    cslice = codes[:100_000].cpu().numpy() if cpu else None
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     index = space.index(codes)
     build_s = time.perf_counter() - t0
     del codes
     torch.cuda.empty_cache()
+    t0 = time.perf_counter()
     server = index.serve(k=10, max_rows=1024, slots=2, kernel_variant=args.kernel_variant)
+    setup_s = time.perf_counter() - t0
     tuning = server.tuning()
-    rates = [float(r) for r in args.rates.split(",")]
     rng = np.random.default_rng(9)
     results = []
     for rate in rates:
@@ -517,7 +619,7 @@ def run_serve(args):
         off = 0
         while True:
             t_next += rng.exponential(1.0 / rate)
-            if t_next - t_start > args.window:
+            if t_next - t_start > window:
                 break
             dt = t_next - time.perf_counter()
             if dt > 0:
@@ -546,19 +648,141 @@ def run_serve(args):
             "p50_ms": round(float(np.percentile(lat, 50)), 2),
             "p99_ms": round(float(np.percentile(lat, 99)), 2),
             "batches": st["batches"], "mean_rows_per_batch": round(st["rows"] / max(1, st["batches"]), 1),
+            "exact_fallback_rows": st["fallback_rows"], "bound_violations": st["bound_violations"],
         })
-        print(json.dumps({"serve_rate": results[-1]}), flush=True)
     server.close()
-    print(json.dumps({
-        "metric": METRIC, "workload": "serve",
+    index.close()
+    cpu_base = None
+    if cpu:
+        cores = cpu_cores()
+        sp, kind, rflags = cpu_space(dim, bits, cores)
+        q = np.ascontiguousarray(pool[:128])
+        sp.distance_m_to_n(q[:8], cslice[:1000])
+        t0 = time.perf_counter()
+        d = sp.distance_m_to_n(q, cslice)
+        np.argsort(d, axis=1, kind="stable")[:, :10]
+        dt = time.perf_counter() - t0
+        rows_s = 128 / (dt * n / cslice.shape[0])
+        cpu_base = {"value": round(rows_s, 4), "unit": "query rows/s over the whole corpus",
+                    "cores": cores, "kind": kind, "build": rflags,
+                    "sample": "128 query rows x 100,000 codes: distance_m_to_n + stable argsort "
+                              "top-10, scaled to the corpus size"}
+    return {
         "config": {"dim": dim, "padded_dim": space.padded_dim(), "bits_per_coord": bits,
                    "n_codes": n, "k": 10, "request_rows": "U{1..256}", "arrivals": "Poisson",
-                   "window_s": args.window, "max_batch_rows": 1024, "slots": 2,
+                   "window_s": window, "max_batch_rows": 1024, "slots": 2,
                    "kernel_variant": "autotuned" if args.kernel_variant < 0 else args.kernel_variant,
+                   "top_k": "exact (tensor-pass candidates rescored with the reference's arithmetic)",
                    "data": "1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 8/9)"},
-        "index_build_s": round(build_s, 2), "tuning": tuning, "results": results,
-    }), flush=True)
-    index.close()
+        "index_build_s": round(build_s, 2), "server_setup_s": round(setup_s, 2), "tuning": tuning,
+        "results": results, "cpu_baseline": cpu_base,
+    }
+
+
+def run_serve(args):
+    rates = [float(r) for r in args.rates.split(",")]
+    r = serve_result(args, rates, args.window, cpu=not args.no_cpu_baseline)
+    print(json.dumps({"metric": METRIC, "workload": "serve", **r}), flush=True)
+
+
+def cfg1_result(args):
+    """The plain-method case: 100,000 x 128 N(0,1) rows (seed 0), 4-bit, one query
+    (seed 1): encode_batch then distance_1_to_n, device-resident (CUDA events)
+    and through the host API; codes against the reference's digest, distances
+    against the checker; the reference's CPU path on the same full workload."""
+    import hashlib
+    import torch
+    import turboquant as tq
+    from turboquant._capi import check, lib
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    L = lib()
+    stream = torch.cuda.Stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    X = np.random.default_rng(0).standard_normal((100_000, 128)).astype(np.float32)
+    q = np.random.default_rng(1).standard_normal(128).astype(np.float32)
+    space = tq.TurboQuantSpace(128, bits_per_coord=4, device=0)
+    h = space._h
+    cs = space.code_size_bytes()
+    Xd, qd = torch.from_numpy(X).to(dev), torch.from_numpy(q).to(dev)
+    codes = torch.empty((100_000, cs), dtype=torch.uint8, device=dev)
+    out = torch.empty(100_000, dtype=torch.float32, device=dev)
+
+    def enc():
+        check(L.tq_encode_batch_device(h, C.c_void_p(Xd.data_ptr()), 100_000, C.c_void_p(codes.data_ptr()), sptr))
+
+    def scan():
+        check(L.tq_distance_1_to_n_device(h, C.c_void_p(qd.data_ptr()), C.c_void_p(codes.data_ptr()),
+                                          100_000, C.c_void_p(out.data_ptr()), sptr))
+
+    res = {}
+    for name, fn in (("encode", enc), ("distance_1_to_n", scan)):
+        for _ in range(5):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(100):
+            fn()
+        e1.record(stream)
+        stream.synchronize()
+        res[name] = {"us": round(e0.elapsed_time(e1) * 10.0, 2)}
+    res["encode"]["Mvec_per_s"] = round(100_000 / res["encode"]["us"], 2)
+    res["distance_1_to_n"]["Gcodes_per_s"] = round(100_000 / res["distance_1_to_n"]["us"] / 1e3, 3)
+    ch = codes.cpu().numpy()
+    digest_ok = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "digests.json")) as f:
+            digest_ok = hashlib.sha256(ch.tobytes()).hexdigest() == json.load(f)["cfg1_codes_sha256"]
+    except OSError:
+        pass
+    d = out.cpu().numpy()
+    ref = O.OracleSpace(128, 4).distance_1_to_n(q, ch)
+    meta = np.frombuffer(ch[:, cs - 12:cs - 8].tobytes(), np.float32).astype(np.float64)
+    tscale = float(np.sum(q.astype(np.float64) ** 2)) + meta ** 2
+    err = float(np.max(np.abs(d - ref) / np.maximum(np.abs(ref), tscale)))
+    # through the host API (numpy in, numpy out: copies included)
+    t0 = time.perf_counter()
+    for _ in range(10):
+        c2 = space.encode_batch(X)
+        space.distance_1_to_n(q, c2)
+    host_ms = (time.perf_counter() - t0) / 10 * 1e3
+    cores = cpu_cores()
+    sp, kind, rflags = cpu_space(128, 4, cores)
+    sp.encode_batch(X[:1000])
+    t0 = time.perf_counter()
+    rc = sp.encode_batch(X)
+    t1 = time.perf_counter()
+    for _ in range(10):
+        sp.distance_1_to_n(q, rc)
+    t2 = time.perf_counter()
+    return {
+        "config": {"dim": 128, "bits_per_coord": 4, "n": 100_000, "code_bytes": cs,
+                   "data": "N(0,1) rows (seed 0), query seed 1, not normalised"},
+        "device": res, "host_api_ms_encode_plus_distance": round(host_ms, 3),
+        "codes_match_reference_digest": digest_ok, "distance_max_rel_err_vs_checker": err,
+        "cpu_baseline": {"encode_ms": round((t1 - t0) * 1e3, 3),
+                         "distance_1_to_n_ms": round((t2 - t1) / 10 * 1e3, 3), "cores": cores,
+                         "kind": kind, "build": rflags, "sample": "the full workload"},
+    }
+
+
+def extra(fn, uuid, *a):
+    """One of the default run's extra workloads, with the clocks seen while it
+    ran; an error is reported in its key instead of ending the run."""
+    import torch
+    try:
+        with ClockSampler(uuid) as clk:
+            r = fn(*a)
+        r["clocks"] = clk.summary()
+        return r
+    except Exception as e:  # report, keep the headline line
+        return {"error": f"{type(e).__name__}: {e}"}
+    finally:
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
 
 
 def main():
@@ -573,6 +797,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="scan: skip the config-1, M x N (mton, sym) and serving keys")
+    ap.add_argument("--extra-rates", default="20,60,1000",
+                    help="scan: request rates (req/s) of the serving key")
+    ap.add_argument("--extra-window", type=float, default=5.0,
+                    help="scan: seconds per rate of the serving key")
     ap.add_argument("--rates", default="5,20,40,60,100,150,1000,50000",
                     help="serve: request rates (req/s) to sweep")
     ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
@@ -763,9 +993,9 @@ def main():
         cores = cpu_cores()
         n_cpu = min(n, 1_000_000)
         ch = codes[:n_cpu].cpu().numpy()
-        val, kind = cpu_scan(ch, Qh[:16], cores)
+        val, kind, flags = cpu_scan(ch, Qh[:16], cores)
         cpu = {"value": round(val, 6), "unit": "Gcodes/s", "cores": cores, "kind": kind,
-               "sample": f"16 queries x {n_cpu} codes of this corpus, distance_1_to_n"}
+               "build": flags, "sample": f"16 queries x {n_cpu} codes of this corpus, distance_1_to_n"}
 
     if rank == 0:
         line = {
@@ -792,6 +1022,18 @@ def main():
             "gpu_launches": args.steps * QUERIES * 2,
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_extras:
+            # the metric's other halves on their own workloads, after the scan's
+            # buffers are released
+            del out, codes, Qd, qrot, sq, nrm, scan_args, optr, qptr, cptr
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            rates = [float(r) for r in args.extra_rates.split(",")]
+            line["cfg1"] = extra(cfg1_result, uuid, args)
+            line["mton"] = extra(mton_result, uuid, args, False, 10, not args.no_cpu_baseline)
+            line["sym"] = extra(mton_result, uuid, args, True, 10, not args.no_cpu_baseline)
+            line["serve"] = extra(serve_result, uuid, args, rates, args.extra_window,
+                                  not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
