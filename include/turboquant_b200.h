@@ -255,6 +255,15 @@ tq_status tq_distance_1_to_n_symmetric_full_device(const tq_space *sp, const flo
  * device). */
 tq_status tq_space_take_device_status(const tq_space *sp, int *code);
 
+/* Kernel timer of the 1->N scan (no counterpart in the reference: a
+ * measurement aid).  While enabled, tq_distance_1_to_n_device and
+ * tq_distance_1_to_n_prepared_device record a pair of CUDA events around
+ * their scan kernel on the call's stream; enabling resets the record.
+ * tq_space_scan_timer_read waits for the recorded launches and returns their
+ * summed kernel time in milliseconds and their count. */
+tq_status tq_space_scan_timer(tq_space *sp, int enable);
+tq_status tq_space_scan_timer_read(tq_space *sp, double *total_ms, uint64_t *launches);
+
 /* Self-test of the device-side failure path: a kernel waits, with a limit of
  * about budget_ms, on a barrier that nothing signals.  Returns TQ_ERR_TIMEOUT
  * when the wait gave up and reported it (the expected outcome; the context

@@ -470,3 +470,34 @@ def test_reference_precision_refused_for_symmetric(cuda_ok):
     codes = s.encode_batch(np.ones((3, 64), np.float32))
     with pytest.raises(tq.TQError):
         s.distance_m_to_n_symmetric(codes, codes, precision="reference")
+
+
+def test_scan_timer_counts_launches(cuda_ok):
+    """The scan kernel timer records one event pair per 1->N scan launch while on."""
+    import ctypes as C
+    import torch
+    from turboquant._capi import check, lib
+    L = lib()
+    s = tq.TurboQuantSpace(256, 8)
+    rng = np.random.default_rng(3)
+    codes = torch.from_numpy(s.encode_batch(rng.standard_normal((50_000, 256)).astype(np.float32))).cuda()
+    q = torch.from_numpy(rng.standard_normal(256).astype(np.float32)).cuda()
+    out = torch.empty(50_000, dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        check(L.tq_distance_1_to_n_device(s._h, C.c_void_p(q.data_ptr()), C.c_void_p(codes.data_ptr()),
+                                          50_000, C.c_void_p(out.data_ptr()), C.c_void_p(st)))
+
+    call()
+    check(L.tq_space_scan_timer(s._h, 1))
+    for _ in range(7):
+        call()
+    check(L.tq_space_scan_timer(s._h, 0))
+    call()
+    ms, k = C.c_double(), C.c_uint64()
+    check(L.tq_space_scan_timer_read(s._h, C.byref(ms), C.byref(k)))
+    assert k.value == 7 and ms.value > 0.0
+    check(L.tq_space_scan_timer(s._h, 1))
+    check(L.tq_space_scan_timer_read(s._h, C.byref(ms), C.byref(k)))
+    assert k.value == 0 and ms.value == 0.0

@@ -426,6 +426,7 @@ void tq_space_destroy(tq_space *sp) {
         DeviceGuard g(sp->device);
         for (auto &s : sp->host_stream)
             if (s) cudaStreamDestroy(s);
+        for (auto e : sp->timer_events) cudaEventDestroy(e);
         if (sp->dev_block) cudaFree(sp->dev_block);
     }
     delete sp;
@@ -532,6 +533,68 @@ tq_status tq_prepare_query(const tq_space *csp, const float *query, float *q_rot
     return TQ_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The 1->N scan launch of every distance_1_to_n entry point; while the space's
+// scan timer is on, it is bracketed by a pair of CUDA events on its stream.
+cudaError_t scan_1_to_n(const tq_space *csp, const float *q_rot, const float *s_q,
+                        const float *norms, const uint8_t *codes, size_t n, float *out,
+                        cudaStream_t s) {
+    auto *sp = const_cast<tq_space *>(csp);
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    {
+        std::lock_guard<std::mutex> lk(sp->timer_mu);
+        if (sp->timer_on) {
+            while (sp->timer_events.size() < 2 * (sp->timer_used + 1)) {
+                cudaEvent_t e = nullptr;
+                const cudaError_t r = cudaEventCreate(&e);
+                if (r != cudaSuccess) return r;
+                sp->timer_events.push_back(e);
+            }
+            ev[0] = sp->timer_events[2 * sp->timer_used];
+            ev[1] = sp->timer_events[2 * sp->timer_used + 1];
+            ++sp->timer_used;
+        }
+    }
+    cudaError_t e = ev[0] ? cudaEventRecord(ev[0], s) : cudaSuccess;
+    if (e == cudaSuccess) e = tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out, s);
+    if (e == cudaSuccess && ev[1]) e = cudaEventRecord(ev[1], s);
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+tq_status tq_space_scan_timer(tq_space *sp, int enable) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    std::lock_guard<std::mutex> lk(sp->timer_mu);
+    sp->timer_on = enable != 0;
+    if (enable) sp->timer_used = 0;
+    return TQ_OK;
+}
+
+tq_status tq_space_scan_timer_read(tq_space *sp, double *total_ms, uint64_t *launches) {
+    tq_status st = need_device(sp);
+    if (st != TQ_OK) return st;
+    DeviceGuard g(sp->device);
+    std::lock_guard<std::mutex> lk(sp->timer_mu);
+    double total = 0.0;
+    for (size_t i = 0; i < sp->timer_used; ++i) {
+        TQ_CUDA(cudaEventSynchronize(sp->timer_events[2 * i + 1]), "scan timer sync");
+        float ms = 0.0f;
+        TQ_CUDA(cudaEventElapsedTime(&ms, sp->timer_events[2 * i], sp->timer_events[2 * i + 1]),
+                "scan timer");
+        total += ms;
+    }
+    if (total_ms) *total_ms = total;
+    if (launches) *launches = sp->timer_used;
+    return TQ_OK;
+}
+
 tq_status tq_distance_1_to_n_device(const tq_space *sp, const float *query,
                                     const uint8_t *codes, size_t n, float *out, void *stream) {
     tq_status st = need_device(sp);
@@ -547,7 +610,7 @@ tq_status tq_distance_1_to_n_device(const tq_space *sp, const float *query,
     TQ_CUDA(scr.alloc(sizeof(float) * (2 * sp->D + 2), s), "cudaMallocAsync(prepared query)");
     float *q_rot = static_cast<float *>(scr.p), *s_q = q_rot + sp->D, *norms = s_q + sp->D;
     TQ_CUDA(tq::launch_prepare(sp->P, sp->T, query, 1, q_rot, s_q, norms, s), "prepare kernel");
-    TQ_CUDA(tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out, s), "scan kernel");
+    TQ_CUDA(scan_1_to_n(sp, q_rot, s_q, norms, codes, n, out, s), "scan kernel");
     return TQ_OK;
 }
 
@@ -573,9 +636,7 @@ tq_status tq_distance_1_to_n_prepared_device(const tq_space *sp, const float *q_
     if ((st = check_dev(codes, n * sp->code_size, "codes")) != TQ_OK) return st;
     if ((st = check_codes_align(codes, "codes")) != TQ_OK) return st;
     if ((st = check_dev(out, n * 4, "out")) != TQ_OK) return st;
-    TQ_CUDA(tq::launch_scan_1_to_n(sp->P, sp->T, q_rot, s_q, norms, codes, n, out,
-                                   (cudaStream_t)stream),
-            "scan kernel");
+    TQ_CUDA(scan_1_to_n(sp, q_rot, s_q, norms, codes, n, out, (cudaStream_t)stream), "scan kernel");
     return TQ_OK;
 }
 

@@ -24,6 +24,12 @@ struct tq_space {
     void *dev_block = nullptr;  // single device allocation holding the tables
     std::mutex host_mu;         // serialises the host-pointer entry points
     cudaStream_t host_stream[2] = {nullptr, nullptr};
+    // scan kernel timer (tq_space_scan_timer): event pairs around each 1->N
+    // scan launch while enabled
+    std::mutex timer_mu;
+    bool timer_on = false;
+    size_t timer_used = 0;
+    std::vector<cudaEvent_t> timer_events;  // 2 per recorded launch
 };
 
 namespace tq {

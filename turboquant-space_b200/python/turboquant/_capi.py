@@ -33,7 +33,8 @@ EXPORTS = (
     "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
     "tq_server_create", "tq_server_create_ex", "tq_server_submit", "tq_request_wait", "tq_request_done",
     "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning",
-    "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status",
+    "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status", "tq_space_scan_timer",
+    "tq_space_scan_timer_read",
     "tq_rotated_coords_batch", "tq_rotated_coords_batch_device",
     "tq_distance_m_to_n_symmetric_qjl", "tq_distance_m_to_n_symmetric_qjl_device",
     "tq_prepare_symmetric_query", "tq_distance_1_to_n_symmetric_full",
@@ -151,6 +152,10 @@ def lib() -> C.CDLL:
     L.tq_server_tuning.argtypes = [vp, vp, vp, vp, C.c_int, C.POINTER(C.c_int)]
     L.tq_selftest_bounded_wait.restype = st
     L.tq_selftest_bounded_wait.argtypes = [C.c_int, C.c_int]
+    L.tq_space_scan_timer.restype = st
+    L.tq_space_scan_timer.argtypes = [vp, C.c_int]
+    L.tq_space_scan_timer_read.restype = st
+    L.tq_space_scan_timer_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.tq_space_take_device_status.restype = st
     L.tq_space_take_device_status.argtypes = [vp, C.POINTER(C.c_int)]
     L.tq_rotated_coords_batch.restype = st
