@@ -289,6 +289,8 @@ typedef struct tq_server_stats {
     int candidates;              /* tensor-pass candidates per query row */
     uint64_t fallback_rows;      /* rows the certificate left open, answered by a full exact pass */
     uint64_t bound_violations;   /* candidates whose two distances differed by more than the bound */
+    size_t pool_rows;            /* query rows of the admission pool (device memory) */
+    size_t pool_used_rows;       /* rows held by queued and in-flight requests */
 } tq_server_stats;
 
 /* Keep n codes (host or device memory) resident in HBM, with their BF16
@@ -304,14 +306,18 @@ typedef struct tq_server_params {
     int max_rows;       /* query rows per batch, a positive multiple of 128 */
     int slots;          /* batches in flight, 1..8 (fewer if they do not fit in half of the
                            free device memory) */
-    int kernel_variant; /* -1: autotune the contraction per batch-size bucket; 0..2 fixed
-                           (0: 128 x 256 tiles; 1, 2: 128 x 128 tiles with 3 or 2 stages) */
+    int kernel_variant; /* -1: autotune the contraction's tile shape per batch-size bucket;
+                           0..5 fixed (tq_topk_variant_shape) */
     size_t queue_rows;  /* queued query rows beyond which submit returns TQ_ERR_BUSY
-                           (0: 16 x max_rows) */
+                           (0: no cap beyond the admission pool) */
     int candidates;     /* tensor-pass candidates per row that the exact stage rescores,
                            k..32 (0: min(32, k + 16)) */
     float bound_scale;  /* multiplier on the certificate's error bound (0: 1); a larger
                            value sends more rows to the exact full pass */
+    size_t memory_budget; /* device bytes of the admission pool that holds the queries of
+                           the queued and in-flight requests, dim * 4 bytes a row (0: an
+                           eighth of the free device memory, at most 16 x max_rows rows);
+                           submit returns TQ_ERR_BUSY when a request's rows do not fit */
 } tq_server_params;
 
 /* A server answering exact top-k for requests of up to max_rows queries:
@@ -338,6 +344,16 @@ tq_status tq_server_reset_stats(tq_server *sv);
    per batch (two slots' launches overlapped, as the server runs them). */
 tq_status tq_server_tuning(tq_server *sv, int *bucket_rows, int *variant, float *ms, int cap,
                            int *n);
+/* Every time the autotuner took, bucket-major: ms[b * n_variants + v]
+   (0 where a variant was not timed); from_cache = 1 when this server reused
+   the process's earlier tuning of the same index shape, candidates and
+   bucket rows. */
+tq_status tq_server_tuning_times(tq_server *sv, float *ms, int cap, int *n_buckets, int *n_variants,
+                                 int *from_cache);
+/* The tile shape of a kernel variant: shape[0] query rows per CTA, shape[1]
+   codes per tile (per pipeline stage), shape[2] pipeline stages, shape[3] K
+   blocks of 64 per promoted accumulation chunk. */
+tq_status tq_topk_variant_shape(int variant, int *shape);
 void tq_server_destroy(tq_server *sv);
 
 #ifdef __cplusplus

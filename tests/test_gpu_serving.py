@@ -70,7 +70,7 @@ def test_index_search_is_the_stable_argsort(corpus, k):
     _assert_exact(D, I, ref[:300], k)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_kernel_variants_give_identical_results(corpus, variant):
     space, codes, X, Q, ref, index = corpus
     with index.serve(k=10, max_rows=256, slots=1, kernel_variant=variant) as sv:
@@ -179,12 +179,67 @@ def test_admission_refuses_when_queue_full(corpus):
     assert st["completed"] == len(accepted)
 
 
-def test_autotuner_reports_each_bucket(corpus):
+def test_admission_by_device_memory_budget(corpus):
+    """The admission pool holds the queries of queued and in-flight requests in
+    device memory: with a budget of 300 query rows, a burst of 100-row requests
+    is partly refused, everything admitted completes exactly, and the pool is
+    empty again afterwards."""
     space, codes, X, Q, ref, index = corpus
-    with index.serve(k=10, max_rows=512, slots=1) as sv:
-        t = sv.tuning()
-    assert [b["bucket_rows"] for b in t] == [128, 256, 512]
-    assert all(b["variant"] in (0, 1, 2) and b["ms"] > 0 for b in t)
+    row_bytes = DIM * 4
+    with index.serve(k=5, max_rows=256, slots=1, memory_budget=300 * row_bytes) as sv:
+        assert sv.stats()["pool_rows"] == 300
+        accepted, refused = [], 0
+        for i in range(40):
+            try:
+                accepted.append((i % 5, sv.submit(Q[100 * (i % 5): 100 * (i % 5) + 100])))
+            except tq.BusyError:
+                refused += 1
+        for j, r in accepted:
+            D, I = r.wait()
+            _assert_exact(D, I, ref[100 * j: 100 * j + 100], 5)
+        st = sv.stats()
+    assert refused > 0 and st["rejected"] == refused
+    assert st["completed"] == len(accepted)
+    assert st["pool_used_rows"] == 0
+    # a larger budget admits the whole burst
+    with index.serve(k=5, max_rows=256, slots=1, memory_budget=4000 * row_bytes) as sv:
+        rs = [sv.submit(Q[:100]) for _ in range(40)]
+        for r in rs:
+            r.wait()
+        assert sv.stats()["rejected"] == 0
+
+
+def test_budget_below_one_batch_is_refused(corpus):
+    space, codes, X, Q, ref, index = corpus
+    with pytest.raises(ValueError):
+        index.serve(k=5, max_rows=256, slots=1, memory_budget=100 * DIM * 4)
+
+
+def test_autotuner_searches_the_tile_space(corpus):
+    space, codes, X, Q, ref, index = corpus
+    shapes = tq.variant_shapes()
+    assert len(shapes) == 6
+    assert {(s["codes_per_tile"], s["stages"], s["chunk_k_blocks"]) for s in shapes} == {
+        (256, 2, 8), (128, 3, 8), (128, 2, 4), (128, 3, 4), (128, 2, 8), (256, 2, 4)}
+    ix = space.index(np.ascontiguousarray(codes[:50_000]))  # an index shape not tuned before
+    try:
+        with ix.serve(k=10, max_rows=512, slots=1) as sv:
+            t = sv.tuning(searched=True)
+            D, I = sv.submit(Q[:64]).wait()
+        _assert_exact(D, I, ref[:64, :50_000], 10)
+        assert [b["bucket_rows"] for b in t] == [128, 256, 512]
+        for b in t:
+            assert not b["from_cache"]
+            assert b["variant"] in range(6) and b["ms"] > 0
+            assert all(x > 0 for x in b["times_ms"])
+            assert b["ms"] == pytest.approx(min(b["times_ms"]))
+        # the same index shape again: the process's tuning cache answers
+        with ix.serve(k=10, max_rows=512, slots=1) as sv:
+            t2 = sv.tuning(searched=True)
+        assert all(b["from_cache"] for b in t2)
+        assert [b["variant"] for b in t2] == [b["variant"] for b in t]
+    finally:
+        ix.close()
 
 
 def test_fewer_codes_than_k(cuda_ok):
@@ -200,7 +255,7 @@ def test_fewer_codes_than_k(cuda_ok):
     _assert_exact(D[:, :5], I[:, :5], want, 5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 5])
 def test_every_column_inserts(corpus, variant):
     """Worst case for the per-row lists: the index holds the codes in order of
     descending distance to the first query, so every column of every slice

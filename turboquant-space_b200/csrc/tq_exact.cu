@@ -536,6 +536,20 @@ __global__ void __launch_bounds__(256) index_bound_kernel(Params P, const uint8_
     }
 }
 
+// Batch row r of the serving path <- pool row rows[r] (r < *m_dev).
+__global__ void __launch_bounds__(256) gather_rows_kernel(const float *__restrict__ pool,
+                                                          const int *__restrict__ rows,
+                                                          const int *__restrict__ m_dev, int dim,
+                                                          float *__restrict__ out) {
+    const int m = *m_dev;
+    const size_t total = (size_t)m * dim;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = t / dim, i = t % dim;
+        out[t] = pool[(size_t)rows[r] * dim + i];
+    }
+}
+
 bool codes_al4(const Params &P, const uint8_t *codes) {
     return (P.cs % 4 == 0) && ((reinterpret_cast<uintptr_t>(codes) & 3) == 0);
 }
@@ -588,6 +602,14 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
     if (e != cudaSuccess) return e;
     fallback_merge_kernel<<<(unsigned)((max_rows + 7) / 8), 256, 0, st>>>(
         counters, fail_rows, fb_ctas, k, part_d, part_i, out_d, out_i);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const float *pool, const int *rows, const int *m_dev, size_t dim,
+                               size_t max_rows, float *out, cudaStream_t st) {
+    const size_t total = max_rows * dim;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 8);
+    gather_rows_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(pool, rows, m_dev, (int)dim, out);
     return cudaGetLastError();
 }
 

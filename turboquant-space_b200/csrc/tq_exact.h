@@ -46,6 +46,11 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
                             int *part_i, float *out_d, long long *out_i, int max_rows,
                             cudaStream_t st);
 
+// Serving admission pool -> batch: out[r] = pool[rows[r]] (dim floats each)
+// for r < *m_dev (at most max_rows).
+cudaError_t launch_gather_rows(const float *pool, const int *rows, const int *m_dev, size_t dim,
+                               size_t max_rows, float *out, cudaStream_t st);
+
 // The reference-order distances of m prepared queries against n codes,
 // out[i * ldo + j]: one thread per pair, the arithmetic the rescoring uses.
 cudaError_t launch_exact_mton(const Params &P, const float *centroids, const float *q_rot,

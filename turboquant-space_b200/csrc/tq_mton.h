@@ -47,15 +47,17 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
 // k (<= kCandMax) smallest (distance, index) pairs, ties to the smaller index.
 // The row count is read from m_dev; `grid` CTAs split the rows into 128-row
 // blocks and the columns into slices.
-// Variant 0: 128 x 256 tiles (n_pad % 256 == 0), two partial lists per (row,
-// slice); variant 1: 128 x 128 tiles, 3 stages, 8-block promoted chunks;
-// variant 2: 128 x 128 tiles, 2 stages, 4-block chunks.  The partial buffers
+// Variants 0 and 5: 128 x 256 tiles (n_pad % 256 == 0), two partial lists per
+// (row, slice); 1-4: 128 x 128 tiles (tc_topk_shape gives each one's stages
+// and chunk length).  The partial buffers
 // hold grid * 128 * tc_topk_lists(variant) * kCandMax entries.
 constexpr int kTopKMax = 16;   // results per row (k) of the serving path
 constexpr int kCandMax = 32;   // list length of the tensor-core top-k (candidates per row)
 constexpr int kTopKListsMax = 2;
 int tc_topk_variants();
 int tc_topk_lists(int variant);
+// {rows per CTA, codes per tile, pipeline stages, K blocks per chunk} of a variant
+bool tc_topk_shape(int variant, int out[4]);
 cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t rows_pad,
                            const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo,
                            const int *m_dev,

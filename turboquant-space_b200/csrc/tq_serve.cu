@@ -17,10 +17,14 @@
 //              other batches are on the GPU join the next batch) and the
 //              bucket's graph is launched on the slot's stream.  Slots run on
 //              separate streams, so one batch's copies and query preparation
-//              overlap another's contraction.  Admission: the slots are sized
-//              from the device's free memory at creation, and submit refuses a
-//              request (TQ_ERR_BUSY) when the queued rows would exceed the
-//              queue capacity.
+//              overlap another's contraction.
+//   admission  an admitted request's queries are copied at submit into a
+//              device pool of query rows whose size is the server's memory
+//              budget (by default a share of the device's free memory at
+//              creation); submit refuses a request (TQ_ERR_BUSY) when its rows
+//              do not fit in the pool's free space, which holds the rows of the
+//              queued and the in-flight requests.  A batch gathers its rows
+//              from the pool on the device.
 //   autotune   per bucket, each kernel variant (tile shape x stage depth) is
 //              timed on the index and the fastest is captured into the graph.
 //   exact      the tensor-core pass keeps `kc` candidates per row; the
@@ -34,13 +38,17 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "tq_exact.h"
@@ -79,6 +87,8 @@ size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 struct tq_request {
     std::vector<float> queries;  // m x dim
     size_t m = 0;
+    size_t pool_off = 0;                // first row of its queries in the server's pool
+    cudaEvent_t uploaded = nullptr;     // the copy into the pool is done
     int k = 0;
     std::vector<float> dist;     // m x k
     std::vector<long long> idx;  // m x k
@@ -107,6 +117,8 @@ struct Slot {
         *d_fpi = nullptr;
     long long *d_ci = nullptr;
     int *h_cnt = nullptr;  // pinned copy of d_cnt after each batch
+    int *h_rows = nullptr;  // pool row of each batch row (pinned)
+    int *d_rows = nullptr;
     void *d_ap = nullptr;  // query planes: max_rows x K x 2 BF16 planes
     long long *d_oi = nullptr;
     std::vector<int> bucket_rows;
@@ -130,8 +142,15 @@ struct tq_server {
     std::vector<Slot> slots;
     std::vector<int> bucket_variant;  // autotuned kernel variant per bucket
     std::vector<double> bucket_ms;
+    std::vector<float> tune_ms;       // bucket x variant times (0: not timed)
+    bool tuned_from_cache = false;
     std::deque<tq_request *> pending;
     size_t pending_rows = 0;
+    // admission pool: pool_rows query rows in device memory, first-fit ranges
+    float *pool = nullptr;
+    size_t pool_rows = 0, pool_used = 0;
+    std::map<size_t, size_t> pool_free;  // offset -> length
+    cudaStream_t up_stream = nullptr;
     std::mutex mu;
     std::condition_variable cv;
     std::thread worker;
@@ -153,6 +172,47 @@ int bucket_index(const tq_server *sv, size_t rows) {
     return (int)b.size() - 1;
 }
 
+// First-fit allocation of `m` pool rows (caller holds sv->mu).
+bool pool_alloc(tq_server *sv, size_t m, size_t *off) {
+    for (auto it = sv->pool_free.begin(); it != sv->pool_free.end(); ++it) {
+        if (it->second < m) continue;
+        *off = it->first;
+        const size_t rest = it->second - m;
+        const size_t at = it->first + m;
+        sv->pool_free.erase(it);
+        if (rest) sv->pool_free.emplace(at, rest);
+        sv->pool_used += m;
+        return true;
+    }
+    return false;
+}
+
+// Returns rows [off, off + m) to the pool, merging with free neighbours
+// (caller holds sv->mu).
+void pool_release(tq_server *sv, size_t off, size_t m) {
+    auto nx = sv->pool_free.lower_bound(off);
+    if (nx != sv->pool_free.begin()) {
+        auto pv = std::prev(nx);
+        if (pv->first + pv->second == off) {
+            off = pv->first;
+            m += pv->second;
+            sv->pool_free.erase(pv);
+        }
+    }
+    if (nx != sv->pool_free.end() && off + m == nx->first) {
+        m += nx->second;
+        sv->pool_free.erase(nx);
+    }
+    sv->pool_free.emplace(off, m);
+}
+
+void release_request_rows(tq_server *sv, tq_request *r) {
+    pool_release(sv, r->pool_off, r->m);
+    sv->pool_used -= r->m;
+    if (r->uploaded) cudaEventDestroy(r->uploaded);
+    r->uploaded = nullptr;
+}
+
 // Enqueue the batch pipeline of `rows_cap` rows with kernel variant `var` on
 // the slot's stream (used both for graph capture and for autotuning runs).
 cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool copies) {
@@ -163,8 +223,11 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     cudaStream_t st = sl.stream;
     cudaError_t e = cudaSuccess;
     if (copies) {
-        e = cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)rows_cap * sp->dim * 4, cudaMemcpyHostToDevice, st);
+        // the batch's rows: their pool rows, then a gather from the pool
+        e = cudaMemcpyAsync(sl.d_rows, sl.h_rows, (size_t)rows_cap * sizeof(int), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(sl.d_m, sl.h_m, sizeof(int), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = tq::launch_gather_rows(sv->pool, sl.d_rows, sl.d_m, sp->dim, rows_cap, sl.d_q, st);
         if (e != cudaSuccess) return e;
     }
     float *q_rot = sl.d_prep, *s_q = q_rot + (size_t)rows_cap * D, *norms = s_q + (size_t)rows_cap * D;
@@ -222,6 +285,8 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     TQ_CUDA(cudaMallocHost(&sl.h_d, R * k * 4), "cudaMallocHost(dist)");
     TQ_CUDA(cudaMallocHost(&sl.h_i, R * k * 8), "cudaMallocHost(idx)");
     TQ_CUDA(cudaMallocHost(&sl.h_cnt, tq::kCntWords * sizeof(int)), "cudaMallocHost(counters)");
+    TQ_CUDA(cudaMallocHost(&sl.h_rows, R * sizeof(int)), "cudaMallocHost(rows)");
+    std::memset(sl.h_rows, 0, R * sizeof(int));
     std::memset(sl.h_cnt, 0, tq::kCntWords * sizeof(int));
     std::memset(sl.h_q, 0, R * sp->dim * 4);
     // device block layout (each part 256-byte aligned)
@@ -239,6 +304,7 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     const size_t kc = (size_t)sv->kc, fparts = R * (size_t)sv->fb_ctas * k;
     const size_t o_cd = take(R * kc * 4), o_ci = take(R * kc * 8), o_fail = take(R * 4);
     const size_t o_cnt = take(tq::kCntWords * 4), o_fpd = take(fparts * 4), o_fpi = take(fparts * 4);
+    const size_t o_rows = take(R * 4);
     TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
     TQ_CUDA(cudaMemset(sl.d_block, 0, off), "cudaMemset(slot)");
     auto *base = static_cast<unsigned char *>(sl.d_block);
@@ -259,6 +325,7 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     sl.d_cnt = reinterpret_cast<int *>(base + o_cnt);
     sl.d_fpd = reinterpret_cast<float *>(base + o_fpd);
     sl.d_fpi = reinterpret_cast<int *>(base + o_fpi);
+    sl.d_rows = reinterpret_cast<int *>(base + o_rows);
     for (int b = 128; b < sv->max_rows; b *= 2) sl.bucket_rows.push_back(b);
     sl.bucket_rows.push_back(sv->max_rows);
     return TQ_OK;
@@ -276,6 +343,7 @@ void slot_free(Slot &sl) {
     if (sl.h_d) cudaFreeHost(sl.h_d);
     if (sl.h_i) cudaFreeHost(sl.h_i);
     if (sl.h_cnt) cudaFreeHost(sl.h_cnt);
+    if (sl.h_rows) cudaFreeHost(sl.h_rows);
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.stream) cudaStreamDestroy(sl.stream);
     sl = Slot();
@@ -290,12 +358,49 @@ void slot_free(Slot &sl) {
 // fixed LCG stream): MMAs on zero operands draw less power, so a tensor-bound
 // variant would otherwise be timed at a clock that real batches under the
 // power cap do not get.
+// Tuning results of this process, per (device, padded dim, bits, corpus size,
+// candidates, slots tuned together, bucket rows): the fastest variant and its
+// time.  A server whose key is present skips timing that bucket.
+struct TuneKey {
+    int device, D, bits, kc, ns, rows;
+    size_t n;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(device, D, bits, kc, ns, rows, n) <
+               std::tie(o.device, o.D, o.bits, o.kc, o.ns, o.rows, o.n);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, double>> g_tune_cache;
+
 tq_status autotune(tq_server *sv, int fixed_variant) {
     const int ns = std::min<int>(2, (int)sv->slots.size());
     Slot &s0 = sv->slots[0];
     const int nb = (int)s0.bucket_rows.size();
+    const int nv = tq::tc_topk_variants();
     sv->bucket_variant.assign(nb, fixed_variant >= 0 ? fixed_variant : 0);
     sv->bucket_ms.assign(nb, 0.0);
+    sv->tune_ms.assign((size_t)nb * nv, 0.0f);
+    const tq_index *ix = sv->index;
+    auto key_of = [&](int rows) {
+        return TuneKey{ix->device, (int)ix->sp->D, ix->sp->bits, sv->kc, ns, rows, ix->n};
+    };
+    if (fixed_variant < 0) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        bool all = true;
+        for (int b = 0; b < nb; ++b) {
+            auto it = g_tune_cache.find(key_of(s0.bucket_rows[b]));
+            if (it == g_tune_cache.end()) {
+                all = false;
+                break;
+            }
+            sv->bucket_variant[b] = it->second.first;
+            sv->bucket_ms[b] = it->second.second;
+        }
+        if (all) {
+            sv->tuned_from_cache = true;
+            return TQ_OK;
+        }
+    }
     const size_t qn = (size_t)s0.max_rows * sv->index->sp->dim;
     uint32_t x = 0x9E3779B9u;
     for (size_t i = 0; i < qn; ++i) {
@@ -312,7 +417,7 @@ tq_status autotune(tq_server *sv, int fixed_variant) {
     TQ_CUDA(cudaEventCreate(&e0), "event");
     TQ_CUDA(cudaEventCreate(&e1[0]), "event");
     TQ_CUDA(cudaEventCreate(&e1[1]), "event");
-    constexpr int kReps = 2;
+    constexpr int kReps = 1;
     for (int b = 0; b < nb; ++b) {
         const int rows = s0.bucket_rows[b];
         for (int si = 0; si < ns; ++si) {
@@ -322,7 +427,7 @@ tq_status autotune(tq_server *sv, int fixed_variant) {
             TQ_CUDA(cudaStreamSynchronize(sl.stream), "sync");
         }
         double best = 1e30;
-        for (int v = 0; v < tq::tc_topk_variants(); ++v) {
+        for (int v = 0; v < nv; ++v) {
             if (fixed_variant >= 0 && v != fixed_variant) continue;
             TQ_CUDA(enqueue_batch(sv, s0, rows, v, false), "autotune warm-up");
             TQ_CUDA(cudaEventRecord(e0, s0.stream), "event");
@@ -340,6 +445,7 @@ tq_status autotune(tq_server *sv, int fixed_variant) {
                 ms = std::max(ms, t);
             }
             ms /= (float)(kReps * ns);
+            sv->tune_ms[(size_t)b * nv + v] = ms;
             if (ms < best) {
                 best = ms;
                 sv->bucket_variant[b] = v;
@@ -354,6 +460,11 @@ tq_status autotune(tq_server *sv, int fixed_variant) {
         int herr = 0;
         TQ_CUDA(cudaMemcpy(&herr, sv->slots[si].d_err, sizeof(int), cudaMemcpyDeviceToHost), "D2H status");
         if (herr) return fail(TQ_ERR_TIMEOUT, "top-k kernel: a pipeline wait timed out (code %d)", herr);
+    }
+    if (fixed_variant < 0) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (int b = 0; b < nb; ++b)
+            g_tune_cache[key_of(s0.bucket_rows[b])] = {sv->bucket_variant[b], sv->bucket_ms[b]};
     }
     return TQ_OK;
 }
@@ -395,7 +506,6 @@ void finish_request(tq_server *sv, tq_request *r, double t) {
 // every free slot.
 void worker_loop(tq_server *sv) {
     DeviceGuard g(sv->index->device);
-    const size_t dim = sv->index->sp->dim;
     const int k = sv->k;
     std::unique_lock<std::mutex> lk(sv->mu);
     while (true) {
@@ -422,6 +532,7 @@ void worker_loop(tq_server *sv) {
                     std::memcpy(r->idx.data(), sl.h_i + row * k, r->m * k * sizeof(long long));
                 }
                 row += r->m;
+                release_request_rows(sv, r);
                 finish_request(sv, r, t);
             }
             sv->completed += sl.batch.size();
@@ -434,11 +545,13 @@ void worker_loop(tq_server *sv) {
         for (auto &sl : sv->slots) {
             if (sl.busy || sv->pending.empty()) continue;
             size_t rows = 0;
+            cudaError_t e = cudaSuccess;
             while (!sv->pending.empty() && rows + sv->pending.front()->m <= (size_t)sv->max_rows) {
                 tq_request *r = sv->pending.front();
                 sv->pending.pop_front();
                 sv->pending_rows -= r->m;
-                std::memcpy(sl.h_q + rows * dim, r->queries.data(), r->m * dim * sizeof(float));
+                for (size_t i = 0; i < r->m; ++i) sl.h_rows[rows + i] = (int)(r->pool_off + i);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(sl.stream, r->uploaded, 0);
                 rows += r->m;
                 sl.batch.push_back(r);
             }
@@ -446,11 +559,12 @@ void worker_loop(tq_server *sv) {
             *sl.h_m = (int)rows;
             sl.batch_rows = rows;
             const int b = bucket_index(sv, rows);
-            cudaError_t e = cudaGraphLaunch(sl.graphs[b], sl.stream);
+            if (e == cudaSuccess) e = cudaGraphLaunch(sl.graphs[b], sl.stream);
             if (e == cudaSuccess) e = cudaEventRecord(sl.done, sl.stream);
             if (e != cudaSuccess) {
                 for (tq_request *r : sl.batch) {
                     r->status = TQ_ERR_CUDA;
+                    release_request_rows(sv, r);
                     finish_request(sv, r, now_ms());
                 }
                 sl.batch.clear();
@@ -565,10 +679,22 @@ tq_status tq_server_create_ex(tq_index *ix, const tq_server_params *prm, tq_serv
     sv->grid = sms;
     sv->fb_ctas = tq::fallback_ctas(sms);
     sv->max_rows = max_rows;
-    sv->queue_rows_cap = prm->queue_rows ? prm->queue_rows : (size_t)16 * max_rows;
-    // admission by free device memory: no more slots than fit in half the free memory
+    sv->queue_rows_cap = prm->queue_rows ? prm->queue_rows : SIZE_MAX;
+    // device memory: no more slots than fit in half the free memory; the
+    // admission pool holds the queries of the queued and in-flight requests
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
+    const size_t dim = ix->sp->dim, row_bytes = dim * sizeof(float);
+    const size_t budget = prm->memory_budget
+                              ? prm->memory_budget
+                              : std::min(free_b / 8, (size_t)16 * max_rows * row_bytes);
+    sv->pool_rows = budget / row_bytes;
+    if (sv->pool_rows < (size_t)max_rows) {
+        delete sv;
+        return fail(TQ_ERR_INVALID_ARGUMENT,
+                    "memory budget of %zu bytes holds %zu query rows, fewer than max_rows (%d)",
+                    budget, budget / row_bytes, max_rows);
+    }
     const size_t D = ix->sp->D, K = (size_t)ix->K, R = (size_t)max_rows;
     const size_t slot_bytes =
         R * (ix->sp->dim * 4 + (2 * D + 2) * 4 + K * 4 + 8 + (size_t)k * 12 + (size_t)kc * 12 + 4 +
@@ -578,8 +704,12 @@ tq_status tq_server_create_ex(tq_index *ix, const tq_server_params *prm, tq_serv
     slots = (int)std::min<size_t>((size_t)slots, fit);
     sv->slots.resize(slots);
     tq_status st = TQ_OK;
+    cudaError_t ce = cudaMalloc(&sv->pool, sv->pool_rows * row_bytes);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&sv->up_stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) st = cuda_fail(ce, "admission pool");
+    sv->pool_free.emplace(0, sv->pool_rows);
     for (auto &sl : sv->slots)
-        if ((st = slot_alloc(sv, sl)) != TQ_OK) break;
+        if (st == TQ_OK && (st = slot_alloc(sv, sl)) != TQ_OK) break;
     if (st == TQ_OK) st = autotune(sv, kernel_variant);
     for (auto &sl : sv->slots) {
         if (st != TQ_OK) break;
@@ -587,6 +717,8 @@ tq_status tq_server_create_ex(tq_index *ix, const tq_server_params *prm, tq_serv
     }
     if (st != TQ_OK) {
         for (auto &sl : sv->slots) slot_free(sl);
+        if (sv->pool) cudaFree(sv->pool);
+        if (sv->up_stream) cudaStreamDestroy(sv->up_stream);
         delete sv;
         return st;
     }
@@ -611,6 +743,9 @@ tq_status tq_server_submit(tq_server *sv, const float *queries, size_t m, tq_req
     *out = nullptr;
     if (m == 0 || m > (size_t)sv->max_rows)
         return fail(TQ_ERR_INVALID_ARGUMENT, "request rows must be in 1..%d", sv->max_rows);
+    if (m > sv->pool_rows)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "request of %zu rows exceeds the admission pool (%zu rows)",
+                    m, sv->pool_rows);
     const size_t dim = sv->index->sp->dim;
     auto *r = new tq_request();
     r->queries.assign(queries, queries + m * dim);
@@ -618,15 +753,34 @@ tq_status tq_server_submit(tq_server *sv, const float *queries, size_t m, tq_req
     r->k = sv->k;
     r->dist.assign(m * sv->k, 0.0f);
     r->idx.assign(m * sv->k, -1);
+    r->t_submit = now_ms();
     {
+        // admission: room in the pool (and under the optional queued-row cap)
         std::lock_guard<std::mutex> lk(sv->mu);
         ++sv->submitted;
-        if (sv->stop || sv->pending_rows + m > sv->queue_rows_cap) {
+        if (sv->stop || sv->pending_rows + m > sv->queue_rows_cap || !pool_alloc(sv, m, &r->pool_off)) {
             ++sv->rejected;
+            const size_t used = sv->pool_used, queued = sv->pending_rows;
             delete r;
-            return fail(TQ_ERR_BUSY, "server queue full (%zu rows queued)", sv->pending_rows);
+            return fail(TQ_ERR_BUSY, "admission refused: %zu of %zu pool rows in use, %zu rows queued",
+                        used, sv->pool_rows, queued);
         }
-        r->t_submit = now_ms();
+    }
+    // the queries go to their pool rows now; the batch that takes them waits
+    // for this copy on the device
+    DeviceGuard g(sv->index->device);
+    cudaError_t e = cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sv->pool + r->pool_off * dim, r->queries.data(), m * dim * sizeof(float),
+                            cudaMemcpyHostToDevice, sv->up_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(r->uploaded, sv->up_stream);
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        if (e != cudaSuccess) {
+            release_request_rows(sv, r);
+            delete r;
+            return cuda_fail(e, "request upload");
+        }
         sv->pending.push_back(r);
         sv->pending_rows += m;
     }
@@ -681,6 +835,8 @@ tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latenc
     out->candidates = sv->kc;
     out->fallback_rows = sv->fallback_rows;
     out->bound_violations = sv->bound_violations;
+    out->pool_rows = sv->pool_rows;
+    out->pool_used_rows = sv->pool_used;
     size_t nl = std::min(cap, sv->latencies_ms.size());
     if (latencies && nl) std::memcpy(latencies, sv->latencies_ms.data(), nl * sizeof(float));
     if (n_lat) *n_lat = latencies ? nl : sv->latencies_ms.size();
@@ -707,6 +863,28 @@ tq_status tq_server_tuning(tq_server *sv, int *bucket_rows, int *variant, float 
         if (ms) ms[i] = (float)sv->bucket_ms[i];
     }
     if (n) *n = (int)b.size();
+    return TQ_OK;
+}
+
+tq_status tq_server_tuning_times(tq_server *sv, float *ms, int cap, int *n_buckets,
+                                 int *n_variants, int *from_cache) {
+    if (!sv) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL server");
+    const int nb = (int)sv->slots[0].bucket_rows.size(), nv = tq::tc_topk_variants();
+    if (ms) {
+        const int c = std::min(cap, nb * nv);
+        for (int i = 0; i < c; ++i) ms[i] = sv->tune_ms.empty() ? 0.0f : sv->tune_ms[(size_t)i];
+    }
+    if (n_buckets) *n_buckets = nb;
+    if (n_variants) *n_variants = nv;
+    if (from_cache) *from_cache = sv->tuned_from_cache ? 1 : 0;
+    return TQ_OK;
+}
+
+tq_status tq_topk_variant_shape(int variant, int *shape) {
+    int v[4];
+    if (!shape || !tq::tc_topk_shape(variant, v))
+        return fail(TQ_ERR_INVALID_ARGUMENT, "unknown kernel variant %d", variant);
+    for (int i = 0; i < 4; ++i) shape[i] = v[i];
     return TQ_OK;
 }
 
@@ -745,6 +923,11 @@ void tq_server_destroy(tq_server *sv) {
     if (sv->worker.joinable()) sv->worker.join();
     DeviceGuard g(sv->index->device);
     for (auto &sl : sv->slots) slot_free(sl);
+    if (sv->up_stream) {
+        cudaStreamSynchronize(sv->up_stream);
+        cudaStreamDestroy(sv->up_stream);
+    }
+    if (sv->pool) cudaFree(sv->pool);
     delete sv;
 }
 

@@ -1199,8 +1199,28 @@ bool bf16_maps(TcMaps &mp, TcShape &sh, const void *Ah, const void *Al, size_t m
 
 }  // namespace
 
-int tc_topk_variants() { return 3; }
-int tc_topk_lists(int variant) { return variant == 0 ? 2 : 1; }
+// The serving top-k's tile space: {rows per CTA, codes per tile (the B tile,
+// i.e. per pipeline stage), stages, K blocks per promoted chunk}.  Every
+// variant keeps 128 query rows per CTA (the UMMA M of cta_group::1); chunks
+// stay at <= 8 K blocks, the length the exact stage's error bound assumes.
+namespace {
+constexpr int kTopkShapes[][4] = {
+    {TC_BM, TW_BN, 2, 8},  // 0: tcw_kernel, two lists per (row, slice)
+    {TC_BM, TC_BN, 3, 8},  // 1
+    {TC_BM, TC_BN, 2, 4},  // 2
+    {TC_BM, TC_BN, 3, 4},  // 3
+    {TC_BM, TC_BN, 2, 8},  // 4
+    {TC_BM, TW_BN, 2, 4},  // 5: tcw_kernel
+};
+}  // namespace
+
+int tc_topk_variants() { return (int)(sizeof(kTopkShapes) / sizeof(kTopkShapes[0])); }
+int tc_topk_lists(int variant) { return kTopkShapes[variant][1] == TW_BN ? 2 : 1; }
+bool tc_topk_shape(int variant, int out[4]) {
+    if (variant < 0 || variant >= tc_topk_variants()) return false;
+    for (int i = 0; i < 4; ++i) out[i] = kTopkShapes[variant][i];
+    return true;
+}
 
 cudaError_t launch_bounded_wait_selftest(int *err, long long budget_cycles, cudaStream_t st) {
     bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(err, budget_cycles);
@@ -1220,18 +1240,22 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
     alignas(64) TcMaps mp;
     TcShape sh{};
     if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
-    if (variant == 0) {
+    if (tc_topk_lists(variant) == 2) {
         // 128 x 256 tiles (tcw_kernel), two partial lists per (row, slice)
         if (n_pad % TW_BN) return cudaErrorInvalidValue;
         if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
             return cudaErrorInvalidValue;
         const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TW_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+        if (variant == 5) return tcw_launch<WTopk, 4>(mp, sh, ep, err, (unsigned)grid, st);
         return tcw_launch<WTopk, 8>(mp, sh, ep, err, (unsigned)grid, st);
     }
     const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
-    // asymmetric planes: 8-block chunks (see launch_tc_dist)
-    if (variant == 2) return tcp_launch<false, 2, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
-    return tcp_launch<false, 3, 8, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    switch (variant) {
+        case 2: return tcp_launch<false, 2, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+        case 3: return tcp_launch<false, 3, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+        case 4: return tcp_launch<false, 2, 8, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+        default: return tcp_launch<false, 3, 8, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    }
 }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,

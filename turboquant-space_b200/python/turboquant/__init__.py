@@ -564,5 +564,5 @@ class TurboQuantSpace:
                 f"device={self.device()})")
 
 
-from .serving import BusyError, Index, Server  # noqa: E402
+from .serving import BusyError, Index, Server, variant_shapes  # noqa: E402
 from .io import load_codes  # noqa: E402

@@ -32,7 +32,7 @@ EXPORTS = (
     "tq_distance_1_to_n_device_noalloc", "tq_distance_m_to_n_device",
     "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
     "tq_server_create", "tq_server_create_ex", "tq_server_submit", "tq_request_wait", "tq_request_done",
-    "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning",
+    "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning", "tq_server_tuning_times", "tq_topk_variant_shape",
     "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status", "tq_space_scan_timer",
     "tq_space_scan_timer_read",
     "tq_rotated_coords_batch", "tq_rotated_coords_batch_device",
@@ -50,6 +50,7 @@ class ServerStats(C.Structure):
         ("batches", C.c_uint64), ("rows", C.c_uint64), ("queued_rows", C.c_size_t),
         ("slots", C.c_int), ("max_rows", C.c_int), ("candidates", C.c_int),
         ("fallback_rows", C.c_uint64), ("bound_violations", C.c_uint64),
+        ("pool_rows", C.c_size_t), ("pool_used_rows", C.c_size_t),
     ]
 
 
@@ -57,6 +58,7 @@ class ServerParams(C.Structure):
     _fields_ = [
         ("k", C.c_int), ("max_rows", C.c_int), ("slots", C.c_int), ("kernel_variant", C.c_int),
         ("queue_rows", C.c_size_t), ("candidates", C.c_int), ("bound_scale", C.c_float),
+        ("memory_budget", C.c_size_t),
     ]
 
 
@@ -148,6 +150,11 @@ def lib() -> C.CDLL:
     L.tq_server_get_stats.argtypes = [vp, C.POINTER(ServerStats), fp, sz, C.POINTER(C.c_size_t)]
     L.tq_server_reset_stats.restype = st
     L.tq_server_reset_stats.argtypes = [vp]
+    L.tq_server_tuning_times.restype = st
+    L.tq_server_tuning_times.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]
+    L.tq_topk_variant_shape.restype = st
+    L.tq_topk_variant_shape.argtypes = [C.c_int, vp]
     L.tq_server_tuning.restype = st
     L.tq_server_tuning.argtypes = [vp, vp, vp, vp, C.c_int, C.POINTER(C.c_int)]
     L.tq_selftest_bounded_wait.restype = st

@@ -21,7 +21,7 @@ from ._capi import TQError, check, lib
 
 
 class BusyError(TQError):
-    """The server's admission refused a request (queue full)."""
+    """The server's admission refused a request (no room in its device pool)."""
 
 
 def _codes_arg(codes, cs):
@@ -74,15 +74,19 @@ class Server:
 
     candidates: rows kept by the tensor-core pass for exact rescoring (0: k + 16,
     at most 32); bound_scale: multiplier on the certificate's error bound (rows
-    it cannot certify are answered by an exact full pass over the codes)."""
+    it cannot certify are answered by an exact full pass over the codes);
+    memory_budget: device bytes of the admission pool holding the queries of
+    queued and in-flight requests (0: derived from the free device memory);
+    queue_rows: an optional cap on queued rows (0: none beyond the pool)."""
 
     def __init__(self, index, k=10, max_rows=1024, slots=2, kernel_variant=-1, queue_rows=0,
-                 candidates=0, bound_scale=0.0):
+                 candidates=0, bound_scale=0.0, memory_budget=0):
         self.index = index
         self.k = int(k)
         p = _capi.ServerParams(k=self.k, max_rows=int(max_rows), slots=int(slots),
                                kernel_variant=int(kernel_variant), queue_rows=int(queue_rows),
-                               candidates=int(candidates), bound_scale=float(bound_scale))
+                               candidates=int(candidates), bound_scale=float(bound_scale),
+                               memory_budget=int(memory_budget))
         h = C.c_void_p()
         check(lib().tq_server_create_ex(index._h, C.byref(p), C.byref(h)))
         self._h = h
@@ -112,13 +116,26 @@ class Server:
     def reset_stats(self):
         check(lib().tq_server_reset_stats(self._h))
 
-    def tuning(self):
+    def tuning(self, searched=False):
+        """The autotuner's choice per bucket; searched=True adds every variant's
+        shape and time, and whether the choice came from the process's cache."""
         rows = (C.c_int * 16)()
         var = (C.c_int * 16)()
         ms = (C.c_float * 16)()
         n = C.c_int()
         check(lib().tq_server_tuning(self._h, rows, var, ms, 16, C.byref(n)))
-        return [{"bucket_rows": rows[i], "variant": var[i], "ms": ms[i]} for i in range(n.value)]
+        out = [{"bucket_rows": rows[i], "variant": var[i], "ms": ms[i]} for i in range(n.value)]
+        if searched:
+            nb, nv, cached = C.c_int(), C.c_int(), C.c_int()
+            check(lib().tq_server_tuning_times(self._h, None, 0, C.byref(nb), C.byref(nv), C.byref(cached)))
+            times = (C.c_float * (nb.value * nv.value))()
+            check(lib().tq_server_tuning_times(self._h, times, nb.value * nv.value, C.byref(nb),
+                                               C.byref(nv), C.byref(cached)))
+            for i, b in enumerate(out):
+                b["times_ms"] = [times[i * nv.value + v] for v in range(nv.value)]
+                b["from_cache"] = bool(cached.value)
+        return out
+
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -152,8 +169,9 @@ class Index:
         self._search_server = None
 
     def serve(self, k=10, max_rows=1024, slots=2, kernel_variant=-1, queue_rows=0, candidates=0,
-              bound_scale=0.0):
-        return Server(self, k, max_rows, slots, kernel_variant, queue_rows, candidates, bound_scale)
+              bound_scale=0.0, memory_budget=0):
+        return Server(self, k, max_rows, slots, kernel_variant, queue_rows, candidates, bound_scale,
+                      memory_budget)
 
     def search(self, queries, k=10):
         """Exact top-k (ascending distance, ties to the smaller index) for each query row."""
@@ -183,3 +201,17 @@ class Index:
             self.close()
         except Exception:
             pass
+
+
+def variant_shapes():
+    """Tile shape of each top-k kernel variant: rows per CTA, codes per tile,
+    pipeline stages, K blocks per promoted chunk."""
+    out = []
+    v = 0
+    while True:
+        sh = (C.c_int * 4)()
+        if lib().tq_topk_variant_shape(v, sh) != 0:
+            return out
+        out.append({"variant": v, "rows_per_cta": sh[0], "codes_per_tile": sh[1], "stages": sh[2],
+                    "chunk_k_blocks": sh[3]})
+        v += 1
