@@ -569,7 +569,7 @@ def run_symq(args):
     }), flush=True)
 
 
-def serve_result(args, rates, window, cpu=True):
+def serve_result(args, rates, window, cpu=True, layout="planes"):
     """Serving over a device-resident corpus: 20,000,000 codes of a 1024-centre
     Gaussian mixture at dim 384 (padded 512), 4-bit; requests of m ~ U{1..256}
     queries from the same mixture ask for exact top-10; Poisson arrivals at each
@@ -601,14 +601,16 @@ def serve_result(args, rates, window, cpu=True):
     cslice = codes[:100_000].cpu().numpy() if cpu else None
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    index = space.index(codes)
+    index = space.index(codes, layout=layout)
     build_s = time.perf_counter() - t0
+    D_pad = space.padded_dim()
+    index_bytes = n * (cs + (6 * D_pad + 8 if layout == "planes" else 16))
     del codes
     torch.cuda.empty_cache()
     t0 = time.perf_counter()
     server = index.serve(k=10, max_rows=1024, slots=2, kernel_variant=args.kernel_variant)
     setup_s = time.perf_counter() - t0
-    tuning = server.tuning()
+    tuning = server.tuning(searched=True)
     rng = np.random.default_rng(9)
     results = []
     for rate in rates:
@@ -673,6 +675,7 @@ def serve_result(args, rates, window, cpu=True):
                    "window_s": window, "max_batch_rows": 1024, "slots": 2,
                    "kernel_variant": "autotuned" if args.kernel_variant < 0 else args.kernel_variant,
                    "top_k": "exact (tensor-pass candidates rescored with the reference's arithmetic)",
+                   "index_layout": layout, "index_bytes": index_bytes,
                    "data": "1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 8/9)"},
         "index_build_s": round(build_s, 2), "server_setup_s": round(setup_s, 2), "tuning": tuning,
         "results": results, "cpu_baseline": cpu_base,
@@ -681,7 +684,7 @@ def serve_result(args, rates, window, cpu=True):
 
 def run_serve(args):
     rates = [float(r) for r in args.rates.split(",")]
-    r = serve_result(args, rates, args.window, cpu=not args.no_cpu_baseline)
+    r = serve_result(args, rates, args.window, cpu=not args.no_cpu_baseline, layout=args.layout)
     print(json.dumps({"metric": METRIC, "workload": "serve", **r}), flush=True)
 
 
@@ -806,6 +809,8 @@ def main():
     ap.add_argument("--rates", default="5,20,40,60,100,150,1000,50000",
                     help="serve: request rates (req/s) to sweep")
     ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
+    ap.add_argument("--layout", choices=("planes", "codes"), default="planes",
+                    help="serve: index layout (operand planes, or codes decoded in shared memory)")
     ap.add_argument("--kernel-variant", type=int, default=-1,
                     help="serve: top-k kernel variant (-1: autotuned per batch bucket; 0: 128 x 256 "
                          "tiles; 1, 2: 128 x 128 tiles)")
@@ -1045,6 +1050,9 @@ def main():
             line["sym"] = extra(mton_result, uuid, args, True, 10, not args.no_cpu_baseline)
             line["serve"] = extra(serve_result, uuid, args, rates, args.extra_window,
                                   not args.no_cpu_baseline)
+            # the same corpus in the codes layout (tiles decoded in shared memory): one rate
+            line["serve_codes_layout"] = extra(serve_result, uuid, args, rates[-1:],
+                                               args.extra_window, False, "codes")
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

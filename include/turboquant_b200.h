@@ -293,10 +293,19 @@ typedef struct tq_server_stats {
     size_t pool_used_rows;       /* rows held by queued and in-flight requests */
 } tq_server_stats;
 
-/* Keep n codes (host or device memory) resident in HBM, with their BF16
- * tensor-core operand planes: the hi plane of 2 * padded_dim values and the
- * lo plane of the padded_dim centroid values (the sign half is exact), so
- * code_size + 6 * padded_dim + 8 bytes per code. */
+/* How an index keeps its corpus for the tensor-core pass. */
+typedef enum tq_index_layout {
+    TQ_INDEX_PLANES = 0, /* the codes plus their exact-sign hi/lo BF16 operand planes:
+                            code_size + 6 * padded_dim + 8 bytes a code; the fastest pass */
+    TQ_INDEX_CODES = 1   /* the codes plus four floats a code (code_size + 16 bytes): the pass
+                            decodes each tile of codes in shared memory (kernel variants 1..4),
+                            for corpora ~10x larger per GPU at a slower pass; padded dim >= 64 */
+} tq_index_layout;
+
+/* Keep n codes (host or device memory) resident in HBM in the given layout. */
+tq_status tq_index_create_ex(const tq_space *sp, const uint8_t *codes, size_t n, int codes_on_device,
+                             tq_index_layout layout, tq_index **out);
+/* tq_index_create_ex with TQ_INDEX_PLANES. */
 tq_status tq_index_create(const tq_space *sp, const uint8_t *codes, size_t n, int codes_on_device,
                           tq_index **out);
 void tq_index_destroy(tq_index *ix);
@@ -307,7 +316,8 @@ typedef struct tq_server_params {
     int slots;          /* batches in flight, 1..8 (fewer if they do not fit in half of the
                            free device memory) */
     int kernel_variant; /* -1: autotune the contraction's tile shape per batch-size bucket;
-                           0..5 fixed (tq_topk_variant_shape) */
+                           else fixed (tq_topk_variant_shape): 0..5 for a TQ_INDEX_PLANES
+                           index, 1..4 for TQ_INDEX_CODES */
     size_t queue_rows;  /* queued query rows beyond which submit returns TQ_ERR_BUSY
                            (0: no cap beyond the admission pool) */
     int candidates;     /* tensor-pass candidates per row that the exact stage rescores,

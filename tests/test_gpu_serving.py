@@ -62,6 +62,15 @@ def corpus(cuda_ok):
     index.close()
 
 
+@pytest.fixture(scope="module")
+def index_codes(corpus):
+    """The same corpus in the codes layout (B tiles decoded in shared memory)."""
+    space, codes, X, Q, ref, _ = corpus
+    ix = space.index(codes, layout="codes")
+    yield ix
+    ix.close()
+
+
 @pytest.mark.parametrize("k", [1, 10, 16])
 def test_index_search_is_the_stable_argsort(corpus, k):
     space, codes, X, Q, ref, index = corpus
@@ -79,6 +88,31 @@ def test_kernel_variants_give_identical_results(corpus, variant):
     _assert_exact(D, I, ref[:200], 10)
     assert st["bound_violations"] == 0
     print(f"variant {variant}: {st['fallback_rows']} of 200 rows took the exact full pass")
+
+
+@pytest.mark.parametrize("k", [1, 10, 16])
+def test_codes_layout_is_the_stable_argsort(corpus, index_codes, k):
+    space, codes, X, Q, ref, _ = corpus
+    D, I = index_codes.search(Q[:300], k=k)
+    _assert_exact(D, I, ref[:300], k)
+
+
+@pytest.mark.parametrize("variant", [2, 4])
+def test_codes_layout_variants(corpus, index_codes, variant):
+    space, codes, X, Q, ref, _ = corpus
+    with index_codes.serve(k=10, max_rows=256, slots=1, kernel_variant=variant) as sv:
+        D, I = sv.submit(Q[:200]).wait()
+        st = sv.stats()
+    _assert_exact(D, I, ref[:200], 10)
+    assert st["bound_violations"] == 0
+
+
+def test_codes_layout_refuses_planes_only_variants(corpus, index_codes):
+    # 0 and 5 need planes; 1 and 3 (three stages) leave no room for a tile of
+    # 268-byte codes in shared memory
+    for v in (0, 1, 3, 5):
+        with pytest.raises(ValueError):
+            index_codes.serve(k=10, max_rows=128, slots=1, kernel_variant=v)
 
 
 def test_same_result_alone_and_in_the_mix(corpus):
@@ -240,6 +274,40 @@ def test_autotuner_searches_the_tile_space(corpus):
         assert [b["variant"] for b in t2] == [b["variant"] for b in t]
     finally:
         ix.close()
+
+
+@pytest.mark.parametrize("layout", ["planes", "codes"])
+@pytest.mark.parametrize("dim,bits", [(256, 8), (200, 3), (1000, 2), (64, 4)])
+def test_other_widths_and_degenerate_codes(cuda_ok, dim, bits, layout):
+    """Byte and nibble codes of other widths, with zero rows and a row equal to a
+    query among them (zero gamma: the sign half left out of the tensor pass)."""
+    rng = np.random.default_rng(dim + bits)
+    X = rng.standard_normal((9_000, dim)).astype(np.float32)
+    X[::97] = 0.0
+    Q = rng.standard_normal((40, dim)).astype(np.float32)
+    X[5] = Q[0]
+    space = tq.TurboQuantSpace(dim, bits)
+    codes = space.encode_batch(X)
+    want = O.OracleSpace(dim, bits).distance_m_to_n(Q, codes)
+    ix = space.index(codes, layout=layout)
+    try:
+        with ix.serve(k=10, max_rows=128, slots=1) as sv:
+            D, I = sv.submit(Q).wait()
+            st = sv.stats()
+        _assert_exact(D, I, want, 10)
+        assert st["bound_violations"] == 0
+    finally:
+        ix.close()
+
+
+@pytest.mark.parametrize("dim,bits", [(32, 4), (1024, 8)])
+def test_codes_layout_refused_where_it_cannot_run(cuda_ok, dim, bits):
+    """Padded dims below 64, and codes whose 128-code tile does not fit in
+    shared memory beside two pipeline stages (1036-byte codes)."""
+    space = tq.TurboQuantSpace(dim, bits)
+    codes = space.encode_batch(np.ones((10, dim), np.float32))
+    with pytest.raises(tq.TQError):
+        space.index(codes, layout="codes")
 
 
 def test_fewer_codes_than_k(cuda_ok):

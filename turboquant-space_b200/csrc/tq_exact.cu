@@ -50,8 +50,9 @@ constexpr float kDegenerateG = 1e-20f;
 
 __device__ __forceinline__ float sgn_s(float s, unsigned bit) { return bit ? s : -s; }
 
+// A 32-bit word of a code in global or shared memory (generic load).
 __device__ __forceinline__ uint32_t ld_u32(const uint8_t *p, bool al4) {
-    if (al4) return __ldg(reinterpret_cast<const unsigned int *>(p));
+    if (al4) return *reinterpret_cast<const unsigned int *>(p);
     return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
 
@@ -391,7 +392,7 @@ struct FallbackArgs {
     const float *q_rot, *s_q, *norms;
     const uint8_t *codes;
     size_t n;
-    bool al4;
+    bool al16;  // codes 16-byte aligned
     const int *fail_rows, *counters;
     float *part_d;
     int *part_i;
@@ -400,18 +401,23 @@ struct FallbackArgs {
 };
 
 // Exact top-k by a full pass over the codes for each row the certificate did
-// not settle: each thread keeps a sorted list of its codes, the warps merge
-// their lanes' lists and warp 0 merges the block's into part[row][cta].
+// not settle.  A CTA stages chunks of `chunk` consecutive codes in shared
+// memory with coalesced 16-byte loads, then each thread scores the codes of
+// the chunk it owns from there (a code's words are cs / 4 apart, an odd
+// stride: no bank conflicts) and keeps a sorted list; the warps merge their
+// lanes' lists and warp 0 merges the block's into part[row][cta].
 template <bool NIBBLE>
-__global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a) {
+__global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a, int chunk) {
     const int nf = a.counters[kCntFallbackRows];
     if (nf == 0) return;
+    extern __shared__ __align__(16) unsigned char fsm[];
     __shared__ float sc[kMaxLevels];
     __shared__ float wd[8][kTopKMax];
     __shared__ int wi[8][kTopKMax];
     load_centroids(sc, a.centroids, a.P.levels);
     const int D = a.P.D, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int k = a.k;
+    const int k = a.k, cs = a.P.cs;
+    const bool al4 = (cs & 3) == 0;
     for (int f = 0; f < nf; ++f) {
         const int row = a.fail_rows[f];
         const float *q = a.q_rot + (size_t)row * D, *s = a.s_q + (size_t)row * D;
@@ -425,10 +431,25 @@ __global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a) {
         }
         float td = INFINITY;
         int ti = kNoIdx;
-        for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.n;
-             j += (size_t)gridDim.x * blockDim.x) {
-            const float d = exact_dist<NIBBLE>(a.P, sc, q, s, qn2, qn, a.codes + j * a.P.cs, a.al4);
-            if (better(d, (int)j, td, ti)) list_insert(bd, bi, k, d, (int)j, &td, &ti);
+        for (size_t c0 = (size_t)blockIdx.x * chunk; c0 < a.n; c0 += (size_t)gridDim.x * chunk) {
+            const int rows = (int)(a.n - c0 < (size_t)chunk ? a.n - c0 : (size_t)chunk);
+            const size_t bytes = (size_t)rows * cs;
+            const uint8_t *src = a.codes + c0 * cs;
+            __syncthreads();  // the previous chunk is scored
+            if (a.al16) {
+                const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+                uint4 *d4 = reinterpret_cast<uint4 *>(fsm);
+                for (size_t i = threadIdx.x; i < bytes / 16; i += blockDim.x) d4[i] = __ldg(s4 + i);
+                for (size_t i = (bytes & ~size_t(15)) + threadIdx.x; i < bytes; i += blockDim.x) fsm[i] = src[i];
+            } else {
+                for (size_t i = threadIdx.x; i < bytes; i += blockDim.x) fsm[i] = src[i];
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+                const int j = (int)(c0 + (size_t)i);
+                const float d = exact_dist<NIBBLE>(a.P, sc, q, s, qn2, qn, fsm + (size_t)i * cs, al4);
+                if (better(d, j, td, ti)) list_insert(bd, bi, k, d, j, &td, &ti);
+            }
         }
         float md;
         int mi;
@@ -592,13 +613,20 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
                             int *part_i, float *out_d, long long *out_i, int max_rows,
                             cudaStream_t st) {
     if (k < 1 || k > kTopKMax || fb_ctas < 1 || max_rows < 1) return cudaErrorInvalidValue;
+    // chunks start chunk * cs bytes apart, a multiple of 64: 16-byte aligned with the base
+    const bool al16 = (reinterpret_cast<uintptr_t>(codes) & 15) == 0;
     const FallbackArgs a{P,     centroids, k,         q_rot,    s_q,    norms,  codes, n,
-                         codes_al4(P, codes), fail_rows, counters, part_d, part_i, out_d, out_i};
-    if (P.nibble)
-        fallback_scan_kernel<true><<<fb_ctas, 256, 0, st>>>(a);
-    else
-        fallback_scan_kernel<false><<<fb_ctas, 256, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+                         al16, fail_rows, counters, part_d, part_i, out_d, out_i};
+    // codes per staged chunk: up to 256, at most 96 KB of shared memory, a
+    // multiple of 16 so that every chunk starts 16-byte aligned
+    int chunk = (int)std::min<size_t>(256, (size_t)(96 * 1024) / (size_t)P.cs) & ~15;
+    if (chunk < 16) chunk = 16;
+    const size_t smem = (size_t)chunk * P.cs;
+    auto kern = P.nibble ? fallback_scan_kernel<true> : fallback_scan_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<fb_ctas, 256, smem, st>>>(a, chunk);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     fallback_merge_kernel<<<(unsigned)((max_rows + 7) / 8), 256, 0, st>>>(
         counters, fail_rows, fb_ctas, k, part_d, part_i, out_d, out_i);

@@ -27,6 +27,8 @@
 // correction term is below 1e-18 of |q| |x| and is left out.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "tq_internal.h"
 #include "tq_mton.h"
 
@@ -110,6 +112,45 @@ __global__ void __launch_bounds__(256) planes_from_codes_kernel(
             s1[r] = sym ? __fmul_rn(sigma, norm) : ratio ? __fmul_rn(sg, norm) : norm;
             s2[r] = __fmul_rn(norm, norm);
         }
+    }
+}
+
+// Scalars of the decoded-B kernels (launch_dec_factors): the same per-code
+// quantities as the planes' s1 / s2 and exact-sign ratio, with the ratio as a
+// chunk factor instead of a division of every value.
+__global__ void __launch_bounds__(256) dec_factors_kernel(const uint8_t *__restrict__ codes,
+                                                          size_t rows, size_t rows_pad, Params P,
+                                                          int sym, float *__restrict__ c1,
+                                                          float *__restrict__ c2,
+                                                          float *__restrict__ fc,
+                                                          float *__restrict__ fs) {
+    for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows_pad;
+         r += (size_t)gridDim.x * blockDim.x) {
+        float a = 0.0f, b = 0.0f, f = 0.0f, g1 = 0.0f;
+        if (r < rows) {
+            const uint8_t *t = codes + r * (size_t)P.cs + P.pb;
+            float meta[3];
+            for (int q = 0; q < 3; ++q) {
+                uint32_t w = 0;
+                for (int k = 0; k < 4; ++k) w |= (uint32_t)t[4 * q + k] << (8 * k);
+                meta[q] = __uint_as_float(w);
+            }
+            const float norm = meta[0], gamma = meta[1], sigma = meta[2];
+            b = __fmul_rn(norm, norm);
+            if (sym) {
+                a = __fmul_rn(sigma, norm);
+            } else {
+                const float sg = __fmul_rn(P.scale, gamma);
+                const bool ratio = sg >= 1e-20f && sg <= 3.0e38f;  // as the exact-sign planes
+                a = ratio ? __fmul_rn(sg, norm) : norm;
+                f = ratio ? __fdiv_rn(sigma, sg) : sigma;
+                g1 = ratio ? 1.0f : 0.0f;
+            }
+        }
+        c1[r] = a;
+        c2[r] = b;
+        if (fc) fc[r] = f;
+        if (fs) fs[r] = g1;
     }
 }
 
@@ -243,6 +284,15 @@ cudaError_t launch_planes_from_codes(const Params &P, const DevTables &T, const 
     const int ldl = (!sym && fmt == kPlaneBF16) ? asym_lo_width(P.D) : K;
     planes_from_codes_kernel<<<grid_for(rows_pad * (K / 4), 256), 256, 0, st>>>(
         codes, rows, rows_pad, P, T, sym ? 1 : 0, fmt, ldl, plane0, plane1, s1, s2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dec_factors(const Params &P, const uint8_t *codes, size_t rows, size_t rows_pad,
+                               bool sym, float *c1, float *c2, float *fc, float *fs, cudaStream_t st) {
+    if (rows_pad == 0) return cudaSuccess;
+    const size_t blocks = std::min<size_t>((rows_pad + 255) / 256, 148 * 16);
+    dec_factors_kernel<<<(unsigned)blocks, 256, 0, st>>>(codes, rows, rows_pad, P, sym ? 1 : 0, c1, c2,
+                                                          fc, fs);
     return cudaGetLastError();
 }
 

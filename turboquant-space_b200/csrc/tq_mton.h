@@ -51,6 +51,36 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
 // (row, slice); 1-4: 128 x 128 tiles (tc_topk_shape gives each one's stages
 // and chunk length).  The partial buffers
 // hold grid * 128 * tc_topk_lists(variant) * kCandMax entries.
+// The column operand of the decoded-B tensor kernels: instead of BF16 planes,
+// four decoder warps per CTA write each K block's B tile into shared memory
+// straight from the codes (a centroid block as the hi/lo pair of the table
+// value c[idx], a sign block as the exact +-1), and the per-code scale of the
+// asymmetric form is applied per column when a chunk is promoted: fc for the
+// centroid half (sigma / (scale gamma), or sigma), fs for the sign half (1, or
+// 0 for a code whose sign half is left out), as launch_dec_factors computes
+// them; c1 / c2 of the epilogue come from the same kernel.
+struct DecSrc {
+    const uint8_t *codes = nullptr;      // column codes, cs bytes apart, 16-byte aligned base,
+                                         // readable up to 15 bytes past the last code
+    unsigned n = 0;                      // columns; tile columns at or past n decode to zero
+    int cs = 0;                          // code bytes (a multiple of 4)
+    int nibble = 0;                      // two units per byte (bits <= 4)
+    int kbc = 0;                         // K blocks (64 values) of the centroid half
+    const float *fc = nullptr, *fs = nullptr;  // per-column factors (asymmetric); null: none
+    const float *centroids = nullptr;    // the space's centroid table (device)
+    int levels = 0;
+    // set by the launcher: shared-memory buffers of one tile of codes (128 codes,
+    // one bulk copy each) and their size
+    int cbufs = 0, ctile_bytes = 0;
+};
+
+// Per-code scalars of the decoded-B kernels for rows [0, rows) of `codes`
+// (zero for rows up to rows_pad): asymmetric: c1 = scale gamma |x| (or |x|),
+// c2 = |x|^2, fc, fs as above; symmetric: c1 = sigma |x|, c2 = |x|^2 (fc, fs
+// may be null).
+cudaError_t launch_dec_factors(const Params &P, const uint8_t *codes, size_t rows, size_t rows_pad,
+                               bool sym, float *c1, float *c2, float *fc, float *fs, cudaStream_t st);
+
 constexpr int kTopKMax = 16;   // results per row (k) of the serving path
 constexpr int kCandMax = 32;   // list length of the tensor-core top-k (candidates per row)
 constexpr int kTopKListsMax = 2;
@@ -64,6 +94,15 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
                            size_t n, const float *r1, const float *r2, const float *c1,
                            const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
                            cudaStream_t st);
+// The same top-k with decoded B tiles (variants 1-4, the 128 x 128 tiles; no
+// planes of the columns).  K = 2D; dec.kbc = D / 64.
+cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size_t rows_pad,
+                               const DecSrc &dec, size_t n_pad, int K, const int *m_dev, size_t n,
+                               const float *r1, const float *r2, const float *c1, const float *c2,
+                               int k, float *part_d, int *part_i, int *err, int grid, cudaStream_t st);
+// Whether `variant` runs with decoded B tiles for codes of cs bytes (a tile of
+// 128 codes must fit in shared memory beside the variant's stages).
+bool tc_topk_dec_ok(int variant, int cs);
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,
                               const int *part_i, int k, size_t max_rows, float *out_d,
                               long long *out_i, cudaStream_t st);

@@ -3,12 +3,18 @@
 // The reference has no index or serving loop (README.md:81-83); this is the
 // north-star serving path built on the same distance contraction:
 //
-//   tq_index   the corpus decoded once into hi/lo BF16 planes
-//              B[j] = [sigma_j c[idx_j] | scale gamma_j (+-1)_j] (K = 2D) plus
-//              |x_j| and |x_j|^2, resident in HBM.
+//   tq_index   the corpus itself resident in HBM (the exact stages read it)
+//              and, by layout:
+//              TQ_INDEX_PLANES: the codes decoded once into exact-sign hi/lo
+//                BF16 planes B[j] = [sigma_j c[idx_j] / g_j | (+-1)_j] (K = 2D;
+//                6 D + 8 more bytes a code) with c1 = g |x| and c2 = |x|^2;
+//              TQ_INDEX_CODES: four floats a code (c1, c2 and the chunk
+//                factors fc, fs of launch_dec_factors); the tensor pass decodes
+//                each B tile in shared memory from the codes.
 //   slot       buffers for one batch of up to `max_rows` query rows and one CUDA
 //              graph per row bucket (128, 256, 512, ... max_rows) capturing
-//              H2D queries -> prepareQuery -> query planes -> tcgen05 top-k ->
+//              rows gathered from the pool -> prepareQuery -> query planes ->
+//              tcgen05 candidates (B decoded in shared memory) ->
 //              merge -> D2H results; the kernels read the batch's row count
 //              from device memory, so the graph replays for any batch size.
 //   server     a scheduler thread.  Requests are queued on submit; whenever a
@@ -59,9 +65,11 @@ struct tq_index {
     tq_space *sp = nullptr;
     size_t n = 0, n_pad = 0;
     int K = 0;
-    int K_lo = 0;            // columns of the lo plane (tq::asym_lo_width)
-    void *planes = nullptr;  // hi plane n_pad x K, then lo plane n_pad x K_lo, BF16
-    float *c1 = nullptr, *c2 = nullptr;
+    int layout = TQ_INDEX_PLANES;
+    int K_lo = 0;             // PLANES: columns of the lo plane (tq::asym_lo_width)
+    void *block = nullptr;    // one allocation: [planes], c1, c2, [fc, fs], codes, bound
+    void *planes = nullptr;   // PLANES: hi plane n_pad x K, then lo plane n_pad x K_lo, BF16
+    float *c1 = nullptr, *c2 = nullptr, *fc = nullptr, *fs = nullptr;
     uint8_t *codes = nullptr;  // the corpus itself (n x code_size), for the exact stages
     float *bound = nullptr;    // kBoundFloats index-wide maxima of the error bound
     float cmax = 0.0f;         // max |centroid|
@@ -165,6 +173,13 @@ struct tq_server {
 
 namespace {
 
+// Kernel variants that serve an index layout: any for planes, the decoded-B
+// ones for codes.
+bool variant_fits(const tq_index *ix, int v) {
+    return ix->layout == TQ_INDEX_CODES ? tq::tc_topk_dec_ok(v, (int)ix->sp->code_size)
+                                        : (v >= 0 && v < tq::tc_topk_variants());
+}
+
 int bucket_index(const tq_server *sv, size_t rows) {
     const auto &b = sv->slots[0].bucket_rows;
     for (size_t i = 0; i < b.size(); ++i)
@@ -238,12 +253,28 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     e = tq::launch_planes_from_prepared(q_rot, s_q, norms, rows_cap, rows_cap, (int)D, tq::kPlaneBF16,
                                         ah, al, sl.d_r1, sl.d_r2, st);
     if (e != cudaSuccess) return e;
-    unsigned char *bh = static_cast<unsigned char *>(ix->planes);
-    unsigned char *bl = bh + ix->n_pad * K * 2;
     // tensor-core pass: each row's kc best candidates by approximate distance
-    e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
-                           sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
-                           sv->grid, st);
+    if (ix->layout == TQ_INDEX_PLANES) {
+        unsigned char *bh = static_cast<unsigned char *>(ix->planes);
+        unsigned char *bl = bh + ix->n_pad * K * 2;
+        e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
+                               sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
+                               sv->grid, st);
+    } else {  // the column tiles decoded in shared memory from the codes
+        tq::DecSrc dec;
+        dec.codes = ix->codes;
+        dec.n = (unsigned)ix->n;
+        dec.cs = (int)sp->code_size;
+        dec.nibble = sp->P.nibble;
+        dec.kbc = (int)(D / 64);
+        dec.fc = ix->fc;
+        dec.fs = ix->fs;
+        dec.centroids = sp->T.centroids;
+        dec.levels = sp->levels;
+        e = tq::launch_tc_topk_dec(var, ah, al, rows_cap, dec, ix->n_pad, (int)K, sl.d_m, ix->n,
+                                   sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
+                                   sv->grid, st);
+    }
     if (e != cudaSuccess) return e;
     e = tq::launch_topk_merge(sl.d_m, sv->grid, tq::tc_topk_lists(var), sl.d_pd, sl.d_pi, sv->kc,
                               rows_cap, sl.d_cd, sl.d_ci, st);
@@ -362,11 +393,11 @@ void slot_free(Slot &sl) {
 // candidates, slots tuned together, bucket rows): the fastest variant and its
 // time.  A server whose key is present skips timing that bucket.
 struct TuneKey {
-    int device, D, bits, kc, ns, rows;
+    int device, D, bits, kc, ns, rows, layout;
     size_t n;
     bool operator<(const TuneKey &o) const {
-        return std::tie(device, D, bits, kc, ns, rows, n) <
-               std::tie(o.device, o.D, o.bits, o.kc, o.ns, o.rows, o.n);
+        return std::tie(device, D, bits, kc, ns, rows, layout, n) <
+               std::tie(o.device, o.D, o.bits, o.kc, o.ns, o.rows, o.layout, o.n);
     }
 };
 std::mutex g_tune_mu;
@@ -377,12 +408,12 @@ tq_status autotune(tq_server *sv, int fixed_variant) {
     Slot &s0 = sv->slots[0];
     const int nb = (int)s0.bucket_rows.size();
     const int nv = tq::tc_topk_variants();
-    sv->bucket_variant.assign(nb, fixed_variant >= 0 ? fixed_variant : 0);
+    sv->bucket_variant.assign(nb, fixed_variant >= 0 ? fixed_variant : 4);  // 4 fits both layouts
     sv->bucket_ms.assign(nb, 0.0);
     sv->tune_ms.assign((size_t)nb * nv, 0.0f);
     const tq_index *ix = sv->index;
     auto key_of = [&](int rows) {
-        return TuneKey{ix->device, (int)ix->sp->D, ix->sp->bits, sv->kc, ns, rows, ix->n};
+        return TuneKey{ix->device, (int)ix->sp->D, ix->sp->bits, sv->kc, ns, rows, ix->layout, ix->n};
     };
     if (fixed_variant < 0) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -429,6 +460,7 @@ tq_status autotune(tq_server *sv, int fixed_variant) {
         double best = 1e30;
         for (int v = 0; v < nv; ++v) {
             if (fixed_variant >= 0 && v != fixed_variant) continue;
+            if (!variant_fits(sv->index, v)) continue;
             TQ_CUDA(enqueue_batch(sv, s0, rows, v, false), "autotune warm-up");
             TQ_CUDA(cudaEventRecord(e0, s0.stream), "event");
             for (int si = 1; si < ns; ++si)
@@ -589,57 +621,78 @@ void worker_loop(tq_server *sv) {
 
 extern "C" {
 
-tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n,
-                          int codes_on_device, tq_index **out) {
+tq_status tq_index_create_ex(const tq_space *csp, const uint8_t *codes, size_t n, int codes_on_device,
+                             tq_index_layout layout, tq_index **out) {
     if (!out) return fail(TQ_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     tq_status st = tq::need_device(csp);
     if (st != TQ_OK) return st;
     if (n == 0 || !codes) return fail(TQ_ERR_INVALID_ARGUMENT, "index: empty corpus");
     if (n > 0x7ffffff0ull) return fail(TQ_ERR_INVALID_ARGUMENT, "index: more than 2^31 codes");
+    if (layout != TQ_INDEX_PLANES && layout != TQ_INDEX_CODES)
+        return fail(TQ_ERR_INVALID_ARGUMENT, "index: unknown layout %d", (int)layout);
     auto *sp = const_cast<tq_space *>(csp);
     const size_t K = 2 * sp->D;
-    if (K % 64) return fail(TQ_ERR_NOT_SUPPORTED, "index: padded dim must be a multiple of 32");
+    if (layout == TQ_INDEX_PLANES && K % 64)
+        return fail(TQ_ERR_NOT_SUPPORTED, "index: padded dim must be a multiple of 32");
+    if (layout == TQ_INDEX_CODES && (sp->D < 64 || sp->code_size % 4))
+        return fail(TQ_ERR_NOT_SUPPORTED, "index: the codes layout needs a padded dim of at least 64");
+    if (layout == TQ_INDEX_CODES && !tq::tc_topk_dec_ok(4, (int)sp->code_size))
+        return fail(TQ_ERR_NOT_SUPPORTED,
+                    "index: a tile of 128 codes of %zu bytes does not fit in shared memory; use the "
+                    "planes layout", sp->code_size);
     DeviceGuard g(sp->device);
     auto *ix = new tq_index();
     ix->sp = sp;
     ix->n = n;
     ix->n_pad = round_up(n, 256);
     ix->K = (int)K;
-    ix->K_lo = tq::asym_lo_width((int)sp->D);
+    ix->layout = layout;
     ix->device = sp->device;
     for (float c : sp->centroids) ix->cmax = std::max(ix->cmax, std::fabs(c));
-    const size_t plane_hi = ix->n_pad * K * 2, plane_lo = ix->n_pad * (size_t)ix->K_lo * 2;
+    const bool planes = layout == TQ_INDEX_PLANES;
+    ix->K_lo = planes ? tq::asym_lo_width((int)sp->D) : 0;
+    const size_t plane_bytes = planes ? ix->n_pad * (K + (size_t)ix->K_lo) * 2 : 0;
     const size_t code_bytes = round_up(n * sp->code_size, 256);
-    cudaError_t e = cudaMalloc(&ix->planes, plane_hi + plane_lo + 2 * ix->n_pad * 4 + code_bytes +
-                                                tq::kBoundFloats * 4 + 256);
+    const size_t nscal = planes ? 2 : 4;  // c1, c2 (+ fc, fs)
+    cudaError_t e = cudaMalloc(&ix->block, plane_bytes + nscal * ix->n_pad * 4 + code_bytes +
+                                               tq::kBoundFloats * 4 + 256);
     if (e != cudaSuccess) {
         delete ix;
         return cuda_fail(e, "cudaMalloc(index)");
     }
-    auto *hi = static_cast<unsigned char *>(ix->planes);
-    auto *lo = hi + plane_hi;
-    ix->c1 = reinterpret_cast<float *>(lo + plane_lo);
+    auto *base = static_cast<unsigned char *>(ix->block);
+    ix->planes = planes ? base : nullptr;
+    ix->c1 = reinterpret_cast<float *>(base + plane_bytes);
     ix->c2 = ix->c1 + ix->n_pad;
-    ix->codes = reinterpret_cast<uint8_t *>(ix->c2 + ix->n_pad);
+    if (!planes) {
+        ix->fc = ix->c2 + ix->n_pad;
+        ix->fs = ix->fc + ix->n_pad;
+    }
+    ix->codes = reinterpret_cast<uint8_t *>(ix->c1 + nscal * ix->n_pad);
     ix->bound = reinterpret_cast<float *>(ix->codes + code_bytes);
-    // the corpus itself stays resident (the exact stages read it); the planes
-    // are decoded from that copy
     e = cudaMemcpy(ix->codes, codes, n * sp->code_size,
                    codes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
-    const size_t chunk = 1 << 20;
-    for (size_t r0 = 0; r0 < ix->n_pad && e == cudaSuccess; r0 += chunk) {
-        const size_t rows_pad = std::min(chunk, ix->n_pad - r0);
-        const size_t rows = r0 < n ? std::min(rows_pad, n - r0) : 0;
-        e = tq::launch_planes_from_codes(sp->P, sp->T, ix->codes + std::min(r0, n - 1) * sp->code_size,
-                                         rows, rows_pad, false, tq::kPlaneBF16, hi + r0 * K * 2,
-                                         lo + r0 * (size_t)ix->K_lo * 2, ix->c1 + r0, ix->c2 + r0,
-                                         nullptr);
+    if (planes) {
+        auto *hi = static_cast<unsigned char *>(ix->planes);
+        auto *lo = hi + ix->n_pad * K * 2;
+        const size_t chunk = 1 << 20;
+        for (size_t r0 = 0; r0 < ix->n_pad && e == cudaSuccess; r0 += chunk) {
+            const size_t rows_pad = std::min(chunk, ix->n_pad - r0);
+            const size_t rows = r0 < n ? std::min(rows_pad, n - r0) : 0;
+            e = tq::launch_planes_from_codes(sp->P, sp->T, ix->codes + std::min(r0, n - 1) * sp->code_size,
+                                             rows, rows_pad, false, tq::kPlaneBF16, hi + r0 * K * 2,
+                                             lo + r0 * (size_t)ix->K_lo * 2, ix->c1 + r0, ix->c2 + r0,
+                                             nullptr);
+        }
+    } else if (e == cudaSuccess) {
+        e = tq::launch_dec_factors(sp->P, ix->codes, n, ix->n_pad, false, ix->c1, ix->c2, ix->fc, ix->fs,
+                                   nullptr);
     }
     if (e == cudaSuccess) e = tq::launch_index_bound(sp->P, ix->codes, n, ix->bound, nullptr);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
-        cudaFree(ix->planes);
+        cudaFree(ix->block);
         delete ix;
         return cuda_fail(e, "index build");
     }
@@ -647,10 +700,15 @@ tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n,
     return TQ_OK;
 }
 
+tq_status tq_index_create(const tq_space *csp, const uint8_t *codes, size_t n, int codes_on_device,
+                          tq_index **out) {
+    return tq_index_create_ex(csp, codes, n, codes_on_device, TQ_INDEX_PLANES, out);
+}
+
 void tq_index_destroy(tq_index *ix) {
     if (!ix) return;
     DeviceGuard g(ix->device);
-    if (ix->planes) cudaFree(ix->planes);
+    if (ix->block) cudaFree(ix->block);
     delete ix;
 }
 
@@ -666,7 +724,9 @@ tq_status tq_server_create_ex(tq_index *ix, const tq_server_params *prm, tq_serv
     if (!(prm->bound_scale >= 0.0f)) return fail(TQ_ERR_INVALID_ARGUMENT, "bound_scale must be >= 0");
     if (max_rows < 128 || max_rows % 128) return fail(TQ_ERR_INVALID_ARGUMENT, "max_rows must be a positive multiple of 128");
     if (slots < 1 || slots > 8) return fail(TQ_ERR_INVALID_ARGUMENT, "slots must be in 1..8");
-    if (kernel_variant >= tq::tc_topk_variants()) return fail(TQ_ERR_INVALID_ARGUMENT, "unknown kernel variant");
+    if (kernel_variant >= 0 && !variant_fits(ix, kernel_variant))
+        return fail(TQ_ERR_INVALID_ARGUMENT, "kernel variant %d does not serve this index layout",
+                    kernel_variant);
     DeviceGuard g(ix->device);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);

@@ -60,8 +60,13 @@ constexpr int TC_B_BYTES = TC_BN * 128;  // 16 KB
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // 64 KB
 constexpr int TC_TMEM_COLS = 512;
 // threads: producer, MMA and 4 epilogue warps; plus 4 finalize warps when the
-// running sum is double-buffered (one K segment)
-constexpr int tc_threads(bool split) { return split ? 320 : 192; }
+// running sum is double-buffered (one K segment); plus 4 decoder warps when the
+// B tiles are decoded from codes in shared memory (DEC)
+constexpr int tc_threads(bool split, bool dec = false) { return (split ? 320 : 192) + (dec ? 128 : 0); }
+// shared bytes after the stages: barriers and the tensor-memory slot; the DEC
+// kernels' decode tables follow (tabc: 256 x 8 B, tabs: 256 x 4 B)
+constexpr int TC_BAR_BYTES = 256;
+constexpr int TC_DEC_TAB_BYTES = 256 * 8 + 256 * 4;
 // error codes written to *err
 constexpr int kErrFull = 1, kErrEmpty = 2, kErrTmemFull = 3, kErrTmemEmpty = 4;
 
@@ -202,6 +207,14 @@ struct TcShape {
     int KB[2], kbx[2], a_exact[2], whole[2];
 };
 
+// End of the promoted chunk that starts at K block c0: CH blocks, the
+// segment's end, or the end of the centroid half (DEC, asymmetric).
+__device__ __forceinline__ int chunk_end(int c0, int chl, int KB, int kbc) {
+    int c1 = c0 + chl < KB ? c0 + chl : KB;
+    if (c0 < kbc && c1 > kbc) c1 = kbc;
+    return c1;
+}
+
 // ---------------------------------------------------------------------------
 // The pipeline.  Epi supplies the tile schedule (tiles(), tile_at()) and the
 // epilogue State (tile() reads the running sums Y0 / Y1 of a finished tile,
@@ -212,11 +225,12 @@ struct TcShape {
 // for Y[t & 1] to be read ("yempty") and signal it complete ("yfull").
 // Otherwise (two segments, Y0 and Y1 per tile) warps 2..5 do both.
 // ---------------------------------------------------------------------------
-template <bool TF32, int STAGES, int CH, bool SPLIT, class Epi>
-__global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_constant__ TcMaps maps,
-                                                                   const TcShape sh,
-                                                                   const typename Epi::Params ep,
-                                                                   int *err) {
+template <bool TF32, int STAGES, int CH, bool SPLIT, class Epi, bool DEC = false>
+__global__ void __launch_bounds__(tc_threads(SPLIT, DEC), 1) tcp_kernel(const __grid_constant__ TcMaps maps,
+                                                                        const TcShape sh,
+                                                                        const typename Epi::Params ep,
+                                                                        int *err, const DecSrc dec) {
+    static_assert(!DEC || (!TF32 && SPLIT), "decoded B tiles: BF16, one K segment");
     constexpr int KBLK = TF32 ? SQ_TBK : TC_BK;  // values per K block
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles
@@ -224,7 +238,9 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * TC_STAGE_BYTES);
     // bars: full[STAGES], empty[STAGES], xfull[2], xempty[2], drain, yfull[2],
     // yempty[2]; then the TMEM slot
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 9);
+    // DEC: cfull[2], cempty[2] (code tile buffers) follow; then the TMEM slot
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 9 + (DEC ? 4 : 0));
+    const uint32_t cfull0 = smem_u32(bars + 2 * STAGES + 9), cempty0 = cfull0 + 16;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
     const uint32_t xfull0 = smem_u32(bars + 2 * STAGES), xempty0 = smem_u32(bars + 2 * STAGES + 2);
@@ -232,7 +248,7 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
     const uint32_t yfull0 = smem_u32(bars + 2 * STAGES + 5), yempty0 = smem_u32(bars + 2 * STAGES + 7);
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(full0 + 8 * s, 1);
+            mbar_init(full0 + 8 * s, DEC ? 1 + 128 : 1);  // DEC: the producer and 128 decoders
             mbar_init(empty0 + 8 * s, 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -242,6 +258,12 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
             mbar_init(yempty0 + 8 * b, 128);
         }
         mbar_init(drain, 1);
+        if constexpr (DEC) {
+            for (int b = 0; b < 2; ++b) {
+                mbar_init(cfull0 + 8 * b, 1);
+                mbar_init(cempty0 + 8 * b, 128);
+            }
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -250,6 +272,33 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
                      "r"(TC_TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // DEC decode tables: nibble codes: tabc[byte] = {hi pair, lo pair} of its
+    // two units' centroids, tabs[byte] = their +-1 pair; byte codes: tabc as
+    // 256 words hi | lo << 16 of c[u >> 1].
+    uint2 *tabc = reinterpret_cast<uint2 *>(smem + STAGES * TC_STAGE_BYTES + TC_BAR_BYTES);
+    uint32_t *tabs = reinterpret_cast<uint32_t *>(tabc + 256);
+    if constexpr (DEC) {
+        auto cpair = [&](unsigned u, uint32_t &h, uint32_t &l) {
+            const unsigned v = u >> 1;
+            const float c = v < (unsigned)dec.levels ? dec.centroids[v] : 0.0f;
+            const __nv_bfloat16 hb = __float2bfloat16_rn(c);
+            const __nv_bfloat16 lb = __float2bfloat16_rn(c - __bfloat162float(hb));
+            h = __bfloat16_as_ushort(hb);
+            l = __bfloat16_as_ushort(lb);
+        };
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+            uint32_t h0, l0, h1, l1;
+            if (dec.nibble) {
+                cpair(i & 15, h0, l0);
+                cpair(i >> 4, h1, l1);
+                tabc[i] = make_uint2(h0 | (h1 << 16), l0 | (l1 << 16));
+                tabs[i] = ((i & 1) ? 0x3F80u : 0xBF80u) | (((i & 16) ? 0x3F80u : 0xBF80u) << 16);
+            } else {
+                cpair(i, h0, l0);
+                reinterpret_cast<uint32_t *>(tabc)[i] = h0 | (l0 << 16);
+            }
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -274,12 +323,18 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
                         const bool blo = kb < sh.kbx[sg];
                         const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
                         const uint32_t fb = full0 + 8 * s;
-                        mbar_expect_tx(fb, (alo ? 2 : 1) * TC_A_BYTES + (blo ? 2 : 1) * TC_B_BYTES);
                         const int kx = kb * KBLK;
-                        tma_load_2d(base, &mp[0], kx, mb * TC_BM, fb);
-                        if (alo) tma_load_2d(base + TC_A_BYTES, &mp[1], kx, mb * TC_BM, fb);
-                        tma_load_2d(base + 2 * TC_A_BYTES, &mp[2], kx, nb * TC_BN, fb);
-                        if (blo) tma_load_2d(base + 2 * TC_A_BYTES + TC_B_BYTES, &mp[3], kx, nb * TC_BN, fb);
+                        if constexpr (DEC) {  // B comes from the decoder warps
+                            mbar_expect_tx(fb, (alo ? 2 : 1) * TC_A_BYTES);
+                            tma_load_2d(base, &mp[0], kx, mb * TC_BM, fb);
+                            if (alo) tma_load_2d(base + TC_A_BYTES, &mp[1], kx, mb * TC_BM, fb);
+                        } else {
+                            mbar_expect_tx(fb, (alo ? 2 : 1) * TC_A_BYTES + (blo ? 2 : 1) * TC_B_BYTES);
+                            tma_load_2d(base, &mp[0], kx, mb * TC_BM, fb);
+                            if (alo) tma_load_2d(base + TC_A_BYTES, &mp[1], kx, mb * TC_BM, fb);
+                            tma_load_2d(base + 2 * TC_A_BYTES, &mp[2], kx, nb * TC_BN, fb);
+                            if (blo) tma_load_2d(base + 2 * TC_A_BYTES + TC_B_BYTES, &mp[3], kx, nb * TC_BN, fb);
+                        }
                     }
                 }
             }
@@ -298,12 +353,13 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
                 for (int sg = 0; sg < sh.nseg && ok; ++sg) {
                     const bool alo = !sh.a_exact[sg];
                     const int chl = sh.whole[sg] ? sh.KB[sg] : CH;
-                    for (int c0 = 0; c0 < sh.KB[sg] && ok; c0 += chl, ++gc) {
+                    const int kbc = DEC ? dec.kbc : sh.KB[sg];
+                    for (int c0 = 0, c1 = 0; c0 < sh.KB[sg] && ok; c0 = c1, ++gc) {
+                        c1 = chunk_end(c0, chl, sh.KB[sg], kbc);
                         const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
                         if (!mbar_wait(xempty0 + 8 * b, xph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
                         tc_fence_after();
                         const uint32_t d_tmem = tmem_base + b * TC_BN;
-                        const int c1 = c0 + chl < sh.KB[sg] ? c0 + chl : sh.KB[sg];
                         uint32_t acc = 0u;
                         for (int kb = c0; kb < c1; ++kb, ++it) {
                             const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
@@ -352,14 +408,21 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
                 if (!mbar_wait(yempty0 + 8 * yb, yph ^ 1u, err, kErrTmemEmpty)) { ok = false; break; }
                 tc_fence_after();
             }
+            int mb_t = 0, nb_t = 0;
+            if constexpr (DEC) Epi::tile_at(ep, t, mb_t, nb_t);
             for (int sg = 0; sg < sh.nseg && ok; ++sg) {
                 const uint32_t Y = lanes + (2 + (SPLIT ? yb : (uint32_t)sg)) * TC_BN;
                 const int chl = sh.whole[sg] ? sh.KB[sg] : CH;
-                for (int c0 = 0; c0 < sh.KB[sg]; c0 += chl, ++gc) {
+                const int kbc = DEC ? dec.kbc : sh.KB[sg];
+                for (int c0 = 0, c1 = 0; c0 < sh.KB[sg]; c0 = c1, ++gc) {
+                    c1 = chunk_end(c0, chl, sh.KB[sg], kbc);
                     const uint32_t b = gc & 1u, xph = (gc >> 1) & 1u;
                     if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t X = lanes + b * TC_BN;
+                    // DEC: this chunk's per-column factor (centroid or sign half)
+                    const float *fsrc = nullptr;
+                    if constexpr (DEC) fsrc = dec.fc ? (c0 < dec.kbc ? dec.fc : dec.fs) : nullptr;
 #pragma unroll 1
                     for (int p = 0; p < TC_BN / 32; ++p) {
                         uint32_t x[32], y[32];
@@ -367,7 +430,15 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
                         tmem_ld32_nw(X + 32 * p, x);
                         if (c0 != 0) tmem_ld32_nw(Y + 32 * p, y);
                         tmem_wait_ld();
-                        if (c0 != 0) {
+                        if (DEC && fsrc) {
+                            const float *f = fsrc + (size_t)nb_t * TC_BN + 32 * p;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const float xv = __uint_as_float(x[j]), fj = __ldg(f + j);
+                                x[j] = __float_as_uint(c0 != 0 ? __fmaf_rn(xv, fj, __uint_as_float(y[j]))
+                                                               : __fmul_rn(xv, fj));
+                            }
+                        } else if (c0 != 0) {
 #pragma unroll
                             for (int j = 0; j < 32; ++j)
                                 x[j] = __float_as_uint(__fadd_rn(__uint_as_float(y[j]), __uint_as_float(x[j])));
@@ -392,7 +463,7 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
         if constexpr (!SPLIT) {
             if (ok) st.finish(ep);
         }
-    } else {
+    } else if (!DEC || warp < 10) {
         // ---------------- tile epilogue (warps 6..9, SPLIT only) ----------------
         const int q = warp & 3;
         const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16);
@@ -410,6 +481,136 @@ __global__ void __launch_bounds__(tc_threads(SPLIT), 1) tcp_kernel(const __grid_
             mbar_arrive(yempty0 + 8 * yb);
         }
         if (ok) st.finish(ep);
+    } else if constexpr (DEC) {
+        // ---------------- decoders (warps 10..13, DEC only) ----------------
+        // Each tile's 128 codes arrive in shared memory as one bulk copy
+        // (dec.cbufs buffers: the next tile's copy is in flight while this one
+        // is decoded).  Thread r writes row r of each B tile (code nb * 128 +
+        // r): eight 16-byte chunks of 8 values, chunk w at (w ^ (r & 7)) * 16
+        // of the row's 128 bytes (the TMA's 128-byte swizzle).  Thread 0 issues
+        // the copies; a buffer is reused once all 128 threads have arrived on
+        // its cempty barrier.
+        const int r = threadIdx.x - 320, sw = r & 7;
+        const int wpb = dec.nibble ? 8 : 16;  // code words per K block
+        const int KB = sh.KB[0];
+        const int nbuf = dec.cbufs;
+        const uint32_t tile_bytes = (uint32_t)dec.ctile_bytes;
+        unsigned char *cbuf0 = reinterpret_cast<unsigned char *>(tabs + 256);
+        // copy of tile tt's codes into buffer bb (rows past n: whatever lies beyond
+        // the corpus in its allocation, which is padded to 256 bytes; unused)
+        auto issue = [&](int tt, int bb) {
+            int mb, nb;
+            Epi::tile_at(ep, tt, mb, nb);
+            const size_t j0 = (size_t)nb * TC_BN;
+            const size_t rows = dec.n - j0 < (size_t)TC_BN ? dec.n - j0 : (size_t)TC_BN;
+            const uint32_t bytes = ((uint32_t)(rows * (size_t)dec.cs) + 15u) & ~15u;
+            const uint32_t bar = cfull0 + 8 * bb;
+            mbar_expect_tx(bar, bytes);
+            bulk_load(smem_u32(cbuf0 + (size_t)bb * tile_bytes), dec.codes + j0 * (size_t)dec.cs, bytes, bar);
+        };
+        uint32_t it = 0;
+        bool ok = true;
+        int issued = 0, waited = 0;  // tiles whose copy thread 0 issued / saw land
+        if (r == 0 && ntiles > 0) {
+            issue(0, 0);
+            issued = 1;
+        }
+        for (int t = 0; t < ntiles && ok; ++t) {
+            const int bb = nbuf == 2 ? (t & 1) : 0;
+            const uint32_t use = nbuf == 2 ? (uint32_t)(t >> 1) : (uint32_t)t;  // uses of bb before
+            if (r == 0 && nbuf == 2 && t + 1 < ntiles) {
+                // the other buffer is free once tile t - 1 was decoded
+                if (t >= 1 && !mbar_wait(cempty0 + 8 * ((t + 1) & 1), (uint32_t)((t - 1) >> 1) & 1u, err,
+                                         kErrEmpty)) {
+                    ok = false;
+                    break;
+                }
+                issue(t + 1, (t + 1) & 1);
+                issued = t + 2;
+            }
+            if (!mbar_wait(cfull0 + 8 * bb, use & 1u, err, kErrFull)) { ok = false; break; }
+            waited = t + 1;
+            int mb, nb;
+            Epi::tile_at(ep, t, mb, nb);
+            const bool live = (unsigned)nb * TC_BN + (unsigned)r < dec.n;
+            const uint32_t *crow = reinterpret_cast<const uint32_t *>(cbuf0 + (size_t)bb * tile_bytes +
+                                                                      (size_t)r * (size_t)dec.cs);
+            for (int kb = 0; kb < KB; ++kb, ++it) {
+                const bool cent = kb < dec.kbc;
+                const int kq = cent ? kb : kb - dec.kbc;  // K block within its half
+                uint32_t w[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) w[i] = (live && i < wpb) ? crow[kq * wpb + i] : 0u;
+                if (kb == KB - 1) mbar_arrive(cempty0 + 8 * bb);  // this thread is done with the tile
+                const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+                if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err, kErrEmpty)) { ok = false; break; }
+                unsigned char *bh = smem + s * TC_STAGE_BYTES + 2 * TC_A_BYTES + r * 128;
+                unsigned char *bl = bh + TC_B_BYTES;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    uint4 hi = make_uint4(0u, 0u, 0u, 0u), lo = hi;
+                    if (live) {
+                        if (dec.nibble) {
+                            const uint32_t x = w[c];
+                            uint32_t hv[4], lv[4];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const uint32_t byte = (x >> (8 * q)) & 0xFFu;
+                                if (cent) {
+                                    const uint2 e = tabc[byte];
+                                    hv[q] = e.x;
+                                    lv[q] = e.y;
+                                } else {
+                                    hv[q] = tabs[byte];
+                                    lv[q] = 0u;
+                                }
+                            }
+                            hi = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                            lo = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+                        } else {
+                            const uint32_t *t1 = reinterpret_cast<const uint32_t *>(tabc);
+                            uint32_t hv[4], lv[4];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const uint32_t x = w[2 * c + (q >> 1)];
+                                const uint32_t u0 = (x >> (16 * (q & 1))) & 0xFFu;
+                                const uint32_t u1 = (x >> (16 * (q & 1) + 8)) & 0xFFu;
+                                if (cent) {
+                                    const uint32_t e0 = t1[u0], e1 = t1[u1];
+                                    hv[q] = __byte_perm(e0, e1, 0x5410u);
+                                    lv[q] = __byte_perm(e0, e1, 0x7632u);
+                                } else {
+                                    hv[q] = ((u0 & 1u) ? 0x3F80u : 0xBF80u) |
+                                            (((u1 & 1u) ? 0x3F80u : 0xBF80u) << 16);
+                                    lv[q] = 0u;
+                                }
+                            }
+                            hi = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                            lo = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+                        }
+                    }
+                    const int off = (c ^ sw) << 4;
+                    *reinterpret_cast<uint4 *>(bh + off) = hi;
+                    if (kb < sh.kbx[0]) *reinterpret_cast<uint4 *>(bl + off) = lo;
+                }
+                fence_proxy_async_smem();  // the tile's generic stores before the MMA's async reads
+                mbar_arrive(full0 + 8 * s);
+            }
+            if (ok && r == 0 && nbuf == 1 && t + 1 < ntiles) {
+                // one buffer: the next tile's copy once every thread read this one
+                if (!mbar_wait(cempty0, (uint32_t)t & 1u, err, kErrEmpty)) { ok = false; break; }
+                issue(t + 1, 0);
+                issued = t + 2;
+            }
+        }
+        if (r == 0) {
+            // the copies issued but not seen to land must do so before the CTA exits
+            for (int tt = waited; tt < issued; ++tt) {
+                const int bb = nbuf == 2 ? (tt & 1) : 0;
+                const uint32_t use = nbuf == 2 ? (uint32_t)(tt >> 1) : (uint32_t)tt;
+                mbar_drain(cfull0 + 8 * bb, use & 1u);
+            }
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -1146,16 +1347,18 @@ bool make_map_f32(CUtensorMap *map, const void *base, int K, size_t rows, int bo
 }
 
 // CH: K blocks per promoted chunk.
-template <bool TF32, int STAGES, int CH, bool SPLIT, class Epi>
+template <bool TF32, int STAGES, int CH, bool SPLIT, class Epi, bool DEC = false>
 cudaError_t tcp_launch(const TcMaps &maps, const TcShape &sh, const typename Epi::Params &ep,
-                       int *err, unsigned grid, cudaStream_t st) {
+                       int *err, unsigned grid, cudaStream_t st, const DecSrc &dec = DecSrc{}) {
     static_assert(CH >= 1, "a chunk holds at least one K block");
     if (SPLIT && sh.nseg != 1) return cudaErrorInvalidValue;  // Y[t & 1] needs the second Y
-    const size_t smem = (size_t)STAGES * TC_STAGE_BYTES + 256 + 1024;
-    auto kern = tcp_kernel<TF32, STAGES, CH, SPLIT, Epi>;
+    const size_t smem = (size_t)STAGES * TC_STAGE_BYTES + TC_BAR_BYTES +
+                        (DEC ? TC_DEC_TAB_BYTES + (size_t)dec.cbufs * dec.ctile_bytes : 0) + 1024;
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    auto kern = tcp_kernel<TF32, STAGES, CH, SPLIT, Epi, DEC>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, tc_threads(SPLIT), smem, st>>>(maps, sh, ep, err);
+    kern<<<grid, tc_threads(SPLIT, DEC), smem, st>>>(maps, sh, ep, err, dec);
     return cudaGetLastError();
 }
 
@@ -1255,6 +1458,66 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
         case 3: return tcp_launch<false, 3, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
         case 4: return tcp_launch<false, 2, 8, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
         default: return tcp_launch<false, 3, 8, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
+    }
+}
+
+namespace {
+
+// A maps of one K segment for the decoded-B kernels (no B planes).
+bool a_maps(TcMaps &mp, TcShape &sh, const void *Ah, const void *Al, size_t m_pad, int K, int kbx) {
+    sh = TcShape{};
+    sh.nseg = 1;
+    sh.KB[0] = K / TC_BK;
+    sh.kbx[0] = kbx;
+    sh.a_exact[0] = 0;
+    return make_map(&mp.m[0][0], Ah, K, m_pad, TC_BM) && make_map(&mp.m[0][1], Al, K, m_pad, TC_BM);
+}
+
+bool dec_ok(const DecSrc &d, int K) {
+    return d.codes && d.centroids && d.cs % 4 == 0 && (reinterpret_cast<uintptr_t>(d.codes) & 15) == 0 &&
+           d.kbc >= 1 && d.kbc <= K / TC_BK && d.levels >= 1 && d.levels <= 256;
+}
+
+// Code-tile buffers of a DEC launch with `stages` pipeline stages: two (the
+// next tile's copy overlaps this one's decode) when they fit, else one.
+DecSrc with_code_buffers(DecSrc d, int stages) {
+    d.ctile_bytes = (int)(((size_t)TC_BN * d.cs + 127) & ~size_t(127));
+    const size_t fixed = (size_t)stages * TC_STAGE_BYTES + TC_BAR_BYTES + TC_DEC_TAB_BYTES + 1024;
+    d.cbufs = fixed + 2 * (size_t)d.ctile_bytes <= 227 * 1024 ? 2
+              : fixed + (size_t)d.ctile_bytes <= 227 * 1024 ? 1 : 0;
+    return d;
+}
+
+}  // namespace
+
+bool tc_topk_dec_ok(int variant, int cs) {
+    if (variant < 1 || variant > 4 || cs <= 0) return false;
+    DecSrc d;
+    d.cs = cs;
+    return with_code_buffers(d, (variant == 2 || variant == 4) ? 2 : 3).cbufs > 0;
+}
+
+cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size_t rows_pad,
+                               const DecSrc &dec, size_t n_pad, int K, const int *m_dev, size_t n,
+                               const float *r1, const float *r2, const float *c1, const float *c2,
+                               int k, float *part_d, int *part_i, int *err, int grid, cudaStream_t st) {
+    if (k < 1 || k > kCandMax || grid < 1 || !tc_topk_dec_ok(variant, dec.cs)) return cudaErrorInvalidValue;
+    if (K % TC_BK || rows_pad % TC_BM || n_pad % TC_BN || !dec_ok(dec, K) || dec.kbc * 2 != K / TC_BK ||
+        !dec.fc || !dec.fs || n > n_pad)
+        return cudaErrorInvalidValue;
+    if (!aligned16({Ah, Al})) return cudaErrorMisalignedAddress;
+    alignas(64) TcMaps mp;
+    TcShape sh{};
+    if (!a_maps(mp, sh, Ah, Al, rows_pad, K, dec.kbc)) return cudaErrorInvalidValue;
+    const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+    const int stages = (variant == 2 || variant == 4) ? 2 : 3;
+    const DecSrc d = with_code_buffers(dec, stages);
+    if (d.cbufs == 0) return cudaErrorInvalidValue;  // the code tile does not fit beside the stages
+    switch (variant) {
+        case 2: return tcp_launch<false, 2, 4, true, TopkEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
+        case 3: return tcp_launch<false, 3, 4, true, TopkEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
+        case 4: return tcp_launch<false, 2, 8, true, TopkEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
+        default: return tcp_launch<false, 3, 8, true, TopkEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
     }
 }
 

@@ -554,9 +554,9 @@ class TurboQuantSpace:
                                                       _ptr(pq.scalars), _ptr(c), n, _ptr(out)))
         return out
 
-    def index(self, codes):
+    def index(self, codes, layout="planes"):
         """A device-resident search index over `codes` (see turboquant.serving)."""
-        return Index(self, codes)
+        return Index(self, codes, layout)
 
     def __repr__(self):
         return (f"TurboQuantSpace(dim={self.dim()}, bits_per_coord={self.bits_per_coord()}, "

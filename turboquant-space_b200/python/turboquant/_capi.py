@@ -30,7 +30,7 @@ EXPORTS = (
     "tq_distance_m_to_n_symmetric", "tq_encode_batch_device", "tq_prepare_queries_device", "tq_prepare_query",
     "tq_distance_1_to_n_device", "tq_distance_1_to_n_prepared_device",
     "tq_distance_1_to_n_device_noalloc", "tq_distance_m_to_n_device",
-    "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_destroy",
+    "tq_distance_m_to_n_symmetric_device", "tq_index_create", "tq_index_create_ex", "tq_index_destroy",
     "tq_server_create", "tq_server_create_ex", "tq_server_submit", "tq_request_wait", "tq_request_done",
     "tq_request_release", "tq_server_get_stats", "tq_server_reset_stats", "tq_server_tuning", "tq_server_tuning_times", "tq_topk_variant_shape",
     "tq_server_destroy", "tq_selftest_bounded_wait", "tq_space_take_device_status", "tq_space_scan_timer",
@@ -130,6 +130,8 @@ def lib() -> C.CDLL:
     L.tq_distance_m_to_n_device.argtypes = [vp, fp, sz, u8p, sz, fp, C.c_int, vp]
     L.tq_distance_m_to_n_symmetric_device.restype = st
     L.tq_distance_m_to_n_symmetric_device.argtypes = [vp, u8p, sz, u8p, sz, fp, C.c_int, vp]
+    L.tq_index_create_ex.restype = st
+    L.tq_index_create_ex.argtypes = [vp, u8p, sz, C.c_int, C.c_int, C.POINTER(vp)]
     L.tq_index_create.restype = st
     L.tq_index_create.argtypes = [vp, u8p, sz, C.c_int, C.POINTER(vp)]
     L.tq_index_destroy.restype = None

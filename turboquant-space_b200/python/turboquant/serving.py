@@ -156,14 +156,26 @@ class Server:
             pass
 
 
-class Index:
-    """A corpus of codes kept in HBM with its tensor-core operand planes."""
+LAYOUTS = {"planes": 0, "codes": 1}
 
-    def __init__(self, space, codes):
+
+class Index:
+    """A corpus of codes kept in HBM for exact top-k search.
+
+    layout "planes" (default) also keeps the codes' BF16 tensor-core operand
+    planes (code_size + 6 * padded_dim + 8 bytes a code, the fastest pass);
+    "codes" keeps only the codes and four floats a code, and the tensor pass
+    decodes each tile of codes in shared memory (about a tenth of the memory,
+    a slower pass)."""
+
+    def __init__(self, space, codes, layout="planes"):
         self.space = space
+        if layout not in LAYOUTS:
+            raise ValueError(f"layout must be one of {sorted(LAYOUTS)}")
+        self.layout = layout
         ptr, n, on_dev, keep = _codes_arg(codes, space.code_size_bytes())
         h = C.c_void_p()
-        check(lib().tq_index_create(space._h, ptr, n, on_dev, C.byref(h)))
+        check(lib().tq_index_create_ex(space._h, ptr, n, on_dev, LAYOUTS[layout], C.byref(h)))
         self._h = h
         self.n = n
         self._search_server = None
