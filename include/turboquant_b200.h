@@ -287,10 +287,12 @@ typedef struct tq_server_stats {
     size_t queued_rows;
     int slots, max_rows;
     int candidates;              /* tensor-pass candidates per query row */
-    uint64_t fallback_rows;      /* rows the certificate left open, answered by a full exact pass */
+    uint64_t fallback_rows;      /* rows the certificate left open, answered by an exact pass */
     uint64_t bound_violations;   /* candidates whose two distances differed by more than the bound */
     size_t pool_rows;            /* query rows of the admission pool (device memory) */
     size_t pool_used_rows;       /* rows held by queued and in-flight requests */
+    uint64_t list_pass_rows;     /* open rows with more codes at or below their threshold than the
+                                    threshold pass collects, answered by the list pass */
 } tq_server_stats;
 
 /* How an index keeps its corpus for the tensor-core pass. */

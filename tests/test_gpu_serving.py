@@ -6,8 +6,9 @@ python/benchmarks/run_benchmark.py:251-255).  Here the bar is exact: every
 returned row must equal the stable argsort of the reference's own distances
 (the checker's, which are bit-identical to the reference build) -- the same
 indices and bit-identical distances -- for k = 1, 10, 16, whether a request runs
-alone or batched with others.  The certificate's fallback (an exact full pass
-over the codes) is exercised by duplicated codes and by an inflated bound.
+alone or batched with others.  The certificate's fallback (an exact pass over
+the codes: a threshold pass, and a list pass for rows it cannot hold) is
+exercised by duplicated codes and by an inflated bound.
 """
 import threading
 
@@ -163,21 +164,67 @@ def test_duplicates_take_the_exact_fallback(corpus):
         _assert_exact(D, I, want, 16)
         assert st["bound_violations"] == 0
         assert st["fallback_rows"] >= 3, st["fallback_rows"]
+        assert st["list_pass_rows"] == 0
     finally:
         ix.close()
 
 
 def test_forced_fallback_is_exact(corpus):
     """bound_scale inflates the certificate's bound so that no row certifies:
-    every row is answered by the exact full pass."""
+    every row is answered by the fallback's threshold pass."""
     space, codes, X, Q, ref, _ = corpus
     ix = space.index(np.ascontiguousarray(codes[:30_000]))
     try:
+        for k in (1, 10, 16):
+            with ix.serve(k=k, max_rows=128, slots=1, bound_scale=1e30) as sv:
+                D, I = sv.submit(Q[:50]).wait()
+                st = sv.stats()
+            assert st["fallback_rows"] == 50 and st["list_pass_rows"] == 0
+            _assert_exact(D, I, ref[:50, :30_000], k)
+    finally:
+        ix.close()
+
+
+@pytest.mark.parametrize("dim,bits", [(256, 8), (200, 3), (1000, 2), (32, 4)])
+def test_forced_fallback_other_widths(cuda_ok, dim, bits):
+    """The threshold pass in each of its forms: term tables for nibble codes
+    with a padded dim of 64 or more (200-d 3-bit, 1000-d 2-bit), the direct
+    arithmetic for byte codes and for smaller nibble dims."""
+    rng = np.random.default_rng(dim * 10 + bits)
+    X = rng.standard_normal((7_000, dim)).astype(np.float32)
+    X[::101] = 0.0
+    Q = rng.standard_normal((24, dim)).astype(np.float32)
+    X[3] = Q[0]
+    space = tq.TurboQuantSpace(dim, bits)
+    codes = space.encode_batch(X)
+    want = O.OracleSpace(dim, bits).distance_m_to_n(Q, codes)
+    ix = space.index(codes)
+    try:
         with ix.serve(k=10, max_rows=128, slots=1, bound_scale=1e30) as sv:
-            D, I = sv.submit(Q[:50]).wait()
+            D, I = sv.submit(Q).wait()
             st = sv.stats()
-        assert st["fallback_rows"] == 50
-        _assert_exact(D, I, ref[:50, :30_000], 10)
+        assert st["fallback_rows"] == 24 and st["list_pass_rows"] == 0
+        _assert_exact(D, I, want, 10)
+    finally:
+        ix.close()
+
+
+def test_collection_overflow_takes_the_list_pass(corpus):
+    """1,100 copies of one code at a query's smallest distance: its open row
+    has more codes at or below its threshold than the threshold pass
+    collects, and the list pass answers it (ties by the smaller index)."""
+    space, codes, X, Q, ref, _ = corpus
+    dup = np.repeat(codes[5:6], 1_100, axis=0)
+    corp = np.ascontiguousarray(np.concatenate([codes[:20_000], dup]))
+    queries = np.ascontiguousarray(np.concatenate([X[5:6], Q[:7]]))
+    want = O.OracleSpace(DIM, BITS).distance_m_to_n(queries, corp)
+    ix = space.index(corp)
+    try:
+        with ix.serve(k=10, max_rows=128, slots=1) as sv:
+            D, I = sv.submit(queries).wait()
+            st = sv.stats()
+        _assert_exact(D, I, want, 10)
+        assert st["list_pass_rows"] >= 1, st
     finally:
         ix.close()
 

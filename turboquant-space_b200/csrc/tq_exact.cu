@@ -266,8 +266,10 @@ __device__ void warp_merge(const float *bd, const int *bi, int k, int lane, floa
     }
 }
 
+// The centroid table in shared memory, zero past the space's levels (an
+// index no encoder writes reads 0 in every kernel of this file alike).
 __device__ __forceinline__ void load_centroids(float *sc, const float *centroids, int levels) {
-    for (int i = threadIdx.x; i < levels; i += blockDim.x) sc[i] = centroids[i];
+    for (int i = threadIdx.x; i < kMaxLevels; i += blockDim.x) sc[i] = i < levels ? centroids[i] : 0.0f;
     __syncthreads();
 }
 
@@ -287,7 +289,9 @@ struct RescoreArgs {
     float bound_scale;
     float *out_d;
     long long *out_i;
-    int *fail_rows, *counters;
+    int *fail_rows;
+    float *thr;
+    int *counters;
 };
 
 // One warp per query row, lane l on candidate l.
@@ -380,7 +384,210 @@ __global__ void __launch_bounds__(256) rescore_kernel(RescoreArgs a) {
         } else if (lane == 0) {
             const int pos = atomicAdd(&a.counters[kCntFallbackRows], 1);
             a.fail_rows[pos] = row;
+            a.thr[pos] = ek;
             if (viol_mask) atomicAdd(&a.counters[kCntBoundViolations], __popc(viol_mask));
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// distSearchScalarB4 in the reference build's order for D >= 64 (nb a
+// multiple of 32), from per-query tables of its per-byte terms:
+//   tip[b * 64 + (lo >> 1) + 8 (hi >> 1)] = fma(q[2b], c[lo >> 1], q[2b+1] * c[hi >> 1]),
+//   tsg[b * 4 + (lo & 1) + 2 (hi & 1)]    = (+-s[2b]) + (+-s[2b+1]),
+// the same FP32 operations as exact_b4 performs per byte, done once per query
+// instead of once per code.  The running sums then take one table value per
+// byte, in the same order.  code: 4-byte aligned.
+__device__ __forceinline__ float exact_b4_tab(const float *__restrict__ tip,
+                                              const float *__restrict__ tsg, float qn2, float qn,
+                                              float scale, int nb, const uint8_t *code) {
+    float A[32], S[32];
+#pragma unroll
+    for (int t = 0; t < 32; ++t) A[t] = S[t] = 0.0f;
+#pragma unroll 1
+    for (int b0 = 0; b0 < nb; b0 += 32) {
+        const float *ti = tip + (size_t)b0 * 64, *ts = tsg + b0 * 4;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t x = *reinterpret_cast<const uint32_t *>(code + b0 + 4 * w);
+            // per byte: (lo >> 1) | (hi >> 1) << 3, and (lo & 1) | (hi & 1) << 1
+            const uint32_t iw = ((x >> 1) & 0x07070707u) | ((x >> 2) & 0x38383838u);
+            const uint32_t sw = (x & 0x01010101u) | ((x >> 3) & 0x02020202u);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int t = 4 * w + e;
+                A[t] = __fadd_rn(A[t], ti[t * 64 + ((iw >> (8 * e)) & 0xFFu)]);
+                S[t] = __fadd_rn(S[t], ts[t * 4 + ((sw >> (8 * e)) & 0xFFu)]);
+            }
+        }
+    }
+    float V[8], W[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        V[j] = __fadd_rn(__fadd_rn(A[16 + j], A[24 + j]), __fadd_rn(A[j], A[8 + j]));
+        W[j] = __fadd_rn(__fadd_rn(S[16 + j], S[24 + j]), __fadd_rn(S[j], S[8 + j]));
+    }
+    const float ip = hsum8(V), dot = hsum8(W);
+    const float xn = ld_f32(code + nb, true), g = ld_f32(code + nb + 4, true);
+    const float sig = ld_f32(code + nb + 8, true);
+    float t = __fmul_rn(__fmul_rn(scale, g), dot);
+    t = __fmul_rn(__fmaf_rn(ip, sig, t), xn);
+    return finish_dist(t, xn, qn2, qn);
+}
+
+struct CollectArgs {
+    Params P;
+    const float *centroids;
+    const float *q_rot, *s_q, *norms;
+    const uint8_t *codes;
+    size_t n;
+    bool al16;  // codes 16-byte aligned
+    const int *fail_rows, *counters;
+    const float *thr;
+    int *coll_n;
+    float *coll_d;
+    int *coll_i;
+};
+
+// The threshold pass of the fallback.  For each open row f in turn, every CTA
+// builds the row's term tables (TAB) in shared memory, then streams its share
+// of the codes through two shared-memory chunk buffers (16-byte cp.async, the
+// next chunk in flight while this one is scored), a thread per code.  A code
+// whose exact distance is at most thr[f] is appended to the row's collection
+// (one atomic per warp).
+template <bool NIBBLE, bool TAB>
+__global__ void __launch_bounds__(256, 1) fallback_collect_kernel(CollectArgs a, int chunk,
+                                                                  int tab_bytes) {
+    const int nf = a.counters[kCntFallbackRows];
+    if (nf == 0) return;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    __shared__ float sc[kMaxLevels];
+    load_centroids(sc, a.centroids, a.P.levels);
+    const int D = a.P.D, nb = a.P.pb, cs = a.P.cs, lane = threadIdx.x & 31;
+    const bool al4 = (cs & 3) == 0;
+    float *tip = reinterpret_cast<float *>(fsm);
+    float *tsg = tip + (size_t)nb * 64;
+    unsigned char *cbuf = fsm + tab_bytes;
+    const size_t cbytes = (size_t)chunk * cs, stride = (size_t)gridDim.x * chunk;
+    auto stage = [&](int bsel, size_t c0) {
+        const size_t rows = a.n - c0 < (size_t)chunk ? a.n - c0 : (size_t)chunk;
+        const size_t bytes = rows * cs;
+        const uint8_t *src = a.codes + c0 * cs;
+        unsigned char *dst = cbuf + bsel * cbytes;
+        size_t done = 0;
+        if (a.al16) {
+            const size_t n16 = bytes >> 4;
+            for (size_t i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(dst + 16 * i, src + 16 * i);
+            done = n16 << 4;
+        }
+        for (size_t i = done + threadIdx.x; i < bytes; i += blockDim.x) dst[i] = src[i];
+        cp_async_commit();
+    };
+    for (int f = 0; f < nf; ++f) {
+        const int row = a.fail_rows[f];
+        const float T = a.thr[f];
+        const float *q = a.q_rot + (size_t)row * D, *s = a.s_q + (size_t)row * D;
+        const float qn2 = a.norms[2 * row], qn = a.norms[2 * row + 1];
+        __syncthreads();  // the previous row's tables and chunks are no longer read
+        if constexpr (TAB) {
+            for (int e = threadIdx.x; e < nb * 64; e += blockDim.x) {
+                const int b = e >> 6;
+                tip[e] = __fmaf_rn(q[2 * b], sc[e & 7], __fmul_rn(q[2 * b + 1], sc[(e >> 3) & 7]));
+            }
+            for (int e = threadIdx.x; e < nb * 4; e += blockDim.x) {
+                const int b = e >> 2;
+                tsg[e] = __fadd_rn(sgn_s(s[2 * b], e & 1), sgn_s(s[2 * b + 1], (e >> 1) & 1));
+            }
+        }
+        size_t c0 = (size_t)blockIdx.x * chunk;
+        int bsel = 0;
+        if (c0 < a.n) stage(0, c0);
+        for (; c0 < a.n; c0 += stride, bsel ^= 1) {
+            if (c0 + stride < a.n)
+                stage(bsel ^ 1, c0 + stride);
+            else
+                cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();  // chunk c0 (and the tables) visible to every thread
+            const int rows = (int)(a.n - c0 < (size_t)chunk ? a.n - c0 : (size_t)chunk);
+            const int rows32 = (rows + 31) & ~31;
+            const unsigned char *cb = cbuf + bsel * cbytes;
+            for (int i = threadIdx.x; i < rows32; i += blockDim.x) {
+                float d = 0.0f;
+                bool pass = false;
+                if (i < rows) {
+                    const uint8_t *code = cb + (size_t)i * cs;
+                    if constexpr (TAB)
+                        d = exact_b4_tab(tip, tsg, qn2, qn, a.P.scale, nb, code);
+                    else
+                        d = exact_dist<NIBBLE>(a.P, sc, q, s, qn2, qn, code, al4);
+                    pass = d <= T;
+                }
+                const unsigned m = __ballot_sync(kFull, pass);
+                if (m) {
+                    const int leader = __ffs(m) - 1;
+                    int base = 0;
+                    if (lane == leader) base = atomicAdd(&a.coll_n[f], __popc(m));
+                    base = __shfl_sync(kFull, base, leader);
+                    const int pos = base + __popc(m & ((1u << lane) - 1u));
+                    if (pass && pos < kCollectCap) {
+                        a.coll_d[(size_t)f * kCollectCap + pos] = d;
+                        a.coll_i[(size_t)f * kCollectCap + pos] = (int)(c0 + (size_t)i);
+                    }
+                }
+            }
+            __syncthreads();  // buffer bsel is free for the chunk after next
+        }
+    }
+}
+
+// One warp per open row: the k best collected codes by (distance, index) to
+// the output; a row whose collection overflowed (or that the threshold pass
+// could not take, collected == false) goes to the list pass's row list.
+__global__ void __launch_bounds__(256) fallback_select_kernel(int *counters, const int *fail_rows,
+                                                              int k, bool collected,
+                                                              const int *__restrict__ coll_n,
+                                                              const float *__restrict__ coll_d,
+                                                              const int *__restrict__ coll_i,
+                                                              int *fail2, float *out_d,
+                                                              long long *out_i) {
+    const int nf = counters[kCntFallbackRows];
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < nf; f += gridDim.x * wpb) {
+        const int row = fail_rows[f];
+        const int cnt = coll_n[f];
+        if (!collected || cnt > kCollectCap) {
+            if (lane == 0) fail2[atomicAdd(&counters[kCntOverflowRows], 1)] = row;
+            continue;
+        }
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+#pragma unroll
+        for (int u = 0; u < kTopKMax; ++u) {
+            bd[u] = INFINITY;
+            bi[u] = kNoIdx;
+        }
+        float td = INFINITY;
+        int ti = kNoIdx;
+        for (int u = lane; u < cnt; u += 32) {
+            const float d = coll_d[(size_t)f * kCollectCap + u];
+            const int i = coll_i[(size_t)f * kCollectCap + u];
+            if (better(d, i, td, ti)) list_insert(bd, bi, k, d, i, &td, &ti);
+        }
+        float md;
+        int mi;
+        warp_merge(bd, bi, k, lane, md, mi);
+        if (lane < k) {
+            out_d[(size_t)row * k + lane] = md;
+            out_i[(size_t)row * k + lane] = mi == kNoIdx ? -1 : (long long)mi;
         }
     }
 }
@@ -393,22 +600,21 @@ struct FallbackArgs {
     const uint8_t *codes;
     size_t n;
     bool al16;  // codes 16-byte aligned
-    const int *fail_rows, *counters;
+    const int *rows, *counters;
     float *part_d;
     int *part_i;
-    float *out_d;
-    long long *out_i;
 };
 
-// Exact top-k by a full pass over the codes for each row the certificate did
-// not settle.  A CTA stages chunks of `chunk` consecutive codes in shared
+// The list pass for the rows the threshold pass could not settle
+// (counters[kCntOverflowRows] of them, in rows): a full pass over the codes
+// for each row.  A CTA stages chunks of `chunk` consecutive codes in shared
 // memory with coalesced 16-byte loads, then each thread scores the codes of
 // the chunk it owns from there (a code's words are cs / 4 apart, an odd
 // stride: no bank conflicts) and keeps a sorted list; the warps merge their
 // lanes' lists and warp 0 merges the block's into part[row][cta].
 template <bool NIBBLE>
 __global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a, int chunk) {
-    const int nf = a.counters[kCntFallbackRows];
+    const int nf = a.counters[kCntOverflowRows];
     if (nf == 0) return;
     extern __shared__ __align__(16) unsigned char fsm[];
     __shared__ float sc[kMaxLevels];
@@ -419,7 +625,7 @@ __global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a, int 
     const int k = a.k, cs = a.P.cs;
     const bool al4 = (cs & 3) == 0;
     for (int f = 0; f < nf; ++f) {
-        const int row = a.fail_rows[f];
+        const int row = a.rows[f];
         const float *q = a.q_rot + (size_t)row * D, *s = a.s_q + (size_t)row * D;
         const float qn2 = a.norms[2 * row], qn = a.norms[2 * row + 1];
         float bd[kTopKMax];
@@ -478,15 +684,14 @@ __global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a, int 
     }
 }
 
-// One warp per fallback row: merge the CTAs' lists into the row's output.
+// One warp per list-pass row: merge the CTAs' lists into the row's output.
 __global__ void __launch_bounds__(256) fallback_merge_kernel(const int *__restrict__ counters,
-                                                             const int *__restrict__ fail_rows,
-                                                             int ctas, int k,
-                                                             const float *__restrict__ part_d,
+                                                             const int *__restrict__ rows, int ctas,
+                                                             int k, const float *__restrict__ part_d,
                                                              const int *__restrict__ part_i,
                                                              float *__restrict__ out_d,
                                                              long long *__restrict__ out_i) {
-    const int nf = counters[kCntFallbackRows];
+    const int nf = counters[kCntOverflowRows];
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < nf; f += gridDim.x * wpb) {
         float bd[kTopKMax];
@@ -508,7 +713,7 @@ __global__ void __launch_bounds__(256) fallback_merge_kernel(const int *__restri
         float md;
         int mi;
         warp_merge(bd, bi, k, lane, md, mi);
-        const int row = fail_rows[f];
+        const int row = rows[f];
         if (lane < k) {
             out_d[(size_t)row * k + lane] = md;
             out_i[(size_t)row * k + lane] = mi == kNoIdx ? -1 : (long long)mi;
@@ -590,13 +795,13 @@ cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, 
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
                            const uint8_t *codes, size_t n, const float *bound, float bound_scale,
-                           float *out_d, long long *out_i, int *fail_rows, int *counters,
-                           int max_rows, cudaStream_t st) {
+                           float *out_d, long long *out_i, int *fail_rows, float *thr,
+                           int *counters, int max_rows, cudaStream_t st) {
     if (kc < 1 || kc > 32 || k < 1 || k > kc || k > kTopKMax || max_rows < 1)
         return cudaErrorInvalidValue;
     const RescoreArgs a{P,     centroids, cmax,  m_dev,     kc,          k,     cand_d,
                         cand_i, q_rot,    s_q,   norms,     codes,       n,     codes_al4(P, codes),
-                        bound, bound_scale, out_d, out_i, fail_rows, counters};
+                        bound, bound_scale, out_d, out_i, fail_rows, thr, counters};
     const unsigned blocks = (unsigned)((max_rows + 7) / 8);
     if (P.nibble)
         rescore_kernel<true><<<blocks, 256, 0, st>>>(a);
@@ -609,27 +814,65 @@ int fallback_ctas(int sms) { return 2 * (sms > 0 ? sms : 148); }
 
 cudaError_t launch_fallback(const Params &P, const float *centroids, int k, const float *q_rot,
                             const float *s_q, const float *norms, const uint8_t *codes, size_t n,
-                            const int *fail_rows, const int *counters, int fb_ctas, float *part_d,
-                            int *part_i, float *out_d, long long *out_i, int max_rows,
-                            cudaStream_t st) {
+                            const int *fail_rows, int *counters, int fb_ctas,
+                            const FallbackBuffers &fb, float *out_d, long long *out_i,
+                            int max_rows, cudaStream_t st) {
     if (k < 1 || k > kTopKMax || fb_ctas < 1 || max_rows < 1) return cudaErrorInvalidValue;
-    // chunks start chunk * cs bytes apart, a multiple of 64: 16-byte aligned with the base
-    const bool al16 = (reinterpret_cast<uintptr_t>(codes) & 15) == 0;
-    const FallbackArgs a{P,     centroids, k,         q_rot,    s_q,    norms,  codes, n,
-                         al16, fail_rows, counters, part_d, part_i, out_d, out_i};
-    // codes per staged chunk: up to 256, at most 96 KB of shared memory, a
-    // multiple of 16 so that every chunk starts 16-byte aligned
-    int chunk = (int)std::min<size_t>(256, (size_t)(96 * 1024) / (size_t)P.cs) & ~15;
-    if (chunk < 16) chunk = 16;
-    const size_t smem = (size_t)chunk * P.cs;
-    auto kern = P.nibble ? fallback_scan_kernel<true> : fallback_scan_kernel<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    kern<<<fb_ctas, 256, smem, st>>>(a, chunk);
+    // chunks start at code indices that are multiples of 16: 16-byte aligned
+    // with the base
+    const bool al16 = (reinterpret_cast<uintptr_t>(codes) & 15) == 0;
+    constexpr int kThreads = 256;
+    constexpr size_t kSmemMax = 224 * 1024;
+    // threshold pass: term tables when nibble codes have D >= 64 and the
+    // tables leave room for two chunks of at least 16 codes
+    const size_t cs = (size_t)P.cs;
+    const size_t tab_bytes = (size_t)P.pb * (64 + 4) * 4;
+    const bool tab = P.nibble && P.D >= 64 && P.pb % 32 == 0 && tab_bytes + 32 * cs <= kSmemMax;
+    const size_t tb = tab ? tab_bytes : 0;
+    const int chunk = (int)std::min<size_t>(256, (kSmemMax - std::min(tb, kSmemMax)) / (2 * cs)) & ~15;
+    const bool collected = chunk >= 16 && (cs & 3) == 0;
+    e = cudaMemsetAsync(fb.coll_n, 0, (size_t)max_rows * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    if (collected) {
+        const CollectArgs ca{P,  centroids, q_rot,    s_q,   norms,     codes,    n,
+                             al16, fail_rows, counters, fb.thr, fb.coll_n, fb.coll_d, fb.coll_i};
+        const size_t smem = tb + 2 * (size_t)chunk * cs;
+        auto kern = !P.nibble ? fallback_collect_kernel<false, false>
+                              : (tab ? fallback_collect_kernel<true, true> : fallback_collect_kernel<true, false>);
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+        if (e != cudaSuccess) return e;
+        const int grid = std::max(1, per_sm) * std::max(1, sms);
+        kern<<<grid, kThreads, smem, st>>>(ca, chunk, (int)tb);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    const unsigned rblocks = (unsigned)((max_rows + 7) / 8);
+    fallback_select_kernel<<<rblocks, 256, 0, st>>>(counters, fail_rows, k, collected, fb.coll_n,
+                                                    fb.coll_d, fb.coll_i, fb.fail2, out_d, out_i);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    fallback_merge_kernel<<<(unsigned)((max_rows + 7) / 8), 256, 0, st>>>(
-        counters, fail_rows, fb_ctas, k, part_d, part_i, out_d, out_i);
+    // list pass: codes per staged chunk up to 256, at most 96 KB of shared
+    // memory, a multiple of 16 so that every chunk starts 16-byte aligned
+    const FallbackArgs a{P, centroids, k, q_rot, s_q, norms, codes, n, al16, fb.fail2, counters,
+                         fb.part_d, fb.part_i};
+    int lchunk = (int)std::min<size_t>(256, (size_t)(96 * 1024) / cs) & ~15;
+    if (lchunk < 16) lchunk = 16;
+    const size_t lsmem = (size_t)lchunk * cs;
+    auto lkern = P.nibble ? fallback_scan_kernel<true> : fallback_scan_kernel<false>;
+    e = cudaFuncSetAttribute(lkern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
+    if (e != cudaSuccess) return e;
+    lkern<<<fb_ctas, 256, lsmem, st>>>(a, lchunk);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    fallback_merge_kernel<<<rblocks, 256, 0, st>>>(counters, fb.fail2, fb_ctas, k, fb.part_d,
+                                                   fb.part_i, out_d, out_i);
     return cudaGetLastError();
 }
 

@@ -120,9 +120,9 @@ struct Slot {
     long long *h_i = nullptr;
     void *d_block = nullptr;  // one device allocation for all buffers below
     float *d_q = nullptr, *d_prep = nullptr, *d_r1 = nullptr, *d_r2 = nullptr, *d_pd = nullptr,
-          *d_od = nullptr, *d_cd = nullptr, *d_fpd = nullptr;
+          *d_od = nullptr, *d_cd = nullptr, *d_fpd = nullptr, *d_thr = nullptr, *d_colld = nullptr;
     int *d_m = nullptr, *d_pi = nullptr, *d_err = nullptr, *d_fail = nullptr, *d_cnt = nullptr,
-        *d_fpi = nullptr;
+        *d_fpi = nullptr, *d_colln = nullptr, *d_colli = nullptr, *d_fail2 = nullptr;
     long long *d_ci = nullptr;
     int *h_cnt = nullptr;  // pinned copy of d_cnt after each batch
     int *h_rows = nullptr;  // pool row of each batch row (pinned)
@@ -165,7 +165,7 @@ struct tq_server {
     bool stop = false;
     // stats
     uint64_t submitted = 0, rejected = 0, completed = 0, batches = 0, rows_done = 0;
-    uint64_t fallback_rows = 0, bound_violations = 0;
+    uint64_t fallback_rows = 0, bound_violations = 0, list_pass_rows = 0;
     std::vector<float> latencies_ms;  // ring of the most recent completions
     size_t lat_pos = 0;
     double busy_ms = 0;
@@ -285,11 +285,12 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     if (e != cudaSuccess) return e;
     e = tq::launch_rescore(sp->P, sp->T.centroids, ix->cmax, sl.d_m, sv->kc, sv->k, sl.d_cd, sl.d_ci,
                            q_rot, s_q, norms, ix->codes, ix->n, ix->bound, sv->bound_scale, sl.d_od,
-                           sl.d_oi, sl.d_fail, sl.d_cnt, rows_cap, st);
+                           sl.d_oi, sl.d_fail, sl.d_thr, sl.d_cnt, rows_cap, st);
     if (e != cudaSuccess) return e;
+    const tq::FallbackBuffers fb{sl.d_thr, sl.d_colln, sl.d_colld, sl.d_colli,
+                                 sl.d_fail2, sl.d_fpd, sl.d_fpi};
     e = tq::launch_fallback(sp->P, sp->T.centroids, sv->k, q_rot, s_q, norms, ix->codes, ix->n,
-                            sl.d_fail, sl.d_cnt, sv->fb_ctas, sl.d_fpd, sl.d_fpi, sl.d_od, sl.d_oi,
-                            rows_cap, st);
+                            sl.d_fail, sl.d_cnt, sv->fb_ctas, fb, sl.d_od, sl.d_oi, rows_cap, st);
     if (e != cudaSuccess) return e;
     if (copies) {
         e = cudaMemcpyAsync(sl.h_d, sl.d_od, (size_t)rows_cap * sv->k * 4, cudaMemcpyDeviceToHost, st);
@@ -335,7 +336,9 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     const size_t kc = (size_t)sv->kc, fparts = R * (size_t)sv->fb_ctas * k;
     const size_t o_cd = take(R * kc * 4), o_ci = take(R * kc * 8), o_fail = take(R * 4);
     const size_t o_cnt = take(tq::kCntWords * 4), o_fpd = take(fparts * 4), o_fpi = take(fparts * 4);
-    const size_t o_rows = take(R * 4);
+    const size_t o_rows = take(R * 4), o_thr = take(R * 4), o_colln = take(R * 4);
+    const size_t o_colld = take(R * tq::kCollectCap * 4), o_colli = take(R * tq::kCollectCap * 4);
+    const size_t o_fail2 = take(R * 4);
     TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
     TQ_CUDA(cudaMemset(sl.d_block, 0, off), "cudaMemset(slot)");
     auto *base = static_cast<unsigned char *>(sl.d_block);
@@ -357,6 +360,11 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     sl.d_fpd = reinterpret_cast<float *>(base + o_fpd);
     sl.d_fpi = reinterpret_cast<int *>(base + o_fpi);
     sl.d_rows = reinterpret_cast<int *>(base + o_rows);
+    sl.d_thr = reinterpret_cast<float *>(base + o_thr);
+    sl.d_colln = reinterpret_cast<int *>(base + o_colln);
+    sl.d_colld = reinterpret_cast<float *>(base + o_colld);
+    sl.d_colli = reinterpret_cast<int *>(base + o_colli);
+    sl.d_fail2 = reinterpret_cast<int *>(base + o_fail2);
     for (int b = 128; b < sv->max_rows; b *= 2) sl.bucket_rows.push_back(b);
     sl.bucket_rows.push_back(sv->max_rows);
     return TQ_OK;
@@ -554,6 +562,7 @@ void worker_loop(tq_server *sv) {
             if (q == cudaSuccess) {
                 sv->fallback_rows += (uint64_t)sl.h_cnt[tq::kCntFallbackRows];
                 sv->bound_violations += (uint64_t)sl.h_cnt[tq::kCntBoundViolations];
+                sv->list_pass_rows += (uint64_t)sl.h_cnt[tq::kCntOverflowRows];
             }
             size_t row = 0;
             for (tq_request *r : sl.batch) {
@@ -895,6 +904,7 @@ tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latenc
     out->candidates = sv->kc;
     out->fallback_rows = sv->fallback_rows;
     out->bound_violations = sv->bound_violations;
+    out->list_pass_rows = sv->list_pass_rows;
     out->pool_rows = sv->pool_rows;
     out->pool_used_rows = sv->pool_used;
     size_t nl = std::min(cap, sv->latencies_ms.size());
@@ -907,7 +917,7 @@ tq_status tq_server_reset_stats(tq_server *sv) {
     if (!sv) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL server");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->submitted = sv->rejected = sv->completed = sv->batches = sv->rows_done = 0;
-    sv->fallback_rows = sv->bound_violations = 0;
+    sv->fallback_rows = sv->bound_violations = sv->list_pass_rows = 0;
     sv->latencies_ms.clear();
     sv->lat_pos = 0;
     return TQ_OK;
