@@ -291,8 +291,10 @@ typedef struct tq_server_stats {
     uint64_t bound_violations;   /* candidates whose two distances differed by more than the bound */
     size_t pool_rows;            /* query rows of the admission pool (device memory) */
     size_t pool_used_rows;       /* rows held by queued and in-flight requests */
-    uint64_t list_pass_rows;     /* open rows with more codes at or below their threshold than the
-                                    threshold pass collects, answered by the list pass */
+    uint64_t scan_pass_rows;     /* open rows answered by an exact scan of every code (the others
+                                    by rescoring a tensor-core threshold pass's list) */
+    uint64_t list_pass_rows;     /* of those, rows with more codes at or below their threshold
+                                    than the scan collects, answered by a full list pass */
 } tq_server_stats;
 
 /* How an index keeps its corpus for the tensor-core pass. */

@@ -6,9 +6,10 @@ python/benchmarks/run_benchmark.py:251-255).  Here the bar is exact: every
 returned row must equal the stable argsort of the reference's own distances
 (the checker's, which are bit-identical to the reference build) -- the same
 indices and bit-identical distances -- for k = 1, 10, 16, whether a request runs
-alone or batched with others.  The certificate's fallback (an exact pass over
-the codes: a threshold pass, and a list pass for rows it cannot hold) is
-exercised by duplicated codes and by an inflated bound.
+alone or batched with others.  The certificate's fallback (a tensor-core
+threshold pass whose lists are rescored, an exact scan, and a list pass for
+rows the scan cannot hold) is exercised by duplicated codes and by inflated
+bounds.
 """
 import threading
 
@@ -170,8 +171,9 @@ def test_duplicates_take_the_exact_fallback(corpus):
 
 
 def test_forced_fallback_is_exact(corpus):
-    """bound_scale inflates the certificate's bound so that no row certifies:
-    every row is answered by the fallback's threshold pass."""
+    """bound_scale = 1e30 makes the certificate's bound infinite: no row
+    certifies, the tensor-core threshold pass would list every code, so every
+    row is answered by the exact scan."""
     space, codes, X, Q, ref, _ = corpus
     ix = space.index(np.ascontiguousarray(codes[:30_000]))
     try:
@@ -179,17 +181,42 @@ def test_forced_fallback_is_exact(corpus):
             with ix.serve(k=k, max_rows=128, slots=1, bound_scale=1e30) as sv:
                 D, I = sv.submit(Q[:50]).wait()
                 st = sv.stats()
-            assert st["fallback_rows"] == 50 and st["list_pass_rows"] == 0
+            assert st["fallback_rows"] == 50 and st["scan_pass_rows"] == 50
+            assert st["list_pass_rows"] == 0
             _assert_exact(D, I, ref[:50, :30_000], k)
     finally:
         ix.close()
 
 
+@pytest.mark.parametrize("layout", ["planes", "codes"])
+@pytest.mark.parametrize("k", [1, 10, 16])
+def test_tensor_threshold_tier_is_exact(corpus, index_codes, layout, k):
+    """Inflated bounds leave many rows open: with more than eight, the
+    tensor-core threshold pass lists each open row's codes within e_k + eps
+    and the rescoring of those lists answers them (rows whose list overflows
+    go to the exact scan).  Every result is exact, and some bound of the sweep
+    has rows answered from the lists."""
+    space, codes, X, Q, ref, index = corpus
+    ix = index if layout == "planes" else index_codes
+    from_lists = 0
+    for bs in (4.0, 8.0, 16.0, 32.0, 64.0):
+        with ix.serve(k=k, max_rows=256, slots=1, kernel_variant=4, bound_scale=bs) as sv:
+            D, I = sv.submit(Q[:256]).wait()
+            st = sv.stats()
+        _assert_exact(D, I, ref[:256], k)
+        assert st["bound_violations"] == 0
+        if st["fallback_rows"] > 8:
+            from_lists += st["fallback_rows"] - st["scan_pass_rows"]
+        print(f"{layout} k={k} bound x{bs}: {st['fallback_rows']} open rows, "
+              f"{st['scan_pass_rows']} by the exact scan")
+    assert from_lists > 0
+
+
 @pytest.mark.parametrize("dim,bits", [(256, 8), (200, 3), (1000, 2), (32, 4)])
 def test_forced_fallback_other_widths(cuda_ok, dim, bits):
-    """The threshold pass in each of its forms: term tables for nibble codes
-    with a padded dim of 64 or more (200-d 3-bit, 1000-d 2-bit), the direct
-    arithmetic for byte codes and for smaller nibble dims."""
+    """The exact scan in each of its forms: term tables for nibble codes with a
+    padded dim of 64 or more (200-d 3-bit, 1000-d 2-bit), the direct arithmetic
+    for byte codes and for smaller nibble dims."""
     rng = np.random.default_rng(dim * 10 + bits)
     X = rng.standard_normal((7_000, dim)).astype(np.float32)
     X[::101] = 0.0
@@ -203,7 +230,8 @@ def test_forced_fallback_other_widths(cuda_ok, dim, bits):
         with ix.serve(k=10, max_rows=128, slots=1, bound_scale=1e30) as sv:
             D, I = sv.submit(Q).wait()
             st = sv.stats()
-        assert st["fallback_rows"] == 24 and st["list_pass_rows"] == 0
+        assert st["fallback_rows"] == 24 and st["scan_pass_rows"] == 24
+        assert st["list_pass_rows"] == 0
         _assert_exact(D, I, want, 10)
     finally:
         ix.close()
@@ -211,8 +239,8 @@ def test_forced_fallback_other_widths(cuda_ok, dim, bits):
 
 def test_collection_overflow_takes_the_list_pass(corpus):
     """1,100 copies of one code at a query's smallest distance: its open row
-    has more codes at or below its threshold than the threshold pass
-    collects, and the list pass answers it (ties by the smaller index)."""
+    has more codes at or below its threshold than the exact scan collects,
+    and the list pass answers it (ties by the smaller index)."""
     space, codes, X, Q, ref, _ = corpus
     dup = np.repeat(codes[5:6], 1_100, axis=0)
     corp = np.ascontiguousarray(np.concatenate([codes[:20_000], dup]))

@@ -290,7 +290,7 @@ struct RescoreArgs {
     float *out_d;
     long long *out_i;
     int *fail_rows;
-    float *thr;
+    float *thr, *tthr;
     int *counters;
 };
 
@@ -385,6 +385,7 @@ __global__ void __launch_bounds__(256) rescore_kernel(RescoreArgs a) {
             const int pos = atomicAdd(&a.counters[kCntFallbackRows], 1);
             a.fail_rows[pos] = row;
             a.thr[pos] = ek;
+            a.tthr[pos] = viol_mask ? -1.0f : __fadd_ru(ek, eps);
             if (viol_mask) atomicAdd(&a.counters[kCntBoundViolations], __popc(viol_mask));
         }
     }
@@ -450,24 +451,25 @@ struct CollectArgs {
     const uint8_t *codes;
     size_t n;
     bool al16;  // codes 16-byte aligned
-    const int *fail_rows, *counters;
+    const int *fail_rows, *scan_rows, *counters;
     const float *thr;
     int *coll_n;
     float *coll_d;
     int *coll_i;
 };
 
-// The threshold pass of the fallback.  For each open row f in turn, every CTA
-// builds the row's term tables (TAB) in shared memory, then streams its share
-// of the codes through two shared-memory chunk buffers (16-byte cp.async, the
-// next chunk in flight while this one is scored), a thread per code.  A code
-// whose exact distance is at most thr[f] is appended to the row's collection
-// (one atomic per warp).
+// The exact scan of the fallback.  For each of its rows g in turn (fail-list
+// position f = scan_rows[g]), every CTA builds the row's term tables (TAB) in
+// shared memory, then streams its share of the codes through two
+// shared-memory chunk buffers (16-byte cp.async, the next chunk in flight
+// while this one is scored), a thread per code.  A code whose exact distance
+// is at most thr[f] is appended to the row's collection g (one atomic per
+// warp).
 template <bool NIBBLE, bool TAB>
 __global__ void __launch_bounds__(256, 1) fallback_collect_kernel(CollectArgs a, int chunk,
                                                                   int tab_bytes) {
-    const int nf = a.counters[kCntFallbackRows];
-    if (nf == 0) return;
+    const int ng = a.counters[kCntScanRows];
+    if (ng == 0) return;
     extern __shared__ __align__(16) unsigned char fsm[];
     __shared__ float sc[kMaxLevels];
     load_centroids(sc, a.centroids, a.P.levels);
@@ -491,7 +493,8 @@ __global__ void __launch_bounds__(256, 1) fallback_collect_kernel(CollectArgs a,
         for (size_t i = done + threadIdx.x; i < bytes; i += blockDim.x) dst[i] = src[i];
         cp_async_commit();
     };
-    for (int f = 0; f < nf; ++f) {
+    for (int g = 0; g < ng; ++g) {
+        const int f = a.scan_rows[g];
         const int row = a.fail_rows[f];
         const float T = a.thr[f];
         const float *q = a.q_rot + (size_t)row * D, *s = a.s_q + (size_t)row * D;
@@ -535,12 +538,12 @@ __global__ void __launch_bounds__(256, 1) fallback_collect_kernel(CollectArgs a,
                 if (m) {
                     const int leader = __ffs(m) - 1;
                     int base = 0;
-                    if (lane == leader) base = atomicAdd(&a.coll_n[f], __popc(m));
+                    if (lane == leader) base = atomicAdd(&a.coll_n[g], __popc(m));
                     base = __shfl_sync(kFull, base, leader);
                     const int pos = base + __popc(m & ((1u << lane) - 1u));
                     if (pass && pos < kCollectCap) {
-                        a.coll_d[(size_t)f * kCollectCap + pos] = d;
-                        a.coll_i[(size_t)f * kCollectCap + pos] = (int)(c0 + (size_t)i);
+                        a.coll_d[(size_t)g * kCollectCap + pos] = d;
+                        a.coll_i[(size_t)g * kCollectCap + pos] = (int)(c0 + (size_t)i);
                     }
                 }
             }
@@ -549,23 +552,24 @@ __global__ void __launch_bounds__(256, 1) fallback_collect_kernel(CollectArgs a,
     }
 }
 
-// One warp per open row: the k best collected codes by (distance, index) to
-// the output; a row whose collection overflowed (or that the threshold pass
-// could not take, collected == false) goes to the list pass's row list.
+// One warp per exact-scan row: the k best collected codes by (distance,
+// index) to the output; a row whose collection overflowed (or that the scan
+// could not take, collected == false) goes to the list pass's rows.
 __global__ void __launch_bounds__(256) fallback_select_kernel(int *counters, const int *fail_rows,
-                                                              int k, bool collected,
+                                                              const int *scan_rows, int k,
+                                                              bool collected,
                                                               const int *__restrict__ coll_n,
                                                               const float *__restrict__ coll_d,
                                                               const int *__restrict__ coll_i,
-                                                              int *fail2, float *out_d,
+                                                              int *list_rows, float *out_d,
                                                               long long *out_i) {
-    const int nf = counters[kCntFallbackRows];
+    const int ng = counters[kCntScanRows];
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < nf; f += gridDim.x * wpb) {
-        const int row = fail_rows[f];
+    for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < ng; f += gridDim.x * wpb) {
+        const int row = fail_rows[scan_rows[f]];
         const int cnt = coll_n[f];
         if (!collected || cnt > kCollectCap) {
-            if (lane == 0) fail2[atomicAdd(&counters[kCntOverflowRows], 1)] = row;
+            if (lane == 0) list_rows[atomicAdd(&counters[kCntListRows], 1)] = row;
             continue;
         }
         float bd[kTopKMax];
@@ -592,6 +596,85 @@ __global__ void __launch_bounds__(256) fallback_select_kernel(int *counters, con
     }
 }
 
+// Tier 1: one warp per open row f.  When the tensor-core threshold pass ran
+// (more than kTensorTierMinRows open rows), its bound held (tthr >= 0) and its
+// list did not overflow, the lanes score the listed codes with the
+// reference's arithmetic and the row's k best by (distance, index) go to the
+// output; every other row goes to the exact scan's rows.
+template <bool NIBBLE>
+__global__ void __launch_bounds__(256) tensor_select_kernel(
+    Params P, const float *centroids, const float *q_rot, const float *s_q, const float *norms,
+    const uint8_t *codes, size_t n, bool al4, int *counters, const int *fail_rows,
+    const float *tthr, bool tensor_pass, int k, const int *__restrict__ coll_n,
+    const int *__restrict__ coll_i, int *scan_rows, float *out_d, long long *out_i) {
+    const int nf = counters[kCntFallbackRows];
+    if (nf == 0) return;
+    __shared__ float sc[kMaxLevels];
+    load_centroids(sc, centroids, P.levels);
+    const int D = P.D, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const bool ran = tensor_pass && nf > kTensorTierMinRows;
+    for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < nf; f += gridDim.x * wpb) {
+        const int cnt = coll_n[f];
+        if (!ran || !(tthr[f] >= 0.0f) || cnt > kCollectCap) {
+            if (lane == 0) scan_rows[atomicAdd(&counters[kCntScanRows], 1)] = f;
+            continue;
+        }
+        const int row = fail_rows[f];
+        const float *q = q_rot + (size_t)row * D, *s = s_q + (size_t)row * D;
+        const float qn2 = norms[2 * row], qn = norms[2 * row + 1];
+        float bd[kTopKMax];
+        int bi[kTopKMax];
+#pragma unroll
+        for (int u = 0; u < kTopKMax; ++u) {
+            bd[u] = INFINITY;
+            bi[u] = kNoIdx;
+        }
+        float td = INFINITY;
+        int ti = kNoIdx;
+        for (int u = lane; u < cnt; u += 32) {
+            const int j = coll_i[(size_t)f * kCollectCap + u];
+            if (j < 0 || (size_t)j >= n) continue;
+            const float d = exact_dist<NIBBLE>(P, sc, q, s, qn2, qn, codes + (size_t)j * P.cs, al4);
+            if (better(d, j, td, ti)) list_insert(bd, bi, k, d, j, &td, &ti);
+        }
+        float md;
+        int mi;
+        warp_merge(bd, bi, k, lane, md, mi);
+        if (lane < k) {
+            out_d[(size_t)row * k + lane] = md;
+            out_i[(size_t)row * k + lane] = mi == kNoIdx ? -1 : (long long)mi;
+        }
+    }
+}
+
+// Open row f's query planes (K BF16 values a row, hi and lo) and scales to
+// row f of the tensor-core threshold pass's operands.
+__global__ void __launch_bounds__(256) gather_open_kernel(const int *__restrict__ counters,
+                                                          const int *__restrict__ fail_rows,
+                                                          const uint4 *__restrict__ ah,
+                                                          const uint4 *__restrict__ al,
+                                                          const float *__restrict__ r1,
+                                                          const float *__restrict__ r2, int w16,
+                                                          uint4 *__restrict__ ah2,
+                                                          uint4 *__restrict__ al2,
+                                                          float *__restrict__ r1o,
+                                                          float *__restrict__ r2o) {
+    const int nf = counters[kCntFallbackRows];
+    if (nf <= kTensorTierMinRows) return;
+    const size_t total = (size_t)nf * w16;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t f = t / w16, w = t % w16;
+        const size_t src = (size_t)fail_rows[f] * w16 + w;
+        ah2[t] = ah[src];
+        al2[t] = al[src];
+        if (w == 0) {
+            r1o[f] = r1[fail_rows[f]];
+            r2o[f] = r2[fail_rows[f]];
+        }
+    }
+}
+
 struct FallbackArgs {
     Params P;
     const float *centroids;
@@ -605,8 +688,8 @@ struct FallbackArgs {
     int *part_i;
 };
 
-// The list pass for the rows the threshold pass could not settle
-// (counters[kCntOverflowRows] of them, in rows): a full pass over the codes
+// The list pass for the rows the exact scan could not settle
+// (counters[kCntListRows] of them, in rows): a full pass over the codes
 // for each row.  A CTA stages chunks of `chunk` consecutive codes in shared
 // memory with coalesced 16-byte loads, then each thread scores the codes of
 // the chunk it owns from there (a code's words are cs / 4 apart, an odd
@@ -614,7 +697,7 @@ struct FallbackArgs {
 // lanes' lists and warp 0 merges the block's into part[row][cta].
 template <bool NIBBLE>
 __global__ void __launch_bounds__(256) fallback_scan_kernel(FallbackArgs a, int chunk) {
-    const int nf = a.counters[kCntOverflowRows];
+    const int nf = a.counters[kCntListRows];
     if (nf == 0) return;
     extern __shared__ __align__(16) unsigned char fsm[];
     __shared__ float sc[kMaxLevels];
@@ -691,7 +774,7 @@ __global__ void __launch_bounds__(256) fallback_merge_kernel(const int *__restri
                                                              const int *__restrict__ part_i,
                                                              float *__restrict__ out_d,
                                                              long long *__restrict__ out_i) {
-    const int nf = counters[kCntOverflowRows];
+    const int nf = counters[kCntListRows];
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     for (int f = blockIdx.x * wpb + (threadIdx.x >> 5); f < nf; f += gridDim.x * wpb) {
         float bd[kTopKMax];
@@ -795,13 +878,13 @@ cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, 
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
                            const uint8_t *codes, size_t n, const float *bound, float bound_scale,
-                           float *out_d, long long *out_i, int *fail_rows, float *thr,
+                           float *out_d, long long *out_i, int *fail_rows, float *thr, float *tthr,
                            int *counters, int max_rows, cudaStream_t st) {
     if (kc < 1 || kc > 32 || k < 1 || k > kc || k > kTopKMax || max_rows < 1)
         return cudaErrorInvalidValue;
     const RescoreArgs a{P,     centroids, cmax,  m_dev,     kc,          k,     cand_d,
                         cand_i, q_rot,    s_q,   norms,     codes,       n,     codes_al4(P, codes),
-                        bound, bound_scale, out_d, out_i, fail_rows, thr, counters};
+                        bound, bound_scale, out_d, out_i, fail_rows, thr, tthr, counters};
     const unsigned blocks = (unsigned)((max_rows + 7) / 8);
     if (P.nibble)
         rescore_kernel<true><<<blocks, 256, 0, st>>>(a);
@@ -812,9 +895,26 @@ cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, 
 
 int fallback_ctas(int sms) { return 2 * (sms > 0 ? sms : 148); }
 
+cudaError_t launch_gather_open(const int *counters, const int *fail_rows, const void *ah,
+                               const void *al, const float *r1, const float *r2, int K,
+                               int max_rows, void *ah2, void *al2, float *r1o, float *r2o,
+                               cudaStream_t st) {
+    if (K % 8 || max_rows < 1) return cudaErrorInvalidValue;
+    const uintptr_t any = reinterpret_cast<uintptr_t>(ah) | reinterpret_cast<uintptr_t>(al) |
+                          reinterpret_cast<uintptr_t>(ah2) | reinterpret_cast<uintptr_t>(al2);
+    if (any & 15) return cudaErrorMisalignedAddress;
+    const int w16 = K / 8;  // 16-byte words of a BF16 row
+    const size_t total = (size_t)max_rows * w16;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 4);
+    gather_open_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(
+        counters, fail_rows, static_cast<const uint4 *>(ah), static_cast<const uint4 *>(al), r1, r2,
+        w16, static_cast<uint4 *>(ah2), static_cast<uint4 *>(al2), r1o, r2o);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fallback(const Params &P, const float *centroids, int k, const float *q_rot,
                             const float *s_q, const float *norms, const uint8_t *codes, size_t n,
-                            const int *fail_rows, int *counters, int fb_ctas,
+                            const int *fail_rows, int *counters, int fb_ctas, bool tensor_pass,
                             const FallbackBuffers &fb, float *out_d, long long *out_i,
                             int max_rows, cudaStream_t st) {
     if (k < 1 || k > kTopKMax || fb_ctas < 1 || max_rows < 1) return cudaErrorInvalidValue;
@@ -822,24 +922,38 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    // chunks start at code indices that are multiples of 16: 16-byte aligned
-    // with the base
+    const unsigned rblocks = (unsigned)((max_rows + 7) / 8);
+    int *scan_n = fb.coll_n + max_rows;
+    // tier 1: the tensor-core pass's lists (coll_n[0..R) was zeroed before it)
+    if (P.nibble)
+        tensor_select_kernel<true><<<rblocks, 256, 0, st>>>(
+            P, centroids, q_rot, s_q, norms, codes, n, codes_al4(P, codes), counters, fail_rows,
+            fb.tthr, tensor_pass, k, fb.coll_n, fb.coll_i, fb.scan_rows, out_d, out_i);
+    else
+        tensor_select_kernel<false><<<rblocks, 256, 0, st>>>(
+            P, centroids, q_rot, s_q, norms, codes, n, codes_al4(P, codes), counters, fail_rows,
+            fb.tthr, tensor_pass, k, fb.coll_n, fb.coll_i, fb.scan_rows, out_d, out_i);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // tier 2: the exact scan.  Chunks start at code indices that are multiples
+    // of 16: 16-byte aligned with the base.
     const bool al16 = (reinterpret_cast<uintptr_t>(codes) & 15) == 0;
     constexpr int kThreads = 256;
     constexpr size_t kSmemMax = 224 * 1024;
-    // threshold pass: term tables when nibble codes have D >= 64 and the
-    // tables leave room for two chunks of at least 16 codes
+    // term tables when nibble codes have D >= 64 and the tables leave room for
+    // two chunks of at least 16 codes
     const size_t cs = (size_t)P.cs;
     const size_t tab_bytes = (size_t)P.pb * (64 + 4) * 4;
     const bool tab = P.nibble && P.D >= 64 && P.pb % 32 == 0 && tab_bytes + 32 * cs <= kSmemMax;
     const size_t tb = tab ? tab_bytes : 0;
     const int chunk = (int)std::min<size_t>(256, (kSmemMax - std::min(tb, kSmemMax)) / (2 * cs)) & ~15;
     const bool collected = chunk >= 16 && (cs & 3) == 0;
-    e = cudaMemsetAsync(fb.coll_n, 0, (size_t)max_rows * sizeof(int), st);
+    e = cudaMemsetAsync(scan_n, 0, (size_t)max_rows * sizeof(int), st);
     if (e != cudaSuccess) return e;
     if (collected) {
-        const CollectArgs ca{P,  centroids, q_rot,    s_q,   norms,     codes,    n,
-                             al16, fail_rows, counters, fb.thr, fb.coll_n, fb.coll_d, fb.coll_i};
+        const CollectArgs ca{P,         centroids,    q_rot,    s_q,    norms,  codes,     n,
+                             al16,      fail_rows,    fb.scan_rows, counters, fb.thr, scan_n,
+                             fb.coll_d, fb.coll_i};
         const size_t smem = tb + 2 * (size_t)chunk * cs;
         auto kern = !P.nibble ? fallback_collect_kernel<false, false>
                               : (tab ? fallback_collect_kernel<true, true> : fallback_collect_kernel<true, false>);
@@ -853,14 +967,15 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    const unsigned rblocks = (unsigned)((max_rows + 7) / 8);
-    fallback_select_kernel<<<rblocks, 256, 0, st>>>(counters, fail_rows, k, collected, fb.coll_n,
-                                                    fb.coll_d, fb.coll_i, fb.fail2, out_d, out_i);
+    fallback_select_kernel<<<rblocks, 256, 0, st>>>(counters, fail_rows, fb.scan_rows, k, collected,
+                                                    scan_n, fb.coll_d, fb.coll_i, fb.list_rows,
+                                                    out_d, out_i);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // list pass: codes per staged chunk up to 256, at most 96 KB of shared
-    // memory, a multiple of 16 so that every chunk starts 16-byte aligned
-    const FallbackArgs a{P, centroids, k, q_rot, s_q, norms, codes, n, al16, fb.fail2, counters,
+    // tier 3: the list pass.  Codes per staged chunk up to 256, at most 96 KB
+    // of shared memory, a multiple of 16 so that every chunk starts 16-byte
+    // aligned.
+    const FallbackArgs a{P,  centroids, k, q_rot, s_q, norms, codes, n, al16, fb.list_rows, counters,
                          fb.part_d, fb.part_i};
     int lchunk = (int)std::min<size_t>(256, (size_t)(96 * 1024) / cs) & ~15;
     if (lchunk < 16) lchunk = 16;
@@ -871,7 +986,7 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
     lkern<<<fb_ctas, 256, lsmem, st>>>(a, lchunk);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    fallback_merge_kernel<<<rblocks, 256, 0, st>>>(counters, fb.fail2, fb_ctas, k, fb.part_d,
+    fallback_merge_kernel<<<rblocks, 256, 0, st>>>(counters, fb.list_rows, fb_ctas, k, fb.part_d,
                                                    fb.part_i, out_d, out_i);
     return cudaGetLastError();
 }

@@ -14,13 +14,21 @@ constexpr int kBoundFloats = 4;
 cudaError_t launch_index_bound(const Params &P, const uint8_t *codes, size_t n, float *bound,
                                cudaStream_t st);
 
-// Counters of the exact stages (device ints, zeroed before each batch):
-// rows the certificate left open, candidates outside the bound, and open rows
-// whose collection overflowed (answered by the list pass).
-enum { kCntFallbackRows = 0, kCntBoundViolations = 1, kCntOverflowRows = 2, kCntWords = 4 };
+// Counters of the exact stages (device ints, zeroed before each batch): rows
+// the certificate left open, candidates outside the bound, open rows taken by
+// the exact scan, and rows taken by the list pass (see launch_fallback).
+enum {
+    kCntFallbackRows = 0,
+    kCntBoundViolations = 1,
+    kCntScanRows = 2,
+    kCntListRows = 3,
+    kCntWords = 4
+};
 
-// Codes collected per open row by the fallback's threshold pass.
+// Codes collected per open row by a threshold pass.
 constexpr int kCollectCap = 1024;
+// The tensor-core threshold pass runs when more rows than this are open.
+constexpr int kTensorTierMinRows = 8;
 
 // Candidate rescoring: one warp per query row (row count read from m_dev).
 // cand_d / cand_i hold each row's kc (<= 32) tensor-pass candidates, ascending
@@ -29,41 +37,56 @@ constexpr int kCollectCap = 1024;
 // (distance, index) go to out_d / out_i.  The row is certified when its k-th
 // exact distance is below the kc-th approximate distance minus the error
 // bound of the tensor pass (so no code outside the candidates can enter the
-// top-k); otherwise its index is appended to fail_rows (counters[0]) and its
-// k-th exact candidate distance to thr at the same position.  A candidate
-// whose approximate and exact distances differ by more than the bound is
-// counted in counters[1] and fails its row as well.
+// top-k); otherwise its index is appended to fail_rows (counters[0]), its k-th
+// exact candidate distance e_k to thr and e_k + eps (rounded up; -1 when a
+// candidate broke the bound) to tthr, at the same position.  A candidate whose
+// approximate and exact distances differ by more than the bound eps is counted
+// in counters[1] and fails its row as well.
 // cmax = max_v |c_v| of the space's centroid table.
 cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, const int *m_dev,
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
                            const uint8_t *codes, size_t n, const float *bound, float bound_scale,
-                           float *out_d, long long *out_i, int *fail_rows, float *thr,
+                           float *out_d, long long *out_i, int *fail_rows, float *thr, float *tthr,
                            int *counters, int max_rows, cudaStream_t st);
 
-// Device buffers of the fallback (max_rows = R open rows at most).
+// The open rows' query planes and scales, gathered to rows 0 .. nf-1 for the
+// tensor-core threshold pass (nothing unless nf = counters[0] exceeds
+// kTensorTierMinRows).  Planes: rows of K BF16 values.
+cudaError_t launch_gather_open(const int *counters, const int *fail_rows, const void *ah,
+                               const void *al, const float *r1, const float *r2, int K,
+                               int max_rows, void *ah2, void *al2, float *r1o, float *r2o,
+                               cudaStream_t st);
+
+// Device buffers of the fallback (R = max_rows open rows at most).
 struct FallbackBuffers {
-    const float *thr;  // R: written by the rescoring
-    int *coll_n;       // R
-    float *coll_d;     // R * kCollectCap
-    int *coll_i;       // R * kCollectCap
-    int *fail2;        // R: rows whose collection overflowed
-    float *part_d;     // R * fb_ctas * k
-    int *part_i;       // R * fb_ctas * k
+    const float *thr;   // R: e_k, from the rescoring
+    const float *tthr;  // R: e_k + eps, from the rescoring
+    int *coll_n;        // 2R: counts of the tensor pass's lists, then of the exact scan's
+    float *coll_d;      // R * kCollectCap
+    int *coll_i;        // R * kCollectCap: the tensor pass's lists, then the exact scan's
+    int *scan_rows;     // R: positions in fail_rows taken by the exact scan
+    int *list_rows;     // R: rows taken by the list pass
+    float *part_d;      // R * fb_ctas * k
+    int *part_i;        // R * fb_ctas * k
 };
 
-// Fallback for the rows in fail_rows, exact by construction:
-//   collect  every code whose exact distance is at most the row's thr (the
-//            k-th exact distance among its candidates, so at least the true
-//            k-th: every member of the true top-k passes);
-//   select   the k best collected by (distance, index) into out_d / out_i;
-//   a row that collected more than kCollectCap codes goes to a full pass
-//   with per-CTA top-k lists (fb_ctas CTAs) merged per row.
+// The rows in fail_rows, exact by construction, in three tiers:
+//   1. (tensor_pass: launch_tc_thresh ran on the gathered open rows with
+//      thr = tthr, lists in coll_i / coll_n[0..R)) when more than
+//      kTensorTierMinRows rows are open and the row's bound held: the k best
+//      of its list by (exact distance, index).  Every code of the true top-k
+//      is in the list: its tensor-pass distance is at most its exact one +
+//      eps <= e_k + eps.
+//   2. the others: an exact scan of every code, collecting those at or below
+//      e_k (every member of the true top-k), then the k best of them.
+//   3. rows with more than kCollectCap codes in tier 2: a full pass with
+//      per-CTA top-k lists (fb_ctas CTAs) merged per row.
 // Every kernel returns at once when it has no row.
 int fallback_ctas(int sms);
 cudaError_t launch_fallback(const Params &P, const float *centroids, int k, const float *q_rot,
                             const float *s_q, const float *norms, const uint8_t *codes, size_t n,
-                            const int *fail_rows, int *counters, int fb_ctas,
+                            const int *fail_rows, int *counters, int fb_ctas, bool tensor_pass,
                             const FallbackBuffers &fb, float *out_d, long long *out_i,
                             int max_rows, cudaStream_t st);
 

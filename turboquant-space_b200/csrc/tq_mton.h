@@ -103,6 +103,16 @@ cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size
 // Whether `variant` runs with decoded B tiles for codes of cs bytes (a tile of
 // 128 codes must fit in shared memory beside the variant's stages).
 bool tc_topk_dec_ok(int variant, int cs);
+// Threshold collection over the corpus for the rows of A (row count *m_dev,
+// nothing unless it exceeds min_rows): every column whose tile distance (as the
+// top-k pass computes it) is at most thr[row] goes to coll_i[row * cap + ...],
+// counted in coll_n[row] (which may exceed cap: overflow).  Planes (Bh, Bl,
+// k_lo) or, with dec, decoded B tiles; variant 4's tile shape.
+cudaError_t launch_tc_thresh(const void *Ah, const void *Al, size_t rows_pad, const void *Bh,
+                             const void *Bl, const DecSrc *dec, size_t n_pad, int K, int k_lo,
+                             const int *m_dev, int min_rows, size_t n, const float *r1,
+                             const float *r2, const float *c1, const float *c2, const float *thr,
+                             int *coll_n, int *coll_i, int cap, int *err, int grid, cudaStream_t st);
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,
                               const int *part_i, int k, size_t max_rows, float *out_d,
                               long long *out_i, cudaStream_t st);

@@ -120,9 +120,12 @@ struct Slot {
     long long *h_i = nullptr;
     void *d_block = nullptr;  // one device allocation for all buffers below
     float *d_q = nullptr, *d_prep = nullptr, *d_r1 = nullptr, *d_r2 = nullptr, *d_pd = nullptr,
-          *d_od = nullptr, *d_cd = nullptr, *d_fpd = nullptr, *d_thr = nullptr, *d_colld = nullptr;
+          *d_od = nullptr, *d_cd = nullptr, *d_fpd = nullptr, *d_thr = nullptr, *d_colld = nullptr,
+          *d_tthr = nullptr, *d_r1o = nullptr, *d_r2o = nullptr;
     int *d_m = nullptr, *d_pi = nullptr, *d_err = nullptr, *d_fail = nullptr, *d_cnt = nullptr,
-        *d_fpi = nullptr, *d_colln = nullptr, *d_colli = nullptr, *d_fail2 = nullptr;
+        *d_fpi = nullptr, *d_colln = nullptr, *d_colli = nullptr, *d_scan = nullptr,
+        *d_list_rows = nullptr;
+    void *d_ap2 = nullptr;  // the open rows' query planes (same shape as d_ap)
     long long *d_ci = nullptr;
     int *h_cnt = nullptr;  // pinned copy of d_cnt after each batch
     int *h_rows = nullptr;  // pool row of each batch row (pinned)
@@ -165,7 +168,7 @@ struct tq_server {
     bool stop = false;
     // stats
     uint64_t submitted = 0, rejected = 0, completed = 0, batches = 0, rows_done = 0;
-    uint64_t fallback_rows = 0, bound_violations = 0, list_pass_rows = 0;
+    uint64_t fallback_rows = 0, bound_violations = 0, scan_pass_rows = 0, list_pass_rows = 0;
     std::vector<float> latencies_ms;  // ring of the most recent completions
     size_t lat_pos = 0;
     double busy_ms = 0;
@@ -254,14 +257,11 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
                                         ah, al, sl.d_r1, sl.d_r2, st);
     if (e != cudaSuccess) return e;
     // tensor-core pass: each row's kc best candidates by approximate distance
-    if (ix->layout == TQ_INDEX_PLANES) {
-        unsigned char *bh = static_cast<unsigned char *>(ix->planes);
-        unsigned char *bl = bh + ix->n_pad * K * 2;
-        e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
-                               sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
-                               sv->grid, st);
-    } else {  // the column tiles decoded in shared memory from the codes
-        tq::DecSrc dec;
+    const bool planes = ix->layout == TQ_INDEX_PLANES;
+    unsigned char *bh = planes ? static_cast<unsigned char *>(ix->planes) : nullptr;
+    unsigned char *bl = planes ? bh + ix->n_pad * K * 2 : nullptr;
+    tq::DecSrc dec;  // codes layout: the column tiles decoded in shared memory
+    if (!planes) {
         dec.codes = ix->codes;
         dec.n = (unsigned)ix->n;
         dec.cs = (int)sp->code_size;
@@ -271,10 +271,15 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
         dec.fs = ix->fs;
         dec.centroids = sp->T.centroids;
         dec.levels = sp->levels;
+    }
+    if (planes)
+        e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
+                               sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
+                               sv->grid, st);
+    else
         e = tq::launch_tc_topk_dec(var, ah, al, rows_cap, dec, ix->n_pad, (int)K, sl.d_m, ix->n,
                                    sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
                                    sv->grid, st);
-    }
     if (e != cudaSuccess) return e;
     e = tq::launch_topk_merge(sl.d_m, sv->grid, tq::tc_topk_lists(var), sl.d_pd, sl.d_pi, sv->kc,
                               rows_cap, sl.d_cd, sl.d_ci, st);
@@ -285,12 +290,25 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     if (e != cudaSuccess) return e;
     e = tq::launch_rescore(sp->P, sp->T.centroids, ix->cmax, sl.d_m, sv->kc, sv->k, sl.d_cd, sl.d_ci,
                            q_rot, s_q, norms, ix->codes, ix->n, ix->bound, sv->bound_scale, sl.d_od,
-                           sl.d_oi, sl.d_fail, sl.d_thr, sl.d_cnt, rows_cap, st);
+                           sl.d_oi, sl.d_fail, sl.d_thr, sl.d_tthr, sl.d_cnt, rows_cap, st);
     if (e != cudaSuccess) return e;
-    const tq::FallbackBuffers fb{sl.d_thr, sl.d_colln, sl.d_colld, sl.d_colli,
-                                 sl.d_fail2, sl.d_fpd, sl.d_fpi};
+    // the open rows' threshold pass on the tensor cores (when enough are open)
+    e = cudaMemsetAsync(sl.d_colln, 0, (size_t)rows_cap * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    unsigned char *ah2 = static_cast<unsigned char *>(sl.d_ap2);
+    unsigned char *al2 = ah2 + (size_t)rows_cap * K * 2;
+    e = tq::launch_gather_open(sl.d_cnt, sl.d_fail, ah, al, sl.d_r1, sl.d_r2, (int)K, rows_cap, ah2, al2,
+                               sl.d_r1o, sl.d_r2o, st);
+    if (e != cudaSuccess) return e;
+    e = tq::launch_tc_thresh(ah2, al2, rows_cap, bh, bl, planes ? nullptr : &dec, ix->n_pad, (int)K,
+                             ix->K_lo, sl.d_cnt + tq::kCntFallbackRows, tq::kTensorTierMinRows, ix->n,
+                             sl.d_r1o, sl.d_r2o, ix->c1, ix->c2, sl.d_tthr, sl.d_colln, sl.d_colli,
+                             tq::kCollectCap, sl.d_err, sv->grid, st);
+    if (e != cudaSuccess) return e;
+    const tq::FallbackBuffers fb{sl.d_thr,  sl.d_tthr,      sl.d_colln, sl.d_colld, sl.d_colli,
+                                 sl.d_scan, sl.d_list_rows, sl.d_fpd,   sl.d_fpi};
     e = tq::launch_fallback(sp->P, sp->T.centroids, sv->k, q_rot, s_q, norms, ix->codes, ix->n,
-                            sl.d_fail, sl.d_cnt, sv->fb_ctas, fb, sl.d_od, sl.d_oi, rows_cap, st);
+                            sl.d_fail, sl.d_cnt, sv->fb_ctas, true, fb, sl.d_od, sl.d_oi, rows_cap, st);
     if (e != cudaSuccess) return e;
     if (copies) {
         e = cudaMemcpyAsync(sl.h_d, sl.d_od, (size_t)rows_cap * sv->k * 4, cudaMemcpyDeviceToHost, st);
@@ -336,9 +354,10 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     const size_t kc = (size_t)sv->kc, fparts = R * (size_t)sv->fb_ctas * k;
     const size_t o_cd = take(R * kc * 4), o_ci = take(R * kc * 8), o_fail = take(R * 4);
     const size_t o_cnt = take(tq::kCntWords * 4), o_fpd = take(fparts * 4), o_fpi = take(fparts * 4);
-    const size_t o_rows = take(R * 4), o_thr = take(R * 4), o_colln = take(R * 4);
+    const size_t o_rows = take(R * 4), o_thr = take(R * 4), o_tthr = take(R * 4), o_colln = take(2 * R * 4);
     const size_t o_colld = take(R * tq::kCollectCap * 4), o_colli = take(R * tq::kCollectCap * 4);
-    const size_t o_fail2 = take(R * 4);
+    const size_t o_scan = take(R * 4), o_list = take(R * 4), o_ap2 = take(R * K * 4);
+    const size_t o_r1o = take(R * 4), o_r2o = take(R * 4);
     TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
     TQ_CUDA(cudaMemset(sl.d_block, 0, off), "cudaMemset(slot)");
     auto *base = static_cast<unsigned char *>(sl.d_block);
@@ -361,10 +380,15 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     sl.d_fpi = reinterpret_cast<int *>(base + o_fpi);
     sl.d_rows = reinterpret_cast<int *>(base + o_rows);
     sl.d_thr = reinterpret_cast<float *>(base + o_thr);
+    sl.d_tthr = reinterpret_cast<float *>(base + o_tthr);
     sl.d_colln = reinterpret_cast<int *>(base + o_colln);
     sl.d_colld = reinterpret_cast<float *>(base + o_colld);
     sl.d_colli = reinterpret_cast<int *>(base + o_colli);
-    sl.d_fail2 = reinterpret_cast<int *>(base + o_fail2);
+    sl.d_scan = reinterpret_cast<int *>(base + o_scan);
+    sl.d_list_rows = reinterpret_cast<int *>(base + o_list);
+    sl.d_ap2 = base + o_ap2;
+    sl.d_r1o = reinterpret_cast<float *>(base + o_r1o);
+    sl.d_r2o = reinterpret_cast<float *>(base + o_r2o);
     for (int b = 128; b < sv->max_rows; b *= 2) sl.bucket_rows.push_back(b);
     sl.bucket_rows.push_back(sv->max_rows);
     return TQ_OK;
@@ -562,7 +586,8 @@ void worker_loop(tq_server *sv) {
             if (q == cudaSuccess) {
                 sv->fallback_rows += (uint64_t)sl.h_cnt[tq::kCntFallbackRows];
                 sv->bound_violations += (uint64_t)sl.h_cnt[tq::kCntBoundViolations];
-                sv->list_pass_rows += (uint64_t)sl.h_cnt[tq::kCntOverflowRows];
+                sv->scan_pass_rows += (uint64_t)sl.h_cnt[tq::kCntScanRows];
+                sv->list_pass_rows += (uint64_t)sl.h_cnt[tq::kCntListRows];
             }
             size_t row = 0;
             for (tq_request *r : sl.batch) {
@@ -904,6 +929,7 @@ tq_status tq_server_get_stats(tq_server *sv, tq_server_stats *out, float *latenc
     out->candidates = sv->kc;
     out->fallback_rows = sv->fallback_rows;
     out->bound_violations = sv->bound_violations;
+    out->scan_pass_rows = sv->scan_pass_rows;
     out->list_pass_rows = sv->list_pass_rows;
     out->pool_rows = sv->pool_rows;
     out->pool_used_rows = sv->pool_used;
@@ -917,7 +943,7 @@ tq_status tq_server_reset_stats(tq_server *sv) {
     if (!sv) return fail(TQ_ERR_INVALID_ARGUMENT, "NULL server");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->submitted = sv->rejected = sv->completed = sv->batches = sv->rows_done = 0;
-    sv->fallback_rows = sv->bound_violations = sv->list_pass_rows = 0;
+    sv->fallback_rows = sv->bound_violations = sv->scan_pass_rows = sv->list_pass_rows = 0;
     sv->latencies_ms.clear();
     sv->lat_pos = 0;
     return TQ_OK;

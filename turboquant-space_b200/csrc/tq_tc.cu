@@ -1029,6 +1029,94 @@ struct TopkEpi {
     };
 };
 
+// The threshold collection of the exact stage's open rows: the tile
+// distances as TopkEpi computes them; every column whose distance is at most
+// the row's thr is appended to the row's list (coll_n / coll_i, cap entries
+// each; the count keeps growing past cap, which tells the reader the list
+// overflowed, and a thread stops appending once it sees that).  No tiles at
+// all unless the row count exceeds min_rows.
+struct ThreshEpi {
+    struct Params {
+        const int *m_dev;
+        int min_rows;
+        unsigned nb_tiles;
+        size_t n;
+        const float *r1, *r2, *c1, *c2;
+        const float *thr;
+        int *coll_n;
+        int *coll_i;
+        int cap;
+    };
+    __device__ static bool slice(const Params &p, int &mb, unsigned &nb0, unsigned &nb1) {
+        const int m = *p.m_dev;
+        if (m <= p.min_rows) return false;
+        const int num_mb = (m + TC_BM - 1) / TC_BM;
+        if (num_mb <= 0 || num_mb > (int)gridDim.x) return false;
+        const int S = (int)gridDim.x / num_mb;
+        if ((int)blockIdx.x >= num_mb * S) return false;
+        mb = (int)blockIdx.x / S;
+        const int sl = (int)blockIdx.x % S;
+        nb0 = (unsigned)(((size_t)p.nb_tiles * sl) / S);
+        nb1 = (unsigned)(((size_t)p.nb_tiles * (sl + 1)) / S);
+        return true;
+    }
+    __device__ static int tiles(const Params &p) {
+        int mb;
+        unsigned nb0, nb1;
+        return slice(p, mb, nb0, nb1) ? (int)(nb1 - nb0) : 0;
+    }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) {
+        unsigned nb0, nb1;
+        slice(p, mb, nb0, nb1);
+        nb = (int)nb0 + t;
+    }
+    struct State {
+        int rit, m;
+        float rr1 = 0.0f, rr2 = 0.0f, T = -INFINITY;
+        bool full = false;
+        __device__ State(const Params &p, int row_in_tile) : rit(row_in_tile) {
+            int mb;
+            unsigned nb0, nb1;
+            m = *p.m_dev;
+            const bool valid = slice(p, mb, nb0, nb1);
+            const int row = valid ? mb * TC_BM + rit : 0;
+            if (valid && row < m) {
+                rr1 = __ldg(p.r1 + row);
+                rr2 = __ldg(p.r2 + row);
+                T = __ldg(p.thr + row);
+            }
+        }
+        __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
+            const int row = mb * TC_BM + rit;
+            const bool row_ok = row < m;
+            const size_t colbase = (size_t)nb * TC_BN;
+#pragma unroll 1
+            for (int ch = 0; ch < TC_BN / 32; ++ch) {
+                float c[32];
+                ld_sum32(y0 + 32 * ch, c);  // warp-collective: every lane loads
+                if (!row_ok || full) continue;
+                const size_t col0 = colbase + ch * 32;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const size_t col = col0 + j;
+                    if (col >= p.n) break;
+                    const float ipt = __fmul_rn(__fmul_rn(c[j], rr1), __ldg(p.c1 + col));
+                    float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
+                    d = d > 0.0f ? d : 0.0f;
+                    if (d <= T && !full) {
+                        const int pos = atomicAdd(p.coll_n + row, 1);
+                        if (pos < p.cap)
+                            p.coll_i[(size_t)row * p.cap + pos] = (int)col;
+                        else
+                            full = true;
+                    }
+                }
+            }
+        }
+        __device__ void finish(const Params &) {}
+    };
+};
+
 // ---- epilogue policies of tcw_kernel: each thread holds one row's running
 // sums of TW_COLS columns (half h of the 256-column tile) in registers.
 struct WDist {
@@ -1519,6 +1607,33 @@ cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size
         case 4: return tcp_launch<false, 2, 8, true, TopkEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
         default: return tcp_launch<false, 3, 8, true, TopkEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
     }
+}
+
+cudaError_t launch_tc_thresh(const void *Ah, const void *Al, size_t rows_pad, const void *Bh,
+                             const void *Bl, const DecSrc *dec, size_t n_pad, int K, int k_lo,
+                             const int *m_dev, int min_rows, size_t n, const float *r1,
+                             const float *r2, const float *c1, const float *c2, const float *thr,
+                             int *coll_n, int *coll_i, int cap, int *err, int grid, cudaStream_t st) {
+    if (grid < 1 || cap < 1 || K % TC_BK || rows_pad % TC_BM || n_pad % TC_BN || n > n_pad)
+        return cudaErrorInvalidValue;
+    if (!aligned16({Ah, Al})) return cudaErrorMisalignedAddress;
+    const ThreshEpi::Params ep{m_dev, min_rows, (unsigned)(n_pad / TC_BN), n,      r1,  r2,
+                               c1,    c2,       thr,                      coll_n, coll_i, cap};
+    alignas(64) TcMaps mp;
+    TcShape sh{};
+    if (dec) {
+        // variant 4's shape with decoded B tiles
+        if (!dec_ok(*dec, K) || dec->kbc * 2 != K / TC_BK || !dec->fc || !dec->fs)
+            return cudaErrorInvalidValue;
+        if (!a_maps(mp, sh, Ah, Al, rows_pad, K, dec->kbc)) return cudaErrorInvalidValue;
+        const DecSrc d = with_code_buffers(*dec, 2);
+        if (d.cbufs == 0) return cudaErrorInvalidValue;
+        return tcp_launch<false, 2, 8, true, ThreshEpi, true>(mp, sh, ep, err, (unsigned)grid, st, d);
+    }
+    if (k_lo % TC_BK || k_lo <= 0 || k_lo > K) return cudaErrorInvalidValue;
+    if (!aligned16({Bh, Bl})) return cudaErrorMisalignedAddress;
+    if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
+    return tcp_launch<false, 2, 8, true, ThreshEpi>(mp, sh, ep, err, (unsigned)grid, st);
 }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,

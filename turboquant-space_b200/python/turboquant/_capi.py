@@ -50,7 +50,8 @@ class ServerStats(C.Structure):
         ("batches", C.c_uint64), ("rows", C.c_uint64), ("queued_rows", C.c_size_t),
         ("slots", C.c_int), ("max_rows", C.c_int), ("candidates", C.c_int),
         ("fallback_rows", C.c_uint64), ("bound_violations", C.c_uint64),
-        ("pool_rows", C.c_size_t), ("pool_used_rows", C.c_size_t), ("list_pass_rows", C.c_uint64),
+        ("pool_rows", C.c_size_t), ("pool_used_rows", C.c_size_t), ("scan_pass_rows", C.c_uint64),
+        ("list_pass_rows", C.c_uint64),
     ]
 
 
