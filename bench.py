@@ -608,7 +608,8 @@ def serve_result(args, rates, window, cpu=True, layout="planes"):
     del codes
     torch.cuda.empty_cache()
     t0 = time.perf_counter()
-    server = index.serve(k=10, max_rows=1024, slots=2, kernel_variant=args.kernel_variant)
+    server = index.serve(k=10, max_rows=1024, slots=2, kernel_variant=args.kernel_variant,
+                         bound_scale=getattr(args, "bound_scale", 0.0))
     setup_s = time.perf_counter() - t0
     tuning = server.tuning(searched=True)
     rng = np.random.default_rng(9)
@@ -651,6 +652,7 @@ def serve_result(args, rates, window, cpu=True, layout="planes"):
             "p99_ms": round(float(np.percentile(lat, 99)), 2),
             "batches": st["batches"], "mean_rows_per_batch": round(st["rows"] / max(1, st["batches"]), 1),
             "exact_fallback_rows": st["fallback_rows"], "bound_violations": st["bound_violations"],
+            "fallback_scan_rows": st["scan_pass_rows"], "fallback_list_rows": st["list_pass_rows"],
         })
     server.close()
     index.close()
@@ -675,6 +677,7 @@ def serve_result(args, rates, window, cpu=True, layout="planes"):
                    "window_s": window, "max_batch_rows": 1024, "slots": 2,
                    "kernel_variant": "autotuned" if args.kernel_variant < 0 else args.kernel_variant,
                    "top_k": "exact (tensor-pass candidates rescored with the reference's arithmetic)",
+                   "bound_scale": getattr(args, "bound_scale", 0.0) or 1.0,
                    "index_layout": layout, "index_bytes": index_bytes,
                    "data": "1024-centre Gaussian mixture, std 0.3, rows L2-normalised (seeds 8/9)"},
         "index_build_s": round(build_s, 2), "server_setup_s": round(setup_s, 2), "tuning": tuning,
@@ -812,8 +815,11 @@ def main():
     ap.add_argument("--layout", choices=("planes", "codes"), default="planes",
                     help="serve: index layout (operand planes, or codes decoded in shared memory)")
     ap.add_argument("--kernel-variant", type=int, default=-1,
-                    help="serve: top-k kernel variant (-1: autotuned per batch bucket; 0: 128 x 256 "
-                         "tiles; 1, 2: 128 x 128 tiles)")
+                    help="serve: top-k kernel variant (-1: autotuned per batch bucket; 0 .. 5: "
+                         "the tile shapes of turboquant.variant_shapes())")
+    ap.add_argument("--bound-scale", type=float, default=0.0,
+                    help="serve: multiple of the certificate's error bound (0: the server's default, "
+                         "1); larger values leave more rows to the exact fallback")
     ap.add_argument("--workload", choices=("scan", "mton", "sym", "symq", "serve"), default="scan",
                     help="scan (default): the 1->N scan benchmark; mton/sym: the dense M x N "
                          "contractions, FP32 vs split-BF16; symq: the QJL-corrected symmetric "
