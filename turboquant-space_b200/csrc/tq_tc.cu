@@ -919,6 +919,29 @@ __device__ __noinline__ TopkEntry topk_insert(float *bd, int *bi, int k, float d
     return TopkEntry{bd[k - 1], bi[k - 1]};
 }
 
+// Inserts (d, i), better than the last entry, into the ascending register
+// list (bd, bi) of kCandMax entries (ties broken by the smaller index).  With
+// b_u = (d, i) better than entry u, slot u takes entry u - 1 when b_{u-1},
+// else (d, i) when b_u, else keeps its entry; each slot reads only old
+// entries (slots are rewritten from the last down), so the slots do not form
+// a dependency chain.
+__device__ __forceinline__ void reg_insert(float (&bd)[kCandMax], int (&bi)[kCandMax], float d, int i) {
+    bool bu = true;  // b_{kCandMax-1}: the caller's test
+#pragma unroll
+    for (int u = kCandMax - 1; u > 0; --u) {
+        const bool bl = better(d, i, bd[u - 1], bi[u - 1]);
+        const float nd = bl ? bd[u - 1] : (bu ? d : bd[u]);
+        const int ni = bl ? bi[u - 1] : (bu ? i : bi[u]);
+        bd[u] = nd;
+        bi[u] = ni;
+        bu = bl;
+    }
+    if (bu) {
+        bd[0] = d;
+        bi[0] = i;
+    }
+}
+
 // Per-row top-k over a device-resident index.  The number of query rows m is
 // read from device memory (so that one captured launch serves batches of any
 // size up to the buffers' capacity).  CTA c takes row block c / S and the
@@ -963,10 +986,10 @@ struct TopkEpi {
         int rit, m;
         bool valid;
         float rr1 = 0.0f, rr2 = 0.0f;
+        // the row's best kCandMax entries (ascending): the first p.k of them
+        // are its best p.k
         float bd[kCandMax];
         int bi[kCandMax];
-        float thr_d = INFINITY;
-        int thr_i = 0x7fffffff;
         __device__ State(const Params &p, int row_in_tile) : rit(row_in_tile) {
             int mb;
             unsigned nb0, nb1;
@@ -983,34 +1006,45 @@ struct TopkEpi {
                 bi[t] = 0x7fffffff;
             }
         }
+        // Each 32-column chunk: the distances in registers and a mask of the
+        // columns that beat the list's last entry; only when some column does,
+        // the chunk's distances go to a local array and the marked columns are
+        // inserted one by one.  Late in a slice few chunks have any.
         __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
             const bool row_ok = mb * TC_BM + rit < m;
             const size_t colbase = (size_t)nb * TC_BN;
-            float td = thr_d;
-            int ti = thr_i;
 #pragma unroll 1
             for (int ch = 0; ch < TC_BN / 32; ++ch) {
                 float c[32];
                 ld_sum32(y0 + 32 * ch, c);
                 if (!row_ok) continue;
                 const size_t col0 = colbase + ch * 32;
+                const float td = bd[kCandMax - 1];
+                const int ti = bi[kCandMax - 1];
+                uint32_t pass = 0u;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
+                for (int j = 0; j < 32; ++j) {  // c[j] <- the column's distance
                     const size_t col = col0 + j;
-                    if (col >= p.n) break;
-                    const float ipt = __fmul_rn(__fmul_rn(c[j], rr1), __ldg(p.c1 + col));
-                    float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
+                    const size_t cc = col < p.n ? col : p.n - 1;
+                    const float ipt = __fmul_rn(__fmul_rn(c[j], rr1), __ldg(p.c1 + cc));
+                    float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + cc)), __fmul_rn(2.0f, ipt));
                     d = d > 0.0f ? d : 0.0f;
-                    const int ci = (int)col;
-                    if (better(d, ci, td, ti)) {
-                        const TopkEntry e = topk_insert(bd, bi, p.k, d, ci);
-                        td = e.d;
-                        ti = e.i;
-                    }
+                    c[j] = d;
+                    if (col < p.n && better(d, (int)col, td, ti)) pass |= 1u << j;
+                }
+                if (pass) {
+                    float sd[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sd[j] = c[j];
+                    do {
+                        const int j = __ffs(pass) - 1;
+                        pass &= pass - 1u;
+                        const float d = sd[j];
+                        const int ci = (int)(col0 + (size_t)j);
+                        if (better(d, ci, bd[kCandMax - 1], bi[kCandMax - 1])) reg_insert(bd, bi, d, ci);
+                    } while (pass);
                 }
             }
-            thr_d = td;
-            thr_i = ti;
         }
         __device__ void finish(const Params &p) {
             if (!valid) return;
