@@ -600,12 +600,14 @@ __global__ void __launch_bounds__(256) fallback_select_kernel(int *counters, con
 // (more than kTensorTierMinRows open rows), its bound held (tthr >= 0) and its
 // list did not overflow, the lanes score the listed codes with the
 // reference's arithmetic and the row's k best by (distance, index) go to the
-// output; every other row goes to the exact scan's rows.
+// output.  The list holds the row's k best candidates (exact distance <= e_k)
+// whenever the bound holds for them, so a k-th distance above e_k means it
+// did not: that row, like every other, goes to the exact scan's rows.
 template <bool NIBBLE>
 __global__ void __launch_bounds__(256) tensor_select_kernel(
     Params P, const float *centroids, const float *q_rot, const float *s_q, const float *norms,
     const uint8_t *codes, size_t n, bool al4, int *counters, const int *fail_rows,
-    const float *tthr, bool tensor_pass, int k, const int *__restrict__ coll_n,
+    const float *thr, const float *tthr, bool tensor_pass, int k, const int *__restrict__ coll_n,
     const int *__restrict__ coll_i, int *scan_rows, float *out_d, long long *out_i) {
     const int nf = counters[kCntFallbackRows];
     if (nf == 0) return;
@@ -640,6 +642,11 @@ __global__ void __launch_bounds__(256) tensor_select_kernel(
         float md;
         int mi;
         warp_merge(bd, bi, k, lane, md, mi);
+        const float kth = __shfl_sync(kFull, md, k - 1);
+        if (!(kth <= thr[f])) {
+            if (lane == 0) scan_rows[atomicAdd(&counters[kCntScanRows], 1)] = f;
+            continue;
+        }
         if (lane < k) {
             out_d[(size_t)row * k + lane] = md;
             out_i[(size_t)row * k + lane] = mi == kNoIdx ? -1 : (long long)mi;
@@ -928,11 +935,11 @@ cudaError_t launch_fallback(const Params &P, const float *centroids, int k, cons
     if (P.nibble)
         tensor_select_kernel<true><<<rblocks, 256, 0, st>>>(
             P, centroids, q_rot, s_q, norms, codes, n, codes_al4(P, codes), counters, fail_rows,
-            fb.tthr, tensor_pass, k, fb.coll_n, fb.coll_i, fb.scan_rows, out_d, out_i);
+            fb.thr, fb.tthr, tensor_pass, k, fb.coll_n, fb.coll_i, fb.scan_rows, out_d, out_i);
     else
         tensor_select_kernel<false><<<rblocks, 256, 0, st>>>(
             P, centroids, q_rot, s_q, norms, codes, n, codes_al4(P, codes), counters, fail_rows,
-            fb.tthr, tensor_pass, k, fb.coll_n, fb.coll_i, fb.scan_rows, out_d, out_i);
+            fb.thr, fb.tthr, tensor_pass, k, fb.coll_n, fb.coll_i, fb.scan_rows, out_d, out_i);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // tier 2: the exact scan.  Chunks start at code indices that are multiples
