@@ -530,8 +530,10 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
     const bool vec4 = ((P.dim & 3) == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
     const size_t nquads = (n + 3) >> 2;
 
-    // The warps of a block step through the phases together (block barriers
-    // between phase groups), so the block executes one phase's code at a time.
+    // Each warp steps through the phases of its own quads on its own: the
+    // buffers are the warp's and the tables read-only, so the phases are
+    // ordered by warp barriers alone, and a warp in a reduction chain overlaps
+    // another warp's transforms (block barriers here cost 11%).
     for (size_t base = (size_t)blockIdx.x * nwarps; base < nquads; base += (size_t)gridDim.x * nwarps) {
         const size_t qd = base + warp;
         const bool active = qd < nquads;
@@ -580,7 +582,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
             norm = __fsqrt_rn(nsq);
             inv_norm = (nsq > f32_bits(kNormSqFloorBits)) ? __fdiv_rn(1.0f, norm) : 0.0f;
         }
-        __syncthreads();
+        __syncwarp();
         // C: rotated = RHT_rot(raw * inv_norm), written back in layout B; D: sigma
         float sigma = 0.0f, inv_sigma = 0.0f;
         if (active) {
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 inv_sigma = __fdiv_rn(1.0f, sigma);
             }
         }
-        __syncthreads();
+        __syncwarp();
         // E: quantize + residual in layout B, four indices per lane-word into
         // the per-warp index array; F: gamma
         float gamma = 0.0f;
@@ -636,7 +638,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
             __syncwarp();
             gamma = __fsqrt_rn(chain_sq_reduce2<E, true>(buf + g * VS, D, lane));
         }
-        __syncthreads();
+        __syncwarp();
         // G: RHT_qjl(residual), pack units + trailer; H: staged codes -> global
         if (active) {
 #pragma unroll 1
@@ -684,7 +686,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 for (int i = lane; i < len; i += 32) dst[i] = stage[i];
             }
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
