@@ -1006,7 +1006,7 @@ struct TopkEpi {
                 bi[t] = 0x7fffffff;
             }
         }
-        // Each 32-column chunk: the distances in registers and a mask of the
+        // Each 16-column chunk: the distances in registers and a mask of the
         // columns that beat the list's last entry; only when some column does,
         // the chunk's distances go to a local array and the marked columns are
         // inserted one by one.  Late in a slice few chunks have any.
@@ -1014,28 +1014,31 @@ struct TopkEpi {
             const bool row_ok = mb * TC_BM + rit < m;
             const size_t colbase = (size_t)nb * TC_BN;
 #pragma unroll 1
-            for (int ch = 0; ch < TC_BN / 32; ++ch) {
-                float c[32];
-                ld_sum32(y0 + 32 * ch, c);
+            for (int ch = 0; ch < TC_BN / 16; ++ch) {
+                uint32_t r[16];
+                __syncwarp();
+                tmem_ld16_nw(y0 + 16 * ch, r);  // warp-collective: every lane loads
+                tmem_wait_ld();
                 if (!row_ok) continue;
-                const size_t col0 = colbase + ch * 32;
+                const size_t col0 = colbase + ch * 16;
                 const float td = bd[kCandMax - 1];
                 const int ti = bi[kCandMax - 1];
+                float c[16];
                 uint32_t pass = 0u;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {  // c[j] <- the column's distance
+                for (int j = 0; j < 16; ++j) {  // c[j] <- the column's distance
                     const size_t col = col0 + j;
                     const size_t cc = col < p.n ? col : p.n - 1;
-                    const float ipt = __fmul_rn(__fmul_rn(c[j], rr1), __ldg(p.c1 + cc));
+                    const float ipt = __fmul_rn(__fmul_rn(__uint_as_float(r[j]), rr1), __ldg(p.c1 + cc));
                     float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + cc)), __fmul_rn(2.0f, ipt));
                     d = d > 0.0f ? d : 0.0f;
                     c[j] = d;
                     if (col < p.n && better(d, (int)col, td, ti)) pass |= 1u << j;
                 }
                 if (pass) {
-                    float sd[32];
+                    float sd[16];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) sd[j] = c[j];
+                    for (int j = 0; j < 16; ++j) sd[j] = c[j];
                     do {
                         const int j = __ffs(pass) - 1;
                         pass &= pass - 1u;
