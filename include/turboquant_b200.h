@@ -320,7 +320,7 @@ typedef struct tq_server_params {
     int slots;          /* batches in flight, 1..8 (fewer if they do not fit in half of the
                            free device memory) */
     int kernel_variant; /* -1: autotune the contraction's tile shape per batch-size bucket;
-                           else fixed (tq_topk_variant_shape): 0..5 for a TQ_INDEX_PLANES
+                           else fixed (tq_topk_variant_shape): 0..6 for a TQ_INDEX_PLANES
                            index, 1..4 for TQ_INDEX_CODES */
     size_t queue_rows;  /* queued query rows beyond which submit returns TQ_ERR_BUSY
                            (0: no cap beyond the admission pool) */
@@ -366,7 +366,8 @@ tq_status tq_server_tuning_times(tq_server *sv, float *ms, int cap, int *n_bucke
                                  int *from_cache);
 /* The tile shape of a kernel variant: shape[0] query rows per CTA, shape[1]
    codes per tile (per pipeline stage), shape[2] pipeline stages, shape[3] K
-   blocks of 64 per promoted accumulation chunk. */
+   blocks of 64 per promoted accumulation chunk (0: the whole K in one
+   accumulator, whose wider error bound the exact stage's certificate uses). */
 tq_status tq_topk_variant_shape(int variant, int *shape);
 void tq_server_destroy(tq_server *sv);
 

@@ -81,7 +81,7 @@ def test_index_search_is_the_stable_argsort(corpus, k):
     _assert_exact(D, I, ref[:300], k)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 def test_kernel_variants_give_identical_results(corpus, variant):
     space, codes, X, Q, ref, index = corpus
     with index.serve(k=10, max_rows=256, slots=1, kernel_variant=variant) as sv:
@@ -110,9 +110,9 @@ def test_codes_layout_variants(corpus, index_codes, variant):
 
 
 def test_codes_layout_refuses_planes_only_variants(corpus, index_codes):
-    # 0 and 5 need planes; 1 and 3 (three stages) leave no room for a tile of
-    # 268-byte codes in shared memory
-    for v in (0, 1, 3, 5):
+    # 0, 5 and 6 need planes; 1 and 3 (three stages) leave no room for a tile
+    # of 268-byte codes in shared memory
+    for v in (0, 1, 3, 5, 6):
         with pytest.raises(ValueError):
             index_codes.serve(k=10, max_rows=128, slots=1, kernel_variant=v)
 
@@ -327,9 +327,9 @@ def test_budget_below_one_batch_is_refused(corpus):
 def test_autotuner_searches_the_tile_space(corpus):
     space, codes, X, Q, ref, index = corpus
     shapes = tq.variant_shapes()
-    assert len(shapes) == 6
+    assert len(shapes) == 7
     assert {(s["codes_per_tile"], s["stages"], s["chunk_k_blocks"]) for s in shapes} == {
-        (256, 2, 8), (128, 3, 8), (128, 2, 4), (128, 3, 4), (128, 2, 8), (256, 2, 4)}
+        (256, 2, 8), (128, 3, 8), (128, 2, 4), (128, 3, 4), (128, 2, 8), (256, 2, 4), (256, 2, 0)}
     ix = space.index(np.ascontiguousarray(codes[:50_000]))  # an index shape not tuned before
     try:
         with ix.serve(k=10, max_rows=512, slots=1) as sv:
@@ -339,7 +339,7 @@ def test_autotuner_searches_the_tile_space(corpus):
         assert [b["bucket_rows"] for b in t] == [128, 256, 512]
         for b in t:
             assert not b["from_cache"]
-            assert b["variant"] in range(6) and b["ms"] > 0
+            assert b["variant"] in range(7) and b["ms"] > 0
             assert all(x > 0 for x in b["times_ms"])
             assert b["ms"] == pytest.approx(min(b["times_ms"]))
         # the same index shape again: the process's tuning cache answers
@@ -398,7 +398,7 @@ def test_fewer_codes_than_k(cuda_ok):
     _assert_exact(D[:, :5], I[:, :5], want, 5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 5])
+@pytest.mark.parametrize("variant", [0, 1, 5, 6])
 def test_every_column_inserts(corpus, variant):
     """Worst case for the per-row lists: the index holds the codes in order of
     descending distance to the first query, so every column of every slice

@@ -41,10 +41,9 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kNoIdx = INT_MAX;
 
-// Relative error bound of the split-BF16 tensor pass (and of the reference's
-// own FP32 sums) against the terms' absolute sum; derivation in
-// rescore_kernel.
-constexpr float kKappa = 2.5e-4f;
+// Error bound of the distance epilogues, against |q|^2 + max |x|^2 (the
+// tensor pass's own bound, kappa, comes with each launch; derivation in
+// rescore_kernel).
 constexpr float kKappaEpi = 1e-6f;
 constexpr float kDegenerateG = 1e-20f;
 
@@ -286,7 +285,7 @@ struct RescoreArgs {
     size_t n;
     bool al4;
     const float *bound;
-    float bound_scale;
+    float kappa, bound_scale;
     float *out_d;
     long long *out_i;
     int *fail_rows;
@@ -310,8 +309,9 @@ struct RescoreArgs {
 // a chunk of at most 8 K blocks issues at most 96 MMAs into one accumulator
 // from zero (96 * 2^-20 of the chunk's |terms|); promotions, the planes' FP32
 // roundings and the reference's own FP32 sums (chains of at most D/64 + 8
-// adds) add a few 1e-7.  Their sum, 1.4e-4, is taken as kKappa = 2.5e-4 of
-// sum_i |terms|, and
+// adds) add a few 1e-7.  Their sum, 1.4e-4, is taken as kappa = 2.5e-4 of
+// sum_i |terms| (a pass with more MMAs per accumulator, as the whole-K
+// variant, brings a kappa grown with their count: tc_topk_kappa), and
 //   sum_i |terms| <= |q| (cmax sigma_j |x_j| sum|q_rot| + scale gamma_j |x_j| sum|s_q|),
 // bounded with the index-wide maxima of sigma |x| and scale gamma |x|.  The
 // distance epilogues of both sides add kKappaEpi (|q|^2 + max |x|^2), and a
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(256) rescore_kernel(RescoreArgs a) {
             ss += __shfl_xor_sync(kFull, ss, off);
         }
         const float eps =
-            a.bound_scale * (2.0f * qn * (kKappa * (a.cmax * a.bound[0] * sq + a.bound[1] * ss) +
+            a.bound_scale * (2.0f * qn * (a.kappa * (a.cmax * a.bound[0] * sq + a.bound[1] * ss) +
                                           kDegenerateG * ss * a.bound[3]) +
                              kKappaEpi * (qn2 + a.bound[2]));
         const bool viol = ci != kNoIdx && !(fabsf(ad - ed) <= eps);
@@ -884,14 +884,15 @@ cudaError_t launch_index_bound(const Params &P, const uint8_t *codes, size_t n, 
 cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, const int *m_dev,
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
-                           const uint8_t *codes, size_t n, const float *bound, float bound_scale,
+                           const uint8_t *codes, size_t n, const float *bound, float kappa,
+                           float bound_scale,
                            float *out_d, long long *out_i, int *fail_rows, float *thr, float *tthr,
                            int *counters, int max_rows, cudaStream_t st) {
-    if (kc < 1 || kc > 32 || k < 1 || k > kc || k > kTopKMax || max_rows < 1)
+    if (kc < 1 || kc > 32 || k < 1 || k > kc || k > kTopKMax || max_rows < 1 || !(kappa > 0.0f))
         return cudaErrorInvalidValue;
     const RescoreArgs a{P,     centroids, cmax,  m_dev,     kc,          k,     cand_d,
                         cand_i, q_rot,    s_q,   norms,     codes,       n,     codes_al4(P, codes),
-                        bound, bound_scale, out_d, out_i, fail_rows, thr, tthr, counters};
+                        bound, kappa, bound_scale, out_d, out_i, fail_rows, thr, tthr, counters};
     const unsigned blocks = (unsigned)((max_rows + 7) / 8);
     if (P.nibble)
         rescore_kernel<true><<<blocks, 256, 0, st>>>(a);

@@ -42,11 +42,14 @@ constexpr int kTensorTierMinRows = 8;
 // candidate broke the bound) to tthr, at the same position.  A candidate whose
 // approximate and exact distances differ by more than the bound eps is counted
 // in counters[1] and fails its row as well.
-// cmax = max_v |c_v| of the space's centroid table.
+// cmax = max_v |c_v| of the space's centroid table; kappa = the tensor pass's
+// relative error bound (tc_topk_kappa of the variant that produced the
+// candidates).
 cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, const int *m_dev,
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
-                           const uint8_t *codes, size_t n, const float *bound, float bound_scale,
+                           const uint8_t *codes, size_t n, const float *bound, float kappa,
+                           float bound_scale,
                            float *out_d, long long *out_i, int *fail_rows, float *thr, float *tthr,
                            int *counters, int max_rows, cudaStream_t st);
 

@@ -85,6 +85,9 @@ constexpr int kTopKMax = 16;   // results per row (k) of the serving path
 constexpr int kCandMax = 32;   // list length of the tensor-core top-k (candidates per row)
 constexpr int kTopKListsMax = 2;
 int tc_topk_variants();
+// Relative error bound of a variant's tensor pass (see the exact stage's
+// certificate), for K columns of which the first k_lo have a lo plane.
+float tc_topk_kappa(int variant, int K, int k_lo);
 int tc_topk_lists(int variant);
 // {rows per CTA, codes per tile, pipeline stages, K blocks per chunk} of a variant
 bool tc_topk_shape(int variant, int out[4]);

@@ -842,6 +842,22 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tcw_kernel(const __grid_constan
         const int q = warp & 3, h = (warp - 2) >> 2;  // lane quadrant, column half
         const uint32_t lanes = tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(TW_COLS * h);
         typename W::State st(ep, 32 * q + lane, h);
+        if constexpr (W::kDirect) {
+            // one chunk per tile (CH >= KB): the tile's sums are read in place
+            bool ok = true;
+            for (int t = 0; t < ntiles && ok; ++t) {
+                int mb, nb;
+                W::tile_at(ep, t, mb, nb);
+                const uint32_t b = (uint32_t)t & 1u, xph = ((uint32_t)t >> 1) & 1u;
+                if (!mbar_wait(xfull0 + 8 * b, xph, err, kErrTmemFull)) { ok = false; break; }
+                tc_fence_after();
+                st.tile_tmem(ep, mb, nb, lanes + b * TW_BN);
+                __syncwarp();
+                tc_fence_before();
+                mbar_arrive(xempty0 + 8 * b);
+            }
+            if (ok) st.finish(ep);
+        } else {
         float y[TW_COLS];
         uint32_t gc = 0;
         bool ok = true;
@@ -877,6 +893,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1) tcw_kernel(const __grid_constan
             st.tile(ep, mb, nb, y);
         }
         if (ok) st.finish(ep);
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -1157,6 +1174,7 @@ struct ThreshEpi {
 // ---- epilogue policies of tcw_kernel: each thread holds one row's running
 // sums of TW_COLS columns (half h of the 256-column tile) in registers.
 struct WDist {
+    static constexpr bool kDirect = false;  // running sums promoted into registers
     using Params = DistEpi::Params;
     __device__ static int tiles(const Params &p) { return GridTiles::count(p.g.num_tiles); }
     __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) { p.g.at(t, mb, nb); }
@@ -1204,6 +1222,7 @@ struct WDist {
 // in the thread's local frame and is touched only on an insertion; the
 // per-column test reads the k-th entry kept in registers.
 struct WTopk {
+    static constexpr bool kDirect = false;
     using Params = TopkEpi::Params;  // nb_tiles counts 256-wide tiles
     __device__ static int tiles(const Params &p) { return TopkEpi::tiles(p); }
     __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) {
@@ -1254,6 +1273,99 @@ struct WTopk {
             }
             thr_d = td;
             thr_i = ti;
+        }
+        __device__ void finish(const Params &p) {
+            if (!valid) return;
+            int mb;
+            unsigned nb0, nb1;
+            TopkEpi::slice(p, mb, nb0, nb1);
+            if (mb * TC_BM + rit >= m) return;
+            const size_t o = (((size_t)blockIdx.x * TC_BM + rit) * 2 + h) * kCandMax;
+#pragma unroll
+            for (int u = 0; u < kCandMax; ++u)
+                if (u < p.k) {
+                    p.part_d[o + u] = bd[u];
+                    p.part_i[o + u] = bi[u];
+                }
+        }
+    };
+};
+
+// The top-k over 256-wide column tiles whose sums run over the whole K in one
+// tensor-memory buffer (no promoted chunks; `kDirect`): the epilogue threads
+// read their row's 128 columns of the finished tile from tensor memory in
+// 16-column pieces and keep a register list of the best kCandMax, as TopkEpi
+// does.  Two partial lists per (row, slice), as WTopk.  Without promotion
+// the 128 x 256 tile needs no running sums in registers, which is what leaves
+// the registers for the list.
+struct WTopkD {
+    static constexpr bool kDirect = true;
+    using Params = TopkEpi::Params;  // nb_tiles counts 256-wide tiles
+    __device__ static int tiles(const Params &p) { return TopkEpi::tiles(p); }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) {
+        TopkEpi::tile_at(p, t, mb, nb);
+    }
+    struct State {
+        int rit, h, m;
+        bool valid;
+        float rr1 = 0.0f, rr2 = 0.0f;
+        float bd[kCandMax];
+        int bi[kCandMax];
+        __device__ State(const Params &p, int row_in_tile, int half) : rit(row_in_tile), h(half) {
+            int mb;
+            unsigned nb0, nb1;
+            m = *p.m_dev;
+            valid = TopkEpi::slice(p, mb, nb0, nb1);
+            const int row = valid ? mb * TC_BM + rit : 0;
+            if (valid && row < m) {
+                rr1 = __ldg(p.r1 + row);
+                rr2 = __ldg(p.r2 + row);
+            }
+#pragma unroll
+            for (int t = 0; t < kCandMax; ++t) {
+                bd[t] = INFINITY;
+                bi[t] = 0x7fffffff;
+            }
+        }
+        // X: this thread's lane and first column of the tile's sums
+        __device__ void tile_tmem(const Params &p, int mb, int nb, uint32_t X) {
+            const bool row_ok = mb * TC_BM + rit < m;
+            const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
+#pragma unroll 1
+            for (int ch = 0; ch < TW_COLS / 16; ++ch) {
+                uint32_t r[16];
+                __syncwarp();
+                tmem_ld16_nw(X + 16 * ch, r);  // warp-collective: every lane loads
+                tmem_wait_ld();
+                if (!row_ok) continue;
+                const size_t col0 = cbase + ch * 16;
+                const float td = bd[kCandMax - 1];
+                const int ti = bi[kCandMax - 1];
+                float c[16];
+                uint32_t pass = 0u;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const size_t col = col0 + j;
+                    const size_t cc = col < p.n ? col : p.n - 1;
+                    const float ipt = __fmul_rn(__fmul_rn(__uint_as_float(r[j]), rr1), __ldg(p.c1 + cc));
+                    float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + cc)), __fmul_rn(2.0f, ipt));
+                    d = d > 0.0f ? d : 0.0f;
+                    c[j] = d;
+                    if (col < p.n && better(d, (int)col, td, ti)) pass |= 1u << j;
+                }
+                if (pass) {
+                    float sd[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) sd[j] = c[j];
+                    do {
+                        const int j = __ffs(pass) - 1;
+                        pass &= pass - 1u;
+                        const float d = sd[j];
+                        const int ci = (int)(col0 + (size_t)j);
+                        if (better(d, ci, bd[kCandMax - 1], bi[kCandMax - 1])) reg_insert(bd, bi, d, ci);
+                    } while (pass);
+                }
+            }
         }
         __device__ void finish(const Params &p) {
             if (!valid) return;
@@ -1539,10 +1651,32 @@ constexpr int kTopkShapes[][4] = {
     {TC_BM, TC_BN, 3, 4},  // 3
     {TC_BM, TC_BN, 2, 8},  // 4
     {TC_BM, TW_BN, 2, 4},  // 5: tcw_kernel
+    {TC_BM, TW_BN, 2, 0},  // 6: tcw_kernel, the whole K in one accumulator (0: no chunks)
 };
+constexpr int kWholeK = 1 << 16;  // chunk length of variant 6: longer than any K
 }  // namespace
 
 int tc_topk_variants() { return (int)(sizeof(kTopkShapes) / sizeof(kTopkShapes[0])); }
+
+// The relative error bound of a variant's tensor pass against the sum of its
+// terms' magnitudes.  Per term the split-BF16 representation leaves 3 * 2^-16;
+// each K = 16 MMA is taken to add at most 2^-20 of (|accumulator| + sum |p|);
+// promotions, the planes' FP32 roundings and the reference's own sums add a
+// few 1e-7.  With n MMAs per accumulator (a chunk of ch K blocks: 12 per
+// block with a lo plane, 8 without; variant 6: every block of K) the sum is
+// 3 * 2^-16 + n * 2^-20 + 5e-7, taken with a factor 1.8 and at least 2.5e-4:
+// 2.5e-4 for the 8-block chunks (n = 96), 3.6e-4 for variant 6 at K = 1024,
+// K_lo = 512 (n = 160).
+float tc_topk_kappa(int variant, int K, int k_lo) {
+    const int KB = K / TC_BK, kbx = k_lo / TC_BK;
+    int n = 0;
+    if (variant >= 0 && variant < tc_topk_variants() && kTopkShapes[variant][3] == 0)
+        n = 4 * (3 * kbx + 2 * (KB - kbx));
+    else
+        n = 4 * 3 * 8;  // the longest chunk of the promoted variants, all with a lo plane
+    const float kappa = 1.8f * (3.0f / 65536.0f + (float)n / 1048576.0f + 5e-7f);
+    return kappa > 2.5e-4f ? kappa : 2.5e-4f;
+}
 int tc_topk_lists(int variant) { return kTopkShapes[variant][1] == TW_BN ? 2 : 1; }
 bool tc_topk_shape(int variant, int out[4]) {
     if (variant < 0 || variant >= tc_topk_variants()) return false;
@@ -1574,6 +1708,7 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
         if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
             return cudaErrorInvalidValue;
         const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TW_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+        if (variant == 6) return tcw_launch<WTopkD, kWholeK>(mp, sh, ep, err, (unsigned)grid, st);
         if (variant == 5) return tcw_launch<WTopk, 4>(mp, sh, ep, err, (unsigned)grid, st);
         return tcw_launch<WTopk, 8>(mp, sh, ep, err, (unsigned)grid, st);
     }

@@ -217,7 +217,8 @@ class Index:
 
 def variant_shapes():
     """Tile shape of each top-k kernel variant: rows per CTA, codes per tile,
-    pipeline stages, K blocks per promoted chunk."""
+    pipeline stages, K blocks per promoted chunk (0: the whole K in one
+    accumulator)."""
     out = []
     v = 0
     while True:
