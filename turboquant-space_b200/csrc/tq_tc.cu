@@ -1450,8 +1450,10 @@ struct SymqEpi {
 };
 
 // Merge of the per-slice candidates: one warp per query row.  Each lane keeps
-// the best k of its slices, then k rounds of a warp arg-min on (d, index)
-// produce the sorted top-k.
+// the best kCandMax of its slices' lists in registers (each list ascends, so a
+// lane stops reading a list at its first entry that does not beat the lane's
+// last), then k rounds of a warp arg-min on (d, index) produce the sorted
+// top-k.
 __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__ m_dev, int lists,
                                                          int grid_ctas, const float *__restrict__ part_d,
                                                          const int *__restrict__ part_i, int k,
@@ -1476,20 +1478,12 @@ __global__ void __launch_bounds__(256) topk_merge_kernel(const int *__restrict__
             const size_t cta = (size_t)mb * S + sl / lists;
             const size_t o = ((cta * TC_BM + rit) * lists + sl % lists) * kCandMax;
             for (int u = 0; u < k; ++u) {
-                float cd = part_d[o + u];
-                int cx = part_i[o + u];
-#pragma unroll
-                for (int v = 0; v < kCandMax; ++v) {
-                    if (v < k) {
-                        const bool sw = better(cd, cx, bd[v], bi[v]);
-                        const float td = bd[v];
-                        const int ti = bi[v];
-                        bd[v] = sw ? cd : td;
-                        bi[v] = sw ? cx : ti;
-                        cd = sw ? td : cd;
-                        cx = sw ? ti : cx;
-                    }
-                }
+                const float cd = part_d[o + u];
+                const int cx = part_i[o + u];
+                // each list ascends: once an entry does not beat this lane's
+                // last kept entry, neither does the rest of the list
+                if (!better(cd, cx, bd[kCandMax - 1], bi[kCandMax - 1])) break;
+                reg_insert(bd, bi, cd, cx);
             }
         }
         // k rounds: warp arg-min of each lane's current head
