@@ -375,6 +375,31 @@ def test_other_widths_and_degenerate_codes(cuda_ok, dim, bits, layout):
         ix.close()
 
 
+@pytest.mark.parametrize("dim,bits", [(256, 8), (200, 3), (1000, 2), (64, 4), (1536, 4)])
+def test_whole_k_variant_other_widths(cuda_ok, dim, bits):
+    """Variant 6 (the whole K in one accumulator) at other widths: its error
+    bound grows with K (1536-d: K = 4096, 640 MMAs per accumulator), and every
+    result stays the stable argsort of the reference's distances."""
+    rng = np.random.default_rng(dim * 3 + bits)
+    X = rng.standard_normal((6_000, dim)).astype(np.float32)
+    X[::89] = 0.0
+    Q = rng.standard_normal((30, dim)).astype(np.float32)
+    X[7] = Q[1]
+    space = tq.TurboQuantSpace(dim, bits)
+    codes = space.encode_batch(X)
+    want = O.OracleSpace(dim, bits).distance_m_to_n(Q, codes)
+    ix = space.index(codes)
+    try:
+        for k in (1, 10, 16):
+            with ix.serve(k=k, max_rows=128, slots=1, kernel_variant=6) as sv:
+                D, I = sv.submit(Q).wait()
+                st = sv.stats()
+            _assert_exact(D, I, want, k)
+            assert st["bound_violations"] == 0
+    finally:
+        ix.close()
+
+
 @pytest.mark.parametrize("dim,bits", [(32, 4), (1024, 8)])
 def test_codes_layout_refused_where_it_cannot_run(cuda_ok, dim, bits):
     """Padded dims below 64, and codes whose 128-code tile does not fit in
