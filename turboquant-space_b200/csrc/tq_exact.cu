@@ -285,7 +285,7 @@ struct RescoreArgs {
     size_t n;
     bool al4;
     const float *bound;
-    float kappa, bound_scale;
+    float kappa, kappa_t, bound_scale;
     float *out_d;
     long long *out_i;
     int *fail_rows;
@@ -347,10 +347,12 @@ __global__ void __launch_bounds__(256) rescore_kernel(RescoreArgs a) {
             sq += __shfl_xor_sync(kFull, sq, off);
             ss += __shfl_xor_sync(kFull, ss, off);
         }
-        const float eps =
-            a.bound_scale * (2.0f * qn * (a.kappa * (a.cmax * a.bound[0] * sq + a.bound[1] * ss) +
-                                          kDegenerateG * ss * a.bound[3]) +
-                             kKappaEpi * (qn2 + a.bound[2]));
+        // eps for this pass's candidates; eps_t for the threshold pass that may
+        // rescan an open row (its own kappa, kappa_t >= kappa)
+        const float terms = a.cmax * a.bound[0] * sq + a.bound[1] * ss;
+        const float rest = 2.0f * qn * kDegenerateG * ss * a.bound[3] + kKappaEpi * (qn2 + a.bound[2]);
+        const float eps = a.bound_scale * (2.0f * qn * a.kappa * terms + rest);
+        const float eps_t = a.bound_scale * (2.0f * qn * a.kappa_t * terms + rest);
         const bool viol = ci != kNoIdx && !(fabsf(ad - ed) <= eps);
         const unsigned viol_mask = __ballot_sync(kFull, viol);
         const float ad_last = __shfl_sync(kFull, ad, a.kc - 1);
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(256) rescore_kernel(RescoreArgs a) {
             const int pos = atomicAdd(&a.counters[kCntFallbackRows], 1);
             a.fail_rows[pos] = row;
             a.thr[pos] = ek;
-            a.tthr[pos] = viol_mask ? -1.0f : __fadd_ru(ek, eps);
+            a.tthr[pos] = viol_mask ? -1.0f : __fadd_ru(ek, eps_t);
             if (viol_mask) atomicAdd(&a.counters[kCntBoundViolations], __popc(viol_mask));
         }
     }
@@ -885,14 +887,15 @@ cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, 
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
                            const uint8_t *codes, size_t n, const float *bound, float kappa,
-                           float bound_scale,
+                           float kappa_t, float bound_scale,
                            float *out_d, long long *out_i, int *fail_rows, float *thr, float *tthr,
                            int *counters, int max_rows, cudaStream_t st) {
     if (kc < 1 || kc > 32 || k < 1 || k > kc || k > kTopKMax || max_rows < 1 || !(kappa > 0.0f))
         return cudaErrorInvalidValue;
     const RescoreArgs a{P,     centroids, cmax,  m_dev,     kc,          k,     cand_d,
                         cand_i, q_rot,    s_q,   norms,     codes,       n,     codes_al4(P, codes),
-                        bound, kappa, bound_scale, out_d, out_i, fail_rows, thr, tthr, counters};
+                        bound, kappa, kappa_t > kappa ? kappa_t : kappa, bound_scale, out_d, out_i,
+                        fail_rows, thr, tthr, counters};
     const unsigned blocks = (unsigned)((max_rows + 7) / 8);
     if (P.nibble)
         rescore_kernel<true><<<blocks, 256, 0, st>>>(a);

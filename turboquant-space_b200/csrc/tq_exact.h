@@ -44,12 +44,13 @@ constexpr int kTensorTierMinRows = 8;
 // in counters[1] and fails its row as well.
 // cmax = max_v |c_v| of the space's centroid table; kappa = the tensor pass's
 // relative error bound (tc_topk_kappa of the variant that produced the
-// candidates).
+// candidates); kappa_t = that of the threshold pass over open rows (tthr is
+// e_k plus the bound with max(kappa, kappa_t)).
 cudaError_t launch_rescore(const Params &P, const float *centroids, float cmax, const int *m_dev,
                            int kc, int k, const float *cand_d, const long long *cand_i,
                            const float *q_rot, const float *s_q, const float *norms,
                            const uint8_t *codes, size_t n, const float *bound, float kappa,
-                           float bound_scale,
+                           float kappa_t, float bound_scale,
                            float *out_d, long long *out_i, int *fail_rows, float *thr, float *tthr,
                            int *counters, int max_rows, cudaStream_t st);
 

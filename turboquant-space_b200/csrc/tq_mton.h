@@ -110,7 +110,10 @@ bool tc_topk_dec_ok(int variant, int cs);
 // nothing unless it exceeds min_rows): every column whose tile distance (as the
 // top-k pass computes it) is at most thr[row] goes to coll_i[row * cap + ...],
 // counted in coll_n[row] (which may exceed cap: overflow).  Planes (Bh, Bl,
-// k_lo) or, with dec, decoded B tiles; variant 4's tile shape.
+// k_lo) or, with dec, decoded B tiles: the tile shape of variant
+// tc_thresh_variant(dec != nullptr, n_pad) (6 on planes, 4 decoded), whose
+// error bound (tc_topk_kappa) the thresholds must allow for.
+int tc_thresh_variant(bool decoded, size_t n_pad);
 cudaError_t launch_tc_thresh(const void *Ah, const void *Al, size_t rows_pad, const void *Bh,
                              const void *Bl, const DecSrc *dec, size_t n_pad, int K, int k_lo,
                              const int *m_dev, int min_rows, size_t n, const float *r1,

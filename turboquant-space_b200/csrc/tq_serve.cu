@@ -290,7 +290,9 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
     if (e != cudaSuccess) return e;
     e = tq::launch_rescore(sp->P, sp->T.centroids, ix->cmax, sl.d_m, sv->kc, sv->k, sl.d_cd, sl.d_ci,
                            q_rot, s_q, norms, ix->codes, ix->n, ix->bound,
-                           tq::tc_topk_kappa(var, (int)K, ix->K_lo), sv->bound_scale, sl.d_od,
+                           tq::tc_topk_kappa(var, (int)K, ix->K_lo),
+                           tq::tc_topk_kappa(tq::tc_thresh_variant(!planes, ix->n_pad), (int)K, ix->K_lo),
+                           sv->bound_scale, sl.d_od,
                            sl.d_oi, sl.d_fail, sl.d_thr, sl.d_tthr, sl.d_cnt, rows_cap, st);
     if (e != cudaSuccess) return e;
     // the open rows' threshold pass on the tensor cores (when enough are open)

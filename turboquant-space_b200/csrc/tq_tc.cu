@@ -1384,6 +1384,64 @@ struct WTopkD {
     };
 };
 
+// The threshold collection (as ThreshEpi) over 256-wide column tiles whose
+// sums run over the whole K in one tensor-memory buffer, read in place.
+struct WThreshD {
+    static constexpr bool kDirect = true;
+    using Params = ThreshEpi::Params;  // nb_tiles counts 256-wide tiles
+    __device__ static int tiles(const Params &p) { return ThreshEpi::tiles(p); }
+    __device__ static void tile_at(const Params &p, int t, int &mb, int &nb) {
+        ThreshEpi::tile_at(p, t, mb, nb);
+    }
+    struct State {
+        int rit, h, m;
+        float rr1 = 0.0f, rr2 = 0.0f, T = -INFINITY;
+        bool full = false;
+        __device__ State(const Params &p, int row_in_tile, int half) : rit(row_in_tile), h(half) {
+            int mb;
+            unsigned nb0, nb1;
+            m = *p.m_dev;
+            const bool valid = ThreshEpi::slice(p, mb, nb0, nb1);
+            const int row = valid ? mb * TC_BM + rit : 0;
+            if (valid && row < m) {
+                rr1 = __ldg(p.r1 + row);
+                rr2 = __ldg(p.r2 + row);
+                T = __ldg(p.thr + row);
+            }
+        }
+        __device__ void tile_tmem(const Params &p, int mb, int nb, uint32_t X) {
+            const int row = mb * TC_BM + rit;
+            const bool row_ok = row < m;
+            const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
+#pragma unroll 1
+            for (int ch = 0; ch < TW_COLS / 16; ++ch) {
+                uint32_t r[16];
+                __syncwarp();
+                tmem_ld16_nw(X + 16 * ch, r);  // warp-collective: every lane loads
+                tmem_wait_ld();
+                if (!row_ok || full) continue;
+                const size_t col0 = cbase + ch * 16;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const size_t col = col0 + j;
+                    if (col >= p.n) break;
+                    const float ipt = __fmul_rn(__fmul_rn(__uint_as_float(r[j]), rr1), __ldg(p.c1 + col));
+                    float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + col)), __fmul_rn(2.0f, ipt));
+                    d = d > 0.0f ? d : 0.0f;
+                    if (d <= T && !full) {
+                        const int pos = atomicAdd(p.coll_n + row, 1);
+                        if (pos < p.cap)
+                            p.coll_i[(size_t)row * p.cap + pos] = (int)col;
+                        else
+                            full = true;
+                    }
+                }
+            }
+        }
+        __device__ void finish(const Params &) {}
+    };
+};
+
 // The QJL-corrected symmetric distances (tq_symq.cu): Y0 = C1, Y1 = C2,
 // ip_mse = C1 s1a s1b, corr = clamp(C2 s2a s2b, +-|ip_mse|),
 // ip = (ip_mse + corr) na nb, d = max(0, na^2 + nb^2 - 2 ip), with the
@@ -1799,8 +1857,18 @@ cudaError_t launch_tc_thresh(const void *Ah, const void *Al, size_t rows_pad, co
     if (k_lo % TC_BK || k_lo <= 0 || k_lo > K) return cudaErrorInvalidValue;
     if (!aligned16({Bh, Bl})) return cudaErrorMisalignedAddress;
     if (!bf16_maps(mp, sh, Ah, Al, rows_pad, Bh, Bl, n_pad, K, k_lo)) return cudaErrorInvalidValue;
+    if (n_pad % TW_BN == 0) {
+        // variant 6's shape: 128 x 256 tiles, the whole K in one accumulator
+        if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
+            return cudaErrorInvalidValue;
+        ThreshEpi::Params ew = ep;
+        ew.nb_tiles = (unsigned)(n_pad / TW_BN);
+        return tcw_launch<WThreshD, kWholeK>(mp, sh, ew, err, (unsigned)grid, st);
+    }
     return tcp_launch<false, 2, 8, true, ThreshEpi>(mp, sh, ep, err, (unsigned)grid, st);
 }
+
+int tc_thresh_variant(bool decoded, size_t n_pad) { return (!decoded && n_pad % TW_BN == 0) ? 6 : 4; }
 
 cudaError_t launch_topk_merge(const int *m_dev, int grid_ctas, int lists, const float *part_d,
                               const int *part_i, int k, size_t max_rows, float *out_d,
