@@ -191,7 +191,7 @@ def test_forced_fallback_is_exact(corpus):
 @pytest.mark.parametrize("layout", ["planes", "codes"])
 @pytest.mark.parametrize("k", [1, 10, 16])
 def test_tensor_threshold_tier_is_exact(corpus, index_codes, layout, k):
-    """Inflated bounds leave many rows open: with more than eight, the
+    """Inflated bounds leave many rows open: with more than four, the
     tensor-core threshold pass lists each open row's codes within e_k + eps
     and the rescoring of those lists answers them (rows whose list overflows
     go to the exact scan).  Every result is exact, and some bound of the sweep
@@ -205,7 +205,7 @@ def test_tensor_threshold_tier_is_exact(corpus, index_codes, layout, k):
             st = sv.stats()
         _assert_exact(D, I, ref[:256], k)
         assert st["bound_violations"] == 0
-        if st["fallback_rows"] > 8:
+        if st["fallback_rows"] > 4:
             from_lists += st["fallback_rows"] - st["scan_pass_rows"]
         print(f"{layout} k={k} bound x{bs}: {st['fallback_rows']} open rows, "
               f"{st['scan_pass_rows']} by the exact scan")

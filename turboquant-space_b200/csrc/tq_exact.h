@@ -27,8 +27,10 @@ enum {
 
 // Codes collected per open row by a threshold pass.
 constexpr int kCollectCap = 1024;
-// The tensor-core threshold pass runs when more rows than this are open.
-constexpr int kTensorTierMinRows = 8;
+// The tensor-core threshold pass runs when more rows than this are open (one
+// pass over the corpus for up to 128 rows costs about what the exact scan
+// costs for five).
+constexpr int kTensorTierMinRows = 4;
 
 // Candidate rescoring: one warp per query row (row count read from m_dev).
 // cand_d / cand_i hold each row's kc (<= 32) tensor-pass candidates, ascending
