@@ -95,14 +95,15 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
                            const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo,
                            const int *m_dev,
                            size_t n, const float *r1, const float *r2, const float *c1,
-                           const float *c2, int k, float *part_d, int *part_i, int *err, int grid,
-                           cudaStream_t st);
+                           const float *c2, int k, float *part_d, int *part_i,
+                           unsigned long long *gthr, int *err, int grid, cudaStream_t st);
 // The same top-k with decoded B tiles (variants 1-4, the 128 x 128 tiles; no
 // planes of the columns).  K = 2D; dec.kbc = D / 64.
 cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size_t rows_pad,
                                const DecSrc &dec, size_t n_pad, int K, const int *m_dev, size_t n,
                                const float *r1, const float *r2, const float *c1, const float *c2,
-                               int k, float *part_d, int *part_i, int *err, int grid, cudaStream_t st);
+                               int k, float *part_d, int *part_i, unsigned long long *gthr, int *err,
+                               int grid, cudaStream_t st);
 // Whether `variant` runs with decoded B tiles for codes of cs bytes (a tile of
 // 128 codes must fit in shared memory beside the variant's stages).
 bool tc_topk_dec_ok(int variant, int cs);

@@ -126,6 +126,7 @@ struct Slot {
         *d_fpi = nullptr, *d_colln = nullptr, *d_colli = nullptr, *d_scan = nullptr,
         *d_list_rows = nullptr;
     void *d_ap2 = nullptr;  // the open rows' query planes (same shape as d_ap)
+    unsigned long long *d_gthr = nullptr;  // per row: the top-k pass's published bound
     long long *d_ci = nullptr;
     int *h_cnt = nullptr;  // pinned copy of d_cnt after each batch
     int *h_rows = nullptr;  // pool row of each batch row (pinned)
@@ -272,14 +273,16 @@ cudaError_t enqueue_batch(tq_server *sv, Slot &sl, int rows_cap, int var, bool c
         dec.centroids = sp->T.centroids;
         dec.levels = sp->levels;
     }
+    e = cudaMemsetAsync(sl.d_gthr, 0xFF, (size_t)rows_cap * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
     if (planes)
         e = tq::launch_tc_topk(var, ah, al, rows_cap, bh, bl, ix->n_pad, (int)K, ix->K_lo, sl.d_m, ix->n,
-                               sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
-                               sv->grid, st);
+                               sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_gthr,
+                               sl.d_err, sv->grid, st);
     else
         e = tq::launch_tc_topk_dec(var, ah, al, rows_cap, dec, ix->n_pad, (int)K, sl.d_m, ix->n,
-                                   sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_err,
-                                   sv->grid, st);
+                                   sl.d_r1, sl.d_r2, ix->c1, ix->c2, sv->kc, sl.d_pd, sl.d_pi, sl.d_gthr,
+                                   sl.d_err, sv->grid, st);
     if (e != cudaSuccess) return e;
     e = tq::launch_topk_merge(sl.d_m, sv->grid, tq::tc_topk_lists(var), sl.d_pd, sl.d_pi, sv->kc,
                               rows_cap, sl.d_cd, sl.d_ci, st);
@@ -360,7 +363,7 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     const size_t o_rows = take(R * 4), o_thr = take(R * 4), o_tthr = take(R * 4), o_colln = take(2 * R * 4);
     const size_t o_colld = take(R * tq::kCollectCap * 4), o_colli = take(R * tq::kCollectCap * 4);
     const size_t o_scan = take(R * 4), o_list = take(R * 4), o_ap2 = take(R * K * 4);
-    const size_t o_r1o = take(R * 4), o_r2o = take(R * 4);
+    const size_t o_r1o = take(R * 4), o_r2o = take(R * 4), o_gthr = take(R * 8);
     TQ_CUDA(cudaMalloc(&sl.d_block, off), "cudaMalloc(slot)");
     TQ_CUDA(cudaMemset(sl.d_block, 0, off), "cudaMemset(slot)");
     auto *base = static_cast<unsigned char *>(sl.d_block);
@@ -392,6 +395,7 @@ tq_status slot_alloc(tq_server *sv, Slot &sl) {
     sl.d_ap2 = base + o_ap2;
     sl.d_r1o = reinterpret_cast<float *>(base + o_r1o);
     sl.d_r2o = reinterpret_cast<float *>(base + o_r2o);
+    sl.d_gthr = reinterpret_cast<unsigned long long *>(base + o_gthr);
     for (int b = 128; b < sv->max_rows; b *= 2) sl.bucket_rows.push_back(b);
     sl.bucket_rows.push_back(sv->max_rows);
     return TQ_OK;

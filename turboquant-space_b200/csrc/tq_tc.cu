@@ -966,6 +966,15 @@ __device__ __forceinline__ void reg_insert(float (&bd)[kCandMax], int (&bi)[kCan
 // epilogue thread keeps its row's best k (distance, index) pairs, ties broken
 // by the smaller index, and writes them to the partial buffers
 // part_d / part_i [(block * S + slice) * 128 + row][kCandMax].
+// A candidate as one unsigned key, ordered as (distance, index): distances are
+// non-negative (or +inf), so their bit patterns order like the values.
+__device__ __forceinline__ unsigned long long topk_key(float d, int i) {
+    return ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)i;
+}
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
+    return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+
 struct TopkEpi {
     struct Params {
         const int *m_dev;
@@ -975,6 +984,14 @@ struct TopkEpi {
         int k;
         float *part_d;
         int *part_i;
+        // per query row, the smallest last-entry key any epilogue thread of the
+        // launch has published (all ones before the launch; nullptr: not kept).
+        // A thread's full list proves kCandMax candidates at or below its last
+        // entry, so no column above the published minimum can be among the
+        // row's best kCandMax: every thread tests its columns against
+        // min(own last entry, published), read once per tile (a stale value is
+        // only larger), and publishes its own last entry after each tile.
+        unsigned long long *gthr;
     };
     // this CTA's row block, column-tile range; false when it has no slice
     __device__ static bool slice(const Params &p, int &mb, unsigned &nb0, unsigned &nb1) {
@@ -1028,8 +1045,10 @@ struct TopkEpi {
         // the chunk's distances go to a local array and the marked columns are
         // inserted one by one.  Late in a slice few chunks have any.
         __device__ void tile(const Params &p, int mb, int nb, uint32_t y0, uint32_t) {
-            const bool row_ok = mb * TC_BM + rit < m;
+            const int row = mb * TC_BM + rit;
+            const bool row_ok = row < m;
             const size_t colbase = (size_t)nb * TC_BN;
+            const unsigned long long g = (row_ok && p.gthr) ? ld_volatile_u64(p.gthr + row) : ~0ull;
 #pragma unroll 1
             for (int ch = 0; ch < TC_BN / 16; ++ch) {
                 uint32_t r[16];
@@ -1038,8 +1057,8 @@ struct TopkEpi {
                 tmem_wait_ld();
                 if (!row_ok) continue;
                 const size_t col0 = colbase + ch * 16;
-                const float td = bd[kCandMax - 1];
-                const int ti = bi[kCandMax - 1];
+                const unsigned long long own = topk_key(bd[kCandMax - 1], bi[kCandMax - 1]);
+                const unsigned long long T = own < g ? own : g;
                 float c[16];
                 uint32_t pass = 0u;
 #pragma unroll
@@ -1050,7 +1069,7 @@ struct TopkEpi {
                     float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + cc)), __fmul_rn(2.0f, ipt));
                     d = d > 0.0f ? d : 0.0f;
                     c[j] = d;
-                    if (col < p.n && better(d, (int)col, td, ti)) pass |= 1u << j;
+                    if (col < p.n && topk_key(d, (int)col) < T) pass |= 1u << j;
                 }
                 if (pass) {
                     float sd[16];
@@ -1061,9 +1080,15 @@ struct TopkEpi {
                         pass &= pass - 1u;
                         const float d = sd[j];
                         const int ci = (int)(col0 + (size_t)j);
-                        if (better(d, ci, bd[kCandMax - 1], bi[kCandMax - 1])) reg_insert(bd, bi, d, ci);
+                        const unsigned long long kj = topk_key(d, ci);
+                        if (kj < topk_key(bd[kCandMax - 1], bi[kCandMax - 1]) && kj < g)
+                            reg_insert(bd, bi, d, ci);
                     } while (pass);
                 }
+            }
+            if (row_ok && p.gthr) {
+                const unsigned long long own = topk_key(bd[kCandMax - 1], bi[kCandMax - 1]);
+                if (own < g) atomicMin(p.gthr + row, own);
             }
         }
         __device__ void finish(const Params &p) {
@@ -1328,9 +1353,12 @@ struct WTopkD {
             }
         }
         // X: this thread's lane and first column of the tile's sums
+        // as TopkEpi::State::tile, with the row's published bound (p.gthr)
         __device__ void tile_tmem(const Params &p, int mb, int nb, uint32_t X) {
-            const bool row_ok = mb * TC_BM + rit < m;
+            const int row = mb * TC_BM + rit;
+            const bool row_ok = row < m;
             const size_t cbase = (size_t)nb * TW_BN + TW_COLS * h;
+            const unsigned long long g = (row_ok && p.gthr) ? ld_volatile_u64(p.gthr + row) : ~0ull;
 #pragma unroll 1
             for (int ch = 0; ch < TW_COLS / 16; ++ch) {
                 uint32_t r[16];
@@ -1339,8 +1367,8 @@ struct WTopkD {
                 tmem_wait_ld();
                 if (!row_ok) continue;
                 const size_t col0 = cbase + ch * 16;
-                const float td = bd[kCandMax - 1];
-                const int ti = bi[kCandMax - 1];
+                const unsigned long long own = topk_key(bd[kCandMax - 1], bi[kCandMax - 1]);
+                const unsigned long long T = own < g ? own : g;
                 float c[16];
                 uint32_t pass = 0u;
 #pragma unroll
@@ -1351,7 +1379,7 @@ struct WTopkD {
                     float d = __fsub_rn(__fadd_rn(rr2, __ldg(p.c2 + cc)), __fmul_rn(2.0f, ipt));
                     d = d > 0.0f ? d : 0.0f;
                     c[j] = d;
-                    if (col < p.n && better(d, (int)col, td, ti)) pass |= 1u << j;
+                    if (col < p.n && topk_key(d, (int)col) < T) pass |= 1u << j;
                 }
                 if (pass) {
                     float sd[16];
@@ -1362,9 +1390,15 @@ struct WTopkD {
                         pass &= pass - 1u;
                         const float d = sd[j];
                         const int ci = (int)(col0 + (size_t)j);
-                        if (better(d, ci, bd[kCandMax - 1], bi[kCandMax - 1])) reg_insert(bd, bi, d, ci);
+                        const unsigned long long kj = topk_key(d, ci);
+                        if (kj < topk_key(bd[kCandMax - 1], bi[kCandMax - 1]) && kj < g)
+                            reg_insert(bd, bi, d, ci);
                     } while (pass);
                 }
+            }
+            if (row_ok && p.gthr) {
+                const unsigned long long own = topk_key(bd[kCandMax - 1], bi[kCandMax - 1]);
+                if (own < g) atomicMin(p.gthr + row, own);
             }
         }
         __device__ void finish(const Params &p) {
@@ -1745,7 +1779,7 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
                            const void *Bh, const void *Bl, size_t n_pad, int K, int k_lo,
                            const int *m_dev, size_t n, const float *r1, const float *r2,
                            const float *c1, const float *c2, int k, float *part_d, int *part_i,
-                           int *err, int grid, cudaStream_t st) {
+                           unsigned long long *gthr, int *err, int grid, cudaStream_t st) {
     if (k < 1 || k > kCandMax || grid < 1 || variant < 0 || variant >= tc_topk_variants())
         return cudaErrorInvalidValue;
     if (K % TC_BK || k_lo % TC_BK || k_lo <= 0 || k_lo > K || rows_pad % TC_BM || n_pad % TC_BN)
@@ -1759,12 +1793,12 @@ cudaError_t launch_tc_topk(int variant, const void *Ah, const void *Al, size_t r
         if (n_pad % TW_BN) return cudaErrorInvalidValue;
         if (!make_map(&mp.m[0][2], Bh, K, n_pad, TW_BN) || !make_map(&mp.m[0][3], Bl, k_lo, n_pad, TW_BN))
             return cudaErrorInvalidValue;
-        const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TW_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+        const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TW_BN), n, r1, r2, c1, c2, k, part_d, part_i, gthr};
         if (variant == 6) return tcw_launch<WTopkD, kWholeK>(mp, sh, ep, err, (unsigned)grid, st);
         if (variant == 5) return tcw_launch<WTopk, 4>(mp, sh, ep, err, (unsigned)grid, st);
         return tcw_launch<WTopk, 8>(mp, sh, ep, err, (unsigned)grid, st);
     }
-    const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+    const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i, gthr};
     switch (variant) {
         case 2: return tcp_launch<false, 2, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
         case 3: return tcp_launch<false, 3, 4, true, TopkEpi>(mp, sh, ep, err, (unsigned)grid, st);
@@ -1812,7 +1846,8 @@ bool tc_topk_dec_ok(int variant, int cs) {
 cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size_t rows_pad,
                                const DecSrc &dec, size_t n_pad, int K, const int *m_dev, size_t n,
                                const float *r1, const float *r2, const float *c1, const float *c2,
-                               int k, float *part_d, int *part_i, int *err, int grid, cudaStream_t st) {
+                               int k, float *part_d, int *part_i, unsigned long long *gthr, int *err,
+                               int grid, cudaStream_t st) {
     if (k < 1 || k > kCandMax || grid < 1 || !tc_topk_dec_ok(variant, dec.cs)) return cudaErrorInvalidValue;
     if (K % TC_BK || rows_pad % TC_BM || n_pad % TC_BN || !dec_ok(dec, K) || dec.kbc * 2 != K / TC_BK ||
         !dec.fc || !dec.fs || n > n_pad)
@@ -1821,7 +1856,7 @@ cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size
     alignas(64) TcMaps mp;
     TcShape sh{};
     if (!a_maps(mp, sh, Ah, Al, rows_pad, K, dec.kbc)) return cudaErrorInvalidValue;
-    const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i};
+    const TopkEpi::Params ep{m_dev, (unsigned)(n_pad / TC_BN), n, r1, r2, c1, c2, k, part_d, part_i, gthr};
     const int stages = (variant == 2 || variant == 4) ? 2 : 3;
     const DecSrc d = with_code_buffers(dec, stages);
     if (d.cbufs == 0) return cudaErrorInvalidValue;  // the code tile does not fit beside the stages
