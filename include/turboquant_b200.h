@@ -52,9 +52,18 @@ typedef enum tq_precision {
     TQ_PRECISION_SPLIT_BF16 = 1, /* tcgen05 tensor cores on hi+lo BF16 pairs, FP32 TMEM accumulators */
     TQ_PRECISION_SPLIT_TF32 = 2, /* tcgen05 tensor cores on hi+lo TF32 pairs, FP32 TMEM accumulators
                                     (the QJL-corrected symmetric distances only) */
-    TQ_PRECISION_REFERENCE = 3   /* the reference's own FP32 arithmetic in its Release build's
+    TQ_PRECISION_REFERENCE = 3,  /* the reference's own FP32 arithmetic in its Release build's
                                     summation order, one code per thread: bit-identical to
                                     distSearchScalarB4 / distSearchAVX (asymmetric M x N only) */
+    TQ_PRECISION_SPLIT_BF16_DECODED = 4 /* as SPLIT_BF16, but the column tiles are decoded from
+                                    the codes in shared memory (128 x 128 tiles) instead of
+                                    being read from BF16 planes written to device memory
+                                    first: 16 bytes of per-code scalars instead of 3-6 KB of
+                                    planes per code.  Padded dims >= 64; a tile of 128 codes
+                                    must fit in shared memory beside the pipeline (nibble
+                                    codes up to padded dim 1024, byte codes up to 512);
+                                    device codes 16-byte aligned.  Otherwise
+                                    TQ_ERR_NOT_SUPPORTED.  Plain M x N entry points only. */
 } tq_precision;
 
 /* The QJL-corrected symmetric distances (space_turbo_quant.h:483-572, 731-945). */

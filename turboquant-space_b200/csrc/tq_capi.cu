@@ -127,7 +127,8 @@ tq_status ensure_host_streams(tq_space *sp) {
 // the reference-order arithmetic for the asymmetric form only (the symmetric
 // distBuild order is not restated).
 tq_status mton_precision_ok(tq_precision p, bool sym) {
-    if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_BF16) return TQ_OK;
+    if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_BF16 || p == TQ_PRECISION_SPLIT_BF16_DECODED)
+        return TQ_OK;
     if (p == TQ_PRECISION_REFERENCE && !sym) return TQ_OK;
     if (p == TQ_PRECISION_REFERENCE || p == TQ_PRECISION_SPLIT_TF32)
         return fail(TQ_ERR_NOT_SUPPORTED, "precision %d is not available for %s distances", (int)p,
@@ -140,6 +141,8 @@ tq_status mton_precision_ok(tq_precision p, bool sym) {
 //   FP32, m < kScanRows:  the HBM-bound scan kernel per row (no planes);
 //   FP32 otherwise:       FP32 planes + CUDA-core SGEMM;
 //   SPLIT_BF16:           hi/lo BF16 planes + tcgen05 GEMM;
+//   SPLIT_BF16_DECODED:   the same row planes; the column tiles decoded from the
+//                         codes in shared memory (per-code scalars only in HBM);
 //   REFERENCE:            the reference build's own arithmetic, one code per thread.
 // Every distance ends in the same epilogue d = max(0, r2 + c2 - 2 C r1 c1).
 class MtonRunner {
@@ -158,8 +161,10 @@ class MtonRunner {
     MtonRunner(tq_space *sp, bool sym, tq_precision prec, size_t m)
         : sp_(sp), sym_(sym), prec_(prec), m_(m) {
         K_ = sym ? (int)sp->D : 2 * (int)sp->D;
-        fmt_ = prec == TQ_PRECISION_SPLIT_BF16 ? tq::kPlaneBF16 : tq::kPlaneF32;
-        planes_ = prec != TQ_PRECISION_REFERENCE && (prec == TQ_PRECISION_SPLIT_BF16 || m >= kScanRows);
+        dec_ = prec == TQ_PRECISION_SPLIT_BF16_DECODED;
+        fmt_ = (prec == TQ_PRECISION_SPLIT_BF16 || dec_) ? tq::kPlaneBF16 : tq::kPlaneF32;
+        planes_ = prec != TQ_PRECISION_REFERENCE &&
+                  (prec == TQ_PRECISION_SPLIT_BF16 || dec_ || m >= kScanRows);
         m_pad_ = round_up(m, tq::kPlaneRowAlign);
         const size_t col_align = prec == TQ_PRECISION_SPLIT_BF16 ? 256 : 128;
         nc_max_ = std::max(col_align, ((kColPlaneBytes / ((size_t)K_ * 4)) / col_align) * col_align);
@@ -170,6 +175,14 @@ class MtonRunner {
             return fail(TQ_ERR_NOT_SUPPORTED,
                         "split-BF16 contraction needs a reduction length that is a multiple of 64 "
                         "(padded dim %zu)", sp_->D);
+        if (dec_ && sp_->D % 64 != 0)
+            return fail(TQ_ERR_NOT_SUPPORTED,
+                        "decoded split-BF16 tiles need a padded dim that is a multiple of 64 (padded dim %zu)",
+                        sp_->D);
+        if (dec_ && !tq::tc_dist_dec_fits((int)sp_->code_size))
+            return fail(TQ_ERR_NOT_SUPPORTED,
+                        "decoded split-BF16 tiles: a tile of 128 codes of %zu bytes does not fit in shared "
+                        "memory beside the pipeline (use split_bf16)", sp_->code_size);
         if (fmt_ == tq::kPlaneF32 && planes_ && (K_ % 16 != 0)) planes_ = false;
         const size_t D = sp_->D;
         if (!sym_) {  // prepared queries (the scan path uses them directly)
@@ -203,6 +216,7 @@ class MtonRunner {
 
     // columns [0, n) of device codes -> out[i * ldo + j]
     tq_status run_cols(const uint8_t *codes, size_t n, float *out, size_t ldo, cudaStream_t s) {
+        if (dec_) return run_cols_decoded(codes, n, out, ldo, s);
         if (!planes_) {
             if (!sym_ && prec_ == TQ_PRECISION_REFERENCE)
                 TQ_CUDA(tq::launch_exact_mton(sp_->P, sp_->T.centroids, q_rot_, s_q_, norms_, m_, codes,
@@ -250,6 +264,64 @@ class MtonRunner {
         return TQ_OK;
     }
 
+    // The decoded form: per chunk of columns, the per-code scalars (16 bytes a
+    // code) and one tensor-core launch whose decoder warps turn each tile of 128
+    // codes into its B tiles in shared memory.  A tile's codes arrive by one bulk
+    // copy rounded up to 16 bytes; whole tiles are multiples of 16 bytes, and a
+    // ragged last tile whose bytes do not end on that boundary is read from a
+    // padded copy, so no copy reads past the caller's codes.
+    tq_status run_cols_decoded(const uint8_t *codes, size_t n, float *out, size_t ldo, cudaStream_t s) {
+        const size_t cs = sp_->code_size;
+        if (reinterpret_cast<uintptr_t>(codes) & 15)
+            return fail(TQ_ERR_NOT_SUPPORTED, "decoded split-BF16 tiles need 16-byte aligned device codes");
+        if (!cols_.p) {
+            nc_alloc_ = std::min(round_up(n, 128), kDecCols);
+            tail_bytes_ = round_up(128 * cs, 16) + 16;
+            TQ_CUDA(cols_.alloc(4 * 4 * nc_alloc_ + 16 + tail_bytes_, s), "cudaMallocAsync(column scalars)");
+            c1_ = static_cast<float *>(cols_.p);
+            c2_ = c1_ + nc_alloc_;
+            fc_ = c2_ + nc_alloc_;
+            fs_ = fc_ + nc_alloc_;
+            err_ = reinterpret_cast<int *>(fs_ + nc_alloc_);
+            tail_ = reinterpret_cast<uint8_t *>(err_ + 4);
+            TQ_CUDA(cudaMemsetAsync(err_, 0, sizeof(int), s), "memset");
+        }
+        tq::DecSrc d;
+        d.cs = (int)cs;
+        d.nibble = sp_->P.nibble;
+        d.kbc = (int)(sp_->D / 64);
+        d.centroids = sp_->T.centroids;
+        d.levels = (int)sp_->levels;
+        auto launch = [&](const uint8_t *src, size_t cols, float *dst) -> tq_status {
+            const size_t cols_pad = round_up(cols, 128);
+            TQ_CUDA(tq::launch_dec_factors(sp_->P, src, cols, cols_pad, sym_, c1_, c2_, sym_ ? nullptr : fc_,
+                                           sym_ ? nullptr : fs_, s),
+                    "column scalars");
+            d.codes = src;
+            d.n = (unsigned)cols;
+            d.fc = sym_ ? nullptr : fc_;
+            d.fs = sym_ ? nullptr : fs_;
+            TQ_CUDA(tq::launch_tc_dist_dec(a0_, a1_, m_, m_pad_, d, cols_pad, K_, r1_, r2_, c1_, c2_, dst, ldo,
+                                           err_, s),
+                    "tcgen05 GEMM kernel (decoded tiles)");
+            return TQ_OK;
+        };
+        for (size_t n0 = 0; n0 < n; n0 += nc_alloc_) {
+            const size_t nc = std::min(nc_alloc_, n - n0);
+            const size_t rem = nc % 128;
+            const size_t n_main = (rem != 0 && (rem * cs) % 16 != 0) ? nc - rem : nc;
+            tq_status st;
+            if (n_main > 0 && (st = launch(codes + n0 * cs, n_main, out + n0)) != TQ_OK) return st;
+            if (n_main < nc) {
+                TQ_CUDA(cudaMemcpyAsync(tail_, codes + (n0 + n_main) * cs, (nc - n_main) * cs,
+                                        cudaMemcpyDeviceToDevice, s),
+                        "copy of the last tile");
+                if ((st = launch(tail_, nc - n_main, out + n0 + n_main)) != TQ_OK) return st;
+            }
+        }
+        return TQ_OK;
+    }
+
     // Reports a bounded wait that gave up inside the tensor-core kernel.
     tq_status finish(cudaStream_t s) {
         if (!err_) return TQ_OK;
@@ -261,9 +333,13 @@ class MtonRunner {
     }
 
   private:
+    static constexpr size_t kDecCols = size_t(1) << 24;  // columns per decoded launch
     static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
     tq_space *sp_;
-    bool sym_;
+    bool sym_, dec_ = false;
+    size_t tail_bytes_ = 0;
+    float *fc_ = nullptr, *fs_ = nullptr;
+    uint8_t *tail_ = nullptr;
     tq_precision prec_;
     size_t m_, m_pad_ = 0, nc_max_ = 0, nc_alloc_ = 0;
     int K_ = 0, fmt_ = 0;
@@ -338,11 +414,15 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
         P.wht_scale = 1.0f / std::sqrt(static_cast<float>(D));
         P.lutq = 0;
         P.qlut_k = 0;
+        P.qflag = 0;
         if (tq::build_quant_lut(sp->boundaries, tq::kQlutBuckets, tq::kQlutMaxK, sp->qlut)) {
             P.lutq = 1;
             P.qlut_k = sp->qlut.k;
             P.qlut_s = sp->qlut.s;
             P.qlut_c = sp->qlut.c;
+            // one boundary at most per bucket and lo < 128: bit 7 can flag the
+            // buckets that hold one (the others need no comparison)
+            P.qflag = (P.qlut_k == 1 && sp->levels <= 128) ? 1 : 0;
         }
 
         // device binding (optional: without a GPU the space answers geometry
@@ -369,7 +449,8 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
             DeviceGuard g(dev);
             const size_t mw = (D + 31) / 32;
             const size_t off_c = 0, off_b = 4 * 256, off_q = off_b + 4 * (256 + tq::kQlutMaxK + 4);
-            const size_t off_r = off_q + tq::kQlutBuckets, off_j = off_r + 4 * mw;
+            const size_t off_qf = off_q + tq::kQlutBuckets;
+            const size_t off_r = off_qf + tq::kQlutBuckets, off_j = off_r + 4 * mw;
             const size_t off_s = (off_j + 4 * mw + 15) & ~size_t(15);
             const size_t total = off_s + 16;
             std::vector<unsigned char> host(total, 0);
@@ -377,7 +458,11 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
             std::vector<float> bnd(256 + tq::kQlutMaxK + 4, INFINITY);
             std::copy(sp->boundaries.begin(), sp->boundaries.end(), bnd.begin());
             std::memcpy(host.data() + off_b, bnd.data(), 4 * bnd.size());
-            if (P.lutq) std::memcpy(host.data() + off_q, sp->qlut.lo.data(), tq::kQlutBuckets);
+            if (P.lutq) {
+                std::memcpy(host.data() + off_q, sp->qlut.lo.data(), tq::kQlutBuckets);
+                for (int j = 0; j < tq::kQlutBuckets; ++j)
+                    host[off_qf + j] = (uint8_t)(sp->qlut.lo[j] | ((P.qflag && sp->qlut.span[j]) ? 0x80 : 0));
+            }
             std::vector<uint32_t> rm(mw, 0), qm(mw, 0);
             for (size_t i = 0; i < D; ++i) {
                 if (sp->rot_signs[i] > 0) rm[i >> 5] |= 1u << (i & 31);
@@ -400,6 +485,7 @@ tq_status tq_space_create(size_t dim, int bits, uint64_t rot_seed, uint64_t qjl_
             sp->T.centroids = reinterpret_cast<const float *>(base + off_c);
             sp->T.boundaries = reinterpret_cast<const float *>(base + off_b);
             sp->T.qlut = base + off_q;
+            sp->T.qlutf = base + off_qf;
             sp->T.rot_mask = reinterpret_cast<const uint32_t *>(base + off_r);
             sp->T.qjl_mask = reinterpret_cast<const uint32_t *>(base + off_j);
             sp->T.status = reinterpret_cast<int *>(base + off_s);
@@ -469,7 +555,10 @@ tq_status tq_space_quantize(const tq_space *sp, const float *z, size_t n, uint8_
             const int j = tq::quant_bucket(z[i], P.qlut_s, P.qlut_c, tq::kQlutBuckets);
             c = sp->qlut.lo[j];
             const int lo = c;
-            for (int t = 0; t < P.qlut_k; ++t) {
+            // as the encode kernel's flagged table (P.qflag): a bucket that holds
+            // no boundary takes lo without a comparison
+            const int kc = (P.qflag && sp->qlut.span[j] == 0) ? 0 : P.qlut_k;
+            for (int t = 0; t < kc; ++t) {
                 const float b = (lo + t < P.nb) ? sp->boundaries[lo + t] : INFINITY;
                 c += (z[i] > b) ? 1 : 0;
             }

@@ -37,6 +37,8 @@ struct Params {
     int cs;            // code size = pb + 12
     int lutq;          // 1: quantize through the bucket table (nb > 15)
     int qlut_k;        // boundaries compared per bucket
+    int qflag;         // 1: T.qlutf holds lo | 0x80 for the buckets that hold a boundary
+                       //    (levels <= 128, qlut_k = 1)
     float qlut_s;      // bucket(v) = clamp(fma(v, qlut_s, qlut_c), 0, NB-1)
     float qlut_c;
     float scale;       // sqrt(pi/2)/sqrt(D)            space_turbo_quant.h:265
@@ -48,6 +50,8 @@ struct DevTables {
     const float *centroids;   // [levels]
     const float *boundaries;  // [nb + kQlutMaxK], padded with +inf
     const uint8_t *qlut;      // [kQlutBuckets]: boundaries below the bucket
+    const uint8_t *qlutf;     // [kQlutBuckets]: the same | 0x80 when a boundary lies in the
+                              // bucket (P.qflag); otherwise a copy of qlut
     const uint32_t *rot_mask; // [D/32 rounded up]: bit i set <=> rot sign +1
     const uint32_t *qjl_mask; // [D/32 rounded up]
     int *status;              // stream-ordered kernels' error word (0 = ok)

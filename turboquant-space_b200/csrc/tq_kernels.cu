@@ -102,6 +102,33 @@ __device__ __forceinline__ void quantize_regs(float (&xr)[CH], float isg, float 
     }
 }
 
+// The bucket quantizer (kQuantBucket) with the flagged bucket table of
+// P.qflag and a lane-replicated centroid table: entry e of bucket y is
+// lo | 0x80 when a boundary lies inside the bucket, and only then is z
+// compared with B[lo] (about 4% of the values at b = 8); crow = table + lane,
+// entry idx at crow[32 idx], so the centroid loads of a warp hit 32 distinct
+// banks.  Same indices and residuals as quantize_regs.
+template <int CH, class Emit>
+__device__ __forceinline__ void quantize_regs_flag(float (&xr)[CH], float isg, float sg,
+                                                   const Params &P, const float *s_bnd,
+                                                   const uint8_t *s_qlutf, const float *crow,
+                                                   Emit emit) {
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const float z = __fmul_rn(xr[t], isg);
+        float y = __fmaf_rn(z, P.qlut_s, P.qlut_c);
+        y = fminf(fmaxf(y, 0.0f), (float)(kQlutBuckets - 1));
+        const int e = s_qlutf[(int)y];
+        int idx = e & 0x7F;
+        if (e & 0x80) idx += (z > s_bnd[idx]) ? 1 : 0;
+        xr[t] = __fmaf_rn(-crow[32 * idx], sg, xr[t]);
+        emit(t, idx);
+    }
+}
+
+// Bytes of encode2's lane-replicated centroid table (P.qflag): levels x 32 floats.
+__host__ __device__ __forceinline__ int crep_bytes(const Params &P) { return P.qflag ? P.levels * 128 : 0; }
+
 // ---------------------------------------------------------------------------
 // encode: one warp per group of VPW consecutive rows (VPW = 4, or 2 at large
 // D, where four vector buffers per warp would leave room for only 4 warps per
@@ -491,12 +518,13 @@ __device__ __forceinline__ void rht2(float *buf, int lane, float pre, uint32_t s
     __syncwarp();
 }
 
-// Per-warp shared bytes of encode2: 4 padded vectors, the quantizer indices
-// of 4 vectors (D bytes each, one 32-bit word per lane and 4 positions), 4
-// staged codes.
+// Per-warp shared bytes of encode2: 4 padded vectors and the quantizer
+// indices of 4 vectors (D bytes each, one 32-bit word per lane and 4
+// positions).  The 4 finished codes are staged in vector 0's buffer, which is
+// dead by then (4 cs <= 4 (D + 12) bytes < its 4 (D + D/8 + 8)).
 template <int LOG_D>
-__host__ __device__ constexpr int encode2_warp_bytes_c(int cs) {
-    return 16 * vec_row_floats<(1 << LOG_D)>() + 4 * (1 << LOG_D) + align16(4 * cs);
+__host__ __device__ constexpr int encode2_warp_bytes_c() {
+    return 16 * vec_row_floats<(1 << LOG_D)>() + 4 * (1 << LOG_D);
 }
 
 template <int LOG_D, bool NIBBLE>
@@ -508,7 +536,10 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
     constexpr int VS = vec_row_floats<D>();
     static_assert(E >= 8 && E <= 32, "encode2 covers D = 256..1024");
     extern __shared__ __align__(16) unsigned char smem[];
-    load_tables(smem, P, T, true);
+    load_tables(smem, P, T, true, P.qflag != 0);
+    float *s_crep = reinterpret_cast<float *>(smem + kTabBytes);  // P.qflag: [levels][32]
+    if (P.qflag)
+        for (int i = threadIdx.x; i < P.levels * 32; i += blockDim.x) s_crep[i] = T.centroids[i >> 5];
     __syncthreads();
     const float *s_cent = reinterpret_cast<const float *>(smem + kTabCentOff);
     const float *s_bnd = reinterpret_cast<const float *>(smem + kTabBndOff);
@@ -517,10 +548,10 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
     const uint8_t *s_qlut = smem + kTabQlutOff;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int cs = P.cs;
-    unsigned char *wbase = smem + kTabBytes + warp * encode2_warp_bytes_c<LOG_D>(cs);
+    unsigned char *wbase = smem + kTabBytes + crep_bytes(P) + warp * encode2_warp_bytes_c<LOG_D>();
     float *buf = reinterpret_cast<float *>(wbase);
     uint32_t *idxw = reinterpret_cast<uint32_t *>(wbase + 16 * VS);  // [4][E/4][32]
-    uint8_t *stage = wbase + 16 * VS + 4 * D;
+    uint8_t *stage = wbase;  // vector 0's buffer, once phase G has transformed it
     const int g = lane >> 3;
     // sign bits of this lane's layout-A elements lane*E .. lane*E + E-1
     const int bit0 = lane * E;
@@ -628,8 +659,11 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 uint32_t wq[E / 4] = {};
 #pragma unroll
                 for (int t = 0; t < E; ++t) xr[t] = b[PadLayout<E>::elem(32 * t + lane)];
-                quantize_regs<E>(xr, isg, sg, qmode, P, breg, s_bnd, s_qlut, s_cent,
-                                 [&](int t, int idx) { wq[t >> 2] |= (uint32_t)idx << (8 * (t & 3)); });
+                auto emit = [&](int t, int idx) { wq[t >> 2] |= (uint32_t)idx << (8 * (t & 3)); };
+                if (P.qflag)
+                    quantize_regs_flag<E>(xr, isg, sg, P, s_bnd, s_qlut, s_crep + lane, emit);
+                else
+                    quantize_regs<E>(xr, isg, sg, qmode, P, breg, s_bnd, s_qlut, s_cent, emit);
 #pragma unroll
                 for (int t = 0; t < E; ++t) b[PadLayout<E>::elem(32 * t + lane)] = xr[t];
 #pragma unroll
@@ -1653,11 +1687,11 @@ constexpr int kSmemBudget = 227 * 1024;
 template <int LOG_D, bool NIBBLE>
 cudaError_t encode2_launch(const Params &P, const DevTables &T, const float *X, size_t n,
                            uint8_t *out, cudaStream_t st) {
-    const int per_warp = encode2_warp_bytes_c<LOG_D>(P.cs);
-    int warps = (kSmemBudget - kTabBytes) / per_warp;
+    const int per_warp = encode2_warp_bytes_c<LOG_D>();
+    int warps = (kSmemBudget - kTabBytes - crep_bytes(P)) / per_warp;
     if (warps > 4) warps = 4;
     if (warps < 1) return cudaErrorInvalidConfiguration;
-    const size_t smem = (size_t)kTabBytes + (size_t)warps * per_warp;
+    const size_t smem = (size_t)kTabBytes + crep_bytes(P) + (size_t)warps * per_warp;
     cudaError_t e = cudaFuncSetAttribute(encode2_kernel<LOG_D, NIBBLE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -107,6 +107,17 @@ cudaError_t launch_tc_topk_dec(int variant, const void *Ah, const void *Al, size
 // Whether `variant` runs with decoded B tiles for codes of cs bytes (a tile of
 // 128 codes must fit in shared memory beside the variant's stages).
 bool tc_topk_dec_ok(int variant, int cs);
+// The M x N distances of launch_tc_dist with decoded B tiles (128 x 128 tiles,
+// two stages): columns [0, dec.n) of dec.codes, out[i * ldo + j] for i < m.
+// Asymmetric (dec.fc, dec.fs set): K = 2D, dec.kbc = D / 64, c1 / c2 / fc / fs
+// from launch_dec_factors; symmetric (dec.fc null): K = D, dec.kbc = D / 64,
+// A the symmetric row planes.  The last tile's copy reads the codes up to a
+// 16-byte boundary past code dec.n - 1: the caller guarantees that memory.
+cudaError_t launch_tc_dist_dec(const void *Ah, const void *Al, size_t m, size_t m_pad, const DecSrc &dec,
+                               size_t n_pad, int K, const float *r1, const float *r2, const float *c1,
+                               const float *c2, float *out, size_t ldo, int *err, cudaStream_t st);
+// Whether a tile of 128 codes of cs bytes fits launch_tc_dist_dec's shared memory.
+bool tc_dist_dec_fits(int cs);
 // Threshold collection over the corpus for the rows of A (row count *m_dev,
 // nothing unless it exceeds min_rows): every column whose tile distance (as the
 // top-k pass computes it) is at most thr[row] goes to coll_i[row * cap + ...],

@@ -192,8 +192,10 @@ constexpr int kTabQlutOff = kTabQjlOff + 4 * 256;               // u8[2048]
 constexpr int kTabBytes = kTabQlutOff + kQlutBuckets;           // 6176 (16-aligned)
 static_assert(kTabBytes % 16 == 0, "table block must keep 16-byte alignment");
 
+// flagged: the bucket table with bit 7 set on the buckets that hold a
+// boundary (T.qlutf, for P.qflag) instead of the plain one.
 __device__ __forceinline__ void load_tables(unsigned char *smem, const Params &P,
-                                            const DevTables &T, bool quant) {
+                                            const DevTables &T, bool quant, bool flagged = false) {
     float *cent = reinterpret_cast<float *>(smem + kTabCentOff);
     float *bnd = reinterpret_cast<float *>(smem + kTabBndOff);
     uint32_t *rot = reinterpret_cast<uint32_t *>(smem + kTabRotOff);
@@ -208,8 +210,10 @@ __device__ __forceinline__ void load_tables(unsigned char *smem, const Params &P
     if (quant) {
         for (int i = tid; i < P.levels; i += nt) cent[i] = T.centroids[i];
         for (int i = tid; i < P.nb + kQlutMaxK; i += nt) bnd[i] = T.boundaries[i];
-        if (P.lutq)
-            for (int i = tid; i < kQlutBuckets; i += nt) qlut[i] = T.qlut[i];
+        if (P.lutq) {
+            const uint8_t *src = flagged ? T.qlutf : T.qlut;
+            for (int i = tid; i < kQlutBuckets; i += nt) qlut[i] = src[i];
+        }
     }
 }
 

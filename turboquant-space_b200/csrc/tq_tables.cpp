@@ -123,6 +123,7 @@ bool build_quant_lut(const std::vector<float> &boundaries, int buckets, int max_
     }
     vmin_key[buckets] = kpos + 1;  // one past +inf
     lut.lo.assign(buckets, 0);
+    lut.span.assign(buckets, 0);
     int kmax = 0;
     for (int j = 0; j < buckets; ++j) {
         // lo: boundaries strictly below every value of the bucket
@@ -138,6 +139,7 @@ bool build_quant_lut(const std::vector<float> &boundaries, int buckets, int max_
         }
         if (lo_j > 255) return false;
         lut.lo[j] = static_cast<uint8_t>(lo_j);
+        lut.span[j] = static_cast<uint8_t>(std::min(hi_j - lo_j, 255));
         kmax = std::max(kmax, hi_j - lo_j);
     }
     if (kmax > max_k) return false;

@@ -21,6 +21,7 @@ struct QuantLut {
     float s = 0.0f, c = 0.0f;
     int buckets = 0, k = 0;
     std::vector<uint8_t> lo;
+    std::vector<uint8_t> span;  // boundaries inside bucket j (0 .. k)
 };
 int quant_bucket(float z, float s, float c, int buckets);
 bool build_quant_lut(const std::vector<float> &boundaries, int buckets, int max_k, QuantLut &lut);

@@ -1948,6 +1948,36 @@ cudaError_t launch_tc_dist(const void *Ah, const void *Al, const void *Bh, const
     return tcp_launch<false, 3, 4, true, DistEpi>(mp, sh, ep, err, sm_grid(tiles), st);
 }
 
+bool tc_dist_dec_fits(int cs) {
+    DecSrc d;
+    d.cs = cs;
+    return cs > 0 && with_code_buffers(d, 2).cbufs > 0;
+}
+
+cudaError_t launch_tc_dist_dec(const void *Ah, const void *Al, size_t m, size_t m_pad, const DecSrc &dec,
+                               size_t n_pad, int K, const float *r1, const float *r2, const float *c1,
+                               const float *c2, float *out, size_t ldo, int *err, cudaStream_t st) {
+    if (m == 0 || dec.n == 0) return cudaSuccess;
+    const bool sym = dec.fc == nullptr;
+    if (K % TC_BK || m_pad % TC_BM || n_pad % TC_BN || m > m_pad || dec.n > n_pad || !dec_ok(dec, K))
+        return cudaErrorInvalidValue;
+    // symmetric: the whole K is centroid values; asymmetric: centroid half + sign half
+    if (sym ? dec.kbc != K / TC_BK : (dec.kbc * 2 != K / TC_BK || !dec.fs)) return cudaErrorInvalidValue;
+    if (!aligned16({Ah, Al})) return cudaErrorMisalignedAddress;
+    alignas(64) TcMaps mp;
+    TcShape sh{};
+    if (!a_maps(mp, sh, Ah, Al, m_pad, K, dec.kbc)) return cudaErrorInvalidValue;
+    const unsigned num_mb = (unsigned)(m_pad / TC_BM);
+    const size_t tiles = (size_t)num_mb * (n_pad / TC_BN);
+    if (tiles > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    const DecSrc d = with_code_buffers(dec, 2);
+    if (d.cbufs == 0) return cudaErrorInvalidValue;  // the code tile does not fit beside the stages
+    const DistEpi::Params ep{GridTiles{num_mb, (unsigned)tiles}, m, dec.n, r1, r2, c1, c2, out, ldo};
+    // chunk lengths as the planes kernels: 8 K blocks asymmetric, 4 symmetric
+    if (sym) return tcp_launch<false, 2, 4, true, DistEpi, true>(mp, sh, ep, err, sm_grid(tiles), st, d);
+    return tcp_launch<false, 2, 8, true, DistEpi, true>(mp, sh, ep, err, sm_grid(tiles), st, d);
+}
+
 cudaError_t launch_tc_symq(const void *A1h, const void *A1l, const void *B1h, const void *B1l,
                            int K1, const void *A2h, const void *A2l, const void *B2h,
                            const void *B2l, int K2, bool exact2, size_t m, size_t m_pad, size_t n,

@@ -21,7 +21,7 @@ TQ_ERR_TIMEOUT = 5
 TQ_ERR_BUSY = 6
 TQ_ERR_NOT_SUPPORTED = 7
 
-PRECISION = {"fp32": 0, "split_bf16": 1, "split_tf32": 2, "reference": 3}
+PRECISION = {"fp32": 0, "split_bf16": 1, "split_tf32": 2, "reference": 3, "split_bf16_decoded": 4}
 
 # Every symbol include/turboquant_b200.h declares.
 EXPORTS = (
