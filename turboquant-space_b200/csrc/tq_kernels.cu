@@ -518,19 +518,28 @@ __device__ __forceinline__ void rht2(float *buf, int lane, float pre, uint32_t s
     __syncwarp();
 }
 
-// Per-warp shared bytes of encode2: 4 padded vectors and the quantizer
-// indices of 4 vectors (D bytes each, one 32-bit word per lane and 4
-// positions).  The 4 finished codes are staged in vector 0's buffer, which is
-// dead by then (4 cs <= 4 (D + 12) bytes < its 4 (D + D/8 + 8)).
-template <int LOG_D>
+// Rows per warp and warps per CTA of encode2.  Byte codes at D = 1024 (168
+// registers) run 3 rows per warp in one CTA of 12 warps per SM, three warps
+// per scheduler to hide the serial reduction chains; shared memory holds 8
+// warps of 4 rows.  Everything else: 4 rows per warp, CTAs of 4 warps.
+template <int LOG_D, bool NIBBLE>
+__host__ __device__ constexpr int enc2_rpw() { return (LOG_D == 10 && !NIBBLE) ? 3 : 4; }
+template <int LOG_D, bool NIBBLE>
+__host__ __device__ constexpr int enc2_max_warps() { return (LOG_D == 10 && !NIBBLE) ? 12 : 4; }
+
+// Per-warp shared bytes of encode2: RPW padded vectors and the quantizer
+// indices of RPW vectors (D bytes each, one 32-bit word per lane and 4
+// positions).  The finished codes are staged in vector 0's buffer, which is
+// dead by then (RPW cs <= 4 (D + 12) bytes < its 4 (D + D/8 + 8)).
+template <int LOG_D, int RPW>
 __host__ __device__ constexpr int encode2_warp_bytes_c() {
-    return 16 * vec_row_floats<(1 << LOG_D)>() + 4 * (1 << LOG_D);
+    return 4 * RPW * vec_row_floats<(1 << LOG_D)>() + RPW * (1 << LOG_D);
 }
 
 template <int LOG_D, bool NIBBLE>
-__global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ X, size_t n,
-                                                      uint8_t *__restrict__ out, Params P,
-                                                      DevTables T) {
+__global__ void __launch_bounds__(32 * enc2_max_warps<LOG_D, NIBBLE>()) encode2_kernel(
+    const float *__restrict__ X, size_t n, uint8_t *__restrict__ out, Params P, DevTables T) {
+    constexpr int RPW = enc2_rpw<LOG_D, NIBBLE>();  // rows per warp
     constexpr int D = 1 << LOG_D;
     constexpr int E = D / 32;
     constexpr int VS = vec_row_floats<D>();
@@ -548,34 +557,37 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
     const uint8_t *s_qlut = smem + kTabQlutOff;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int cs = P.cs;
-    unsigned char *wbase = smem + kTabBytes + crep_bytes(P) + warp * encode2_warp_bytes_c<LOG_D>();
+    unsigned char *wbase = smem + kTabBytes + crep_bytes(P) + warp * encode2_warp_bytes_c<LOG_D, RPW>();
     float *buf = reinterpret_cast<float *>(wbase);
-    uint32_t *idxw = reinterpret_cast<uint32_t *>(wbase + 16 * VS);  // [4][E/4][32]
+    uint32_t *idxw = reinterpret_cast<uint32_t *>(wbase + 4 * RPW * VS);  // [RPW][E/4][32]
     uint8_t *stage = wbase;  // vector 0's buffer, once phase G has transformed it
+    // 8-lane group g runs the reduction chains of row g; with 3 rows per warp
+    // group 3 repeats row 2's (its results are not used)
     const int g = lane >> 3;
+    const int gv = g < RPW ? g : RPW - 1;
     // sign bits of this lane's layout-A elements lane*E .. lane*E + E-1
     const int bit0 = lane * E;
     const uint32_t emask = (E >= 32) ? 0xffffffffu : ((1u << E) - 1u);
     const uint32_t rbits = (s_rot[bit0 >> 5] >> (bit0 & 31)) & emask;
     const uint32_t qbits = (s_qjl[bit0 >> 5] >> (bit0 & 31)) & emask;
     const bool vec4 = ((P.dim & 3) == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
-    const size_t nquads = (n + 3) >> 2;
+    const size_t ngroups = (n + RPW - 1) / RPW;
 
-    // Each warp steps through the phases of its own quads on its own: the
-    // buffers are the warp's and the tables read-only, so the phases are
+    // Each warp steps through the phases of its own row groups on its own:
+    // the buffers are the warp's and the tables read-only, so the phases are
     // ordered by warp barriers alone, and a warp in a reduction chain overlaps
     // another warp's transforms (block barriers here cost 11%).
-    for (size_t base = (size_t)blockIdx.x * nwarps; base < nquads; base += (size_t)gridDim.x * nwarps) {
+    for (size_t base = (size_t)blockIdx.x * nwarps; base < ngroups; base += (size_t)gridDim.x * nwarps) {
         const size_t qd = base + warp;
-        const bool active = qd < nquads;
-        const size_t row0 = qd << 2;
-        const int nv = !active ? 0 : ((n - row0 < 4) ? (int)(n - row0) : 4);
+        const bool active = qd < ngroups;
+        const size_t row0 = qd * RPW;
+        const int nv = !active ? 0 : ((n - row0 < (size_t)RPW) ? (int)(n - row0) : RPW);
         float norm = 0.0f, inv_norm = 0.0f;
-        // the rows of this warp's next quad go to L2 while this one is encoded
+        // the rows of this warp's next group go to L2 while this one is encoded
         if (vec4 && lane == 0) {
-            const size_t nrow0 = (qd + (size_t)gridDim.x * nwarps) << 2;
+            const size_t nrow0 = (qd + (size_t)gridDim.x * nwarps) * RPW;
             if (nrow0 < n) {
-                const size_t rows = (n - nrow0 < 4) ? (n - nrow0) : 4;
+                const size_t rows = (n - nrow0 < (size_t)RPW) ? (n - nrow0) : RPW;
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(X + nrow0 * (size_t)P.dim),
                              "r"((uint32_t)(rows * (size_t)P.dim * 4)) : "memory");
             }
@@ -587,7 +599,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 // once); the zero padding past dim as plain stores
                 const int d4 = P.dim >> 2;
 #pragma unroll 4
-                for (int i = lane; i < D; i += 32) {  // i = v * (D/4) + chunk
+                for (int i = lane; i < RPW * (D / 4); i += 32) {  // i = v * (D/4) + chunk
                     const int v = i / (D / 4), i4 = i % (D / 4);
                     float *dst = buf + v * VS + PadLayout<E>::chunk(i4);
                     if (v < nv && i4 < d4) {
@@ -601,7 +613,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
             } else {
 #pragma unroll 1
-                for (int v = 0; v < 4; ++v) {
+                for (int v = 0; v < RPW; ++v) {
                     const float *src = X + (row0 + v) * (size_t)P.dim;
 #pragma unroll 1
                     for (int i = lane; i < D; i += 32)
@@ -609,7 +621,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 }
             }
             __syncwarp();
-            const float nsq = chain_sq_reduce2<E, false>(buf + g * VS, P.dim, lane);
+            const float nsq = chain_sq_reduce2<E, false>(buf + gv * VS, P.dim, lane);
             norm = __fsqrt_rn(nsq);
             inv_norm = (nsq > f32_bits(kNormSqFloorBits)) ? __fdiv_rn(1.0f, norm) : 0.0f;
         }
@@ -618,7 +630,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
         float sigma = 0.0f, inv_sigma = 0.0f;
         if (active) {
 #pragma unroll 1
-            for (int v = 0; v < 4; ++v) {
+            for (int v = 0; v < RPW; ++v) {
                 float *b = buf + v * VS;
                 float x[E];
                 rht2<E, true>(b, lane, __shfl_sync(kFull, inv_norm, 8 * v), rbits, P.wht_scale, x);
@@ -626,7 +638,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 for (int t = 0; t < E; ++t) b[PadLayout<E>::elem(32 * t + lane)] = x[t];
             }
             __syncwarp();
-            const float var = chain_sq_reduce2<E, true>(buf + g * VS, D, lane);
+            const float var = chain_sq_reduce2<E, true>(buf + gv * VS, D, lane);
             sigma = __fsqrt_rn(__fdiv_rn(var, (float)D));
             if (f32_bits(kSigmaFloorBits) > sigma) {
                 sigma = f32_bits(kSigmaFloorBits);
@@ -647,7 +659,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
             float breg[15];
             load_bound_regs(breg, P, s_bnd);
 #pragma unroll 1
-            for (int v = 0; v < 4; ++v) {
+            for (int v = 0; v < RPW; ++v) {
                 const float sg = __shfl_sync(kFull, sigma, 8 * v);
                 const float isg = __shfl_sync(kFull, inv_sigma, 8 * v);
                 float *b = buf + v * VS;
@@ -670,7 +682,7 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 for (int t4 = 0; t4 < E / 4; ++t4) idxw[(v * (E / 4) + t4) * 32 + lane] = wq[t4];
             }
             __syncwarp();
-            gamma = __fsqrt_rn(chain_sq_reduce2<E, true>(buf + g * VS, D, lane));
+            gamma = __fsqrt_rn(chain_sq_reduce2<E, true>(buf + gv * VS, D, lane));
         }
         __syncwarp();
         // G: RHT_qjl(residual), pack units + trailer; H: staged codes -> global
@@ -715,6 +727,12 @@ __global__ void __launch_bounds__(128) encode2_kernel(const float *__restrict__ 
                 uint4 *d4 = reinterpret_cast<uint4 *>(dst);
 #pragma unroll 1
                 for (int i = lane; i < (len >> 4); i += 32) __stcs(d4 + i, s4[i]);
+            } else if (((reinterpret_cast<uintptr_t>(dst) & 3) == 0) && ((len & 3) == 0)) {
+                // groups of 3 codes of 4k + 12 bytes start on 4-byte boundaries
+                const uint32_t *s1 = reinterpret_cast<const uint32_t *>(stage);
+                uint32_t *d1 = reinterpret_cast<uint32_t *>(dst);
+#pragma unroll 1
+                for (int i = lane; i < (len >> 2); i += 32) __stcs(d1 + i, s1[i]);
             } else {
 #pragma unroll 1
                 for (int i = lane; i < len; i += 32) dst[i] = stage[i];
@@ -1687,9 +1705,10 @@ constexpr int kSmemBudget = 227 * 1024;
 template <int LOG_D, bool NIBBLE>
 cudaError_t encode2_launch(const Params &P, const DevTables &T, const float *X, size_t n,
                            uint8_t *out, cudaStream_t st) {
-    const int per_warp = encode2_warp_bytes_c<LOG_D>();
+    constexpr int RPW = enc2_rpw<LOG_D, NIBBLE>();
+    const int per_warp = encode2_warp_bytes_c<LOG_D, RPW>();
     int warps = (kSmemBudget - kTabBytes - crep_bytes(P)) / per_warp;
-    if (warps > 4) warps = 4;
+    if (warps > enc2_max_warps<LOG_D, NIBBLE>()) warps = enc2_max_warps<LOG_D, NIBBLE>();
     if (warps < 1) return cudaErrorInvalidConfiguration;
     const size_t smem = (size_t)kTabBytes + crep_bytes(P) + (size_t)warps * per_warp;
     cudaError_t e = cudaFuncSetAttribute(encode2_kernel<LOG_D, NIBBLE>,
@@ -1699,8 +1718,8 @@ cudaError_t encode2_launch(const Params &P, const DevTables &T, const float *X, 
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode2_kernel<LOG_D, NIBBLE>, 32 * warps, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    const size_t quads = (n + 3) / 4;
-    size_t blocks = (quads + warps - 1) / warps;
+    const size_t groups = (n + RPW - 1) / RPW;
+    size_t blocks = (groups + warps - 1) / warps;
     const size_t cap = (size_t)sm_count() * per_sm;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
