@@ -619,7 +619,8 @@ def serve_result(args, rates, window, cpu=True, layout="planes"):
     del codes
     torch.cuda.empty_cache()
     t0 = time.perf_counter()
-    server = index.serve(k=10, max_rows=1024, slots=2, kernel_variant=args.kernel_variant,
+    max_rows, slots = getattr(args, "max_rows", 1024), getattr(args, "slots", 2)
+    server = index.serve(k=10, max_rows=max_rows, slots=slots, kernel_variant=args.kernel_variant,
                          bound_scale=getattr(args, "bound_scale", 0.0))
     setup_s = time.perf_counter() - t0
     tuning = server.tuning(searched=True)
@@ -685,7 +686,7 @@ def serve_result(args, rates, window, cpu=True, layout="planes"):
     return {
         "config": {"dim": dim, "padded_dim": space.padded_dim(), "bits_per_coord": bits,
                    "n_codes": n, "k": 10, "request_rows": "U{1..256}", "arrivals": "Poisson",
-                   "window_s": window, "max_batch_rows": 1024, "slots": 2,
+                   "window_s": window, "max_batch_rows": max_rows, "slots": slots,
                    "kernel_variant": "autotuned" if args.kernel_variant < 0 else args.kernel_variant,
                    "top_k": "exact (tensor-pass candidates rescored with the reference's arithmetic)",
                    "bound_scale": getattr(args, "bound_scale", 0.0) or 1.0,
@@ -823,6 +824,9 @@ def main():
     ap.add_argument("--rates", default="5,20,40,60,100,150,1000,50000",
                     help="serve: request rates (req/s) to sweep")
     ap.add_argument("--window", type=float, default=30.0, help="serve: seconds per rate")
+    ap.add_argument("--max-rows", type=int, default=1024,
+                    help="serve: query rows per batch (a request holds at most 256)")
+    ap.add_argument("--slots", type=int, default=2, help="serve: batches in flight")
     ap.add_argument("--layout", choices=("planes", "codes"), default="planes",
                     help="serve: index layout (operand planes, or codes decoded in shared memory)")
     ap.add_argument("--kernel-variant", type=int, default=-1,

@@ -145,3 +145,13 @@ def test_compute_without_gpu_fails_loudly():
     code = ctypes.c_int(-1)
     st = _capi.lib().tq_space_take_device_status(s._h, ctypes.byref(code))
     assert st != 0 and code.value == 0
+
+
+def test_precision_names_match_the_header():
+    """The Python mirror's precision keywords are the header's tq_precision
+    values: "split_bf16_decoded" is TQ_PRECISION_SPLIT_BF16_DECODED, and so on."""
+    text = open(os.path.join(ROOT, "include", "turboquant_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    enum = {m.group(1).lower(): int(m.group(2))
+            for m in re.finditer(r"\bTQ_PRECISION_([A-Z0-9_]+)\s*=\s*(\d+)", text)}
+    assert enum == _capi.PRECISION, (enum, _capi.PRECISION)
