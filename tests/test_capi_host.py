@@ -142,6 +142,9 @@ def test_compute_without_gpu_fails_loudly():
         s.encode_batch(np.zeros((2, 64), np.float32))
     with pytest.raises(tq.TQError, match="no CUDA device"):
         s.distance_1_to_n(np.zeros(64, np.float32), np.zeros(44, np.uint8))
+    for prec in _capi.PRECISION:
+        with pytest.raises(tq.TQError, match="no CUDA device"):
+            s.distance_m_to_n(np.zeros((2, 64), np.float32), np.zeros((3, 44), np.uint8), precision=prec)
     code = ctypes.c_int(-1)
     st = _capi.lib().tq_space_take_device_status(s._h, ctypes.byref(code))
     assert st != 0 and code.value == 0
