@@ -38,7 +38,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import oracle as O  # noqa: E402
 
-# (dim, bits): every BASELINE shape plus the edge cases of the layout
+# (dim, bits): the benchmark workloads' shapes (128-d and 384-d 4-bit, 768-d 8- and
+# 4-bit, 1536-d 4-bit) plus the edge cases of the layout
 # (nibble vs byte, padding, dim < 4, 9-bit overflow of the unit byte).
 CASES = [
     (128, 4), (768, 8), (768, 4), (1536, 4), (384, 4),
