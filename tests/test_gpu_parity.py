@@ -34,7 +34,7 @@ def test_encode_bit_exact_vs_golden(cuda_ok, dim, bits):
                                       (4096, 8), (8192, 4)])
 def test_encode_bit_exact_vs_oracle(cuda_ok, dim, bits):
     rng = np.random.default_rng(dim * 13 + bits)
-    n = 257 if dim <= 1024 else 33          # not a multiple of 4: a ragged last quad
+    n = 257 if dim <= 1024 else 33          # not a multiple of 3 or 4: a ragged last row group
     X = (rng.standard_normal((n, dim)) * rng.uniform(1e-3, 1e3, (n, 1))).astype(np.float32)
     X[0] = 0.0
     X[1, : max(1, dim // 2)] = 0.0
