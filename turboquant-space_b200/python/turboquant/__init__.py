@@ -396,6 +396,13 @@ class TurboQuantSpace:
         return out
 
     def distance_m_to_n(self, queries, codes, precision="fp32", out=None):
+        """distanceBatchMToN: queries [m, dim] float32 x codes [n, cs] -> [m, n].
+
+        precision: "fp32" (CUDA cores, the drop-in), "split_bf16" (tcgen05
+        tensor cores on hi+lo BF16 operand planes), "split_bf16_decoded" (the
+        same arithmetic, column tiles decoded from the codes in shared memory:
+        less device memory, somewhat slower) or "reference" (the reference
+        build's own summation order, bit-identical distances)."""
         cs = self.code_size_bytes()
         prec = _capi.PRECISION[precision]
         if _is_device(queries) or _is_device(codes):
@@ -416,6 +423,10 @@ class TurboQuantSpace:
         return out
 
     def distance_m_to_n_symmetric(self, codes_a, codes_b, precision="fp32", out=None):
+        """distanceBatchMToNSymmetric: codes_a [m, cs] x codes_b [n, cs] -> [m, n].
+
+        precision: "fp32", "split_bf16" or "split_bf16_decoded", as for
+        distance_m_to_n ("reference" is not available for this form)."""
         cs = self.code_size_bytes()
         prec = _capi.PRECISION[precision]
         if _is_device(codes_a) or _is_device(codes_b):
