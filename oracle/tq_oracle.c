@@ -428,20 +428,96 @@ static float dist_search(const tqo_space *sp, const float *q_rot, const float *s
                          : dist_search_b8(sp, q_rot, s_q, norms, code);
 }
 
-/* distBuildScalar / distBuildScalarB4: space_turbo_quant.h:688-714, 985-1019 */
-static float dist_build(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+/* Symmetric distances in the pinned build's own order (read from the x86
+ * assembly of the reference compiled here, and checked bit for bit against it
+ * at every padded dim).  Both functions end in the same epilogue:
+ *   d = max(0, fma(-(ip + ip), |a| |b|, fma(|a|, |a|, |b| |b|))).
+ * The sigma factors leave the per-coordinate products: the loops sum products
+ * of centroid values. */
+static float sym_epilogue(float ip, float na, float nb) {
+    const float d = fmaf(-(ip + ip), na * nb, fmaf(na, na, nb * nb));
+    return 0.0f < d ? d : 0.0f;
+}
+
+/* distBuildAVX (:1541-1612), byte codes.  D >= 8: eight running sums,
+ * coordinate i into sum i mod 8, as fma(c_a[i] * c_b[i], sigma_a sigma_b, sum);
+ * ip = hsum8.  D < 8: the same fma in coordinate order into one sum. */
+static float dist_build_b8(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+    const size_t D = sp->D;
+    const float *c = sp->centroids;
     float ma[3], mb[3];
     code_meta(sp, a, ma);
     code_meta(sp, b, mb);
-    float ip_rot = 0.0f;
-    for (size_t i = 0; i < sp->D; ++i) {
-        float ca = sp->centroids[code_unit(a, i, sp->bits) >> 1] * ma[2];
-        float cb = sp->centroids[code_unit(b, i, sp->bits) >> 1] * mb[2];
-        ip_rot = ip_rot + ca * cb;
+    const float sab = ma[2] * mb[2];
+    float ip = 0.0f;
+    size_t i = 0;
+    if (D >= 8) {
+        float S[8];
+        for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+        for (; i + 8 <= D; i += 8)
+            for (int j = 0; j < 8; ++j)
+                S[j] = fmaf(c[a[i + (size_t)j] >> 1] * c[b[i + (size_t)j] >> 1], sab, S[j]);
+        ip = hsum8(S);
     }
-    float ip = ip_rot * ma[0] * mb[0];
-    float d = ma[0] * ma[0] + mb[0] * mb[0] - 2.0f * ip;
-    return d > 0.0f ? d : 0.0f;
+    for (; i < D; ++i) ip = fmaf(c[a[i] >> 1] * c[b[i] >> 1], sab, ip);
+    return sym_epilogue(ip, ma[0], mb[0]);
+}
+
+/* distBuildScalarB4 (:985-1019), nibble codes, as vectorised by the build.
+ * Let lo(x, k) / hi(x, k) be the centroid values of byte k's low / high nibble
+ * and pair(f, k0, k1) = fma(f(a, k0), f(b, k0), f(a, k1) * f(b, k1)).
+ *  - >= 32 bytes, per block of 32 bytes at k and lane j < 8:
+ *      s = ((pair(hi, k+16+j, k+24+j) + pair(hi, k+j, k+8+j))
+ *           + pair(lo, k+j, k+8+j)) + pair(lo, k+16+j, k+24+j),
+ *    S[j] = fma(s * sigma_a, sigma_b, S[j]); ip = hsum8(S).
+ *  - 16 bytes (D == 32), lane j < 4: the same with offsets 0/4 and 8/12,
+ *    S[j] = (s * sigma_a) * sigma_b; ip = hsum4(S).
+ *  - <= 8 bytes: in byte order, ip = fma(fma(lo_a, lo_b, hi_a * hi_b),
+ *    sigma_a sigma_b, ip). */
+static float dist_build_b4(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+    const size_t nb = sp->packed_bytes;
+    const float *c = sp->centroids;
+    float ma[3], mb[3];
+    code_meta(sp, a, ma);
+    code_meta(sp, b, mb);
+    #define LO_(x, k) c[((x)[k] & 15u) >> 1]
+    #define HI_(x, k) c[((x)[k] >> 4) >> 1]
+    #define PAIR_(F, k0, k1) fmaf(F(a, k0), F(b, k0), F(a, k1) * F(b, k1))
+    float ip = 0.0f;
+    size_t k = 0;
+    if (nb >= 32) {
+        float S[8];
+        for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+        for (; k + 32 <= nb; k += 32)
+            for (int j = 0; j < 8; ++j) {
+                const size_t l0 = k + (size_t)j, l1 = l0 + 16;
+                const float s = ((PAIR_(HI_, l1, l1 + 8) + PAIR_(HI_, l0, l0 + 8)) +
+                                 PAIR_(LO_, l0, l0 + 8)) + PAIR_(LO_, l1, l1 + 8);
+                S[j] = fmaf(s * ma[2], mb[2], S[j]);
+            }
+        ip = hsum8(S);
+    }
+    if (nb - k >= 16) {
+        float S4[4];
+        for (int j = 0; j < 4; ++j) {
+            const size_t l0 = k + (size_t)j, l1 = l0 + 8;
+            const float s = ((PAIR_(HI_, l1, l1 + 4) + PAIR_(HI_, l0, l0 + 4)) +
+                             PAIR_(LO_, l0, l0 + 4)) + PAIR_(LO_, l1, l1 + 4);
+            S4[j] = (s * ma[2]) * mb[2];
+        }
+        ip = ip + hsum4(S4);
+        k += 16;
+    }
+    const float sab = ma[2] * mb[2];
+    for (; k < nb; ++k) ip = fmaf(fmaf(LO_(a, k), LO_(b, k), HI_(a, k) * HI_(b, k)), sab, ip);
+    #undef LO_
+    #undef HI_
+    #undef PAIR_
+    return sym_epilogue(ip, ma[0], mb[0]);
+}
+
+static float dist_build(const tqo_space *sp, const uint8_t *a, const uint8_t *b) {
+    return sp->bits <= 4 ? dist_build_b4(sp, a, b) : dist_build_b8(sp, a, b);
 }
 
 void tqo_distance_1_to_n(const tqo_space *sp, const float *q, const uint8_t *codes,

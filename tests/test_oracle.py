@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from conftest import GOLDEN, GOLDEN_CASES, asym_term_scale, dist_close, load_case, sym_term_scale
+from conftest import GOLDEN, GOLDEN_CASES, asym_term_scale, load_case
 
 
 @pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
@@ -40,16 +40,15 @@ def test_oracle_encode_bit_exact_vs_golden(dim, bits):
 def test_oracle_distances_vs_golden(dim, bits):
     g = load_case(dim, bits)
     o = O.OracleSpace(dim, bits)
-    cs, pb = o.cs, o.cs - 12
     codes = g["codes"]
     # asymmetric distances: the pinned build's summation order, bit for bit
     np.testing.assert_array_equal(o.distance_1_to_n(g["q"], codes).view(np.uint32),
                                   g["d1n"].view(np.uint32))
     np.testing.assert_array_equal(o.distance_m_to_n(g["Q"], codes).view(np.uint32),
                                   g["dmn"].view(np.uint32))
+    # symmetric distances: the same, bit for bit
     ds = o.distance_m_to_n_symmetric(codes[:8], codes)
-    err, ok = dist_close(ds, g["dsym"], sym_term_scale(codes[:8], codes, cs, pb))
-    assert ok, err.max()
+    np.testing.assert_array_equal(ds.view(np.uint32), g["dsym"].view(np.uint32))
 
 
 def _digests():
@@ -127,6 +126,22 @@ def test_oracle_asym_distances_bit_exact_every_dim(bits):
         codes = r.encode_batch(X)
         np.testing.assert_array_equal(o.distance_m_to_n(Q, codes).view(np.uint32),
                                       r.distance_m_to_n(Q, codes).view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("bits", [2, 3, 4, 5, 8, 9])
+def test_oracle_sym_distances_bit_exact_every_dim(bits):
+    """Symmetric distances in the pinned build's order, bit for bit, at every
+    padded dim 4 .. 4096: the nibble shapes (<= 8 bytes, 16 bytes, blocks of 32)
+    and the byte shapes (D < 8, D >= 8); zero rows and scaled rows included."""
+    for dim in (1, 3, 5, 9, 17, 33, 64, 100, 256, 384, 768, 1024, 2048, 4096):
+        rng = np.random.default_rng(dim * 11 + bits)
+        X = (rng.standard_normal((120, dim)) * rng.uniform(1e-3, 1e3, (120, 1))).astype(np.float32)
+        X[0] = 0.0
+        o, r = O.OracleSpace(dim, bits), O.RefSpace(dim, bits)
+        codes = r.encode_batch(X)
+        np.testing.assert_array_equal(o.distance_m_to_n_symmetric(codes[:7], codes).view(np.uint32),
+                                      r.distance_m_to_n_symmetric(codes[:7], codes).view(np.uint32))
 
 
 @needs_ref
