@@ -53,8 +53,9 @@ typedef enum tq_precision {
     TQ_PRECISION_SPLIT_TF32 = 2, /* tcgen05 tensor cores on hi+lo TF32 pairs, FP32 TMEM accumulators
                                     (the QJL-corrected symmetric distances only) */
     TQ_PRECISION_REFERENCE = 3,  /* the reference's own FP32 arithmetic in its Release build's
-                                    summation order, one code per thread: bit-identical to
-                                    distSearchScalarB4 / distSearchAVX (asymmetric M x N only) */
+                                    summation order, one pair per thread: bit-identical to
+                                    distSearchScalarB4 / distSearchAVX (asymmetric M x N) and
+                                    distBuildScalarB4 / distBuildAVX (symmetric M x N) */
     TQ_PRECISION_SPLIT_BF16_DECODED = 4 /* as SPLIT_BF16, but the column tiles are decoded from
                                     the codes in shared memory (128 x 128 tiles) instead of
                                     being read from BF16 planes written to device memory

@@ -465,11 +465,38 @@ def test_reference_precision_bit_identical_to_oracle(cuda_ok, dim, bits):
     np.testing.assert_array_equal(dev.cpu().numpy().view(np.uint32), want.view(np.uint32))
 
 
-def test_reference_precision_refused_for_symmetric(cuda_ok):
-    s = tq.TurboQuantSpace(64, 4)
-    codes = s.encode_batch(np.ones((3, 64), np.float32))
-    with pytest.raises(tq.TQError):
-        s.distance_m_to_n_symmetric(codes, codes, precision="reference")
+@pytest.mark.parametrize("dim,bits", GOLDEN_CASES)
+def test_reference_precision_symmetric_bit_identical_to_golden(cuda_ok, dim, bits):
+    """distBuildAVX / distBuildScalarB4 in the pinned build's order: the golden
+    symmetric distances, bit for bit."""
+    g = load_case(dim, bits)
+    s = tq.TurboQuantSpace(dim, bits)
+    codes = g["codes"]
+    got = s.distance_m_to_n_symmetric(codes[:8], codes, precision="reference")
+    np.testing.assert_array_equal(got.view(np.uint32), g["dsym"].view(np.uint32))
+
+
+@pytest.mark.parametrize("dim,bits", [(3, 4), (17, 3), (31, 2), (33, 4), (100, 4), (384, 4),
+                                      (768, 4), (1536, 4), (5, 8), (9, 5), (200, 8), (768, 8),
+                                      (2048, 9), (4096, 7)])
+def test_reference_precision_symmetric_bit_identical_to_oracle(cuda_ok, dim, bits):
+    """Every loop shape of both symmetric reference functions (nibble: <= 8
+    bytes, 16 bytes, blocks of 32; byte: D < 8, D >= 8); zero and tiny rows;
+    codes against themselves; the device path too."""
+    import torch
+    rng = np.random.default_rng(dim * 7 + bits)
+    X = (rng.standard_normal((600, dim)) * rng.uniform(1e-3, 1e3, (600, 1))).astype(np.float32)
+    X[0] = 0.0
+    s = tq.TurboQuantSpace(dim, bits)
+    codes = s.encode_batch(X)
+    A = codes[:11]
+    want = O.OracleSpace(dim, bits).distance_m_to_n_symmetric(A, codes)
+    got = s.distance_m_to_n_symmetric(A, codes, precision="reference")
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    dev = s.distance_m_to_n_symmetric(torch.from_numpy(A).cuda(), torch.from_numpy(codes).cuda(),
+                                      precision="reference")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dev.cpu().numpy().view(np.uint32), want.view(np.uint32))
 
 
 def test_scan_timer_counts_launches(cuda_ok):

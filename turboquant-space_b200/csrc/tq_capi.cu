@@ -123,14 +123,13 @@ tq_status ensure_host_streams(tq_space *sp) {
     return TQ_OK;
 }
 
-// Precisions of the M x N entry points: FP32 and split-BF16 for both forms;
-// the reference-order arithmetic for the asymmetric form only (the symmetric
-// distBuild order is not restated).
+// Precisions of the M x N entry points: FP32, split-BF16 (planes or decoded
+// tiles) and the reference-order arithmetic, for both forms.
 tq_status mton_precision_ok(tq_precision p, bool sym) {
-    if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_BF16 || p == TQ_PRECISION_SPLIT_BF16_DECODED)
+    if (p == TQ_PRECISION_FP32 || p == TQ_PRECISION_SPLIT_BF16 || p == TQ_PRECISION_SPLIT_BF16_DECODED ||
+        p == TQ_PRECISION_REFERENCE)
         return TQ_OK;
-    if (p == TQ_PRECISION_REFERENCE && !sym) return TQ_OK;
-    if (p == TQ_PRECISION_REFERENCE || p == TQ_PRECISION_SPLIT_TF32)
+    if (p == TQ_PRECISION_SPLIT_TF32)
         return fail(TQ_ERR_NOT_SUPPORTED, "precision %d is not available for %s distances", (int)p,
                     sym ? "symmetric" : "asymmetric");
     return fail(TQ_ERR_INVALID_ARGUMENT, "unknown precision %d", (int)p);
@@ -143,7 +142,7 @@ tq_status mton_precision_ok(tq_precision p, bool sym) {
 //   SPLIT_BF16:           hi/lo BF16 planes + tcgen05 GEMM;
 //   SPLIT_BF16_DECODED:   the same row planes; the column tiles decoded from the
 //                         codes in shared memory (per-code scalars only in HBM);
-//   REFERENCE:            the reference build's own arithmetic, one code per thread.
+//   REFERENCE:            the reference build's own arithmetic, one pair per thread.
 // Every distance ends in the same epilogue d = max(0, r2 + c2 - 2 C r1 c1).
 class MtonRunner {
   public:
@@ -226,6 +225,10 @@ class MtonRunner {
                 TQ_CUDA(tq::launch_mton_fp32(sp_->P, sp_->T, q_rot_, s_q_, norms_, m_, codes, n, out,
                                              ldo, s),
                         "m_to_n scan kernel");
+            else if (prec_ == TQ_PRECISION_REFERENCE)
+                TQ_CUDA(tq::launch_exact_mton_sym(sp_->P, sp_->T.centroids, codes_a_, m_, codes, n, out,
+                                                  ldo, s),
+                        "reference-order symmetric m_to_n kernel");
             else
                 TQ_CUDA(tq::launch_mton_sym_fp32(sp_->P, sp_->T, codes_a_, m_, codes, n, out, ldo, s),
                         "symmetric m_to_n scan kernel");

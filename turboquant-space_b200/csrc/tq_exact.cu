@@ -830,6 +830,97 @@ __global__ void __launch_bounds__(256) exact_mton_kernel(Params P, const float *
     }
 }
 
+// The reference build's symmetric distance of codes a and b
+// (distBuildAVX :1541-1612 / distBuildScalarB4 :985-1019 as its compiler
+// vectorised them), in that build's own summation order:
+//   byte codes, D >= 8: 8 running sums fma(c_a c_b, sigma_a sigma_b, S[i mod 8]),
+//     folded as hsum8; D < 8: one sum in coordinate order;
+//   nibble codes, with pair(f, k0, k1) = fma(f_a(k0), f_b(k0), f_a(k1) f_b(k1)):
+//     blocks of 32 bytes k, lanes j < 8:
+//       s = ((pair(hi, k+16+j, k+24+j) + pair(hi, k+j, k+8+j)) + pair(lo, k+j, k+8+j))
+//           + pair(lo, k+16+j, k+24+j),  S[j] = fma(s sigma_a, sigma_b, S[j]), hsum8;
+//     16 bytes (D = 32): 4 lanes, offsets 4 / 8 / 12, S[j] = (s sigma_a) sigma_b, hsum4;
+//     <= 8 bytes: ip = fma(fma(lo_a, lo_b, hi_a hi_b), sigma_a sigma_b, ip) in byte order;
+//   d = max(0, fma(-(ip + ip), |a| |b|, fma(|a|, |a|, |b| |b|))).
+template <bool NIBBLE>
+__device__ float exact_sym_dist(const Params &P, const float *sc, const uint8_t *a, const uint8_t *b,
+                                bool al4) {
+    const int nb = P.pb;
+    const float na = ld_f32(a + nb, al4), sa = ld_f32(a + nb + 8, al4);
+    const float nbn = ld_f32(b + nb, al4), sb = ld_f32(b + nb + 8, al4);
+    const float sab = __fmul_rn(sa, sb);
+    float ip = 0.0f;
+    if constexpr (!NIBBLE) {
+        const int D = P.D;
+        int i = 0;
+        if (D >= 8) {
+            float S[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            for (; i + 8 <= D; i += 8)
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    S[j] = __fmaf_rn(__fmul_rn(sc[a[i + j] >> 1], sc[b[i + j] >> 1]), sab, S[j]);
+            ip = hsum8(S);
+        }
+        for (; i < D; ++i) ip = __fmaf_rn(__fmul_rn(sc[a[i] >> 1], sc[b[i] >> 1]), sab, ip);
+    } else {
+        auto lo = [&](const uint8_t *x, int k) { return sc[(x[k] & 15u) >> 1]; };
+        auto hi = [&](const uint8_t *x, int k) { return sc[(x[k] >> 4) >> 1]; };
+        auto pair_lo = [&](int k0, int k1) {
+            return __fmaf_rn(lo(a, k0), lo(b, k0), __fmul_rn(lo(a, k1), lo(b, k1)));
+        };
+        auto pair_hi = [&](int k0, int k1) {
+            return __fmaf_rn(hi(a, k0), hi(b, k0), __fmul_rn(hi(a, k1), hi(b, k1)));
+        };
+        int k = 0;
+        if (nb >= 32) {
+            float S[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            for (; k + 32 <= nb; k += 32)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int l0 = k + j, l1 = l0 + 16;
+                    const float s = __fadd_rn(__fadd_rn(__fadd_rn(pair_hi(l1, l1 + 8), pair_hi(l0, l0 + 8)),
+                                                        pair_lo(l0, l0 + 8)),
+                                              pair_lo(l1, l1 + 8));
+                    S[j] = __fmaf_rn(__fmul_rn(s, sa), sb, S[j]);
+                }
+            ip = hsum8(S);
+        }
+        if (nb - k >= 16) {
+            float S4[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int l0 = k + j, l1 = l0 + 8;
+                const float s = __fadd_rn(__fadd_rn(__fadd_rn(pair_hi(l1, l1 + 4), pair_hi(l0, l0 + 4)),
+                                                    pair_lo(l0, l0 + 4)),
+                                          pair_lo(l1, l1 + 4));
+                S4[j] = __fmul_rn(__fmul_rn(s, sa), sb);
+            }
+            ip = __fadd_rn(ip, hsum4(S4));
+            k += 16;
+        }
+        for (; k < nb; ++k)
+            ip = __fmaf_rn(__fmaf_rn(lo(a, k), lo(b, k), __fmul_rn(hi(a, k), hi(b, k))), sab, ip);
+    }
+    const float d = __fmaf_rn(-__fadd_rn(ip, ip), __fmul_rn(na, nbn), __fmaf_rn(na, na, __fmul_rn(nbn, nbn)));
+    return 0.0f < d ? d : 0.0f;
+}
+
+// Symmetric distances of m codes A against n codes B in the reference build's
+// order: one thread per pair.
+template <bool NIBBLE>
+__global__ void __launch_bounds__(256) exact_sym_kernel(Params P, const float *centroids,
+                                                        const uint8_t *A, size_t m, const uint8_t *B,
+                                                        size_t n, bool al4, float *out, size_t ldo) {
+    __shared__ float sc[kMaxLevels];
+    load_centroids(sc, centroids, P.levels);
+    const size_t total = m * n;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = t / n, j = t % n;
+        out[r * ldo + j] = exact_sym_dist<NIBBLE>(P, sc, A + r * P.cs, B + j * P.cs, al4);
+    }
+}
+
 // Index-wide maxima of sigma |x|, scale gamma |x|, |x|^2 and |x| (bound must
 // be zeroed; non-negative floats order like their bit patterns, NaN counts as
 // +inf).
@@ -1022,6 +1113,19 @@ cudaError_t launch_exact_mton(const Params &P, const float *centroids, const flo
     else
         exact_mton_kernel<false><<<blocks, 256, 0, st>>>(P, centroids, q_rot, s_q, norms, m, codes, n,
                                                          codes_al4(P, codes), out, ldo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact_mton_sym(const Params &P, const float *centroids, const uint8_t *A, size_t m,
+                                  const uint8_t *B, size_t n, float *out, size_t ldo, cudaStream_t st) {
+    if (m == 0 || n == 0) return cudaSuccess;
+    const size_t total = m * n;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+    const bool al4 = codes_al4(P, A) && codes_al4(P, B);
+    if (P.nibble)
+        exact_sym_kernel<true><<<blocks, 256, 0, st>>>(P, centroids, A, m, B, n, al4, out, ldo);
+    else
+        exact_sym_kernel<false><<<blocks, 256, 0, st>>>(P, centroids, A, m, B, n, al4, out, ldo);
     return cudaGetLastError();
 }
 

@@ -106,5 +106,10 @@ cudaError_t launch_gather_rows(const float *pool, const int *rows, const int *m_
 cudaError_t launch_exact_mton(const Params &P, const float *centroids, const float *q_rot,
                               const float *s_q, const float *norms, size_t m, const uint8_t *codes,
                               size_t n, float *out, size_t ldo, cudaStream_t st);
+// The reference-order symmetric distances of m codes A against n codes B,
+// out[i * ldo + j]: one thread per pair (distBuildAVX / distBuildScalarB4 as
+// the reference's Release build evaluates them).
+cudaError_t launch_exact_mton_sym(const Params &P, const float *centroids, const uint8_t *A, size_t m,
+                                  const uint8_t *B, size_t n, float *out, size_t ldo, cudaStream_t st);
 
 }  // namespace tq

@@ -425,8 +425,8 @@ class TurboQuantSpace:
     def distance_m_to_n_symmetric(self, codes_a, codes_b, precision="fp32", out=None):
         """distanceBatchMToNSymmetric: codes_a [m, cs] x codes_b [n, cs] -> [m, n].
 
-        precision: "fp32", "split_bf16" or "split_bf16_decoded", as for
-        distance_m_to_n ("reference" is not available for this form)."""
+        precision: "fp32", "split_bf16", "split_bf16_decoded" or "reference",
+        as for distance_m_to_n."""
         cs = self.code_size_bytes()
         prec = _capi.PRECISION[precision]
         if _is_device(codes_a) or _is_device(codes_b):
